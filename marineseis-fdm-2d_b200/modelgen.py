@@ -1,0 +1,243 @@
+"""Seeded synthetic marine models in the reference's on-disk format.
+
+The solver reads a JSON config plus little-endian float32 ``[rows][nx]``
+binaries (reference ``json_template.json`` and ``docs/io.md``). This module
+builds such models with the conventions of the reference's generator scripts
+(``tools/run_models/model_FANDS_PANDF_wavy.py:100-177``,
+``tools/run_models/model_ortho_freesurface_scholte.py:93-184``):
+
+* three frozen rows on top, the free surface on global row 3;
+* the fluid-solid interface on fluid row ``nz_f - 1`` == solid row 0
+  (global row ``nz_f - 1``); the metric arrays cover ``nz_f + nz_s - 1`` rows;
+* ``x = h * xi`` (vertical grid columns), so ``xi_x = 1/h``, ``xi_z = 0``,
+  ``J = h * z_zeta``, ``ze_x = -z_xi / J``, ``ze_z = h / J``
+  (``model_FANDS_PANDF_wavy.py:139-144``), evaluated in FP64 from analytic
+  derivatives of the grid map;
+* the vertical undulation envelope vanishes inside the bottom PML band, so the
+  band has the same thickness in every column (``docs/io.md:65-66``);
+* ``beta0 = min(vs, vp_fluid) / (0.5 * ppw * h * fpeak)`` and
+  ``thickness = (npd - 1) * h`` (``model_FANDS_PANDF_wavy.py:174-177``).
+
+Every array is returned in FP64; ``write_model`` rounds to float32 on disk.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+
+SOLID_FIELDS = ("C11", "C13", "C33", "C55", "rho")
+FLUID_FIELDS = ("K", "rho")
+METRIC_FIELDS = ("J", "xi_x", "xi_z", "ze_x", "ze_z")
+
+
+@dataclass
+class Model:
+    """A fluid-over-solid model on a curvilinear grid (calc_type 1, boundary_type 2)."""
+
+    nx: int
+    nz_f: int
+    nz_s: int
+    h: float
+    fpeak: float
+    dt: float
+    nt: int
+    snapshot: int
+    src_x: List[int]
+    src_z: List[int]
+    npd: int
+    npow: int
+    thickness: float
+    vp_max: float
+    rc: float
+    beta0: float
+    fluid: Dict[str, np.ndarray] = field(default_factory=dict)   # [nz_f][nx]
+    solid: Dict[str, np.ndarray] = field(default_factory=dict)   # [nz_s][nx]
+    metric: Dict[str, np.ndarray] = field(default_factory=dict)  # [nz_f+nz_s-1][nx]
+
+    @property
+    def nz(self) -> int:
+        return self.nz_f + self.nz_s - 1
+
+    @property
+    def cells(self) -> int:
+        """Cells the reference updates per step (the interface row counts twice)."""
+        return self.nx * (self.nz_f + self.nz_s)
+
+    def config(self, paths: Dict[str, str]) -> dict:
+        """JSON document in the reference schema (json_template.json:1-50)."""
+        return {
+            "base": {"fpeak": self.fpeak, "dt": self.dt, "nt": int(self.nt),
+                     "snapshot": int(self.snapshot)},
+            "grid": {
+                "calc_type": 1,
+                "boundary_type": 2,
+                "src_pos": {"posx": [int(v) for v in self.src_x],
+                            "posz": [int(v) for v in self.src_z]},
+                "solid": {"nx": self.nx, "nz": self.nz_s,
+                          **{k: paths["solid/" + k] for k in SOLID_FIELDS}},
+                "jacob": {k: paths["jacob/" + k] for k in METRIC_FIELDS},
+                "fluid": {"nx": self.nx, "nz": self.nz_f,
+                          **{k: paths["fluid/" + k] for k in FLUID_FIELDS}},
+            },
+            "PML": {"npd": self.npd, "thickness": self.thickness, "NPOW": self.npow,
+                    "Vp_max": self.vp_max, "Rc": self.rc, "beta0": self.beta0},
+        }
+
+
+def write_model(model: Model, directory: str, name: str = "model",
+                relative_to: Optional[str] = None) -> str:
+    """Writes ``<directory>/<name>.json`` and the float32 binaries; returns the JSON path.
+
+    Paths in the JSON are absolute unless ``relative_to`` is given, in which
+    case they are relative to that directory (the reference resolves them
+    against the working directory, ``src/elements.cu:161``).
+    """
+    os.makedirs(directory, exist_ok=True)
+    paths = {}
+    groups = (("solid", model.solid, SOLID_FIELDS), ("fluid", model.fluid, FLUID_FIELDS),
+              ("jacob", model.metric, METRIC_FIELDS))
+    for sub, arrays, names in groups:
+        os.makedirs(os.path.join(directory, sub), exist_ok=True)
+        for k in names:
+            p = os.path.abspath(os.path.join(directory, sub, k + ".bin"))
+            np.ascontiguousarray(arrays[k], dtype="<f4").tofile(p)
+            paths[sub + "/" + k] = os.path.relpath(p, relative_to) if relative_to else p
+    jpath = os.path.join(directory, name + ".json")
+    with open(jpath, "w") as f:
+        json.dump(model.config(paths), f, indent=2)
+        f.write("\n")
+    return jpath
+
+
+def _smootherstep(t: np.ndarray) -> np.ndarray:
+    t = np.clip(t, 0.0, 1.0)
+    return t * t * t * (t * (6.0 * t - 15.0) + 10.0)
+
+
+def _dsmootherstep(t: np.ndarray) -> np.ndarray:
+    inside = (t > 0.0) & (t < 1.0)
+    tc = np.clip(t, 0.0, 1.0)
+    return np.where(inside, 30.0 * tc * tc * (tc - 1.0) ** 2, 0.0)
+
+
+def _grid_metric(nx: int, nz_f: int, nz_s: int, npd: int, h: float,
+                 amp: float, wavelength: float) -> Dict[str, np.ndarray]:
+    """FP64 metric of z(xi, zeta) = h (zeta - 3) + amp sin(2 pi x / wavelength) u(zeta) v(zeta).
+
+    u rises 0 -> 1 between the free surface (row 3) and the interface row;
+    v falls 1 -> 0 between the interface row and b = nz - 4 - npd, the last
+    undamped row above the bottom band (``model_FANDS_PANDF_wavy.py:97``).
+    """
+    nz = nz_f + nz_s - 1
+    zeta = np.arange(nz, dtype=np.float64)
+    zeta0 = float(nz_f - 1)
+    b = float(nz - 4 - npd)
+    tu = (zeta - 3.0) / (zeta0 - 3.0)
+    u, du = _smootherstep(tu), _dsmootherstep(tu) / (zeta0 - 3.0)
+    v = np.ones(nz)
+    dv = np.zeros(nz)
+    if b > zeta0:
+        seg = zeta > zeta0
+        t = np.clip((zeta[seg] - zeta0) / (b - zeta0), 0.0, 1.0)
+        v[seg] = np.cos(0.5 * math.pi * t) ** 2
+        dv[seg] = np.where(t < 1.0, -0.5 * math.pi / (b - zeta0) * np.sin(math.pi * t), 0.0)
+    w, dw = u * v, du * v + u * dv
+    x = h * np.arange(nx, dtype=np.float64)
+    s = np.sin(2.0 * math.pi * x / wavelength) if amp else np.zeros(nx)
+    c = np.cos(2.0 * math.pi * x / wavelength) if amp else np.zeros(nx)
+    z_xi = amp * (2.0 * math.pi * h / wavelength) * c[None, :] * w[:, None]
+    z_ze = h + amp * s[None, :] * dw[:, None]
+    if np.any(z_ze <= 0.0):
+        raise ValueError("grid folds: z_zeta <= 0")
+    J = h * z_ze
+    return {"J": J, "xi_x": np.full((nz, nx), 1.0 / h), "xi_z": np.zeros((nz, nx)),
+            "ze_x": -z_xi / J, "ze_z": h / J,
+            "x": np.broadcast_to(x[None, :], (nz, nx)).copy(),
+            "z": h * (zeta[:, None] - 3.0) + amp * s[None, :] * w[:, None]}
+
+
+def _correlated_field(rng: np.random.Generator, shape, corr_cells: float) -> np.ndarray:
+    """Zero-mean Gaussian-correlated field scaled to max |value| = 1 (FFT filter)."""
+    noise = rng.standard_normal(shape)
+    ky = np.fft.fftfreq(shape[0])[:, None]
+    kx = np.fft.rfftfreq(shape[1])[None, :]
+    kern = np.exp(-2.0 * (math.pi * corr_cells) ** 2 * (kx * kx + ky * ky))
+    f = np.fft.irfft2(np.fft.rfft2(noise) * kern, s=shape)
+    f -= f.mean()
+    return f / np.max(np.abs(f))
+
+
+def make_model(nx: int, nz_f: int, nz_s: int, *, h: float = 5.0, npd: int = 20,
+               fpeak: float = 15.0, dt: float = 5e-4, nt: int = 2000, snapshot: Optional[int] = None,
+               src_x: Optional[List[int]] = None, src_z: Optional[List[int]] = None,
+               vp_f: float = 1500.0, rho_f: float = 1000.0,
+               vp: float = 3000.0, vs: float = 1732.0, rho: float = 2000.0,
+               amp: float = 0.0, wavelength: float = 600.0,
+               perturb: float = 0.0, corr_len: float = 50.0, seed: int = 0,
+               ppw: float = 8.0, npow: int = 2, rc: float = 1e-3) -> Model:
+    """Builds a fluid-over-solid model; ``amp > 0`` gives a sinusoidal seafloor."""
+    metric = _grid_metric(nx, nz_f, nz_s, npd, h, amp, wavelength)
+    solid_shape = (nz_s, nx)
+    vp_s = np.full(solid_shape, vp)
+    vs_s = np.full(solid_shape, vs)
+    rho_s = np.full(solid_shape, rho)
+    if perturb:
+        rng = np.random.default_rng(seed)
+        corr = corr_len / h
+        vp_s *= 1.0 + perturb * _correlated_field(rng, solid_shape, corr)
+        vs_s *= 1.0 + perturb * _correlated_field(rng, solid_shape, corr)
+        rho_s *= 1.0 + perturb * _correlated_field(rng, solid_shape, corr)
+    mu = rho_s * vs_s ** 2
+    lam = rho_s * (vp_s ** 2 - 2.0 * vs_s ** 2)
+    solid = {"C11": lam + 2.0 * mu, "C13": lam, "C33": lam + 2.0 * mu, "C55": mu, "rho": rho_s}
+    fluid = {"K": np.full((nz_f, nx), rho_f * vp_f ** 2), "rho": np.full((nz_f, nx), rho_f)}
+    vpmax = float(max(np.max(vp_s), vp_f))
+    beta0 = round(min(float(np.min(vs_s)), vp_f) / (0.5 * ppw * h * fpeak), 4)
+    if src_x is None:
+        src_x = [nx // 2]
+    if src_z is None:
+        src_z = [max(3 + 3, nz_f - 1 - int(round(50.0 / h)))]
+    return Model(nx=nx, nz_f=nz_f, nz_s=nz_s, h=h, fpeak=fpeak, dt=dt, nt=nt,
+                 snapshot=snapshot if snapshot is not None else nt + 1,
+                 src_x=list(src_x), src_z=list(src_z), npd=npd, npow=npow,
+                 thickness=(npd - 1) * h, vp_max=vpmax, rc=rc, beta0=beta0,
+                 fluid=fluid, solid=solid, metric=metric)
+
+
+# --- named workloads ---------------------------------------------------------
+
+def flat_400x400(nt: int = 2000) -> Model:
+    """400x400, h = 5 m, flat seafloor 1000 m below the free surface (global row 203),
+    water 1500/1000 over vp 3000, vs 1732, rho 2000; 20-cell CFS-PML; 15 Hz Ricker
+    50 m above the seafloor (column 200, fluid row 193); dt = 0.5 ms."""
+    return make_model(400, 204, 197, h=5.0, npd=20, fpeak=15.0, dt=5e-4, nt=nt,
+                      src_x=[200], src_z=[193])
+
+
+def curvilinear(nx: int, nz: int, *, zeta0: Optional[int] = None, nt: int = 6000,
+                dt: float = 4e-4, seed: int = 1, perturb: float = 0.05) -> Model:
+    """Curvilinear forward model: sinusoidal seafloor 40 sin(2 pi x / 600 m) on global
+    row ``zeta0`` (default: 1500 m below the free surface, row 303), blended into the
+    grid, +-5% Gaussian-correlated vp/vs/rho (50 m), dt = 0.4 ms."""
+    h = 5.0
+    if zeta0 is None:
+        zeta0 = min(303, nz // 2)
+    nz_f = zeta0 + 1
+    nz_s = nz - nz_f + 1
+    return make_model(nx, nz_f, nz_s, h=h, npd=20, fpeak=15.0, dt=dt, nt=nt,
+                      src_x=[nx // 2], src_z=[zeta0 - 10], amp=40.0, wavelength=600.0,
+                      perturb=perturb, corr_len=50.0, seed=seed)
+
+
+def curvilinear_1200x800(nt: int = 6000) -> Model:
+    return curvilinear(1200, 800, nt=nt)
+
+
+def curvilinear_4096x2048(nt: int = 6000) -> Model:
+    """4096x2048 with the seafloor on the middle row (half fluid, half solid)."""
+    return curvilinear(4096, 2048, zeta0=1023, nt=nt)

@@ -1,0 +1,61 @@
+"""Golden cases: seeded models whose records were produced by the reference's
+own CUDA build (oracle/_ref/main_debug, compiled from the reference sources for
+sm_100a) on a B200. make_golden.py writes the fixtures; the tests regenerate the
+same models from these definitions and compare against the stored records.
+"""
+from __future__ import annotations
+
+import importlib
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+modelgen = importlib.import_module("marineseis-fdm-2d_b200.modelgen")
+
+GOLDEN_DIR = os.path.dirname(os.path.abspath(__file__))
+
+
+def flat_small():
+    """120 x 107 flat seafloor, 10-cell PML, 25 Hz, dt 0.5 ms, 600 steps."""
+    return modelgen.make_model(120, 48, 60, npd=10, fpeak=25.0, dt=5e-4, nt=600,
+                               src_x=[60], src_z=[40])
+
+
+def curv_small():
+    """128 x 115 sinusoidal seafloor + 5% perturbations, dt 0.4 ms (record gap 3), 500 steps."""
+    return modelgen.make_model(128, 52, 64, npd=12, fpeak=25.0, dt=4e-4, nt=500,
+                               src_x=[70], src_z=[44], amp=20.0, wavelength=300.0,
+                               perturb=0.05, seed=3)
+
+
+def shallow_src():
+    """Source 2 rows below the free surface (source cells on the surface row), 300 steps."""
+    return modelgen.make_model(96, 40, 48, npd=8, fpeak=30.0, dt=4e-4, nt=300,
+                               src_x=[30], src_z=[5], amp=10.0, wavelength=200.0,
+                               perturb=0.03, seed=7)
+
+
+def flat_400x400():
+    """The 400x400 flat-seafloor forward model, 2000 steps."""
+    return modelgen.flat_400x400(nt=2000)
+
+
+def curvilinear_1200x800():
+    """The 1200x800 curvilinear forward model, 6000 steps."""
+    return modelgen.curvilinear_1200x800(nt=6000)
+
+
+# name -> (builder, receiver stride kept in the fixture, keep final snapshot)
+CASES = {
+    "flat_small": (flat_small, 1, True),
+    "curv_small": (curv_small, 1, True),
+    "shallow_src": (shallow_src, 1, True),
+    "flat_400x400": (flat_400x400, 8, False),
+    "curvilinear_1200x800": (curvilinear_1200x800, 40, False),
+}
+
+
+def fixture_path(name: str) -> str:
+    return os.path.join(GOLDEN_DIR, name + ".npz")
