@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Benchmark of the fluid-solid RK4 time step (Gcell-updates/s, % of HBM roofline).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+One "step" is one RK4 time step of the whole model (four fused stage launches
+plus the interface filter / receiver launch). The default workload is the
+4096 x 2048 curvilinear model (sinusoidal seafloor on the middle row, +-5%
+correlated perturbations, 20-cell CFS-PML), seeded and synthetic; its state
+and coefficients (~0.7 GB) exceed the 126 MB L2, so no flush is needed.
+
+value  = cells x steps / device time (CUDA events on the solver's stream, max
+         over ranks), cells = nx (nz_f + nz_s) as the reference counts them.
+e2e    = the same metric through the public API with host buffers: model
+         upload from pinned host memory, the steps, and the receiver read-back.
+roofline: algorithmic bytes per step (16 S + 4 M floats per cell: 464 B solid,
+         288 B fluid, +256 B per PML strip cell and direction) over the summed
+         average durations of the four stage launches.
+With N > 1 every rank runs its own copy of the workload (independent shots):
+weak scaling, no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+modelgen = importlib.import_module("marineseis-fdm-2d_b200.modelgen")
+
+WORKLOADS = {
+    "curvilinear_4096x2048": lambda: modelgen.curvilinear_4096x2048(nt=10),
+    "curvilinear_1200x800": lambda: modelgen.curvilinear_1200x800(nt=10),
+    "flat_400x400": lambda: modelgen.flat_400x400(nt=10),
+}
+DEFAULT_WORKLOAD = "curvilinear_4096x2048"
+METRIC = "Gcell-updates/s (fluid-solid RK4 step, % HBM roofline)"
+
+
+def algorithmic_bytes(m) -> int:
+    """Bytes per step a classical-RK4 sweep must move (16 S + 4 M floats per cell)."""
+    fluid = m.nx * m.nz_f * (16 * 3 + 4 * 6) * 4
+    solid = m.nx * m.nz_s * (16 * 5 + 4 * 9) * 4
+    strips = 2 * m.npd * (m.nz_f - 3) + 2 * m.npd * (m.nz_s - 3) + m.npd * (m.nx - 6)
+    return fluid + solid + strips * 16 * 4 * 4
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.device), "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.25)
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            parts = [p.strip() for p in l.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_oracle_rate(model, target_s: float, max_steps: int):
+    """Times the oracle (FP32 CPU restatement, all host threads) on a bounded sample."""
+    from oracle import pyoracle
+    pyoracle.build()
+    st = pyoracle.Stepper(model, 32)
+    threads = pyoracle.max_threads()
+    st.step(1)  # warm-up (first touch, thread pool)
+    done, t0 = 0, time.perf_counter()
+    while done < max_steps and (time.perf_counter() - t0) < target_s:
+        st.step(1)
+        done += 1
+    secs = time.perf_counter() - t0
+    st.close()
+    return model.cells * done / secs / 1e9, threads, done, secs
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as td
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=timedelta(seconds=300))
+        dist = td
+    return world, rank, local, dist
+
+
+def max_over_ranks(dist, value: float, local: int) -> float:
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, local: int):
+    if dist is not None:
+        dist.barrier(device_ids=[local])
+
+
+def run_reference(args, model, world, rank):
+    """Reference arm: the reference has no CPU implementation of this path, so the
+    CPU restatement in oracle/ (its operation order, FP32) is timed on the host."""
+    if rank != 0:
+        return
+    budget = 150.0  # seconds of CPU work for warm-up + timed steps together
+    from oracle import pyoracle
+    pyoracle.build()
+    st = pyoracle.Stepper(model, 32)
+    threads = pyoracle.max_threads()
+    t0 = time.perf_counter()
+    st.step(1)
+    per_step = time.perf_counter() - t0
+    warm = max(0, min(args.warmup - 1, int(budget * 0.1 / max(per_step, 1e-6))))
+    st.step(warm)
+    steps = max(1, min(args.steps, int(budget * 0.9 / max(per_step, 1e-6))))
+    t0 = time.perf_counter()
+    st.step(steps)
+    secs = time.perf_counter() - t0
+    st.close()
+    value = model.cells * steps / secs / 1e9
+    sample = (f"{steps} of {args.steps} requested steps of {args.workload} "
+              f"({model.cells} cells) after {warm + 1} warm-up steps")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "Gcell/s",
+        "n_gpus": args.gpus, "steps": steps, "warmup": warm + 1,
+        "ms_per_step": round(secs / steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "nx": model.nx, "nz_f": model.nz_f,
+                   "nz_s": model.nz_s, "cells": model.cells},
+        "cpu_baseline": {"value": round(value, 4), "unit": "Gcell/s", "cores": threads,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": round(value, 4), "unit": "Gcell/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world, rank, local, dist = dist_setup(args)
+    model = WORKLOADS[args.workload]()
+    if args.impl == "reference":
+        run_reference(args, model, world, rank)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    mfdm = importlib.import_module("marineseis-fdm-2d_b200")
+    mfdm.load_library()
+    solver = mfdm.Solver.from_model(model, device=local)
+    solver.set_shot(0, reset=True)
+    solver.step(args.warmup)
+
+    # ---- timed region: K steps through the captured time loop ----
+    barrier(dist, local)
+    with ClockSampler(local) as clk:
+        total_ms, _ = solver.time_steps(args.steps)
+    ms = max_over_ranks(dist, total_ms, local)
+    secs = ms / 1e3
+    value = world * model.cells * args.steps / secs / 1e9
+
+    # ---- per-kernel durations (events around every launch) ----
+    nk = min(args.steps, 40)
+    _, kms = solver.time_steps(nk, per_kernel=True)
+    stage_ms = sum(kms[:4]) / nk  # the four stage launches of one step
+    alg = algorithmic_bytes(model)
+    peak, peak_kind = peaks()
+    achieved = alg / (stage_ms / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "stage_kernel_traffic.json")
+    if os.path.exists(tp):
+        tj = json.load(open(tp))
+        if tj.get("workload") == args.workload:
+            traffic = tj.get("dram_bytes_per_launch")
+
+    # ---- end to end through the public API with host buffers ----
+    import torch
+    pinned = {}
+    for grp in ("fluid", "solid", "metric"):
+        for k, v in getattr(model, grp).items():
+            t = torch.empty(v.shape, dtype=torch.float32, pin_memory=True)
+            t.numpy()[...] = v
+            pinned[(grp, k)] = t
+    host_model = modelgen.Model(**{f: getattr(model, f) for f in (
+        "nx", "nz_f", "nz_s", "h", "fpeak", "dt", "nt", "snapshot", "src_x", "src_z", "npd",
+        "npow", "thickness", "vp_max", "rc", "beta0")})
+    for (grp, k), t in pinned.items():
+        getattr(host_model, grp)[k] = t.numpy()
+    h2d = sum(t.numel() * 4 for (grp, k), t in pinned.items()
+              if k in ("K", "rho", "C11", "C13", "C33", "C55", "J", "xi_x", "xi_z", "ze_x", "ze_z"))
+    barrier(dist, local)
+    t0 = time.perf_counter()
+    solver.load_model(host_model)
+    solver.set_shot(0, reset=True)
+    solver.step(args.steps)
+    rec = solver.records()
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(dist, e2e_s, local)
+    d2h = sum(a.nbytes for a in rec.values())
+    e2e = world * model.cells * args.steps / e2e_s / 1e9
+
+    # ---- CPU baseline (rank 0, single GPU runs only) ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, threads, n, s = cpu_oracle_rate(model, target_s=15.0, max_steps=50)
+        cpu = {"value": round(rate, 5), "unit": "Gcell/s", "cores": threads, "kind": "port",
+               "sample": f"{n} RK4 steps of {args.workload} in {s:.1f} s (FP32 oracle, OpenMP)"}
+
+    # a second, smaller workload for context (configs[1]-sized)
+    other = {}
+    if rank == 0 and args.workload == DEFAULT_WORKLOAD:
+        small = modelgen.curvilinear_1200x800(nt=10)
+        with mfdm.Solver.from_model(small, device=local) as s2:
+            s2.set_shot(0, reset=True)
+            s2.step(args.warmup)
+            n2 = max(args.steps, 200)
+            t2, _ = s2.time_steps(n2)
+            other["curvilinear_1200x800"] = {
+                "value": round(small.cells * n2 / (t2 / 1e3) / 1e9, 3), "unit": "Gcell/s",
+                "ms_per_step": round(t2 / n2, 4)}
+
+    clocks = clk.summary()
+    solver.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Gcell/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generator, no dataset)",
+            "config": {"workload": args.workload, "nx": model.nx, "nz_f": model.nz_f,
+                       "nz_s": model.nz_s, "cells": model.cells, "npd": model.npd,
+                       "parallelism": f"independent shots x{world}",
+                       "l2": "inputs larger than L2 (state + coefficients > 126 MB)"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_step": alg,
+                         "stage_launch_ms": [round(k / nk, 5) for k in kms[:4]],
+                         "filter_launch_ms": round(kms[4] / nk, 5)},
+            "gpu_launches": 5 * args.steps,
+            "e2e": {"value": round(e2e, 3), "unit": "Gcell/s",
+                    "h2d_bytes_per_step": int(h2d // args.steps),
+                    "d2h_bytes_per_step": int(d2h // args.steps)},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "other_workloads": other,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

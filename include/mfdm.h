@@ -1,0 +1,156 @@
+/*
+ * mfdm.h - C ABI of the B200 fluid-solid time-stepping library (libmfdm.so).
+ *
+ * Drop-in replacement of MarineSeis-FDM-2D's time-stepping path for the
+ * pressure-free-top configuration (calc_type 1 = FANDS, boundary_type 2 =
+ * PANDF): a fluid layer over an elastic solid on a curvilinear grid, classical
+ * RK4 with alternating DRP MacCormack-type operators, ADE CFS-PML on the left,
+ * right and bottom, the free surface on row 3, seafloor coupling, a Ricker
+ * point source and interface receivers. The reference exposes this path only
+ * as a C++ function and a command line, so every entry point below cites the
+ * reference code it replaces (paths inside the reference project).
+ *
+ * Conventions: every function returns MFDM_OK (0) or a negative MFDM_ERR_*
+ * code and never exits the process; mfdm_last_error() returns the message of
+ * the calling thread's last failure. Handles are opaque and must be used by
+ * one host thread at a time. Host arrays are caller-owned, row-major
+ * [rows][nx] float32; device memory is owned by the handle.
+ */
+#ifndef MFDM_H
+#define MFDM_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MFDM_OK 0
+#define MFDM_ERR_ARG (-1)         /* bad argument or unsupported configuration   */
+#define MFDM_ERR_IO (-2)          /* file missing, short read, write failure     */
+#define MFDM_ERR_CONFIG (-3)      /* JSON syntax, missing key or type mismatch   */
+#define MFDM_ERR_CUDA (-4)        /* CUDA runtime error                          */
+#define MFDM_ERR_NONFINITE (-5)   /* NaN/Inf reached the interface rows          */
+#define MFDM_ERR_NOMEM (-6)       /* device allocation failed                    */
+
+typedef struct mfdm_model mfdm_model;
+
+/* In-memory model description; field meaning follows json_template.json:1-50
+ * and src/elements.cu:72-154. nz_f and nz_s both include the interface row;
+ * the metric arrays cover nz_f + nz_s - 1 global rows. */
+typedef struct mfdm_desc {
+  int nx, nz_f, nz_s;
+  float fpeak, dt;
+  int nt, snapshot;
+  int npd, npow;
+  float thickness, vp_max, rc, beta0;
+  int nsrc;
+  const int* src_x;               /* [nsrc] source columns            */
+  const int* src_z;               /* [nsrc] source fluid rows         */
+  const float* K;                 /* [nz_f][nx] fluid bulk modulus    */
+  const float* rho_f;             /* [nz_f][nx] fluid density         */
+  const float* C11;               /* [nz_s][nx] solid stiffness       */
+  const float* C13;
+  const float* C33;
+  const float* C55;
+  const float* rho_s;             /* [nz_s][nx] solid density         */
+  const float* J;                 /* [nz_f+nz_s-1][nx] metric         */
+  const float* xi_x;
+  const float* xi_z;
+  const float* ze_x;
+  const float* ze_z;
+} mfdm_desc;
+
+typedef struct mfdm_info {
+  int nx, nz_f, nz_s, pitch;
+  int nt, snapshot, gap, nsrc, shot;
+  int step;                       /* time index of the next step      */
+  int nsamples;                   /* receiver samples recorded so far */
+  long long cells;                /* nx * (nz_f + nz_s): cells updated per step */
+  long long device_bytes;         /* device memory held by the handle */
+} mfdm_info;
+
+/* Field ids for mfdm_get_field / mfdm_set_field. */
+#define MFDM_FLUID_VX 0
+#define MFDM_FLUID_VZ 1
+#define MFDM_FLUID_P 2
+#define MFDM_SOLID_VX 3
+#define MFDM_SOLID_VZ 4
+#define MFDM_SOLID_SX 5
+#define MFDM_SOLID_SZ 6
+#define MFDM_SOLID_SXZ 7
+
+/* Thread-local message of the last failing call ("" if none). */
+const char* mfdm_last_error(void);
+
+/* Reads a JSON config and its .bin arrays and uploads them to `device`.
+ * Replaces MemManager::MemManager(const char*) + grid_cp_h2d()
+ * (src/elements.cu:64-183, 307-333); relative paths resolve against the
+ * working directory as in the reference. */
+int mfdm_open_json(const char* json_path, int device, mfdm_model** out);
+
+/* Same from host arrays (no files); the arrays are copied. */
+int mfdm_open_desc(const mfdm_desc* desc, int device, mfdm_model** out);
+
+/* Re-uploads the model arrays and scalars of `desc` into an open handle with
+ * the same nx, nz_f, nz_s and npd (a new model for the next shot or
+ * iteration without reallocating). The wavefield is left untouched; call
+ * mfdm_set_shot to restart. */
+int mfdm_load_desc(mfdm_model* m, const mfdm_desc* desc);
+
+/* Frees the handle and its device memory (MemManager::~MemManager, src/elements.cu:186-304). */
+int mfdm_close(mfdm_model* m);
+
+int mfdm_get_info(const mfdm_model* m, mfdm_info* info);
+
+/* Selects shot `isrc` (source position), rewinds the time index to 0 and
+ * clears the receiver buffer. reset_state = 1 also zeroes the wavefield and
+ * ADE memory; 0 keeps them, which is what the reference's shot loop does
+ * (src/main.cu:94-136 never clears the fields between shots). */
+int mfdm_set_shot(mfdm_model* m, int isrc, int reset_state);
+
+/* One RK4 step for time index `it` (direction order FBFB for even it, BFBF
+ * for odd, src/main.cu:137-138) followed by the interface filter and the
+ * receiver sample when it % gap == 0. Replaces PmlFs::FluidSolid::update_RK4
+ * (include/pml_fs_kernels.cuh:848-852, src/pml_fs_kernels.cu:765-868) plus
+ * MemManager::RK4_reset (src/elements.cu:345-383), which is fused away.
+ * `stream` is a cudaStream_t (NULL = the handle's stream); asynchronous. */
+int mfdm_update_rk4(mfdm_model* m, int it, void* stream);
+
+/* Advances `nsteps` steps from the current time index on the handle's stream
+ * through a captured CUDA graph (the time loop of src/main.cu:136-213 without
+ * the host I/O), then synchronises and checks the non-finite flag. */
+int mfdm_step(mfdm_model* m, int nsteps);
+
+/* Advances `nsteps` steps like mfdm_step and reports device time measured
+ * with CUDA events on the handle's stream: *total_ms for the whole run. With
+ * per_kernel != 0 the steps are launched one by one with an event pair around
+ * every kernel, and kernel_ms[0..3] receive the summed time of the four RK
+ * stage launches and kernel_ms[4] that of the filter/receiver launch. */
+int mfdm_time_steps(mfdm_model* m, int nsteps, int per_kernel, float* total_ms, float* kernel_ms);
+
+/* Waits for the handle's stream. */
+int mfdm_synchronize(mfdm_model* m);
+
+/* Copies receiver samples [first, first + count) to host arrays of
+ * [count][nx] floats each (any may be NULL): solid vx and vz on solid row 0
+ * and fluid pressure on fluid row nz_f - 1, the rows the reference appends to
+ * record/solid_vx.bin, solid_vz.bin and fluid_p.bin (src/main.cu:245-295). */
+int mfdm_get_records(mfdm_model* m, int first, int count, float* solid_vx, float* solid_vz,
+                     float* fluid_p);
+
+/* Copies one state field to/from a host array of [rows][nx] floats
+ * (MemManager::U_cp_d2h, src/elements.cu:335-343, for the snapshot writer). */
+int mfdm_get_field(mfdm_model* m, int field, float* host);
+int mfdm_set_field(mfdm_model* m, int field, const float* host);
+
+/* The drop-in command line: `main_debug <model.json> <out_root>`
+ * (src/main.cu:58-216). Clears out_root, runs every shot and writes
+ * <out_root>/<shot>/record/{solid_vx,solid_vz,fluid_p}.bin and
+ * <out_root>/<shot>/snapshot/{solid,fluid}/{vx,vz}/<f>_%06d.bin byte for byte
+ * in the reference layout. Returns MFDM_OK or an error code (the CLI exits 1). */
+int mfdm_run_cli(const char* json_path, const char* out_root, int device);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MFDM_H */

@@ -1,0 +1,253 @@
+"""B200-native MarineSeis-FDM-2D time stepping: Python binding of libmfdm.so.
+
+The compute path is the CUDA library built from ``csrc/`` for sm_100a
+(``builder.build()``); this module only marshals arguments through ctypes. There
+is no CPU fallback: if the library is missing or no GPU is present the calls
+raise ``MfdmError``.
+
+Mirrors the reference's interfaces for the fluid-solid PANDF path:
+
+* ``Solver.from_json(path)``      MemManager(json) + grid_cp_h2d (src/elements.cu:64-183, 307-333)
+* ``Solver.update_rk4(it)``       PmlFs::FluidSolid::update_RK4 (src/pml_fs_kernels.cu:765-868)
+* ``Solver.step(n)``              the time loop of src/main.cu:136-213 (graph-captured)
+* ``Solver.records()``            record/{solid_vx,solid_vz,fluid_p}.bin rows (src/main.cu:245-295)
+* ``Solver.field(name)``          MemManager::U_cp_d2h (src/elements.cu:335-343)
+* ``run_cli(json, out_root)``     ``main_debug <model.json> <out_root>`` (src/main.cu:58-216)
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Dict, Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmfdm.so")
+CLI_PATH = os.path.join(HERE, "bin", "main_debug")
+
+FIELDS = {"fluid_vx": 0, "fluid_vz": 1, "fluid_p": 2, "solid_vx": 3, "solid_vz": 4,
+          "solid_sx": 5, "solid_sz": 6, "solid_sxz": 7}
+
+# Entry points declared in include/mfdm.h (checked by the CPU test suite).
+EXPORTS = ("mfdm_last_error", "mfdm_open_json", "mfdm_open_desc", "mfdm_load_desc", "mfdm_close",
+           "mfdm_get_info", "mfdm_set_shot", "mfdm_update_rk4", "mfdm_step", "mfdm_time_steps",
+           "mfdm_synchronize", "mfdm_get_records", "mfdm_get_field", "mfdm_set_field",
+           "mfdm_run_cli")
+
+
+class MfdmError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"mfdm error {code}: {message}")
+        self.code = code
+
+
+_fp = ctypes.POINTER(ctypes.c_float)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+class Desc(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("nz_f", ctypes.c_int), ("nz_s", ctypes.c_int),
+                ("fpeak", ctypes.c_float), ("dt", ctypes.c_float),
+                ("nt", ctypes.c_int), ("snapshot", ctypes.c_int),
+                ("npd", ctypes.c_int), ("npow", ctypes.c_int),
+                ("thickness", ctypes.c_float), ("vp_max", ctypes.c_float),
+                ("rc", ctypes.c_float), ("beta0", ctypes.c_float),
+                ("nsrc", ctypes.c_int), ("src_x", _ip), ("src_z", _ip),
+                ("K", _fp), ("rho_f", _fp), ("C11", _fp), ("C13", _fp), ("C33", _fp),
+                ("C55", _fp), ("rho_s", _fp), ("J", _fp), ("xi_x", _fp), ("xi_z", _fp),
+                ("ze_x", _fp), ("ze_z", _fp)]
+
+
+class Info(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("nz_f", ctypes.c_int), ("nz_s", ctypes.c_int),
+                ("pitch", ctypes.c_int), ("nt", ctypes.c_int), ("snapshot", ctypes.c_int),
+                ("gap", ctypes.c_int), ("nsrc", ctypes.c_int), ("shot", ctypes.c_int),
+                ("step", ctypes.c_int), ("nsamples", ctypes.c_int),
+                ("cells", ctypes.c_longlong), ("device_bytes", ctypes.c_longlong)]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads libmfdm.so (raises if it was not built; there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise MfdmError(-1, f"{path} is missing: build it with marineseis-fdm-2d_b200/builder.py")
+    lib = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    sig = {
+        "mfdm_last_error": (ctypes.c_char_p, []),
+        "mfdm_open_json": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(vp)]),
+        "mfdm_open_desc": (ctypes.c_int, [ctypes.POINTER(Desc), ctypes.c_int, ctypes.POINTER(vp)]),
+        "mfdm_load_desc": (ctypes.c_int, [vp, ctypes.POINTER(Desc)]),
+        "mfdm_close": (ctypes.c_int, [vp]),
+        "mfdm_get_info": (ctypes.c_int, [vp, ctypes.POINTER(Info)]),
+        "mfdm_set_shot": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+        "mfdm_update_rk4": (ctypes.c_int, [vp, ctypes.c_int, vp]),
+        "mfdm_step": (ctypes.c_int, [vp, ctypes.c_int]),
+        "mfdm_time_steps": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, _fp, _fp]),
+        "mfdm_synchronize": (ctypes.c_int, [vp]),
+        "mfdm_get_records": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, _fp, _fp, _fp]),
+        "mfdm_get_field": (ctypes.c_int, [vp, ctypes.c_int, _fp]),
+        "mfdm_set_field": (ctypes.c_int, [vp, ctypes.c_int, _fp]),
+        "mfdm_run_cli": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(rc: int):
+    if rc != 0:
+        msg = load_library().mfdm_last_error().decode(errors="replace")
+        raise MfdmError(rc, msg)
+
+
+def _f32(a: np.ndarray) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def make_desc(model):
+    """mfdm_desc for a modelgen.Model; returns (desc, arrays kept alive)."""
+    keep = []
+
+    def ptr(a):
+        a = _f32(a)
+        keep.append(a)
+        return a.ctypes.data_as(_fp)
+
+    d = Desc()
+    d.nx, d.nz_f, d.nz_s = model.nx, model.nz_f, model.nz_s
+    d.fpeak, d.dt, d.nt, d.snapshot = model.fpeak, model.dt, model.nt, model.snapshot
+    d.npd, d.npow, d.thickness = model.npd, model.npow, model.thickness
+    d.vp_max, d.rc, d.beta0 = model.vp_max, model.rc, model.beta0
+    sx = np.ascontiguousarray(model.src_x, dtype=np.int32)
+    sz = np.ascontiguousarray(model.src_z, dtype=np.int32)
+    keep += [sx, sz]
+    d.nsrc, d.src_x, d.src_z = len(sx), sx.ctypes.data_as(_ip), sz.ctypes.data_as(_ip)
+    d.K, d.rho_f = ptr(model.fluid["K"]), ptr(model.fluid["rho"])
+    d.C11, d.C13 = ptr(model.solid["C11"]), ptr(model.solid["C13"])
+    d.C33, d.C55, d.rho_s = ptr(model.solid["C33"]), ptr(model.solid["C55"]), ptr(model.solid["rho"])
+    d.J, d.xi_x, d.xi_z = ptr(model.metric["J"]), ptr(model.metric["xi_x"]), ptr(model.metric["xi_z"])
+    d.ze_x, d.ze_z = ptr(model.metric["ze_x"]), ptr(model.metric["ze_z"])
+    return d, keep
+
+
+class Solver:
+    """One model resident on one GPU (an opaque libmfdm handle)."""
+
+    def __init__(self, handle: ctypes.c_void_p):
+        self._h = handle
+        self._lib = load_library()
+        self.info()
+
+    # -- construction -------------------------------------------------------
+    @classmethod
+    def from_json(cls, path: str, device: int = 0) -> "Solver":
+        h = ctypes.c_void_p()
+        _check(load_library().mfdm_open_json(os.fsencode(path), device, ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_model(cls, model, device: int = 0) -> "Solver":
+        """From a modelgen.Model held in host memory (no files)."""
+        d, keep = make_desc(model)
+        h = ctypes.c_void_p()
+        _check(load_library().mfdm_open_desc(ctypes.byref(d), device, ctypes.byref(h)))
+        del keep
+        return cls(h)
+
+    def load_model(self, model):
+        """Uploads a model of the same shape into this handle (mfdm_load_desc)."""
+        d, keep = make_desc(model)
+        _check(self._lib.mfdm_load_desc(self._h, ctypes.byref(d)))
+        del keep
+
+    def close(self):
+        if self._h:
+            self._lib.mfdm_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- queries ------------------------------------------------------------
+    def info(self) -> Dict[str, int]:
+        i = Info()
+        _check(self._lib.mfdm_get_info(self._h, ctypes.byref(i)))
+        return {k: getattr(i, k) for k, _ in Info._fields_}
+
+    # -- time stepping ------------------------------------------------------
+    def set_shot(self, isrc: int = 0, reset: bool = True):
+        _check(self._lib.mfdm_set_shot(self._h, int(isrc), 1 if reset else 0))
+
+    def update_rk4(self, it: int, stream: Optional[int] = None):
+        """One RK4 step for time index ``it`` (asynchronous on ``stream`` or the handle's)."""
+        _check(self._lib.mfdm_update_rk4(self._h, int(it), ctypes.c_void_p(stream or 0)))
+
+    def step(self, nsteps: int):
+        _check(self._lib.mfdm_step(self._h, int(nsteps)))
+
+    def time_steps(self, nsteps: int, per_kernel: bool = False):
+        """Runs nsteps and returns (total_ms, per-kernel ms [4 stages + filter] or None),
+        measured with CUDA events on the handle's stream."""
+        total = ctypes.c_float()
+        k = (ctypes.c_float * 5)()
+        _check(self._lib.mfdm_time_steps(self._h, int(nsteps), 1 if per_kernel else 0,
+                                         ctypes.byref(total), k))
+        return total.value, (list(k) if per_kernel else None)
+
+    def synchronize(self):
+        _check(self._lib.mfdm_synchronize(self._h))
+
+    # -- data out -----------------------------------------------------------
+    def records(self, first: int = 0, count: Optional[int] = None) -> Dict[str, np.ndarray]:
+        info = self.info()
+        if count is None:
+            count = info["nsamples"] - first
+        nx = info["nx"]
+        out = {k: np.zeros((count, nx), dtype=np.float32) for k in ("svx", "svz", "fp")}
+        _check(self._lib.mfdm_get_records(self._h, int(first), int(count),
+                                          out["svx"].ctypes.data_as(_fp),
+                                          out["svz"].ctypes.data_as(_fp),
+                                          out["fp"].ctypes.data_as(_fp)))
+        return out
+
+    def field(self, name: str) -> np.ndarray:
+        info = self.info()
+        fid = FIELDS[name]
+        rows = info["nz_f"] if fid < 3 else info["nz_s"]
+        out = np.zeros((rows, info["nx"]), dtype=np.float32)
+        _check(self._lib.mfdm_get_field(self._h, fid, out.ctypes.data_as(_fp)))
+        return out
+
+    def set_field(self, name: str, values: np.ndarray):
+        a = _f32(values)
+        _check(self._lib.mfdm_set_field(self._h, FIELDS[name], a.ctypes.data_as(_fp)))
+
+
+def run_cli(json_path: str, out_root: str, device: int = 0):
+    """In-process equivalent of ``main_debug <model.json> <out_root>``."""
+    _check(load_library().mfdm_run_cli(os.fsencode(json_path), os.fsencode(out_root), device))
+
+
+def build(verbose: bool = False, force: bool = False) -> str:
+    """Compiles libmfdm.so and bin/main_debug for sm_100a (see builder.py)."""
+    from . import builder
+    return builder.build(verbose=verbose, force=force)

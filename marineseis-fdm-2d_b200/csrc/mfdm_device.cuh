@@ -1,0 +1,421 @@
+// Device-side building blocks of the fluid-solid time step: stencil operators,
+// per-cell right-hand sides, interface coupling and the RK4 stage update.
+//
+// Layout in HBM (all FP32, row-major, x fastest, row pitch P floats, P a
+// multiple of 32 so every row starts on a 128-byte boundary):
+//   fluid fields  vx, vz, p              [nz_f][P]
+//   solid fields  vx, vz, sx, sz, sxz    [nz_s][P]
+//   metric        J, xi_x, xi_z, ze_x, ze_z over global rows [nz_f+nz_s-1][P]
+//                 (fluid row r = global row r; solid row r = global row r+nz_f-1)
+//   ADE memory    fluid xi strips [nz_f][Ps], solid xi strips [nz_s][Ps]
+//                 (left columns 3..2+npd then right columns nx-3-npd..nx-4),
+//                 solid zeta strip [npd][P] (solid rows nz_s-3-npd..nz_s-4).
+// The reference keeps ADE memory over the full grid (src/elements.cu:737-758);
+// only the strip cells are ever non-zero, so only those are stored here.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mfdm {
+
+// DRP-optimised biased 5-point first derivative (reference include/tools_func.cuh:6-10).
+// The literals sum to -6e-5, not 0: they are kept exactly.
+constexpr float kAm1 = -0.30874f;
+constexpr float kA0 = -0.63260f;
+constexpr float kA1 = +1.23300f;
+constexpr float kA2 = -0.33340f;
+constexpr float kA3 = +0.04168f;
+// One-sided 4-2 and 2-2 operators near boundaries (include/tools_func.cuh:12-17).
+constexpr float kM42_0 = -7.0f / 6.0f;
+constexpr float kM42_1 = +8.0f / 6.0f;
+constexpr float kM42_2 = -1.0f / 6.0f;
+
+enum { kDirF = 0, kDirB = 1 };
+enum { kStageFirst = 0, kStageMid = 1, kStageLast = 2 };
+
+// Everything a stage kernel needs besides the four RK state sets.
+struct Coef {
+  int nx, nzf, nzs, P, npd, Ps;
+  const float* __restrict__ K;     // fluid bulk modulus [nz_f][P]
+  const float* __restrict__ rhof;  // fluid density
+  const float* __restrict__ C11;   // solid stiffness [nz_s][P]
+  const float* __restrict__ C13;
+  const float* __restrict__ C33;
+  const float* __restrict__ C55;
+  const float* __restrict__ rhos;  // solid density
+  const float* __restrict__ J;     // metric, global rows
+  const float* __restrict__ xix;
+  const float* __restrict__ xiz;
+  const float* __restrict__ zex;
+  const float* __restrict__ zez;
+  const float4* __restrict__ pmlx;  // per column: d/beta, alpha + d/beta, 1/beta
+  const float4* __restrict__ pmlz;  // per solid row (zeta strip)
+  const float2* __restrict__ nrm;   // interface unit normal per column
+  const float* __restrict__ src_amp;  // Ricker value per (step, stage): [steps][4]
+  int src_steps;
+  int srcx, srcz;                   // source column / fluid row (srcx < 0: none)
+  float rk_c[4];                    // dt/2, dt/2, dt, dt/6
+  float rk_w[3];                    // dt/6, dt/3, dt/3
+  int gap;                          // record interval in steps
+  int rec_cap;                      // record ring capacity in samples
+  float* rec;                       // [rec_cap][3][nx]: solid vx, solid vz, fluid p
+  int* step;                        // device step counter (time index of the running step)
+  unsigned* done;                   // block arrival counter of the finish kernel
+  float* ipre;                      // interface rows before the filter [8][P]
+  int* status;                      // sticky error word (non-finite detector)
+};
+
+// One RK4 state set (state, stage ping/pong or accumulator).
+struct Fields {
+  float* fvx; float* fvz; float* fp;
+  float* svx; float* svz; float* ssx; float* ssz; float* ssxz;
+  float* fx[4];  // fluid xi ADE: Vx, Vz, Ex, Ez
+  float* sx[4];  // solid xi ADE
+  float* sz[4];  // solid zeta ADE
+};
+
+__constant__ float c_srcw[25];  // 5x5 source spreading weights (src/elements.cu:34-40)
+__constant__ float c_w7[7];     // interface filter weights (src/elements.cu:30-33)
+
+template <class T>
+__device__ __forceinline__ T ldg(const T* p) { return __ldg(p); }
+
+// Biased derivative from five taps f(-3..+3) around the centre (tools_func.cuh:50-92).
+template <int DIR>
+__device__ __forceinline__ float d5(float m3, float m2, float m1, float c0, float p1, float p2,
+                                    float p3) {
+  if (DIR == kDirF) return kAm1 * m1 + kA0 * c0 + kA1 * p1 + kA2 * p2 + kA3 * p3;
+  return -kAm1 * p1 - kA0 * c0 - kA1 * m1 - kA2 * m2 - kA3 * m3;
+}
+
+// Zeta derivative with the order lowered near a boundary (tools_func.cuh:94-140).
+// `col(j)` returns the value j rows away in the same column.
+template <int DIR, class Col>
+__device__ __forceinline__ float dz_near(const Col& col, int dist, bool solid_side) {
+  if (dist >= 3) return d5<DIR>(col(-3), col(-2), col(-1), col(0), col(1), col(2), col(3));
+  if (dist == 2) {
+    if (DIR == kDirF) return kM42_0 * col(0) + kM42_1 * col(1) + kM42_2 * col(2);
+    return -kM42_0 * col(0) - kM42_1 * col(-1) - kM42_2 * col(-2);
+  }
+  const bool fwd = (dist == 1) ? (DIR == kDirF) : solid_side;
+  if (fwd) return -1.0f * col(0) + 1.0f * col(1);
+  return 1.0f * col(0) - 1.0f * col(-1);
+}
+
+// The biased derivative of a two-component flux (tools_func.cuh:142-188).
+template <int DIR, class Fn>
+__device__ __forceinline__ float2 dflux(const Fn& F) {
+  if (DIR == kDirF) {
+    const float2 m1 = F(-1), c0 = F(0), p1 = F(1), p2 = F(2), p3 = F(3);
+    return make_float2(kAm1 * m1.x + kA0 * c0.x + kA1 * p1.x + kA2 * p2.x + kA3 * p3.x,
+                       kAm1 * m1.y + kA0 * c0.y + kA1 * p1.y + kA2 * p2.y + kA3 * p3.y);
+  }
+  const float2 p1 = F(1), c0 = F(0), m1 = F(-1), m2 = F(-2), m3 = F(-3);
+  return make_float2(-(kAm1 * p1.x + kA0 * c0.x + kA1 * m1.x + kA2 * m2.x + kA3 * m3.x),
+                     -(kAm1 * p1.y + kA0 * c0.y + kA1 * m1.y + kA2 * m2.y + kA3 * m3.y));
+}
+
+// Slot of column ix in the xi-strip arrays (valid only where the cell is in a side strip).
+__device__ __forceinline__ int xstrip_col(int ix, int nx, int npd) {
+  return (ix - 3 < npd) ? ix - 3 : npd + ix - (nx - 3 - npd);
+}
+
+// Output of the right-hand side at one fluid cell.
+struct FluidK {
+  float vx, vz, p;
+  float V0, V1, E0, E1;  // xi-ADE RHS (valid only in the side strips)
+  bool has_E;            // false on the free-surface row (p fixed)
+};
+
+// Output of the right-hand side at one solid cell.
+struct SolidK {
+  float vx, vz, sx, sz, sxz;
+  float XV0, XV1, XE0, XE1;  // xi-ADE RHS (side strips)
+  float ZV0, ZV1, ZE0, ZE1;  // zeta-ADE RHS (bottom strip)
+};
+
+// Fluid RHS at (iz, ix), iz in [3, nz_f-1] (pml_fs_kernels.cuh:333-507).
+// `A` reads the stage input: A.fp(dz, dx), A.fvx(dz, dx), A.fvz(dz, dx) relative
+// to the cell; `ade` holds the stage-input ADE memory (V0, V1, E0, E1) of the cell.
+template <int DIR, class Acc>
+__device__ __forceinline__ FluidK fluid_rhs(const Coef& C, const Acc& A, int iz, int ix,
+                                            bool side, const float* ade) {
+  FluidK o;
+  const int P = C.P, nzf = C.nzf;
+  const size_t g = (size_t)iz * P + ix;
+  const float xix = ldg(C.xix + g), xiz = ldg(C.xiz + g), zex = ldg(C.zex + g),
+              zez = ldg(C.zez + g);
+  const float gxx = xix * xix + xiz * xiz;
+  const int d_if = nzf - 1 - iz, d_fs = iz - 3;
+  float4 pml = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (side) pml = ldg(C.pmlx + ix);
+
+  // ---- momentum: rho dv/dt = -grad p ----
+  {
+    float rvx, rvz, divx = 0.f, divz = 0.f;
+    if (d_if < 3 || d_fs < 3) {
+      // conservative flux form with mirrored ghosts (pml_fs_kernels.cuh:356-415)
+      auto Ff = [&](int r) -> float2 {
+        const size_t k = (size_t)r * P + ix;
+        const float Jk = ldg(C.J + k), pk = A.fp(r - iz, 0);
+        return make_float2(-Jk * ldg(C.zex + k) * pk, -Jk * ldg(C.zez + k) * pk);
+      };
+      auto Fxi = [&](int j) -> float2 {
+        const size_t k = g + j;
+        const float Jk = ldg(C.J + k), pk = A.fp(0, j);
+        return make_float2(-Jk * ldg(C.xix + k) * pk, -Jk * ldg(C.xiz + k) * pk);
+      };
+      auto Fze = [&](int j) -> float2 {
+        const int r = iz + j;
+        if (d_if < 3) {
+          if (r <= nzf - 1) return Ff(r);
+          const float2 a = Ff(nzf - 1), b = Ff(2 * (nzf - 1) - r);  // G = 2F0 - Fn
+          return make_float2(2 * a.x - b.x, 2 * a.y - b.y);
+        }
+        if (r >= 3) return Ff(r);
+        const float2 b = Ff(6 - r);  // free-surface image: G = -Fn
+        return make_float2(-b.x, -b.y);
+      };
+      const float2 a = dflux<DIR>(Fxi), b = dflux<DIR>(Fze);
+      const float Sx = a.x + b.x, Sz = a.y + b.y, Jc = ldg(C.J + g);
+      rvx = Sx / Jc;
+      rvz = Sz / Jc;
+      if (side) {
+        divx = xix * (xix * Sx + xiz * Sz) / (gxx * Jc);
+        divz = xiz * (xix * Sx + xiz * Sz) / (gxx * Jc);
+      }
+    } else {
+      const float dpdx = d5<DIR>(A.fp(0, -3), A.fp(0, -2), A.fp(0, -1), A.fp(0, 0), A.fp(0, 1),
+                                 A.fp(0, 2), A.fp(0, 3));
+      const float dpdz = d5<DIR>(A.fp(-3, 0), A.fp(-2, 0), A.fp(-1, 0), A.fp(0, 0), A.fp(1, 0),
+                                 A.fp(2, 0), A.fp(3, 0));
+      rvx = -(xix * dpdx + zex * dpdz);
+      rvz = -(xiz * dpdx + zez * dpdz);
+      if (side) {
+        const float gxz = xix * zex + xiz * zez;
+        divx = -xix * (gxx * dpdx + gxz * dpdz) / gxx;
+        divz = -xiz * (gxx * dpdx + gxz * dpdz) / gxx;
+      }
+    }
+    const float rho = ldg(C.rhof + g);
+    o.vx = rvx / rho;
+    o.vz = rvz / rho;
+    if (side) {
+      const float dpb = pml.x, apdpb = pml.y, invb = pml.z;
+      o.V0 = -apdpb * ade[0] + dpb * divx;
+      o.V1 = -apdpb * ade[1] + dpb * divz;
+      o.vx += ((invb - 1.0f) * divx - invb * ade[0]) / rho;
+      o.vz += ((invb - 1.0f) * divz - invb * ade[1]) / rho;
+    }
+  }
+  // ---- pressure: dp/dt = -K div v ----
+  o.has_E = (iz != 3);
+  if (iz == 3) {
+    o.p = 0.0f;  // pressure-free surface row
+  } else {
+    auto vxc = [&](int j) { return A.fvx(j, 0); };
+    auto vzc = [&](int j) { return A.fvz(j, 0); };
+    const float dvxdx = d5<DIR>(A.fvx(0, -3), A.fvx(0, -2), A.fvx(0, -1), A.fvx(0, 0),
+                                A.fvx(0, 1), A.fvx(0, 2), A.fvx(0, 3));
+    const float dvzdx = d5<DIR>(A.fvz(0, -3), A.fvz(0, -2), A.fvz(0, -1), A.fvz(0, 0),
+                                A.fvz(0, 1), A.fvz(0, 2), A.fvz(0, 3));
+    const int dn = min(iz - 3, nzf - 1 - iz);
+    const float dvxdz = dz_near<DIR>(vxc, dn, false);
+    const float dvzdz = dz_near<DIR>(vzc, dn, false);
+    const float Kc = ldg(C.K + g);
+    o.p = -Kc * (xix * dvxdx + zex * dvxdz + xiz * dvzdx + zez * dvzdz);
+    if (side) {
+      const float gxz = xix * zex + xiz * zez;
+      const float Dvx = dvxdx + (gxz / gxx) * dvxdz, Dvz = dvzdx + (gxz / gxx) * dvzdz;
+      const float dpb = pml.x, apdpb = pml.y, invb = pml.z;
+      o.E0 = -apdpb * ade[2] + dpb * Dvx;
+      o.E1 = -apdpb * ade[3] + dpb * Dvz;
+      o.p += Kc * (-(invb - 1.0f) * xix * Dvx - (invb - 1.0f) * xiz * Dvz + invb * xix * ade[2] +
+                   invb * xiz * ade[3]);
+    }
+  }
+  return o;
+}
+
+// Solid RHS at (iz, ix), iz in [0, nz_s-4] (pml_fs_kernels.cuh:509-752).
+// `A` reads the stage input: A.svx, A.svz, A.ssx, A.ssz, A.ssxz (dz, dx);
+// `xade` / `zade` are the stage-input xi / zeta ADE memory of the cell.
+template <int DIR, class Acc>
+__device__ __forceinline__ SolidK solid_rhs(const Coef& C, const Acc& A, int iz, int ix, bool side,
+                                            bool bottom, const float* xade, const float* zade) {
+  SolidK o;
+  const int P = C.P, nzf = C.nzf;
+  const size_t m = (size_t)iz * P + ix;
+  const size_t g = m + (size_t)(nzf - 1) * P;
+  const float xix = ldg(C.xix + g), xiz = ldg(C.xiz + g), zex = ldg(C.zex + g),
+              zez = ldg(C.zez + g);
+  float4 px = make_float4(0.f, 0.f, 0.f, 0.f), pz = px;
+  if (side) px = ldg(C.pmlx + ix);
+  if (bottom) pz = ldg(C.pmlz + iz);
+
+  // ---- momentum: rho dv/dt = div sigma ----
+  {
+    float rvx, rvz, dxx = 0.f, dxz = 0.f, dzx = 0.f, dzz = 0.f;
+    if (iz < 3) {
+      // conservative flux form with the interface ghost G = 2F0 - Fn (pml_fs_kernels.cuh:654-680)
+      auto Fs = [&](int r) -> float2 {
+        const size_t k = (size_t)(r + nzf - 1) * P + ix;
+        const float Jk = ldg(C.J + k), ax = ldg(C.zex + k), az = ldg(C.zez + k);
+        const int dz = r - iz;
+        return make_float2(Jk * (ax * A.ssx(dz, 0) + az * A.ssxz(dz, 0)),
+                           Jk * (ax * A.ssxz(dz, 0) + az * A.ssz(dz, 0)));
+      };
+      auto Fxi = [&](int j) -> float2 {
+        const size_t k = g + j;
+        const float Jk = ldg(C.J + k), ax = ldg(C.xix + k), az = ldg(C.xiz + k);
+        return make_float2(Jk * (ax * A.ssx(0, j) + az * A.ssxz(0, j)),
+                           Jk * (ax * A.ssxz(0, j) + az * A.ssz(0, j)));
+      };
+      auto Fze = [&](int j) -> float2 {
+        const int r = iz + j;
+        if (r >= 0) return Fs(r);
+        const float2 a = Fs(0), b = Fs(-r);
+        return make_float2(2 * a.x - b.x, 2 * a.y - b.y);
+      };
+      const float2 a = dflux<DIR>(Fxi), b = dflux<DIR>(Fze);
+      const float Sx = a.x + b.x, Sz = a.y + b.y, Jc = ldg(C.J + g);
+      rvx = Sx / Jc;
+      rvz = Sz / Jc;
+      if (side) {
+        const float gxx = xix * xix + xiz * xiz;
+        dxx = xix * (xix * Sx + xiz * Sz) / (gxx * Jc);
+        dxz = xiz * (xix * Sx + xiz * Sz) / (gxx * Jc);
+      }
+      if (bottom) {
+        const float gzz = zex * zex + zez * zez;
+        dzx = zex * (zex * Sx + zez * Sz) / (gzz * Jc);
+        dzz = zez * (zex * Sx + zez * Sz) / (gzz * Jc);
+      }
+    } else {
+      const float sxdx = d5<DIR>(A.ssx(0, -3), A.ssx(0, -2), A.ssx(0, -1), A.ssx(0, 0),
+                                 A.ssx(0, 1), A.ssx(0, 2), A.ssx(0, 3));
+      const float sxdz = d5<DIR>(A.ssx(-3, 0), A.ssx(-2, 0), A.ssx(-1, 0), A.ssx(0, 0),
+                                 A.ssx(1, 0), A.ssx(2, 0), A.ssx(3, 0));
+      const float szdx = d5<DIR>(A.ssz(0, -3), A.ssz(0, -2), A.ssz(0, -1), A.ssz(0, 0),
+                                 A.ssz(0, 1), A.ssz(0, 2), A.ssz(0, 3));
+      const float szdz = d5<DIR>(A.ssz(-3, 0), A.ssz(-2, 0), A.ssz(-1, 0), A.ssz(0, 0),
+                                 A.ssz(1, 0), A.ssz(2, 0), A.ssz(3, 0));
+      const float tdx = d5<DIR>(A.ssxz(0, -3), A.ssxz(0, -2), A.ssxz(0, -1), A.ssxz(0, 0),
+                                A.ssxz(0, 1), A.ssxz(0, 2), A.ssxz(0, 3));
+      const float tdz = d5<DIR>(A.ssxz(-3, 0), A.ssxz(-2, 0), A.ssxz(-1, 0), A.ssxz(0, 0),
+                                A.ssxz(1, 0), A.ssxz(2, 0), A.ssxz(3, 0));
+      rvx = xix * sxdx + zex * sxdz + xiz * tdx + zez * tdz;
+      rvz = xix * tdx + zex * tdz + xiz * szdx + zez * szdz;
+      if (side || bottom) {
+        const float gxz = xix * zex + xiz * zez;
+        if (side) {
+          const float gxx = xix * xix + xiz * xiz;
+          dxx = xix * (sxdx + gxz / gxx * sxdz) + xiz * (tdx + gxz / gxx * tdz);
+          dxz = xix * (tdx + gxz / gxx * tdz) + xiz * (szdx + gxz / gxx * szdz);
+        }
+        if (bottom) {
+          const float gzz = zex * zex + zez * zez;
+          dzx = zex * (sxdz + gxz / gzz * sxdx) + zez * (gxz / gzz * tdx + tdz);
+          dzz = zex * (gxz / gzz * tdx + tdz) + zez * (gxz / gzz * szdx + szdz);
+        }
+      }
+    }
+    const float rho = ldg(C.rhos + m);
+    o.vx = rvx / rho;
+    o.vz = rvz / rho;
+    if (side) {
+      const float dpb = px.x, apdpb = px.y, invb = px.z;
+      o.XV0 = -apdpb * xade[0] + dpb * dxx;
+      o.XV1 = -apdpb * xade[1] + dpb * dxz;
+      o.vx += ((invb - 1.0f) * dxx - invb * xade[0]) / rho;
+      o.vz += ((invb - 1.0f) * dxz - invb * xade[1]) / rho;
+    }
+    if (bottom) {
+      const float dpb = pz.x, apdpb = pz.y, invb = pz.z;
+      o.ZV0 = -apdpb * zade[0] + dpb * dzx;
+      o.ZV1 = -apdpb * zade[1] + dpb * dzz;
+      o.vx += ((invb - 1.0f) * dzx - invb * zade[0]) / rho;
+      o.vz += ((invb - 1.0f) * dzz - invb * zade[1]) / rho;
+    }
+  }
+  // ---- stress: VTI constitutive law ----
+  {
+    auto vxc = [&](int j) { return A.svx(j, 0); };
+    auto vzc = [&](int j) { return A.svz(j, 0); };
+    const float dvxdx = d5<DIR>(A.svx(0, -3), A.svx(0, -2), A.svx(0, -1), A.svx(0, 0),
+                                A.svx(0, 1), A.svx(0, 2), A.svx(0, 3));
+    const float dvzdx = d5<DIR>(A.svz(0, -3), A.svz(0, -2), A.svz(0, -1), A.svz(0, 0),
+                                A.svz(0, 1), A.svz(0, 2), A.svz(0, 3));
+    const float dvxdz = dz_near<DIR>(vxc, iz, true);
+    const float dvzdz = dz_near<DIR>(vzc, iz, true);
+    const float c11 = ldg(C.C11 + m), c13 = ldg(C.C13 + m), c33 = ldg(C.C33 + m),
+                c55 = ldg(C.C55 + m);
+    o.sx = c11 * (xix * dvxdx + zex * dvxdz) + c13 * (xiz * dvzdx + zez * dvzdz);
+    o.sz = c13 * (xix * dvxdx + zex * dvxdz) + c33 * (xiz * dvzdx + zez * dvzdz);
+    o.sxz = c55 * (xiz * dvxdx + zez * dvxdz + xix * dvzdx + zex * dvzdz);
+    if (side || bottom) {
+      const float gxz = xix * zex + xiz * zez;
+      if (side) {
+        const float gxx = xix * xix + xiz * xiz;
+        const float Dvx = dvxdx + (gxz / gxx) * dvxdz, Dvz = dvzdx + (gxz / gxx) * dvzdz;
+        const float dpb = px.x, apdpb = px.y, invb = px.z;
+        const float E0 = xade[2], E1 = xade[3];
+        o.XE0 = -apdpb * E0 + dpb * Dvx;
+        o.XE1 = -apdpb * E1 + dpb * Dvz;
+        o.sx += c11 * (invb - 1.0f) * xix * Dvx + c13 * (invb - 1.0f) * xiz * Dvz -
+                invb * c11 * xix * E0 - invb * c13 * xiz * E1;
+        o.sz += c13 * (invb - 1.0f) * xix * Dvx + c33 * (invb - 1.0f) * xiz * Dvz -
+                invb * c13 * xix * E0 - invb * c33 * xiz * E1;
+        o.sxz += c55 * (invb - 1.0f) * (xiz * Dvx + xix * Dvz) - invb * c55 * xiz * E0 -
+                 invb * c55 * xix * E1;
+      }
+      if (bottom) {
+        const float gzz = zex * zex + zez * zez;
+        const float Dvx = dvxdz + (gxz / gzz) * dvxdx, Dvz = dvzdz + (gxz / gzz) * dvzdx;
+        const float dpb = pz.x, apdpb = pz.y, invb = pz.z;
+        const float E0 = zade[2], E1 = zade[3];
+        o.ZE0 = -apdpb * E0 + dpb * Dvx;
+        o.ZE1 = -apdpb * E1 + dpb * Dvz;
+        o.sx += c11 * (invb - 1.0f) * zex * Dvx + c13 * (invb - 1.0f) * zez * Dvz -
+                invb * c11 * zex * E0 - invb * c13 * zez * E1;
+        o.sz += c13 * (invb - 1.0f) * zex * Dvx + c33 * (invb - 1.0f) * zez * Dvz -
+                invb * c13 * zex * E0 - invb * c33 * zez * E1;
+        o.sxz += c55 * (invb - 1.0f) * (zez * Dvx + zex * Dvz) - invb * c55 * zez * E0 -
+                 invb * c55 * zex * E1;
+      }
+    }
+  }
+  return o;
+}
+
+// Source term of stage `s` at fluid cell (iz, ix): 5x5 Gaussian spreading of the
+// Ricker value, skipped within 3 cells of any edge (tools_func.cuh:21-37).
+__device__ __forceinline__ float source_term(const Coef& C, int iz, int ix, int it, int s) {
+  const int dx = ix - C.srcx, dz = iz - C.srcz;
+  if (C.srcx < 0 || dx < -2 || dx > 2 || dz < -2 || dz > 2) return 0.0f;
+  if (ix <= 2 || ix >= C.nx - 3 || iz <= 2 || iz >= C.nzf - 3) return 0.0f;
+  if (it < 0 || it >= C.src_steps) return 0.0f;
+  const float amp = ldg(C.src_amp + (size_t)it * 4 + s);
+  return amp * c_srcw[(dz + 2) * 5 + (dx + 2)];
+}
+
+// RK4 bookkeeping for one value (src/pml_fs_kernels.cu:663-763, fused):
+//   first stage: out = u + c k,  acc = u + w k
+//   middle:      out = Un + c k, acc += w k
+//   last:        out = acc + c k
+template <int KIND>
+__device__ __forceinline__ void rk_update(float k, float uin, const float* __restrict__ Un,
+                                          float* __restrict__ out, float* __restrict__ acc,
+                                          size_t i, float c, float w) {
+  if (KIND == kStageFirst) {
+    out[i] = fmaf(c, k, uin);
+    acc[i] = fmaf(w, k, uin);
+  } else if (KIND == kStageMid) {
+    out[i] = fmaf(c, k, Un[i]);
+    acc[i] = fmaf(w, k, acc[i]);
+  } else {
+    out[i] = fmaf(c, k, acc[i]);
+  }
+}
+
+}  // namespace mfdm

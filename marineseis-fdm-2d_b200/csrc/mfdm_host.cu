@@ -1,0 +1,853 @@
+// Host side of libmfdm: the C ABI declared in include/mfdm.h.
+//
+// Replaces the reference's MemManager (src/elements.cu), the stream handshake
+// and the launch sequence of PmlFs::FluidSolid::update_RK4
+// (src/pml_fs_kernels.cu:533-868) and the drop-in CLI (src/main.cu). One
+// non-blocking stream per handle; the time loop is captured once as a CUDA
+// graph of kGraphSteps steps and replayed; receivers are sampled on the
+// device into a buffer drained once per shot.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/mfdm.h"
+#include "json_config.h"
+#include "mfdm_kernels.h"
+
+namespace fs = std::filesystem;
+using mfdm::Coef;
+using mfdm::Fields;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define MFDM_CU(call)                                                                  \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail(e_ == cudaErrorMemoryAllocation ? MFDM_ERR_NOMEM : MFDM_ERR_CUDA,     \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                  \
+  } while (0)
+
+constexpr int kGraphSteps = 32;  // steps per captured graph (must be even)
+
+// 5x5 source weights (src/elements.cu:34-40) and the interface filter (src/elements.cu:30-33).
+const float kSrcW[25] = {0.0030f, 0.0133f, 0.0219f, 0.0133f, 0.0030f, 0.0133f, 0.0596f,
+                         0.0983f, 0.0596f, 0.0133f, 0.0219f, 0.0983f, 0.1621f, 0.0983f,
+                         0.0219f, 0.0133f, 0.0596f, 0.0983f, 0.0596f, 0.0133f, 0.0030f,
+                         0.0133f, 0.0219f, 0.0133f, 0.0030f};
+const float kW7[7] = {1.1e-13f, 1.678e-06f, 0.03419f, 0.93163f, 0.03419f, 1.678e-06f, 1.1e-13f};
+
+struct HostModel {
+  int nx = 0, nzf = 0, nzs = 0;
+  float fpeak = 0.f, dt = 0.f;
+  int nt = 0, snapshot = 1;
+  int npd = 0, npow = 2;
+  float thickness = 0.f, vp_max = 0.f, rc = 0.f, beta0 = 1.f;
+  std::vector<int> srcx, srcz;
+  // host arrays, [rows][nx]
+  std::vector<float> K, rhof, C11, C13, C33, C55, rhos, J, xix, xiz, zex, zez;
+};
+
+int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// Ricker wavelet in the reference's host arithmetic (src/elements.cu:385-392):
+// float time, T = 1.2 / fpeak, the phase product in double rounded to float.
+float ricker_ref(float fpeak, float time) {
+  const float T = float(1.2 / double(fpeak));
+  const float t = time - T;
+  if (t > T) return 0.0f;
+  float temp = float(M_PI * double(fpeak) * double(t));
+  temp *= temp;
+  return (1 - 2 * temp) * expf(-temp);
+}
+
+}  // namespace
+
+struct mfdm_model {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  HostModel cfg;  // scalars (arrays released after upload)
+  int P = 0, Ps = 0, nz = 0, gap = 1;
+  int isrc = 0;
+  int host_step = 0;
+  char* dmem = nullptr;
+  size_t dbytes = 0;
+  Fields S[4];  // U, stage A, stage B, accumulator
+  Coef C{};
+  float* d_src = nullptr;
+  int src_steps = 0;
+  float* d_rec = nullptr;
+  int rec_cap = 0;
+  cudaGraphExec_t graph = nullptr;
+  int cur_device_saved = -1;
+};
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+int validate(const HostModel& h) {
+  if (h.nx < 8 || h.nzf < 8 || h.nzs < 8)
+    return fail(MFDM_ERR_ARG, "grid too small: need nx, nz_f, nz_s >= 8");
+  if (h.npd < 0 || 2 * h.npd > h.nx - 6 || h.npd > h.nzs)
+    return fail(MFDM_ERR_ARG, "PML width npd does not fit the grid");
+  if (!(h.dt > 0.f) || !(h.fpeak > 0.f)) return fail(MFDM_ERR_ARG, "dt and fpeak must be > 0");
+  if (h.nt < 0) return fail(MFDM_ERR_ARG, "nt must be >= 0");
+  if (h.snapshot <= 0) return fail(MFDM_ERR_ARG, "snapshot interval must be > 0");
+  if (h.srcx.size() != h.srcz.size()) return fail(MFDM_ERR_ARG, "posx/posz length mismatch");
+  const size_t nf = size_t(h.nx) * h.nzf, ns = size_t(h.nx) * h.nzs,
+               ng = size_t(h.nx) * (h.nzf + h.nzs - 1);
+  if (h.K.size() != nf || h.rhof.size() != nf || h.C11.size() != ns || h.C13.size() != ns ||
+      h.C33.size() != ns || h.C55.size() != ns || h.rhos.size() != ns || h.J.size() != ng ||
+      h.xix.size() != ng || h.xiz.size() != ng || h.zex.size() != ng || h.zez.size() != ng)
+    return fail(MFDM_ERR_ARG, "array sizes do not match the grid");
+  return MFDM_OK;
+}
+
+// CFS-PML profile of one axis in FP64 (src/elements.cu:121-124, 824-873):
+// d = d0 r^NPOW, beta = 1 + (beta0-1) r^2, alpha = alpha0 (1 - r), r = k/npd,
+// k counted from the inner edge of the band of npd cells inside 3 frozen cells.
+// Stored per cell as (d/beta, alpha + d/beta, 1/beta), the factors the
+// reference derives inside every kernel.
+void pml_profile(const HostModel& h, int n, bool lo, bool hi, std::vector<float4>& out) {
+  const double alpha0 = 2.0 * M_PI * double(h.fpeak);
+  const double d0 = -(h.npow + 1) * double(h.vp_max) * std::log(double(h.rc)) /
+                    (2.0 * double(h.thickness));
+  out.assign(size_t(n), make_float4(0.f, 1.f, 1.f, 0.f));
+  for (int i = 0; i < n; ++i) {
+    int k = -1;
+    if (lo && i >= 3 && i <= 2 + h.npd) k = 3 + h.npd - i;
+    if (hi && i >= n - 3 - h.npd && i <= n - 4) k = i - (n - 4 - h.npd);
+    double d = 0.0, be = 1.0, al = alpha0;
+    if (k > 0) {
+      const double r = double(k) / double(h.npd);
+      d = d0 * std::pow(r, double(h.npow));
+      be = 1.0 + (double(h.beta0) - 1.0) * r * r;
+      al = alpha0 * (1.0 - r);
+    }
+    const double dpb = d / be;
+    out[size_t(i)] = make_float4(float(dpb), float(al + dpb), float(1.0 / be), 0.f);
+  }
+}
+
+int read_bin(const std::string& path, size_t count, std::vector<float>& out) {
+  out.resize(count);
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) return fail(MFDM_ERR_IO, "Failed to open file: " + path);
+  const size_t got = std::fread(out.data(), sizeof(float), count, f);
+  std::fclose(f);
+  if (got != count) return fail(MFDM_ERR_IO, "Failed to read data from file: " + path);
+  return MFDM_OK;
+}
+
+// Reads the JSON schema of json_template.json (src/elements.cu:64-176).
+int load_json(const char* path, HostModel& h) {
+  try {
+    const mfdm::JsonConfig J = mfdm::JsonConfig::from_file(path);
+    h.fpeak = J.get_float("base.fpeak");
+    h.dt = J.get_float("base.dt");
+    h.nt = J.get_int("base.nt");
+    h.snapshot = J.get_int("base.snapshot");
+    const int calc_type = J.get_int("grid.calc_type");
+    const int bdy = J.get_int("grid.boundary_type");
+    if (calc_type != 1 || bdy != 2)
+      return fail(MFDM_ERR_ARG,
+                  "unsupported configuration: only calc_type 1 (fluid over solid) with "
+                  "boundary_type 2 (CFS-PML sides and bottom, free surface on top)");
+    const size_t nsrc = J.size("grid.src_pos.posx");
+    for (size_t i = 0; i < nsrc; ++i) {
+      h.srcx.push_back(J.get_int("grid.src_pos.posx", i));
+      h.srcz.push_back(J.get_int("grid.src_pos.posz", i));
+    }
+    h.nx = J.get_int("grid.solid.nx");
+    h.nzs = J.get_int("grid.solid.nz");
+    const int nxf = J.get_int("grid.fluid.nx");
+    h.nzf = J.get_int("grid.fluid.nz");
+    if (nxf != h.nx) return fail(MFDM_ERR_CONFIG, "nx_fluid doesn't match nx_solid!");
+    h.npd = J.get_int("PML.npd");
+    h.thickness = J.get_float("PML.thickness");
+    h.npow = J.get_int("PML.NPOW");
+    h.vp_max = J.get_float("PML.Vp_max");
+    h.rc = J.get_float("PML.Rc");
+    h.beta0 = J.get_float("PML.beta0");
+    if (h.nx <= 0 || h.nzf <= 0 || h.nzs <= 0) return fail(MFDM_ERR_CONFIG, "bad grid size");
+    const size_t nf = size_t(h.nx) * h.nzf, ns = size_t(h.nx) * h.nzs,
+                 ng = size_t(h.nx) * (h.nzf + h.nzs - 1);
+    struct Item { const char* key; std::vector<float>* dst; size_t n; } items[] = {
+        {"grid.solid.C11", &h.C11, ns}, {"grid.solid.C13", &h.C13, ns},
+        {"grid.solid.C33", &h.C33, ns}, {"grid.solid.C55", &h.C55, ns},
+        {"grid.solid.rho", &h.rhos, ns}, {"grid.fluid.K", &h.K, nf},
+        {"grid.fluid.rho", &h.rhof, nf}, {"grid.jacob.J", &h.J, ng},
+        {"grid.jacob.xi_x", &h.xix, ng}, {"grid.jacob.xi_z", &h.xiz, ng},
+        {"grid.jacob.ze_x", &h.zex, ng}, {"grid.jacob.ze_z", &h.zez, ng}};
+    for (const Item& it : items) {
+      const int rc = read_bin(J.get_string(it.key), it.n, *it.dst);
+      if (rc != MFDM_OK) return rc;
+    }
+  } catch (const std::exception& e) {
+    return fail(MFDM_ERR_CONFIG, e.what());
+  }
+  return MFDM_OK;
+}
+
+void fill_src_table(const HostModel& h, int steps, std::vector<float>& amp) {
+  amp.assign(size_t(steps) * 4, 0.f);
+  const float dt = h.dt;
+  const float half = float(double(dt) * 0.5);
+  for (int it = 0; it < steps; ++it) {
+    const float t = float(it) * dt;  // `const float time = it * mem.dt` (src/pml_fs_kernels.cu:770)
+    amp[size_t(it) * 4 + 0] = ricker_ref(h.fpeak, t);
+    amp[size_t(it) * 4 + 1] = ricker_ref(h.fpeak, t + half);
+    amp[size_t(it) * 4 + 2] = ricker_ref(h.fpeak, t + half);
+    amp[size_t(it) * 4 + 3] = ricker_ref(h.fpeak, t + dt);
+  }
+}
+
+void release_graph(mfdm_model* m) {
+  if (m->graph) {
+    cudaGraphExecDestroy(m->graph);
+    m->graph = nullptr;
+  }
+}
+
+// Grows the source table and the receiver buffer so that steps up to `steps` fit.
+int ensure_capacity(mfdm_model* m, int steps) {
+  if (steps > m->src_steps) {
+    const int cap = std::max(steps, m->src_steps * 2);
+    std::vector<float> amp;
+    fill_src_table(m->cfg, cap, amp);
+    float* d = nullptr;
+    MFDM_CU(cudaMalloc(&d, amp.size() * sizeof(float)));
+    MFDM_CU(cudaMemcpy(d, amp.data(), amp.size() * sizeof(float), cudaMemcpyHostToDevice));
+    if (m->d_src) cudaFree(m->d_src);
+    m->d_src = d;
+    m->src_steps = cap;
+    release_graph(m);
+  }
+  const int need = (steps + m->gap - 1) / m->gap;
+  if (need > m->rec_cap) {
+    const int cap = std::max(need, m->rec_cap * 2);
+    const size_t row = size_t(3) * m->cfg.nx * sizeof(float);
+    float* d = nullptr;
+    MFDM_CU(cudaMalloc(&d, size_t(cap) * row));
+    MFDM_CU(cudaMemsetAsync(d, 0, size_t(cap) * row, m->stream));
+    if (m->d_rec) {
+      MFDM_CU(cudaMemcpyAsync(d, m->d_rec, size_t(m->rec_cap) * row, cudaMemcpyDeviceToDevice,
+                              m->stream));
+      MFDM_CU(cudaStreamSynchronize(m->stream));
+      cudaFree(m->d_rec);
+    }
+    m->d_rec = d;
+    m->rec_cap = cap;
+    release_graph(m);
+  }
+  m->C.src_amp = m->d_src;
+  m->C.src_steps = m->src_steps;
+  m->C.rec = m->d_rec;
+  m->C.rec_cap = m->rec_cap;
+  return MFDM_OK;
+}
+
+// Enqueues the five launches of one step. With `ev` (6 events) an event is
+// recorded before the first launch and after every launch.
+int enqueue_step(mfdm_model* m, int it, cudaStream_t st, cudaEvent_t* ev = nullptr) {
+  const int d0 = (it & 1) ? mfdm::kDirB : mfdm::kDirF, d1 = 1 - d0;
+  const Fields &U = m->S[0], &A = m->S[1], &B = m->S[2], &Acc = m->S[3];
+  const Coef& C = m->C;
+  // stage s reads in[s] and writes out[s]: U -> A -> B -> A -> U
+  const Fields* in[4] = {&U, &A, &B, &A};
+  const Fields* out[4] = {&A, &B, &A, &U};
+  const int dir[4] = {d0, d1, d0, d1};
+  if (ev) MFDM_CU(cudaEventRecord(ev[0], st));
+  for (int s = 0; s < 4; ++s) {
+    MFDM_CU(mfdm::launch_stage(C, *in[s], *out[s], U, Acc, s, dir[s], st));
+    if (ev) MFDM_CU(cudaEventRecord(ev[s + 1], st));
+  }
+  MFDM_CU(mfdm::launch_finish(C, U, st));
+  if (ev) MFDM_CU(cudaEventRecord(ev[5], st));
+  return MFDM_OK;
+}
+
+// Enqueues `nsteps` steps from host_step: graph replays where possible.
+int enqueue_steps(mfdm_model* m, int nsteps);
+
+int capture_graph(mfdm_model* m) {
+  cudaGraph_t g = nullptr;
+  MFDM_CU(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = MFDM_OK;
+  for (int k = 0; k < kGraphSteps && rc == MFDM_OK; ++k) rc = enqueue_step(m, k, m->stream);
+  cudaError_t e = cudaStreamEndCapture(m->stream, &g);
+  if (rc != MFDM_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(MFDM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&m->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(MFDM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  return MFDM_OK;
+}
+
+int check_status(mfdm_model* m) {
+  int st = 0;
+  MFDM_CU(cudaMemcpy(&st, m->C.status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st) return fail(MFDM_ERR_NONFINITE, "non-finite values reached the interface rows");
+  return MFDM_OK;
+}
+
+// Uploads the model arrays, the FP64-derived PML tables and normals, and the
+// scalars of `h` into the buffers of `m` (shape already checked).
+int upload_model(mfdm_model* m, const HostModel& h) {
+  const int nx = h.nx, nzf = h.nzf, nzs = h.nzs, nz = nzf + nzs - 1, P = m->P;
+  Coef& C = m->C;
+  auto up = [&](const float* dst_c, const std::vector<float>& v, int rows) -> int {
+    float* dst = const_cast<float*>(dst_c);
+    MFDM_CU(cudaMemcpy2DAsync(dst, size_t(P) * sizeof(float), v.data(), size_t(nx) * sizeof(float),
+                              size_t(nx) * sizeof(float), size_t(rows), cudaMemcpyHostToDevice,
+                              m->stream));
+    return MFDM_OK;
+  };
+  int rc;
+  if ((rc = up(C.K, h.K, nzf)) || (rc = up(C.rhof, h.rhof, nzf)) || (rc = up(C.C11, h.C11, nzs)) ||
+      (rc = up(C.C13, h.C13, nzs)) || (rc = up(C.C33, h.C33, nzs)) ||
+      (rc = up(C.C55, h.C55, nzs)) || (rc = up(C.rhos, h.rhos, nzs)) || (rc = up(C.J, h.J, nz)) ||
+      (rc = up(C.xix, h.xix, nz)) || (rc = up(C.xiz, h.xiz, nz)) || (rc = up(C.zex, h.zex, nz)) ||
+      (rc = up(C.zez, h.zez, nz)))
+    return rc;
+  std::vector<float4> px, pz;
+  pml_profile(h, nx, true, true, px);
+  pml_profile(h, nzs, false, true, pz);
+  // Interface unit normal n = grad(zeta)/|grad(zeta)| in FP64 (src/elements.cu:892-905).
+  std::vector<float2> nrm(static_cast<size_t>(nx));
+  for (int ix = 0; ix < nx; ++ix) {
+    const size_t i = size_t(nzf - 1) * nx + ix;
+    const double a = h.zex[i], b = h.zez[i], s = std::sqrt(a * a + b * b);
+    nrm[size_t(ix)] = s > 0 ? make_float2(float(a / s), float(b / s)) : make_float2(0.f, 1.f);
+  }
+  MFDM_CU(cudaMemcpyAsync(const_cast<float4*>(C.pmlx), px.data(), px.size() * sizeof(float4),
+                          cudaMemcpyHostToDevice, m->stream));
+  MFDM_CU(cudaMemcpyAsync(const_cast<float4*>(C.pmlz), pz.data(), pz.size() * sizeof(float4),
+                          cudaMemcpyHostToDevice, m->stream));
+  MFDM_CU(cudaMemcpyAsync(const_cast<float2*>(C.nrm), nrm.data(), nrm.size() * sizeof(float2),
+                          cudaMemcpyHostToDevice, m->stream));
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+
+  const float dt = h.dt;
+  // RK4 coefficients exactly as the reference forms them in float (src/pml_fs_kernels.cu:735,781-806).
+  C.rk_c[0] = dt / 2; C.rk_c[1] = dt / 2; C.rk_c[2] = dt; C.rk_c[3] = dt / 6.0f;
+  C.rk_w[0] = dt / 6; C.rk_w[1] = dt / 3; C.rk_w[2] = dt / 3;
+  m->gap = std::max(1, int(1e-3 / double(h.dt) + 0.5));  // src/main.cu:92
+  C.gap = m->gap;
+  // Keep the scalars only.
+  HostModel& c = m->cfg;
+  c.nx = h.nx; c.nzf = h.nzf; c.nzs = h.nzs;
+  c.fpeak = h.fpeak; c.dt = h.dt; c.nt = h.nt; c.snapshot = h.snapshot;
+  c.npd = h.npd; c.npow = h.npow; c.thickness = h.thickness;
+  c.vp_max = h.vp_max; c.rc = h.rc; c.beta0 = h.beta0;
+  c.srcx = h.srcx; c.srcz = h.srcz;
+  if (m->isrc >= int(c.srcx.size())) m->isrc = 0;
+  C.srcx = c.srcx.empty() ? -1 : c.srcx[size_t(m->isrc)];
+  C.srcz = c.srcx.empty() ? 0 : c.srcz[size_t(m->isrc)];
+  // The source table depends on fpeak and dt: rebuild it.
+  if (m->d_src) cudaFree(m->d_src);
+  m->d_src = nullptr;
+  m->src_steps = 0;
+  release_graph(m);
+  return ensure_capacity(m, std::max(h.nt, 1));
+}
+
+// Carves every fixed-size device buffer out of one allocation and uploads the model.
+int build(mfdm_model* m, HostModel&& h, int device) {
+  int rc = validate(h);
+  if (rc != MFDM_OK) return rc;
+  m->device = device;
+  int ndev = 0;
+  MFDM_CU(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(MFDM_ERR_ARG, "no such CUDA device");
+  MFDM_CU(cudaSetDevice(device));
+  MFDM_CU(mfdm::configure_device());
+  MFDM_CU(mfdm::upload_constants(kSrcW, kW7));
+  MFDM_CU(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+
+  const int nx = h.nx, nzf = h.nzf, nzs = h.nzs, nz = nzf + nzs - 1;
+  const int P = round_up(nx, 32), Ps = round_up(std::max(2 * h.npd, 1), 4);
+  const int npdr = std::max(h.npd, 1);
+  m->P = P; m->Ps = Ps; m->nz = nz;
+
+  // Byte offsets of every buffer (256-byte aligned).
+  size_t off = 0;
+  auto take = [&](size_t nfloats) {
+    const size_t o = off;
+    off += (nfloats * sizeof(float) + 255) / 256 * 256;
+    return o;
+  };
+  const size_t nf = size_t(nzf) * P, ns = size_t(nzs) * P, ng = size_t(nz) * P;
+  const size_t o_K = take(nf), o_rf = take(nf);
+  const size_t o_C11 = take(ns), o_C13 = take(ns), o_C33 = take(ns), o_C55 = take(ns),
+               o_rs = take(ns);
+  const size_t o_J = take(ng), o_xix = take(ng), o_xiz = take(ng), o_zex = take(ng),
+               o_zez = take(ng);
+  const size_t o_pmlx = take(size_t(nx) * 4), o_pmlz = take(size_t(nzs) * 4),
+               o_nrm = take(size_t(nx) * 2), o_ipre = take(size_t(8) * P), o_misc = take(64);
+  size_t o_set[4][20];
+  for (int s = 0; s < 4; ++s) {
+    for (int f = 0; f < 3; ++f) o_set[s][f] = take(nf);
+    for (int f = 3; f < 8; ++f) o_set[s][f] = take(ns);
+    for (int q = 0; q < 4; ++q) o_set[s][8 + q] = take(size_t(nzf) * Ps);
+    for (int q = 0; q < 4; ++q) o_set[s][12 + q] = take(size_t(nzs) * Ps);
+    for (int q = 0; q < 4; ++q) o_set[s][16 + q] = take(size_t(npdr) * P);
+  }
+  m->dbytes = off;
+  MFDM_CU(cudaMalloc(&m->dmem, off));
+  MFDM_CU(cudaMemsetAsync(m->dmem, 0, off, m->stream));
+  char* base = m->dmem;
+  auto F = [&](size_t o) { return reinterpret_cast<float*>(base + o); };
+  for (int s = 0; s < 4; ++s) {
+    Fields& S = m->S[s];
+    S.fvx = F(o_set[s][0]); S.fvz = F(o_set[s][1]); S.fp = F(o_set[s][2]);
+    S.svx = F(o_set[s][3]); S.svz = F(o_set[s][4]); S.ssx = F(o_set[s][5]);
+    S.ssz = F(o_set[s][6]); S.ssxz = F(o_set[s][7]);
+    for (int q = 0; q < 4; ++q) {
+      S.fx[q] = F(o_set[s][8 + q]);
+      S.sx[q] = F(o_set[s][12 + q]);
+      S.sz[q] = F(o_set[s][16 + q]);
+    }
+  }
+  Coef& C = m->C;
+  C.nx = nx; C.nzf = nzf; C.nzs = nzs; C.P = P; C.npd = h.npd; C.Ps = Ps;
+  C.K = F(o_K); C.rhof = F(o_rf);
+  C.C11 = F(o_C11); C.C13 = F(o_C13); C.C33 = F(o_C33); C.C55 = F(o_C55); C.rhos = F(o_rs);
+  C.J = F(o_J); C.xix = F(o_xix); C.xiz = F(o_xiz); C.zex = F(o_zex); C.zez = F(o_zez);
+  C.pmlx = reinterpret_cast<const float4*>(F(o_pmlx));
+  C.pmlz = reinterpret_cast<const float4*>(F(o_pmlz));
+  C.nrm = reinterpret_cast<const float2*>(F(o_nrm));
+  C.ipre = F(o_ipre);
+  int* misc = reinterpret_cast<int*>(F(o_misc));
+  C.step = misc;
+  C.done = reinterpret_cast<unsigned*>(misc + 1);
+  C.status = misc + 2;
+  if ((rc = upload_model(m, h)) != MFDM_OK) return rc;
+  MFDM_CU(mfdm::launch_set_step(m->C, 0, m->stream));
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  return MFDM_OK;
+}
+
+void destroy(mfdm_model* m) {
+  if (!m) return;
+  DeviceGuard g(m->device);
+  release_graph(m);
+  if (m->stream) cudaStreamSynchronize(m->stream);
+  if (m->d_src) cudaFree(m->d_src);
+  if (m->d_rec) cudaFree(m->d_rec);
+  if (m->dmem) cudaFree(m->dmem);
+  if (m->stream) cudaStreamDestroy(m->stream);
+  delete m;
+}
+
+int open_common(HostModel&& h, int device, mfdm_model** out) {
+  if (!out) return fail(MFDM_ERR_ARG, "null output handle");
+  *out = nullptr;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  mfdm_model* m = new mfdm_model();
+  const int rc = build(m, std::move(h), device);
+  if (prev >= 0) cudaSetDevice(prev);
+  if (rc != MFDM_OK) {
+    const std::string msg = g_err;
+    destroy(m);
+    g_err = msg;
+    return rc;
+  }
+  *out = m;
+  return MFDM_OK;
+}
+
+int field_ptr(mfdm_model* m, int field, float** p, int* rows) {
+  const Fields& U = m->S[0];
+  float* const ptrs[8] = {U.fvx, U.fvz, U.fp, U.svx, U.svz, U.ssx, U.ssz, U.ssxz};
+  if (field < 0 || field > 7) return fail(MFDM_ERR_ARG, "bad field id");
+  *p = ptrs[field];
+  *rows = field < 3 ? m->cfg.nzf : m->cfg.nzs;
+  return MFDM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* mfdm_last_error(void) { return g_err.c_str(); }
+
+int mfdm_open_json(const char* json_path, int device, mfdm_model** out) {
+  if (!json_path) return fail(MFDM_ERR_ARG, "null JSON path");
+  HostModel h;
+  const int rc = load_json(json_path, h);
+  if (rc != MFDM_OK) return rc;
+  return open_common(std::move(h), device, out);
+}
+
+}  // extern "C"
+
+namespace {
+int desc_to_host(const mfdm_desc* d, HostModel& h) {
+  if (!d) return fail(MFDM_ERR_ARG, "null descriptor");
+  h.nx = d->nx; h.nzf = d->nz_f; h.nzs = d->nz_s;
+  h.fpeak = d->fpeak; h.dt = d->dt; h.nt = d->nt; h.snapshot = d->snapshot;
+  h.npd = d->npd; h.npow = d->npow; h.thickness = d->thickness; h.vp_max = d->vp_max;
+  h.rc = d->rc; h.beta0 = d->beta0;
+  if (h.nx <= 0 || h.nzf <= 0 || h.nzs <= 0) return fail(MFDM_ERR_ARG, "bad grid size");
+  for (int i = 0; i < d->nsrc; ++i) {
+    if (!d->src_x || !d->src_z) return fail(MFDM_ERR_ARG, "null source arrays");
+    h.srcx.push_back(d->src_x[i]);
+    h.srcz.push_back(d->src_z[i]);
+  }
+  const size_t nf = size_t(h.nx) * h.nzf, ns = size_t(h.nx) * h.nzs,
+               ng = size_t(h.nx) * (h.nzf + h.nzs - 1);
+  struct Item { const float* src; std::vector<float>* dst; size_t n; } items[] = {
+      {d->K, &h.K, nf}, {d->rho_f, &h.rhof, nf}, {d->C11, &h.C11, ns}, {d->C13, &h.C13, ns},
+      {d->C33, &h.C33, ns}, {d->C55, &h.C55, ns}, {d->rho_s, &h.rhos, ns}, {d->J, &h.J, ng},
+      {d->xi_x, &h.xix, ng}, {d->xi_z, &h.xiz, ng}, {d->ze_x, &h.zex, ng}, {d->ze_z, &h.zez, ng}};
+  for (const Item& it : items) {
+    if (!it.src) return fail(MFDM_ERR_ARG, "null model array");
+    it.dst->assign(it.src, it.src + it.n);
+  }
+  return MFDM_OK;
+}
+
+int enqueue_steps(mfdm_model* m, int nsteps) {
+  int rc;
+  while (nsteps > 0) {
+    if ((m->host_step & 1) == 0 && nsteps >= kGraphSteps) {
+      if (!m->graph && (rc = capture_graph(m)) != MFDM_OK) return rc;
+      MFDM_CU(cudaGraphLaunch(m->graph, m->stream));
+      m->host_step += kGraphSteps;
+      nsteps -= kGraphSteps;
+    } else {
+      if ((rc = enqueue_step(m, m->host_step, m->stream)) != MFDM_OK) return rc;
+      ++m->host_step;
+      --nsteps;
+    }
+  }
+  return MFDM_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int mfdm_open_desc(const mfdm_desc* d, int device, mfdm_model** out) {
+  HostModel h;
+  const int rc = desc_to_host(d, h);
+  if (rc != MFDM_OK) return rc;
+  return open_common(std::move(h), device, out);
+}
+
+int mfdm_load_desc(mfdm_model* m, const mfdm_desc* d) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  HostModel h;
+  int rc = desc_to_host(d, h);
+  if (rc != MFDM_OK) return rc;
+  if ((rc = validate(h)) != MFDM_OK) return rc;
+  if (h.nx != m->cfg.nx || h.nzf != m->cfg.nzf || h.nzs != m->cfg.nzs || h.npd != m->cfg.npd)
+    return fail(MFDM_ERR_ARG, "model shape differs from the open handle");
+  DeviceGuard g(m->device);
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  return upload_model(m, h);
+}
+
+int mfdm_close(mfdm_model* m) {
+  destroy(m);
+  return MFDM_OK;
+}
+
+int mfdm_get_info(const mfdm_model* m, mfdm_info* info) {
+  if (!m || !info) return fail(MFDM_ERR_ARG, "null argument");
+  info->nx = m->cfg.nx; info->nz_f = m->cfg.nzf; info->nz_s = m->cfg.nzs; info->pitch = m->P;
+  info->nt = m->cfg.nt; info->snapshot = m->cfg.snapshot; info->gap = m->gap;
+  info->nsrc = int(m->cfg.srcx.size()); info->shot = m->isrc; info->step = m->host_step;
+  info->nsamples = (m->host_step + m->gap - 1) / m->gap;
+  info->cells = (long long)m->cfg.nx * (m->cfg.nzf + m->cfg.nzs);
+  info->device_bytes = (long long)m->dbytes + (long long)m->src_steps * 16 +
+                       (long long)m->rec_cap * 12 * m->cfg.nx;
+  return MFDM_OK;
+}
+
+int mfdm_set_shot(mfdm_model* m, int isrc, int reset_state) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  if (isrc < 0 || (isrc >= int(m->cfg.srcx.size()) && !m->cfg.srcx.empty()))
+    return fail(MFDM_ERR_ARG, "shot index out of range");
+  DeviceGuard g(m->device);
+  m->isrc = isrc;
+  m->C.srcx = m->cfg.srcx.empty() ? -1 : m->cfg.srcx[size_t(isrc)];
+  m->C.srcz = m->cfg.srcx.empty() ? 0 : m->cfg.srcz[size_t(isrc)];
+  release_graph(m);  // the source position is baked into the kernel arguments
+  if (reset_state) {
+    // every state set, the stage buffers and the accumulator (the coefficient block is untouched)
+    for (int s = 0; s < 4; ++s) {
+      const Fields& S = m->S[s];
+      const size_t nf = size_t(m->cfg.nzf) * m->P, ns = size_t(m->cfg.nzs) * m->P;
+      float* fl[3] = {S.fvx, S.fvz, S.fp};
+      float* so[5] = {S.svx, S.svz, S.ssx, S.ssz, S.ssxz};
+      for (float* p : fl) MFDM_CU(cudaMemsetAsync(p, 0, nf * sizeof(float), m->stream));
+      for (float* p : so) MFDM_CU(cudaMemsetAsync(p, 0, ns * sizeof(float), m->stream));
+      for (int q = 0; q < 4; ++q) {
+        MFDM_CU(cudaMemsetAsync(S.fx[q], 0, size_t(m->cfg.nzf) * m->Ps * sizeof(float), m->stream));
+        MFDM_CU(cudaMemsetAsync(S.sx[q], 0, size_t(m->cfg.nzs) * m->Ps * sizeof(float), m->stream));
+        MFDM_CU(cudaMemsetAsync(S.sz[q], 0, size_t(std::max(m->cfg.npd, 1)) * m->P * sizeof(float), m->stream));
+      }
+    }
+    MFDM_CU(cudaMemsetAsync(m->C.ipre, 0, size_t(8) * m->P * sizeof(float), m->stream));
+  }
+  MFDM_CU(cudaMemsetAsync(m->d_rec, 0, size_t(m->rec_cap) * 3 * m->cfg.nx * sizeof(float), m->stream));
+  MFDM_CU(cudaMemsetAsync(m->C.status, 0, sizeof(int), m->stream));
+  m->host_step = 0;
+  MFDM_CU(mfdm::launch_set_step(m->C, 0, m->stream));
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  return MFDM_OK;
+}
+
+int mfdm_update_rk4(mfdm_model* m, int it, void* stream) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  if (it < 0) return fail(MFDM_ERR_ARG, "negative time index");
+  DeviceGuard g(m->device);
+  int rc = ensure_capacity(m, it + 1);
+  if (rc != MFDM_OK) return rc;
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : m->stream;
+  if (st != m->stream) MFDM_CU(cudaStreamSynchronize(m->stream));
+  MFDM_CU(mfdm::launch_set_step(m->C, it, st));
+  rc = enqueue_step(m, it, st);
+  if (rc != MFDM_OK) return rc;
+  m->host_step = it + 1;
+  return MFDM_OK;
+}
+
+int mfdm_step(mfdm_model* m, int nsteps) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  if (nsteps < 0) return fail(MFDM_ERR_ARG, "negative step count");
+  DeviceGuard g(m->device);
+  int rc = ensure_capacity(m, m->host_step + nsteps);
+  if (rc != MFDM_OK) return rc;
+  if ((rc = enqueue_steps(m, nsteps)) != MFDM_OK) return rc;
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  return check_status(m);
+}
+
+int mfdm_time_steps(mfdm_model* m, int nsteps, int per_kernel, float* total_ms, float* kernel_ms) {
+  if (!m || !total_ms || (per_kernel && !kernel_ms)) return fail(MFDM_ERR_ARG, "null argument");
+  if (nsteps < 0) return fail(MFDM_ERR_ARG, "negative step count");
+  DeviceGuard g(m->device);
+  int rc = ensure_capacity(m, m->host_step + nsteps);
+  if (rc != MFDM_OK) return rc;
+  cudaEvent_t ev[8] = {};
+  for (auto& e : ev) MFDM_CU(cudaEventCreate(&e));
+  struct Free { cudaEvent_t* e; ~Free() { for (int i = 0; i < 8; ++i) cudaEventDestroy(e[i]); } } fr{ev};
+  if (!per_kernel) {
+    MFDM_CU(cudaEventRecord(ev[6], m->stream));
+    if ((rc = enqueue_steps(m, nsteps)) != MFDM_OK) return rc;
+    MFDM_CU(cudaEventRecord(ev[7], m->stream));
+    MFDM_CU(cudaEventSynchronize(ev[7]));
+    MFDM_CU(cudaEventElapsedTime(total_ms, ev[6], ev[7]));
+    return check_status(m);
+  }
+  float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, tot = 0.f;
+  for (int k = 0; k < nsteps; ++k) {
+    if ((rc = enqueue_step(m, m->host_step, m->stream, ev)) != MFDM_OK) return rc;
+    ++m->host_step;
+    MFDM_CU(cudaEventSynchronize(ev[5]));
+    for (int i = 0; i < 5; ++i) {
+      float t = 0.f;
+      MFDM_CU(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
+      acc[i] += t;
+    }
+    float t = 0.f;
+    MFDM_CU(cudaEventElapsedTime(&t, ev[0], ev[5]));
+    tot += t;
+  }
+  for (int i = 0; i < 5; ++i) kernel_ms[i] = acc[i];
+  *total_ms = tot;
+  return check_status(m);
+}
+
+int mfdm_synchronize(mfdm_model* m) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  DeviceGuard g(m->device);
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  return check_status(m);
+}
+
+int mfdm_get_records(mfdm_model* m, int first, int count, float* svx, float* svz, float* fp) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  const int avail = (m->host_step + m->gap - 1) / m->gap;
+  if (first < 0 || count < 0 || first + count > avail || first + count > m->rec_cap)
+    return fail(MFDM_ERR_ARG, "record range out of bounds");
+  if (count == 0) return MFDM_OK;
+  DeviceGuard g(m->device);
+  const int nx = m->cfg.nx;
+  float* outs[3] = {svx, svz, fp};
+  for (int q = 0; q < 3; ++q) {
+    if (!outs[q]) continue;
+    MFDM_CU(cudaMemcpy2DAsync(outs[q], size_t(nx) * sizeof(float),
+                              m->d_rec + (size_t(first) * 3 + q) * nx, size_t(3) * nx * sizeof(float),
+                              size_t(nx) * sizeof(float), size_t(count), cudaMemcpyDeviceToHost,
+                              m->stream));
+  }
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  return MFDM_OK;
+}
+
+int mfdm_get_field(mfdm_model* m, int field, float* host) {
+  if (!m || !host) return fail(MFDM_ERR_ARG, "null argument");
+  float* p = nullptr;
+  int rows = 0;
+  int rc = field_ptr(m, field, &p, &rows);
+  if (rc != MFDM_OK) return rc;
+  DeviceGuard g(m->device);
+  MFDM_CU(cudaMemcpy2DAsync(host, size_t(m->cfg.nx) * sizeof(float), p, size_t(m->P) * sizeof(float),
+                            size_t(m->cfg.nx) * sizeof(float), size_t(rows), cudaMemcpyDeviceToHost,
+                            m->stream));
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  return MFDM_OK;
+}
+
+int mfdm_set_field(mfdm_model* m, int field, const float* host) {
+  if (!m || !host) return fail(MFDM_ERR_ARG, "null argument");
+  float* p = nullptr;
+  int rows = 0;
+  int rc = field_ptr(m, field, &p, &rows);
+  if (rc != MFDM_OK) return rc;
+  DeviceGuard g(m->device);
+  MFDM_CU(cudaMemcpy2DAsync(p, size_t(m->P) * sizeof(float), host, size_t(m->cfg.nx) * sizeof(float),
+                            size_t(m->cfg.nx) * sizeof(float), size_t(rows), cudaMemcpyHostToDevice,
+                            m->stream));
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  return MFDM_OK;
+}
+
+}  // extern "C"
+
+// ---- drop-in command line (src/main.cu:58-339) -------------------------------
+
+namespace {
+
+int write_floats(const fs::path& file, const float* data, size_t n, bool append) {
+  std::ofstream f(file, std::ios::binary | (append ? std::ios::app : std::ios::trunc));
+  if (!f) return fail(MFDM_ERR_IO, "cannot write " + file.string());
+  f.write(reinterpret_cast<const char*>(data), std::streamsize(n * sizeof(float)));
+  if (!f) return fail(MFDM_ERR_IO, "failed to write " + file.string());
+  return MFDM_OK;
+}
+
+int make_dirs(const fs::path& p) {
+  std::error_code ec;
+  fs::create_directories(p, ec);
+  if (ec) return fail(MFDM_ERR_IO, "cannot create " + p.string() + ": " + ec.message());
+  return MFDM_OK;
+}
+
+// Snapshot files <field>_%06d.bin of solid and fluid vx, vz (src/main.cu:227-243, 327-339).
+int write_snapshot(mfdm_model* m, const fs::path& shot_dir, int it) {
+  const int nx = m->cfg.nx;
+  std::vector<float> buf(size_t(nx) * std::max(m->cfg.nzf, m->cfg.nzs));
+  struct S { int field; const char* medium; const char* comp; } order[] = {
+      {MFDM_SOLID_VZ, "solid", "vz"}, {MFDM_SOLID_VX, "solid", "vx"},
+      {MFDM_FLUID_VZ, "fluid", "vz"}, {MFDM_FLUID_VX, "fluid", "vx"}};
+  for (const S& s : order) {
+    int rc = mfdm_get_field(m, s.field, buf.data());
+    if (rc != MFDM_OK) return rc;
+    const fs::path dir = shot_dir / "snapshot" / s.medium / s.comp;
+    if ((rc = make_dirs(dir)) != MFDM_OK) return rc;
+    std::ostringstream name;
+    name << s.comp << "_" << std::setw(6) << std::setfill('0') << it << ".bin";
+    const int rows = s.field < 3 ? m->cfg.nzf : m->cfg.nzs;
+    if ((rc = write_floats(dir / name.str(), buf.data(), size_t(rows) * nx, false)) != MFDM_OK)
+      return rc;
+  }
+  return MFDM_OK;
+}
+
+int run_cli(const char* json_path, const char* out_root_c, int device) {
+  const fs::path out_root = out_root_c;
+  const std::string s = out_root.string();
+  if (s.empty() || s == "/" || s == "." || s == "..")
+    return fail(MFDM_ERR_ARG, "Invalid output dir: " + s);
+  mfdm_model* m = nullptr;
+  int rc = mfdm_open_json(json_path, device, &m);
+  if (rc != MFDM_OK) return rc;
+  struct Closer { mfdm_model* m; ~Closer() { mfdm_close(m); } } closer{m};
+  const HostModel& h = m->cfg;
+  std::printf("[PML] beta0 = %.3f, p_beta = %.2f, p_alpha = %.2f, alpha0 = %.1f 1/s, d0 = %.1f 1/s\n",
+              h.beta0, 2.0, 1.0, 2.0 * M_PI * h.fpeak,
+              -(h.npow + 1) * double(h.vp_max) * std::log(double(h.rc)) / (2.0 * h.thickness));
+  std::error_code ec;
+  fs::remove_all(out_root, ec);
+  if (ec) return fail(MFDM_ERR_IO, "cannot clear " + s + ": " + ec.message());
+  if ((rc = make_dirs(out_root)) != MFDM_OK) return rc;
+  std::printf("[output] cleared %s\n", s.c_str());
+  const int nx = h.nx;
+  const int nsrc = int(h.srcx.size());
+  for (int isrc = 0; isrc < nsrc; ++isrc) {
+    const fs::path shot_dir = out_root / std::to_string(isrc);
+    if ((rc = make_dirs(shot_dir / "snapshot")) != MFDM_OK) return rc;
+    if ((rc = make_dirs(shot_dir / "record")) != MFDM_OK) return rc;
+    // The reference keeps the wavefield across shots (src/main.cu:94-136).
+    if ((rc = mfdm_set_shot(m, isrc, 0)) != MFDM_OK) return rc;
+    int it = 0;
+    while (it < h.nt) {
+      // run through the next snapshot step (it % snapshot == 0), inclusive
+      const int next_snap = ((it + h.snapshot - 1) / h.snapshot) * h.snapshot;
+      const int last = std::min(h.nt - 1, next_snap);
+      if ((rc = mfdm_step(m, last - it + 1)) != MFDM_OK) return rc;
+      it = last + 1;
+      if (last % h.snapshot == 0) {
+        std::printf("finished %0.2f%%\r", 100.0 * last / h.nt);
+        std::fflush(stdout);
+        if ((rc = write_snapshot(m, shot_dir, last)) != MFDM_OK) return rc;
+      }
+    }
+    const int ns = (h.nt + m->gap - 1) / m->gap;
+    std::vector<float> a(size_t(ns) * nx), b(size_t(ns) * nx), c(size_t(ns) * nx);
+    if (ns > 0 && (rc = mfdm_get_records(m, 0, ns, a.data(), b.data(), c.data())) != MFDM_OK) return rc;
+    const fs::path rd = shot_dir / "record";
+    if ((rc = write_floats(rd / "solid_vx.bin", a.data(), a.size(), false)) != MFDM_OK) return rc;
+    if ((rc = write_floats(rd / "solid_vz.bin", b.data(), b.size(), false)) != MFDM_OK) return rc;
+    if ((rc = write_floats(rd / "fluid_p.bin", c.data(), c.size(), false)) != MFDM_OK) return rc;
+  }
+  return MFDM_OK;
+}
+
+}  // namespace
+
+extern "C" int mfdm_run_cli(const char* json_path, const char* out_root, int device) {
+  if (!json_path || !out_root) return fail(MFDM_ERR_ARG, "null argument");
+  try {
+    return run_cli(json_path, out_root, device);
+  } catch (const std::exception& e) {
+    return fail(MFDM_ERR_IO, e.what());
+  }
+}

@@ -1,0 +1,26 @@
+// Host-side launchers of the time-step kernels (internal to the library).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "mfdm_device.cuh"
+
+namespace mfdm {
+
+// Sets the dynamic shared-memory limit of every stage kernel on the current device.
+cudaError_t configure_device();
+// Launches RK stage `stage` (0..3) with operator direction `dir` (0 = F, 1 = B).
+// Stage 0 reads `in` == U^n; stages 1-2 read `in` and U^n (`un`); stage 3 writes U.
+cudaError_t launch_stage(const Coef& C, const Fields& in, const Fields& out, const Fields& un,
+                         const Fields& acc, int stage, int dir, cudaStream_t st);
+// Interface filter, receiver sampling and step-counter advance.
+cudaError_t launch_finish(const Coef& C, const Fields& U, cudaStream_t st);
+// Sets the device step counter to `it`.
+cudaError_t launch_set_step(const Coef& C, int it, cudaStream_t st);
+// Dynamic shared memory of one stage block.
+size_t stage_smem_bytes();
+// Block counts of one stage launch: column tiles, fluid tiles, solid tiles, interface blocks.
+void stage_grid(int nx, int nzf, int nzs, int* ntx, int* nbf, int* nbs, int* nbi);
+// Uploads the 5x5 source weights and the 7-point interface filter weights.
+cudaError_t upload_constants(const float* srcw25, const float* w7);
+
+}  // namespace mfdm

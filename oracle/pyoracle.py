@@ -47,6 +47,12 @@ def lib():
         _lib.orc_forward.argtypes = [ctypes.POINTER(_Model), ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int, _dp, _dp, _dp, _dp, _dp, ctypes.c_int]
         _lib.orc_max_threads.restype = ctypes.c_int
+        _lib.orc_create.restype = ctypes.c_void_p
+        _lib.orc_create.argtypes = [ctypes.POINTER(_Model), ctypes.c_int]
+        _lib.orc_step.restype = ctypes.c_int
+        _lib.orc_step.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        _lib.orc_destroy.restype = None
+        _lib.orc_destroy.argtypes = [ctypes.c_void_p]
     return _lib
 
 
@@ -65,6 +71,22 @@ def forward(model, nsteps: int, gap: int, precision: int = 32, shot: int = 0,
     Returns records ``svx, svz, fp`` of shape [ceil(nsteps/gap)][nx] and,
     when asked, the final ``fluid`` [3][nz_f][nx] and ``solid`` [5][nz_s][nx].
     """
+    m, keep = _model_struct(model, shot, round_inputs)
+    ns = -(-nsteps // gap) if gap > 0 else 0
+    out = {k: np.zeros((ns, model.nx)) for k in ("svx", "svz", "fp")}
+    fl = np.zeros((3, model.nz_f, model.nx)) if final_fields else None
+    so = np.zeros((5, model.nz_s, model.nx)) if final_fields else None
+    rc = lib().orc_forward(ctypes.byref(m), int(precision), int(nsteps), int(gap),
+                           _ptr(out["svx"]), _ptr(out["svz"]), _ptr(out["fp"]),
+                           _ptr(fl), _ptr(so), int(nthreads))
+    if rc != 0:
+        raise RuntimeError(f"oracle failed ({rc})")
+    if final_fields:
+        out["fluid"], out["solid"] = fl, so
+    return out
+
+
+def _model_struct(model, shot=0, round_inputs=True):
     keep = []
 
     def arr(a):
@@ -87,18 +109,29 @@ def forward(model, nsteps: int, gap: int, precision: int = 32, shot: int = 0,
     m.rho_s = arr(model.solid["rho"])
     m.J, m.xi_x, m.xi_z = arr(model.metric["J"]), arr(model.metric["xi_x"]), arr(model.metric["xi_z"])
     m.ze_x, m.ze_z = arr(model.metric["ze_x"]), arr(model.metric["ze_z"])
-    ns = -(-nsteps // gap) if gap > 0 else 0
-    out = {k: np.zeros((ns, model.nx)) for k in ("svx", "svz", "fp")}
-    fl = np.zeros((3, model.nz_f, model.nx)) if final_fields else None
-    so = np.zeros((5, model.nz_s, model.nx)) if final_fields else None
-    rc = lib().orc_forward(ctypes.byref(m), int(precision), int(nsteps), int(gap),
-                           _ptr(out["svx"]), _ptr(out["svz"]), _ptr(out["fp"]),
-                           _ptr(fl), _ptr(so), int(nthreads))
-    if rc != 0:
-        raise RuntimeError(f"oracle failed ({rc})")
-    if final_fields:
-        out["fluid"], out["solid"] = fl, so
-    return out
+    return m, keep
+
+
+class Stepper:
+    """Persistent oracle state for timing the CPU restatement step by step."""
+
+    def __init__(self, model, precision: int = 32, shot: int = 0):
+        m, keep = _model_struct(model, shot, True)
+        self._h = lib().orc_create(ctypes.byref(m), int(precision))
+        if not self._h:
+            raise RuntimeError("oracle create failed")
+
+    def step(self, nsteps: int, nthreads: int = 0):
+        if lib().orc_step(self._h, int(nsteps), int(nthreads)) != 0:
+            raise RuntimeError("oracle step failed")
+
+    def close(self):
+        if self._h:
+            lib().orc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 def record_gap(dt: float) -> int:
