@@ -39,6 +39,7 @@ modelgen = importlib.import_module("marineseis-fdm-2d_b200.modelgen")
 
 WORKLOADS = {
     "curvilinear_4096x2048": lambda: modelgen.curvilinear_4096x2048(nt=10),
+    "curvilinear_2048x1024": lambda: modelgen.curvilinear(2048, 1024, zeta0=511, nt=10),
     "curvilinear_1200x800": lambda: modelgen.curvilinear_1200x800(nt=10),
     "flat_400x400": lambda: modelgen.flat_400x400(nt=10),
 }
@@ -207,6 +208,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="only the warm-up and timed steps (a short launch list for ncu)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -231,6 +234,15 @@ def main():
     ms = max_over_ranks(dist, total_ms, local)
     secs = ms / 1e3
     value = world * model.cells * args.steps / secs / 1e9
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": round(value, 3), "unit": "Gcell/s",
+                              "steps": args.steps, "warmup": args.warmup,
+                              "config": {"workload": args.workload}, "profile_run": True}))
+        solver.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
 
     # ---- per-kernel durations (events around every launch) ----
     nk = min(args.steps, 40)

@@ -8,6 +8,7 @@ plus the largest relative L2 difference between the two runs (the reference's
 own run-to-run spread; its in-place interface filter races across blocks).
 
     python tests/golden/make_golden.py [case ...] [--work DIR]
+    python tests/golden/make_golden.py --fp64 [case ...]   (CPU: FP64 oracle records)
 """
 from __future__ import annotations
 
@@ -55,13 +56,41 @@ def rel(a, b):
     return float(np.linalg.norm(np.asarray(a, np.float64) - b) / d) if d > 0 else 0.0
 
 
+def add_fp64_records(name: str, outdir: str):
+    """Adds the FP64 oracle's records (same receiver stride) to an existing fixture.
+
+    Runs on the CPU. Over long runs the FP32 rounding noise of this scheme grows
+    above 1e-5 (the reference build itself drifts from the FP64 solution), so
+    the fixture also stores the FP64 records that both FP32 implementations are
+    measured against."""
+    sys.path.insert(0, cases.ROOT)
+    from oracle import pyoracle
+    build, stride, _ = cases.CASES[name]
+    model = build()
+    path = os.path.join(outdir, name + ".npz")
+    data = dict(np.load(path))
+    nt = int(data["nt"])
+    r = pyoracle.forward(model, nt, pyoracle.record_gap(model.dt), 64)
+    for k in ("svx", "svz", "fp"):
+        data["fp64_" + k] = r[k][:, ::stride].astype(np.float64)
+    data["fp64_ref_rel_l2"] = np.float64(max(rel(data[k], data["fp64_" + k]) for k in ("svx", "svz", "fp")))
+    np.savez_compressed(path, **data)
+    print(name, "reference build vs FP64 oracle:", float(data["fp64_ref_rel_l2"]), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("names", nargs="*")
+    ap.add_argument("--fp64", action="store_true",
+                    help="add FP64 oracle records to existing fixtures (CPU only)")
     ap.add_argument("--work", default=os.path.join(cases.ROOT, "gpurun_out", "golden_work"))
     ap.add_argument("--outdir", default=cases.GOLDEN_DIR)
     args = ap.parse_args()
     names = args.names or list(cases.CASES)
+    if args.fp64:
+        for name in names:
+            add_fp64_records(name, args.outdir)
+        return
     summary = {}
     for name in names:
         build, stride, keep_snap = cases.CASES[name]
