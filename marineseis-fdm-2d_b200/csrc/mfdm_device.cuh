@@ -120,6 +120,19 @@ __device__ __forceinline__ int xstrip_col(int ix, int nx, int npd) {
   return (ix - 3 < npd) ? ix - 3 : npd + ix - (nx - 3 - npd);
 }
 
+// Centre-cell coefficients of a fluid / solid cell (metric at the cell's global row).
+struct FluidCoefs { float xix, xiz, zex, zez, rho, K; };
+struct SolidCoefs { float xix, xiz, zex, zez, rho, c11, c13, c33, c55; };
+
+__device__ __forceinline__ FluidCoefs fluid_coefs_global(const Coef& C, size_t g) {
+  return {ldg(C.xix + g), ldg(C.xiz + g), ldg(C.zex + g), ldg(C.zez + g), ldg(C.rhof + g),
+          ldg(C.K + g)};
+}
+__device__ __forceinline__ SolidCoefs solid_coefs_global(const Coef& C, size_t m, size_t g) {
+  return {ldg(C.xix + g), ldg(C.xiz + g), ldg(C.zex + g), ldg(C.zez + g), ldg(C.rhos + m),
+          ldg(C.C11 + m), ldg(C.C13 + m), ldg(C.C33 + m), ldg(C.C55 + m)};
+}
+
 // Output of the right-hand side at one fluid cell.
 struct FluidK {
   float vx, vz, p;
@@ -139,12 +152,11 @@ struct SolidK {
 // to the cell; `ade` holds the stage-input ADE memory (V0, V1, E0, E1) of the cell.
 template <int DIR, class Acc>
 __device__ __forceinline__ FluidK fluid_rhs(const Coef& C, const Acc& A, int iz, int ix,
-                                            bool side, const float* ade) {
+                                            bool side, const float* ade, const FluidCoefs& cf) {
   FluidK o;
   const int P = C.P, nzf = C.nzf;
   const size_t g = (size_t)iz * P + ix;
-  const float xix = ldg(C.xix + g), xiz = ldg(C.xiz + g), zex = ldg(C.zex + g),
-              zez = ldg(C.zez + g);
+  const float xix = cf.xix, xiz = cf.xiz, zex = cf.zex, zez = cf.zez;
   const float gxx = xix * xix + xiz * xiz;
   const int d_if = nzf - 1 - iz, d_fs = iz - 3;
   float4 pml = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -197,7 +209,7 @@ __device__ __forceinline__ FluidK fluid_rhs(const Coef& C, const Acc& A, int iz,
         divz = -xiz * (gxx * dpdx + gxz * dpdz) / gxx;
       }
     }
-    const float rho = ldg(C.rhof + g);
+    const float rho = cf.rho;
     o.vx = rvx / rho;
     o.vz = rvz / rho;
     if (side) {
@@ -222,7 +234,7 @@ __device__ __forceinline__ FluidK fluid_rhs(const Coef& C, const Acc& A, int iz,
     const int dn = min(iz - 3, nzf - 1 - iz);
     const float dvxdz = dz_near<DIR>(vxc, dn, false);
     const float dvzdz = dz_near<DIR>(vzc, dn, false);
-    const float Kc = ldg(C.K + g);
+    const float Kc = cf.K;
     o.p = -Kc * (xix * dvxdx + zex * dvxdz + xiz * dvzdx + zez * dvzdz);
     if (side) {
       const float gxz = xix * zex + xiz * zez;
@@ -242,13 +254,13 @@ __device__ __forceinline__ FluidK fluid_rhs(const Coef& C, const Acc& A, int iz,
 // `xade` / `zade` are the stage-input xi / zeta ADE memory of the cell.
 template <int DIR, class Acc>
 __device__ __forceinline__ SolidK solid_rhs(const Coef& C, const Acc& A, int iz, int ix, bool side,
-                                            bool bottom, const float* xade, const float* zade) {
+                                            bool bottom, const float* xade, const float* zade,
+                                            const SolidCoefs& cf) {
   SolidK o;
   const int P = C.P, nzf = C.nzf;
   const size_t m = (size_t)iz * P + ix;
   const size_t g = m + (size_t)(nzf - 1) * P;
-  const float xix = ldg(C.xix + g), xiz = ldg(C.xiz + g), zex = ldg(C.zex + g),
-              zez = ldg(C.zez + g);
+  const float xix = cf.xix, xiz = cf.xiz, zex = cf.zex, zez = cf.zez;
   float4 px = make_float4(0.f, 0.f, 0.f, 0.f), pz = px;
   if (side) px = ldg(C.pmlx + ix);
   if (bottom) pz = ldg(C.pmlz + iz);
@@ -320,7 +332,7 @@ __device__ __forceinline__ SolidK solid_rhs(const Coef& C, const Acc& A, int iz,
         }
       }
     }
-    const float rho = ldg(C.rhos + m);
+    const float rho = cf.rho;
     o.vx = rvx / rho;
     o.vz = rvz / rho;
     if (side) {
@@ -348,8 +360,7 @@ __device__ __forceinline__ SolidK solid_rhs(const Coef& C, const Acc& A, int iz,
                                 A.svz(0, 1), A.svz(0, 2), A.svz(0, 3));
     const float dvxdz = dz_near<DIR>(vxc, iz, true);
     const float dvzdz = dz_near<DIR>(vzc, iz, true);
-    const float c11 = ldg(C.C11 + m), c13 = ldg(C.C13 + m), c33 = ldg(C.C33 + m),
-                c55 = ldg(C.C55 + m);
+    const float c11 = cf.c11, c13 = cf.c13, c33 = cf.c33, c55 = cf.c55;
     o.sx = c11 * (xix * dvxdx + zex * dvxdz) + c13 * (xiz * dvzdx + zez * dvzdz);
     o.sz = c13 * (xix * dvxdx + zex * dvxdz) + c33 * (xiz * dvzdx + zez * dvzdz);
     o.sxz = c55 * (xiz * dvxdx + zez * dvxdz + xix * dvzdx + zex * dvzdz);

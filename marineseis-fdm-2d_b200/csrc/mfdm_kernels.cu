@@ -10,41 +10,65 @@
 // device step counter. Reference: src/pml_fs_kernels.cu:533-868.
 //
 // Block roles inside one stage launch (blockIdx.x ranges):
-//   [0, nbf)            fluid tiles: kTX columns x kTZ rows of fluid rows 3..nz_f-2
-//   [nbf, nbf+nbs)      solid tiles: kTX columns x kTZ rows of solid rows 1..nz_s-4
-//   [nbf+nbs, ...)      interface strip: one thread per column, fluid row nz_f-1
-//                       and solid row 0 together, so the normal/tangential
-//                       coupling happens in registers.
-// Tiles stage the stencil fields of the stage input in shared memory with a
-// halo of 3 rows and 4 columns (float4-aligned), so every stencil tap is a
-// shared-memory read; point-wise fields (coefficients, U^n, accumulator, ADE
-// strips) stream straight from HBM, coalesced along x.
+//   [0, nbf)          fluid segments: a 64-column strip of up to kSeg fluid rows
+//                     (rows 3..nz_f-2)
+//   [nbf, nbf+nbs)    solid segments: the same over solid rows 1..nz_s-4
+//   [nbf+nbs, ...)    interface strip: one thread per column, fluid row nz_f-1
+//                     and solid row 0 together, so the normal/tangential
+//                     coupling happens in registers.
+//
+// A segment block is a producer/consumer pipeline. Warp 8 streams the segment
+// down in chunks of kR rows with bulk asynchronous copies (cp.async.bulk, one
+// per field row, completing on an mbarrier): the stencil fields of the stage
+// input with a 4-column halo into a 16-row ring (kNS chunk slots), and the
+// point-wise inputs (coefficients, U^n, accumulator) into per-slot buffers.
+// Warps 0-7 compute one cell each per chunk purely from shared memory and
+// store the stage output and accumulator straight to HBM, coalesced along x.
+// Each field row thus crosses HBM once per stage; only the 3-row halo above
+// and below a segment and the 4-column halo of a strip are read twice.
+#include "mfdm_async.cuh"
 #include "mfdm_device.cuh"
 #include "mfdm_kernels.h"
 
 namespace mfdm {
 
-constexpr int kTX = 64;                 // tile width (columns)
-constexpr int kTZ = 32;                 // tile height (rows)
-constexpr int kThreads = 256;           // threads per block (64 x 4)
-constexpr int kHX = 4, kHZ = 3;         // tile halo
-constexpr int kTW = kTX + 2 * kHX;      // 72 floats per staged row
-constexpr int kTH = kTZ + 2 * kHZ;      // 38 staged rows
-constexpr int kRowsPerThread = kTZ / (kThreads / kTX);
+constexpr int kTX = 64;                  // computed columns per strip
+constexpr int kSW = kTX + 8;             // staged row width (4-column halo each side)
+constexpr int kR = 4;                    // rows per chunk
+constexpr int kNS = 4;                   // chunk slots in flight
+constexpr int kRing = kR * kNS;          // ring rows (power of two)
+constexpr int kConsumers = 256;          // warps 0-7
+constexpr int kThreads = kConsumers + 32;  // + producer warp
+constexpr int kSeg = 64;                 // rows per segment block
+constexpr int kBarBytes = 128;           // full[kNS] + empty[kNS], padded
+constexpr int kFinishThreads = 256;      // filter / receiver kernel
 
-struct TileAcc {
-  const float* t;  // staged fields, [nf][kTH][kTW]
-  int r, c;        // cell position inside the tile
+static_assert(kTX * kR == kConsumers, "one cell per consumer thread per chunk");
+static_assert((kRing & (kRing - 1)) == 0, "ring rows must be a power of two");
+
+// Point-wise inputs staged per chunk, by stage kind.
+template <int KIND> struct FluidPW { static constexpr int n = KIND == kStageFirst ? 6 : (KIND == kStageMid ? 12 : 9); };
+template <int KIND> struct SolidPW { static constexpr int n = KIND == kStageFirst ? 9 : (KIND == kStageMid ? 19 : 14); };
+
+template <int NST, int NPW>
+__host__ __device__ constexpr size_t segment_smem() {
+  return size_t(kBarBytes) + size_t(NST) * kRing * kSW * 4 + size_t(kNS) * NPW * kR * kTX * 4;
+}
+
+// Reads the stage input from the ring: row (cell row + dz) mod kRing, column c + dx.
+struct RingAcc {
+  const float* ring;
+  int rr, c;
   __device__ __forceinline__ float at(int f, int dz, int dx) const {
-    return t[(f * kTH + r + dz) * kTW + c + dx];
+    return ring[(f * kRing + ((rr + dz) & (kRing - 1))) * kSW + c + dx];
   }
 };
-struct FluidTile : TileAcc {
+struct FluidRing : RingAcc {
   __device__ __forceinline__ float fvx(int dz, int dx) const { return at(0, dz, dx); }
   __device__ __forceinline__ float fvz(int dz, int dx) const { return at(1, dz, dx); }
   __device__ __forceinline__ float fp(int dz, int dx) const { return at(2, dz, dx); }
 };
-struct SolidTile : TileAcc {
+struct SolidRing : RingAcc {
   __device__ __forceinline__ float svx(int dz, int dx) const { return at(0, dz, dx); }
   __device__ __forceinline__ float svz(int dz, int dx) const { return at(1, dz, dx); }
   __device__ __forceinline__ float ssx(int dz, int dx) const { return at(2, dz, dx); }
@@ -71,96 +95,217 @@ struct SolidGlobal {
   __device__ __forceinline__ float ssxz(int dz, int dx) const { return __ldg(sxz + base + (ptrdiff_t)dz * P + dx); }
 };
 
-// Stages nf fields of rows [z0-3, z0+kTZ+3) x columns [x0-4, x0+kTX+4) into
-// shared memory with float4 loads; cells outside the array read as zero.
-template <int NF>
-__device__ __forceinline__ void stage_tile(float* tile, const float* const (&src)[NF], int rows,
-                                           int P, int x0, int z0) {
-  constexpr int kQ = kTW / 4;
-  for (int f = 0; f < NF; ++f) {
-    const float* s = src[f];
-    for (int q = threadIdx.x; q < kTH * kQ; q += kThreads) {
-      const int r = q / kQ, c4 = q - r * kQ;
-      const int z = z0 - kHZ + r, x = x0 - kHX + 4 * c4;
-      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (z >= 0 && z < rows && x >= 0 && x < P)
-        v = __ldg(reinterpret_cast<const float4*>(s + (size_t)z * P + x));
-      *reinterpret_cast<float4*>(tile + (f * kTH + r) * kTW + 4 * c4) = v;
+// Geometry of one segment block.
+struct Segment {
+  int x0;     // first computed column of the strip
+  int z0;     // first computed row
+  int z1;     // one past the last computed row
+  int rows;   // rows of the arrays (fluid nz_f or solid nz_s)
+  int nch;    // computed chunks
+};
+
+// Producer warp: chunk k (k = -1 .. nch, the two ends carry only halo rows)
+// goes to slot (k + 1) % kNS once the slot's previous chunk is released.
+// The byte count announced on the barrier is accumulated from exactly the
+// copies issued below it.
+template <int NST, int NPW>
+__device__ __forceinline__ void produce(const Segment& sg, int P, const float* const* st_src,
+                                        const float* const* pw_src, float* ring, float* slots,
+                                        uint64_t* full, uint64_t* empty, int* status) {
+  const int lane = threadIdx.x & 31;
+  const int s0 = max(0, sg.x0 - 4), s1 = min(P, sg.x0 + kTX + 4);  // staged stencil columns
+  const int p0 = sg.x0, p1 = min(P, sg.x0 + kTX);                   // staged point-wise columns
+  const unsigned st_bytes = unsigned(s1 - s0) * 4u, pw_bytes = unsigned(p1 - p0) * 4u;
+  for (int k = -1; k <= sg.nch; ++k) {
+    const int u = k + 1, slot = u % kNS;
+    if (u >= kNS && !mbar_wait(&empty[slot], ((u / kNS) - 1) & 1)) {
+      if (lane == 0) atomicOr(status, 2);
+      return;
+    }
+    const int r0 = sg.z0 + k * kR;
+    const bool pw = k >= 0 && k < sg.nch;
+    unsigned bytes = 0;
+    for (int rr = 0; rr < kR; ++rr) {
+      const int r = r0 + rr;
+      if (r >= 0 && r < sg.rows) bytes += NST * st_bytes;
+      if (pw && r < sg.z1) bytes += NPW * pw_bytes;
+    }
+    if (lane == 0) mbar_arrive_expect_tx(&full[slot], bytes);
+    __syncwarp();
+    for (int q = lane; q < (NST + NPW) * kR; q += 32) {
+      if (q < NST * kR) {
+        const int f = q / kR, r = r0 + q % kR;
+        if (r < 0 || r >= sg.rows) continue;
+        float* dst = ring + (f * kRing + ((r - sg.z0 + kR) & (kRing - 1))) * kSW + (s0 - sg.x0 + 4);
+        bulk_g2s(dst, st_src[f] + (size_t)r * P + s0, st_bytes, &full[slot]);
+      } else {
+        const int qq = q - NST * kR, p = qq / kR, rr = qq % kR, r = r0 + rr;
+        if (!pw || r >= sg.z1) continue;
+        float* dst = slots + ((size_t)(slot * NPW + p) * kR + rr) * kTX;
+        bulk_g2s(dst, pw_src[p] + (size_t)r * P + p0, pw_bytes, &full[slot]);
+      }
     }
   }
 }
 
+// Consumer side of the pipeline: waits for chunk c+1 (the halo below chunk c),
+// hands each thread its cell, then releases chunk c-1.
+template <class Body>
+__device__ __forceinline__ void consume(const Segment& sg, uint64_t* full, uint64_t* empty,
+                                        int* status, const Body& body) {
+  const int lane = threadIdx.x & 31;
+  // chunks -1 and 0 (slots 0 and 1, first use)
+  if (!mbar_wait(&full[0], 0) || !mbar_wait(&full[1], 0)) {
+    if (lane == 0) atomicOr(status, 2);
+    return;
+  }
+  for (int c = 0; c < sg.nch; ++c) {
+    const int un = c + 2;  // use index of chunk c+1
+    if (!mbar_wait(&full[un % kNS], (un / kNS) & 1)) {
+      if (lane == 0) atomicOr(status, 2);
+      return;
+    }
+    body(c, (c + 1) % kNS);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[c % kNS]);  // chunk c-1 is no longer needed
+  }
+}
+
 template <int DIR, int KIND>
-__device__ __forceinline__ void fluid_tile(const Coef& C, const Fields& in, const Fields& out,
-                                           const Fields& un, const Fields& acc, int s, int it,
-                                           int tile, int ntx, float* sm) {
-  const int nx = C.nx, P = C.P, nzf = C.nzf;
-  const int x0 = (tile % ntx) * kTX, z0 = 3 + (tile / ntx) * kTZ;
-  const int zend = min(z0 + kTZ, nzf - 1);
-  const float* const src[3] = {in.fvx, in.fvz, in.fp};
-  stage_tile<3>(sm, src, nzf, P, x0, z0);
+__device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, const Fields& out,
+                                              const Fields& un, const Fields& acc, int s, int it,
+                                              int blk, int ntx, char* smem) {
+  constexpr int NST = 3, NPW = FluidPW<KIND>::n;
+  const int P = C.P, nx = C.nx;
+  Segment sg;
+  sg.x0 = (blk % ntx) * kTX;
+  sg.z0 = 3 + (blk / ntx) * kSeg;
+  sg.z1 = min(sg.z0 + kSeg, C.nzf - 1);
+  sg.rows = C.nzf;
+  sg.nch = (sg.z1 - sg.z0 + kR - 1) / kR;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* empty = full + kNS;
+  float* ring = reinterpret_cast<float*>(smem + kBarBytes);
+  float* slots = ring + NST * kRing * kSW;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kNS; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], kConsumers / 32);
+    }
+    mbar_fence_init();
+  }
   __syncthreads();
+  if (threadIdx.x >= kConsumers) {
+    const float* st_src[NST] = {in.fvx, in.fvz, in.fp};
+    const float* pw_src[12] = {C.xix, C.xiz, C.zex, C.zez, C.rhof, C.K,
+                               KIND == kStageMid ? un.fvx : acc.fvx,
+                               KIND == kStageMid ? un.fvz : acc.fvz,
+                               KIND == kStageMid ? un.fp : acc.fp, acc.fvx, acc.fvz, acc.fp};
+    produce<NST, NPW>(sg, P, st_src, pw_src, ring, slots, full, empty, C.status);
+    return;
+  }
   const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
-  const int ix = x0 + tx;
-  if (ix < 3 || ix > nx - 4) return;
-  const bool side = min(ix - 3, nx - 4 - ix) < C.npd;
+  const int ix = sg.x0 + tx;
+  const bool colok = ix >= 3 && ix <= nx - 4;
+  const bool side = colok && min(ix - 3, nx - 4 - ix) < C.npd;
   const int scol = side ? xstrip_col(ix, nx, C.npd) : 0;
-  const float c = C.rk_c[s], w = (KIND == kStageLast) ? 0.f : C.rk_w[s];
-#pragma unroll 1
-  for (int j = 0; j < kRowsPerThread; ++j) {
-    const int zr = ty + j * (kThreads / kTX);
-    const int iz = z0 + zr;
-    if (iz >= zend) break;
-    FluidTile A;
-    A.t = sm; A.r = zr + kHZ; A.c = tx + kHX;
+  const float cc = C.rk_c[s], w = (KIND == kStageLast) ? 0.f : C.rk_w[s];
+  consume(sg, full, empty, C.status, [&](int c, int slot) {
+    const int iz = sg.z0 + c * kR + ty;
+    if (!colok || iz >= sg.z1) return;
+    FluidRing A;
+    A.ring = ring; A.rr = (iz - sg.z0 + kR) & (kRing - 1); A.c = tx + 4;
+    const float* pw = slots + ((size_t)slot * NPW * kR + ty) * kTX + tx;  // field p at pw[p * kR * kTX]
+    constexpr int F = kR * kTX;
+    const FluidCoefs cf{pw[0], pw[F], pw[2 * F], pw[3 * F], pw[4 * F], pw[5 * F]};
     float ade[4] = {0.f, 0.f, 0.f, 0.f};
     const size_t si = (size_t)iz * C.Ps + scol;
     if (side) {
 #pragma unroll
       for (int q = 0; q < 4; ++q) ade[q] = __ldg(in.fx[q] + si);
     }
-    FluidK k = fluid_rhs<DIR>(C, A, iz, ix, side, ade);
+    FluidK k = fluid_rhs<DIR>(C, A, iz, ix, side, ade, cf);
     k.p += source_term(C, iz, ix, it, s);
     const size_t i = (size_t)iz * P + ix;
-    rk_update<KIND>(k.vx, A.fvx(0, 0), un.fvx, out.fvx, acc.fvx, i, c, w);
-    rk_update<KIND>(k.vz, A.fvz(0, 0), un.fvz, out.fvz, acc.fvz, i, c, w);
-    rk_update<KIND>(k.p, A.fp(0, 0), un.fp, out.fp, acc.fp, i, c, w);
-    if (side) {
-      rk_update<KIND>(k.V0, ade[0], un.fx[0], out.fx[0], acc.fx[0], si, c, w);
-      rk_update<KIND>(k.V1, ade[1], un.fx[1], out.fx[1], acc.fx[1], si, c, w);
-      if (k.has_E) {
-        rk_update<KIND>(k.E0, ade[2], un.fx[2], out.fx[2], acc.fx[2], si, c, w);
-        rk_update<KIND>(k.E1, ade[3], un.fx[3], out.fx[3], acc.fx[3], si, c, w);
+    const float kv[3] = {k.vx, k.vz, k.p};
+    float* const outs[3] = {out.fvx, out.fvz, out.fp};
+    float* const accs[3] = {acc.fvx, acc.fvz, acc.fp};
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      if (KIND == kStageFirst) {
+        const float u0 = A.at(f, 0, 0);
+        outs[f][i] = fmaf(cc, kv[f], u0);
+        accs[f][i] = fmaf(w, kv[f], u0);
+      } else if (KIND == kStageMid) {
+        outs[f][i] = fmaf(cc, kv[f], pw[(6 + f) * F]);
+        accs[f][i] = fmaf(w, kv[f], pw[(9 + f) * F]);
+      } else {
+        outs[f][i] = fmaf(cc, kv[f], pw[(6 + f) * F]);
       }
     }
-  }
+    if (side) {
+      rk_update<KIND>(k.V0, ade[0], un.fx[0], out.fx[0], acc.fx[0], si, cc, w);
+      rk_update<KIND>(k.V1, ade[1], un.fx[1], out.fx[1], acc.fx[1], si, cc, w);
+      if (k.has_E) {
+        rk_update<KIND>(k.E0, ade[2], un.fx[2], out.fx[2], acc.fx[2], si, cc, w);
+        rk_update<KIND>(k.E1, ade[3], un.fx[3], out.fx[3], acc.fx[3], si, cc, w);
+      }
+    }
+  });
 }
 
 template <int DIR, int KIND>
-__device__ __forceinline__ void solid_tile(const Coef& C, const Fields& in, const Fields& out,
-                                           const Fields& un, const Fields& acc, int s, int tile,
-                                           int ntx, float* sm) {
-  const int nx = C.nx, P = C.P, nzs = C.nzs, npd = C.npd;
-  const int x0 = (tile % ntx) * kTX, z0 = 1 + (tile / ntx) * kTZ;
-  const int zend = min(z0 + kTZ, nzs - 3);
-  const float* const src[5] = {in.svx, in.svz, in.ssx, in.ssz, in.ssxz};
-  stage_tile<5>(sm, src, nzs, P, x0, z0);
+__device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, const Fields& out,
+                                              const Fields& un, const Fields& acc, int s, int blk,
+                                              int ntx, char* smem) {
+  constexpr int NST = 5, NPW = SolidPW<KIND>::n;
+  const int P = C.P, nx = C.nx, npd = C.npd, nzs = C.nzs;
+  Segment sg;
+  sg.x0 = (blk % ntx) * kTX;
+  sg.z0 = 1 + (blk / ntx) * kSeg;
+  sg.z1 = min(sg.z0 + kSeg, nzs - 3);
+  sg.rows = nzs;
+  sg.nch = (sg.z1 - sg.z0 + kR - 1) / kR;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* empty = full + kNS;
+  float* ring = reinterpret_cast<float*>(smem + kBarBytes);
+  float* slots = ring + NST * kRing * kSW;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kNS; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], kConsumers / 32);
+    }
+    mbar_fence_init();
+  }
   __syncthreads();
+  if (threadIdx.x >= kConsumers) {
+    const size_t goff = (size_t)(C.nzf - 1) * P;  // solid row r -> global metric row r + nz_f - 1
+    const float* st_src[NST] = {in.svx, in.svz, in.ssx, in.ssz, in.ssxz};
+    const Fields& a = KIND == kStageMid ? un : acc;
+    const float* pw_src[19] = {C.xix + goff, C.xiz + goff, C.zex + goff, C.zez + goff, C.rhos,
+                               C.C11, C.C13, C.C33, C.C55,
+                               a.svx, a.svz, a.ssx, a.ssz, a.ssxz,
+                               acc.svx, acc.svz, acc.ssx, acc.ssz, acc.ssxz};
+    produce<NST, NPW>(sg, P, st_src, pw_src, ring, slots, full, empty, C.status);
+    return;
+  }
   const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
-  const int ix = x0 + tx;
-  if (ix < 3 || ix > nx - 4) return;
-  const bool side = min(ix - 3, nx - 4 - ix) < npd;
+  const int ix = sg.x0 + tx;
+  const bool colok = ix >= 3 && ix <= nx - 4;
+  const bool side = colok && min(ix - 3, nx - 4 - ix) < npd;
   const int scol = side ? xstrip_col(ix, nx, npd) : 0;
   const int zb0 = nzs - 3 - npd;  // first row of the bottom strip
-  const float c = C.rk_c[s], w = (KIND == kStageLast) ? 0.f : C.rk_w[s];
-#pragma unroll 1
-  for (int j = 0; j < kRowsPerThread; ++j) {
-    const int zr = ty + j * (kThreads / kTX);
-    const int iz = z0 + zr;
-    if (iz >= zend) break;
+  const float cc = C.rk_c[s], w = (KIND == kStageLast) ? 0.f : C.rk_w[s];
+  consume(sg, full, empty, C.status, [&](int c, int slot) {
+    const int iz = sg.z0 + c * kR + ty;
+    if (!colok || iz >= sg.z1) return;
     const bool bottom = iz >= zb0;
-    SolidTile A;
-    A.t = sm; A.r = zr + kHZ; A.c = tx + kHX;
+    SolidRing A;
+    A.ring = ring; A.rr = (iz - sg.z0 + kR) & (kRing - 1); A.c = tx + 4;
+    const float* pw = slots + ((size_t)slot * NPW * kR + ty) * kTX + tx;
+    constexpr int F = kR * kTX;
+    const SolidCoefs cf{pw[0], pw[F], pw[2 * F], pw[3 * F], pw[4 * F],
+                        pw[5 * F], pw[6 * F], pw[7 * F], pw[8 * F]};
     float xade[4] = {0.f, 0.f, 0.f, 0.f}, zade[4] = {0.f, 0.f, 0.f, 0.f};
     const size_t sxi = (size_t)iz * C.Ps + scol;
     const size_t szi = (size_t)(iz - zb0) * P + ix;
@@ -172,26 +317,37 @@ __device__ __forceinline__ void solid_tile(const Coef& C, const Fields& in, cons
 #pragma unroll
       for (int q = 0; q < 4; ++q) zade[q] = __ldg(in.sz[q] + szi);
     }
-    SolidK k = solid_rhs<DIR>(C, A, iz, ix, side, bottom, xade, zade);
+    SolidK k = solid_rhs<DIR>(C, A, iz, ix, side, bottom, xade, zade, cf);
     const size_t i = (size_t)iz * P + ix;
-    rk_update<KIND>(k.vx, A.svx(0, 0), un.svx, out.svx, acc.svx, i, c, w);
-    rk_update<KIND>(k.vz, A.svz(0, 0), un.svz, out.svz, acc.svz, i, c, w);
-    rk_update<KIND>(k.sx, A.ssx(0, 0), un.ssx, out.ssx, acc.ssx, i, c, w);
-    rk_update<KIND>(k.sz, A.ssz(0, 0), un.ssz, out.ssz, acc.ssz, i, c, w);
-    rk_update<KIND>(k.sxz, A.ssxz(0, 0), un.ssxz, out.ssxz, acc.ssxz, i, c, w);
+    const float kv[5] = {k.vx, k.vz, k.sx, k.sz, k.sxz};
+    float* const outs[5] = {out.svx, out.svz, out.ssx, out.ssz, out.ssxz};
+    float* const accs[5] = {acc.svx, acc.svz, acc.ssx, acc.ssz, acc.ssxz};
+#pragma unroll
+    for (int f = 0; f < 5; ++f) {
+      if (KIND == kStageFirst) {
+        const float u0 = A.at(f, 0, 0);
+        outs[f][i] = fmaf(cc, kv[f], u0);
+        accs[f][i] = fmaf(w, kv[f], u0);
+      } else if (KIND == kStageMid) {
+        outs[f][i] = fmaf(cc, kv[f], pw[(9 + f) * F]);
+        accs[f][i] = fmaf(w, kv[f], pw[(14 + f) * F]);
+      } else {
+        outs[f][i] = fmaf(cc, kv[f], pw[(9 + f) * F]);
+      }
+    }
     if (side) {
-      rk_update<KIND>(k.XV0, xade[0], un.sx[0], out.sx[0], acc.sx[0], sxi, c, w);
-      rk_update<KIND>(k.XV1, xade[1], un.sx[1], out.sx[1], acc.sx[1], sxi, c, w);
-      rk_update<KIND>(k.XE0, xade[2], un.sx[2], out.sx[2], acc.sx[2], sxi, c, w);
-      rk_update<KIND>(k.XE1, xade[3], un.sx[3], out.sx[3], acc.sx[3], sxi, c, w);
+      rk_update<KIND>(k.XV0, xade[0], un.sx[0], out.sx[0], acc.sx[0], sxi, cc, w);
+      rk_update<KIND>(k.XV1, xade[1], un.sx[1], out.sx[1], acc.sx[1], sxi, cc, w);
+      rk_update<KIND>(k.XE0, xade[2], un.sx[2], out.sx[2], acc.sx[2], sxi, cc, w);
+      rk_update<KIND>(k.XE1, xade[3], un.sx[3], out.sx[3], acc.sx[3], sxi, cc, w);
     }
     if (bottom) {
-      rk_update<KIND>(k.ZV0, zade[0], un.sz[0], out.sz[0], acc.sz[0], szi, c, w);
-      rk_update<KIND>(k.ZV1, zade[1], un.sz[1], out.sz[1], acc.sz[1], szi, c, w);
-      rk_update<KIND>(k.ZE0, zade[2], un.sz[2], out.sz[2], acc.sz[2], szi, c, w);
-      rk_update<KIND>(k.ZE1, zade[3], un.sz[3], out.sz[3], acc.sz[3], szi, c, w);
+      rk_update<KIND>(k.ZV0, zade[0], un.sz[0], out.sz[0], acc.sz[0], szi, cc, w);
+      rk_update<KIND>(k.ZV1, zade[1], un.sz[1], out.sz[1], acc.sz[1], szi, cc, w);
+      rk_update<KIND>(k.ZE0, zade[2], un.sz[2], out.sz[2], acc.sz[2], szi, cc, w);
+      rk_update<KIND>(k.ZE1, zade[3], un.sz[3], out.sz[3], acc.sz[3], szi, cc, w);
     }
-  }
+  });
 }
 
 // Interface strip: fluid row nz_f-1 and solid row 0 of one column, their RHS,
@@ -202,7 +358,8 @@ __device__ __forceinline__ void interface_strip(const Coef& C, const Fields& in,
                                                 const Fields& un, const Fields& acc, int s,
                                                 int blk) {
   const int nx = C.nx, P = C.P, nzf = C.nzf, nzs = C.nzs, npd = C.npd;
-  const int ix = blk * kThreads + threadIdx.x;
+  if (threadIdx.x >= kConsumers) return;
+  const int ix = blk * kConsumers + threadIdx.x;
   if (ix < 3 || ix > nx - 4) return;
   const bool side = min(ix - 3, nx - 4 - ix) < npd;
   const int scol = side ? xstrip_col(ix, nx, npd) : 0;
@@ -229,8 +386,9 @@ __device__ __forceinline__ void interface_strip(const Coef& C, const Fields& in,
 #pragma unroll
     for (int q = 0; q < 4; ++q) zade[q] = __ldg(in.sz[q] + szi);
   }
-  FluidK kf = fluid_rhs<DIR>(C, Af, nzf - 1, ix, side, fade);
-  SolidK ks = solid_rhs<DIR>(C, As, 0, ix, side, bottom, xade, zade);
+  FluidK kf = fluid_rhs<DIR>(C, Af, nzf - 1, ix, side, fade, fluid_coefs_global(C, fi));
+  SolidK ks = solid_rhs<DIR>(C, As, 0, ix, side, bottom, xade, zade,
+                             solid_coefs_global(C, si, si + (size_t)(nzf - 1) * P));
 
   // ---- coupling of the stage RHS on the interface ----
   const float2 n = __ldg(C.nrm + ix);
@@ -294,17 +452,16 @@ __device__ __forceinline__ void interface_strip(const Coef& C, const Fields& in,
 }
 
 template <int DIR, int KIND>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
     stage_kernel(Coef C, Fields in, Fields out, Fields un, Fields acc, int s, int ntx, int nbf,
                  int nbs) {
-  extern __shared__ float4 smem_f4[];
-  float* sm = reinterpret_cast<float*>(smem_f4);
+  extern __shared__ __align__(128) char smem[];
   const int b = blockIdx.x;
   if (b < nbf) {
     const int it = __ldg(C.step);
-    fluid_tile<DIR, KIND>(C, in, out, un, acc, s, it, b, ntx, sm);
+    fluid_segment<DIR, KIND>(C, in, out, un, acc, s, it, b, ntx, smem);
   } else if (b < nbf + nbs) {
-    solid_tile<DIR, KIND>(C, in, out, un, acc, s, b - nbf, ntx, sm);
+    solid_segment<DIR, KIND>(C, in, out, un, acc, s, b - nbf, ntx, smem);
   } else {
     interface_strip<DIR, KIND>(C, in, out, un, acc, s, b - nbf - nbs);
   }
@@ -315,9 +472,9 @@ __global__ void __launch_bounds__(kThreads)
 // evaluated out of place from C.ipre, so no block reads values another block
 // already filtered. Then the receiver rows are sampled (src/main.cu:195-211)
 // and the last block to finish advances the device step counter.
-__global__ void __launch_bounds__(kThreads) finish_kernel(Coef C, Fields U) {
+__global__ void __launch_bounds__(kFinishThreads) finish_kernel(Coef C, Fields U) {
   const int nx = C.nx, P = C.P, nzf = C.nzf;
-  const int ix = blockIdx.x * kThreads + threadIdx.x;
+  const int ix = blockIdx.x * kFinishThreads + threadIdx.x;
   const int it = *C.step;
   float r0 = 0.f, r1 = 0.f, r2 = 0.f;
   if (ix >= 3 && ix <= nx - 4) {
@@ -380,15 +537,21 @@ __global__ void set_step_kernel(int* step, unsigned* done, int it) {
 
 // ---- host-side launchers ----------------------------------------------------
 
-size_t stage_smem_bytes() { return size_t(5) * kTH * kTW * sizeof(float); }
+template <int KIND>
+static size_t smem_for_kind() {
+  const size_t f = segment_smem<3, FluidPW<KIND>::n>(), so = segment_smem<5, SolidPW<KIND>::n>();
+  return f > so ? f : so;
+}
+
+size_t stage_smem_bytes() { return smem_for_kind<kStageMid>(); }
 
 void stage_grid(int nx, int nzf, int nzs, int* ntx, int* nbf, int* nbs, int* nbi) {
   *ntx = (nx + kTX - 1) / kTX;
   const int frows = nzf - 1 - 3;  // fluid rows 3..nz_f-2
   const int srows = nzs - 4;      // solid rows 1..nz_s-4
-  *nbf = frows > 0 ? *ntx * ((frows + kTZ - 1) / kTZ) : 0;
-  *nbs = srows > 0 ? *ntx * ((srows + kTZ - 1) / kTZ) : 0;
-  *nbi = (nx + kThreads - 1) / kThreads;
+  *nbf = frows > 0 ? *ntx * ((frows + kSeg - 1) / kSeg) : 0;
+  *nbs = srows > 0 ? *ntx * ((srows + kSeg - 1) / kSeg) : 0;
+  *nbi = (nx + kConsumers - 1) / kConsumers;
 }
 
 template <int DIR, int KIND>
@@ -396,16 +559,15 @@ static cudaError_t launch_one(const Coef& C, const Fields& in, const Fields& out
                               const Fields& acc, int s, cudaStream_t st) {
   int ntx, nbf, nbs, nbi;
   stage_grid(C.nx, C.nzf, C.nzs, &ntx, &nbf, &nbs, &nbi);
-  const size_t smem = stage_smem_bytes();
-  stage_kernel<DIR, KIND><<<nbf + nbs + nbi, kThreads, smem, st>>>(C, in, out, un, acc, s, ntx,
-                                                                   nbf, nbs);
+  stage_kernel<DIR, KIND><<<nbf + nbs + nbi, kThreads, smem_for_kind<KIND>(), st>>>(
+      C, in, out, un, acc, s, ntx, nbf, nbs);
   return cudaGetLastError();
 }
 
 template <int DIR, int KIND>
 static cudaError_t configure_one() {
   return cudaFuncSetAttribute(stage_kernel<DIR, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)stage_smem_bytes());
+                              (int)smem_for_kind<KIND>());
 }
 
 cudaError_t configure_device() {
@@ -432,8 +594,8 @@ cudaError_t launch_stage(const Coef& C, const Fields& in, const Fields& out, con
 }
 
 cudaError_t launch_finish(const Coef& C, const Fields& U, cudaStream_t st) {
-  const int nb = (C.nx + kThreads - 1) / kThreads;
-  finish_kernel<<<nb, kThreads, 0, st>>>(C, U);
+  const int nb = (C.nx + kFinishThreads - 1) / kFinishThreads;
+  finish_kernel<<<nb, kFinishThreads, 0, st>>>(C, U);
   return cudaGetLastError();
 }
 
