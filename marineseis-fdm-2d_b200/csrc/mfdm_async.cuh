@@ -5,6 +5,7 @@
 // up and reports failure, so a mis-counted transaction can never hang a GPU;
 // the kernel then records the failure in its status word and returns.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -72,6 +73,17 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
           "r"(smem_addr(dst)),
       "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// 3-D tiled tensor load (TMA) of one box into shared memory, completing on
+// `bar`; out-of-range elements (negative or past-the-end coordinates) read 0.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
       : "memory");
 }
 

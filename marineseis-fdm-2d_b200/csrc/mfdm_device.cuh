@@ -13,10 +13,27 @@
 // The reference keeps ADE memory over the full grid (src/elements.cu:737-758);
 // only the strip cells are ever non-zero, so only those are stored here.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 namespace mfdm {
+
+// Geometry of the streaming stage kernel, shared with the host (tensor-map boxes).
+constexpr int kStageTX = 64;             // computed columns per strip
+constexpr int kStageSW = kStageTX + 8;   // staged stencil row width (4-column halo each side)
+constexpr int kStageR = 4;               // rows per chunk
+
+// TMA descriptors of one stage launch. Each maps a block [field][rows][P] of
+// one RK set (fluid: vx, vz, p; solid: vx, vz, sx, sz, sxz) or of the
+// coefficients (fluid: xi_x, xi_z, ze_x, ze_z, rho, K; solid: xi_x, xi_z,
+// ze_x, ze_z, rho, C11, C13, C33, C55); one box = all fields of kStageR rows.
+struct StageMaps {
+  CUtensorMap fin, sin;    // stage input, box {kStageSW, kStageR, nfield}
+  CUtensorMap fun, sun;    // U^n, box {kStageTX, kStageR, nfield}
+  CUtensorMap facc, sacc;  // accumulator, box {kStageTX, kStageR, nfield}
+  CUtensorMap fcoef, scoef;  // coefficients, box {kStageTX, kStageR, 6 | 9}
+};
 
 // DRP-optimised biased 5-point first derivative (reference include/tools_func.cuh:6-10).
 // The literals sum to -6e-5, not 0: they are kept exactly.

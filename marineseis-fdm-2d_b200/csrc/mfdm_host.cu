@@ -98,7 +98,11 @@ struct mfdm_model {
   float* d_rec = nullptr;
   int rec_cap = 0;
   cudaGraphExec_t graph = nullptr;
-  int cur_device_saved = -1;
+  // TMA descriptors: per RK set (U, A, B, acc) the stencil box and the
+  // point-wise box of the fluid and solid blocks, and the coefficient blocks.
+  CUtensorMap fst[4], sst[4], fpw[4], spw[4], fco, sco;
+  float* fcoef = nullptr;  // [6][nz_f][P]: xi_x, xi_z, ze_x, ze_z, rho, K
+  float* scoef = nullptr;  // [9][nz_s][P]: xi_x, xi_z, ze_x, ze_z, rho, C11, C13, C33, C55
 };
 
 namespace {
@@ -231,6 +235,34 @@ void fill_src_table(const HostModel& h, int steps, std::vector<float>& amp) {
   }
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// Map of a block [nf][rows][P] of floats read in boxes {box_x, kStageR, nf}.
+int encode_block(CUtensorMap* map, const float* base, int P, int rows, int nf, int box_x) {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    MFDM_CU(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    if (!p || q != cudaDriverEntryPointSuccess)
+      return fail(MFDM_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  const cuuint64_t dims[3] = {cuuint64_t(P), cuuint64_t(rows), cuuint64_t(nf)};
+  const cuuint64_t strides[2] = {cuuint64_t(P) * 4, cuuint64_t(rows) * P * 4};
+  const cuuint32_t box[3] = {cuuint32_t(box_x), cuuint32_t(mfdm::kStageR), cuuint32_t(nf)};
+  const cuuint32_t es[3] = {1, 1, 1};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims,
+                        strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(MFDM_ERR_CUDA, "tensor map encoding failed (" + std::to_string(int(r)) + ")");
+  return MFDM_OK;
+}
+
 void release_graph(mfdm_model* m) {
   if (m->graph) {
     cudaGraphExecDestroy(m->graph);
@@ -285,10 +317,20 @@ int enqueue_step(mfdm_model* m, int it, cudaStream_t st, cudaEvent_t* ev = nullp
   // stage s reads in[s] and writes out[s]: U -> A -> B -> A -> U
   const Fields* in[4] = {&U, &A, &B, &A};
   const Fields* out[4] = {&A, &B, &A, &U};
+  const int in_set[4] = {0, 1, 2, 1};
   const int dir[4] = {d0, d1, d0, d1};
   if (ev) MFDM_CU(cudaEventRecord(ev[0], st));
   for (int s = 0; s < 4; ++s) {
-    MFDM_CU(mfdm::launch_stage(C, *in[s], *out[s], U, Acc, s, dir[s], st));
+    mfdm::StageMaps maps;
+    maps.fin = m->fst[in_set[s]];
+    maps.sin = m->sst[in_set[s]];
+    maps.fun = m->fpw[0];
+    maps.sun = m->spw[0];
+    maps.facc = m->fpw[3];
+    maps.sacc = m->spw[3];
+    maps.fcoef = m->fco;
+    maps.scoef = m->sco;
+    MFDM_CU(mfdm::launch_stage(C, *in[s], *out[s], U, Acc, maps, s, dir[s], st));
     if (ev) MFDM_CU(cudaEventRecord(ev[s + 1], st));
   }
   MFDM_CU(mfdm::launch_finish(C, U, st));
@@ -335,6 +377,13 @@ int upload_model(mfdm_model* m, const HostModel& h) {
                               m->stream));
     return MFDM_OK;
   };
+  auto up_rows = [&](const float* dst_c, const std::vector<float>& v, int row0, int rows) -> int {
+    float* dst = const_cast<float*>(dst_c);
+    MFDM_CU(cudaMemcpy2DAsync(dst, size_t(P) * sizeof(float), v.data() + size_t(row0) * nx,
+                              size_t(nx) * sizeof(float), size_t(nx) * sizeof(float), size_t(rows),
+                              cudaMemcpyHostToDevice, m->stream));
+    return MFDM_OK;
+  };
   int rc;
   if ((rc = up(C.K, h.K, nzf)) || (rc = up(C.rhof, h.rhof, nzf)) || (rc = up(C.C11, h.C11, nzs)) ||
       (rc = up(C.C13, h.C13, nzs)) || (rc = up(C.C33, h.C33, nzs)) ||
@@ -342,6 +391,14 @@ int upload_model(mfdm_model* m, const HostModel& h) {
       (rc = up(C.xix, h.xix, nz)) || (rc = up(C.xiz, h.xiz, nz)) || (rc = up(C.zex, h.zex, nz)) ||
       (rc = up(C.zez, h.zez, nz)))
     return rc;
+  // Per-medium copies of the metric for the streamed coefficient blocks: fluid
+  // rows are global rows 0..nz_f-1, solid rows are global rows nz_f-1..nz-1.
+  const size_t nfe = size_t(nzf) * P, nse = size_t(nzs) * P;
+  const std::vector<float>* met[4] = {&h.xix, &h.xiz, &h.zex, &h.zez};
+  for (int q = 0; q < 4; ++q) {
+    if ((rc = up_rows(m->fcoef + q * nfe, *met[q], 0, nzf)) != MFDM_OK) return rc;
+    if ((rc = up_rows(m->scoef + q * nse, *met[q], nzf - 1, nzs)) != MFDM_OK) return rc;
+  }
   std::vector<float4> px, pz;
   pml_profile(h, nx, true, true, px);
   pml_profile(h, nzs, false, true, pz);
@@ -398,7 +455,8 @@ int build(mfdm_model* m, HostModel&& h, int device) {
   MFDM_CU(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
 
   const int nx = h.nx, nzf = h.nzf, nzs = h.nzs, nz = nzf + nzs - 1;
-  const int P = round_up(nx, 32), Ps = round_up(std::max(2 * h.npd, 1), 4);
+  // pitch: 128-byte rows, and never narrower than the 72-column TMA stencil box
+  const int P = round_up(std::max(nx, mfdm::kStageSW), 32), Ps = round_up(std::max(2 * h.npd, 1), 4);
   const int npdr = std::max(h.npd, 1);
   m->P = P; m->Ps = Ps; m->nz = nz;
 
@@ -410,20 +468,20 @@ int build(mfdm_model* m, HostModel&& h, int device) {
     return o;
   };
   const size_t nf = size_t(nzf) * P, ns = size_t(nzs) * P, ng = size_t(nz) * P;
-  const size_t o_K = take(nf), o_rf = take(nf);
-  const size_t o_C11 = take(ns), o_C13 = take(ns), o_C33 = take(ns), o_C55 = take(ns),
-               o_rs = take(ns);
+  const size_t o_fco = take(6 * nf), o_sco = take(9 * ns);
   const size_t o_J = take(ng), o_xix = take(ng), o_xiz = take(ng), o_zex = take(ng),
                o_zez = take(ng);
   const size_t o_pmlx = take(size_t(nx) * 4), o_pmlz = take(size_t(nzs) * 4),
                o_nrm = take(size_t(nx) * 2), o_ipre = take(size_t(8) * P), o_misc = take(64);
-  size_t o_set[4][20];
+  // Each RK set: one fluid block [3][nz_f][P] and one solid block [5][nz_s][P]
+  // (the TMA boxes span the fields), then the ADE strips.
+  size_t o_fb[4], o_sb[4], o_ade[4][12];
   for (int s = 0; s < 4; ++s) {
-    for (int f = 0; f < 3; ++f) o_set[s][f] = take(nf);
-    for (int f = 3; f < 8; ++f) o_set[s][f] = take(ns);
-    for (int q = 0; q < 4; ++q) o_set[s][8 + q] = take(size_t(nzf) * Ps);
-    for (int q = 0; q < 4; ++q) o_set[s][12 + q] = take(size_t(nzs) * Ps);
-    for (int q = 0; q < 4; ++q) o_set[s][16 + q] = take(size_t(npdr) * P);
+    o_fb[s] = take(3 * nf);
+    o_sb[s] = take(5 * ns);
+    for (int q = 0; q < 4; ++q) o_ade[s][q] = take(size_t(nzf) * Ps);
+    for (int q = 0; q < 4; ++q) o_ade[s][4 + q] = take(size_t(nzs) * Ps);
+    for (int q = 0; q < 4; ++q) o_ade[s][8 + q] = take(size_t(npdr) * P);
   }
   m->dbytes = off;
   MFDM_CU(cudaMalloc(&m->dmem, off));
@@ -432,19 +490,23 @@ int build(mfdm_model* m, HostModel&& h, int device) {
   auto F = [&](size_t o) { return reinterpret_cast<float*>(base + o); };
   for (int s = 0; s < 4; ++s) {
     Fields& S = m->S[s];
-    S.fvx = F(o_set[s][0]); S.fvz = F(o_set[s][1]); S.fp = F(o_set[s][2]);
-    S.svx = F(o_set[s][3]); S.svz = F(o_set[s][4]); S.ssx = F(o_set[s][5]);
-    S.ssz = F(o_set[s][6]); S.ssxz = F(o_set[s][7]);
+    float* fb = F(o_fb[s]);
+    float* sb = F(o_sb[s]);
+    S.fvx = fb; S.fvz = fb + nf; S.fp = fb + 2 * nf;
+    S.svx = sb; S.svz = sb + ns; S.ssx = sb + 2 * ns; S.ssz = sb + 3 * ns; S.ssxz = sb + 4 * ns;
     for (int q = 0; q < 4; ++q) {
-      S.fx[q] = F(o_set[s][8 + q]);
-      S.sx[q] = F(o_set[s][12 + q]);
-      S.sz[q] = F(o_set[s][16 + q]);
+      S.fx[q] = F(o_ade[s][q]);
+      S.sx[q] = F(o_ade[s][4 + q]);
+      S.sz[q] = F(o_ade[s][8 + q]);
     }
   }
+  m->fcoef = F(o_fco);
+  m->scoef = F(o_sco);
   Coef& C = m->C;
   C.nx = nx; C.nzf = nzf; C.nzs = nzs; C.P = P; C.npd = h.npd; C.Ps = Ps;
-  C.K = F(o_K); C.rhof = F(o_rf);
-  C.C11 = F(o_C11); C.C13 = F(o_C13); C.C33 = F(o_C33); C.C55 = F(o_C55); C.rhos = F(o_rs);
+  C.rhof = m->fcoef + 4 * nf; C.K = m->fcoef + 5 * nf;
+  C.rhos = m->scoef + 4 * ns; C.C11 = m->scoef + 5 * ns; C.C13 = m->scoef + 6 * ns;
+  C.C33 = m->scoef + 7 * ns; C.C55 = m->scoef + 8 * ns;
   C.J = F(o_J); C.xix = F(o_xix); C.xiz = F(o_xiz); C.zex = F(o_zex); C.zez = F(o_zez);
   C.pmlx = reinterpret_cast<const float4*>(F(o_pmlx));
   C.pmlz = reinterpret_cast<const float4*>(F(o_pmlz));
@@ -454,6 +516,16 @@ int build(mfdm_model* m, HostModel&& h, int device) {
   C.step = misc;
   C.done = reinterpret_cast<unsigned*>(misc + 1);
   C.status = misc + 2;
+  for (int s = 0; s < 4; ++s) {
+    if ((rc = encode_block(&m->fst[s], F(o_fb[s]), P, nzf, 3, mfdm::kStageSW)) ||
+        (rc = encode_block(&m->sst[s], F(o_sb[s]), P, nzs, 5, mfdm::kStageSW)) ||
+        (rc = encode_block(&m->fpw[s], F(o_fb[s]), P, nzf, 3, mfdm::kStageTX)) ||
+        (rc = encode_block(&m->spw[s], F(o_sb[s]), P, nzs, 5, mfdm::kStageTX)))
+      return rc;
+  }
+  if ((rc = encode_block(&m->fco, m->fcoef, P, nzf, 6, mfdm::kStageTX)) ||
+      (rc = encode_block(&m->sco, m->scoef, P, nzs, 9, mfdm::kStageTX)))
+    return rc;
   if ((rc = upload_model(m, h)) != MFDM_OK) return rc;
   MFDM_CU(mfdm::launch_set_step(m->C, 0, m->stream));
   MFDM_CU(cudaStreamSynchronize(m->stream));

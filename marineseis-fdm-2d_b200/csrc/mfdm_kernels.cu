@@ -32,9 +32,9 @@
 
 namespace mfdm {
 
-constexpr int kTX = 64;                  // computed columns per strip
-constexpr int kSW = kTX + 8;             // staged row width (4-column halo each side)
-constexpr int kR = 4;                    // rows per chunk
+constexpr int kTX = kStageTX;            // computed columns per strip
+constexpr int kSW = kStageSW;            // staged row width (4-column halo each side)
+constexpr int kR = kStageR;              // rows per chunk
 constexpr int kNS = 4;                   // chunk slots in flight
 constexpr int kRing = kR * kNS;          // ring rows (power of two)
 constexpr int kConsumers = 256;          // warps 0-7
@@ -46,29 +46,39 @@ constexpr int kFinishThreads = 256;      // filter / receiver kernel
 static_assert(kTX * kR == kConsumers, "one cell per consumer thread per chunk");
 static_assert((kRing & (kRing - 1)) == 0, "ring rows must be a power of two");
 
-// Point-wise inputs staged per chunk, by stage kind.
-template <int KIND> struct FluidPW { static constexpr int n = KIND == kStageFirst ? 6 : (KIND == kStageMid ? 12 : 9); };
-template <int KIND> struct SolidPW { static constexpr int n = KIND == kStageFirst ? 9 : (KIND == kStageMid ? 19 : 14); };
+// Point-wise inputs staged per chunk, by stage kind: coefficients, then U^n
+// (middle stages), then the accumulator (middle and last stages).
+template <int NST, int NCOEF, int KIND>
+struct PW {
+  static constexpr int n = NCOEF + (KIND == kStageMid ? 2 * NST : (KIND == kStageLast ? NST : 0));
+};
 
+// Shared memory of one segment block: barriers, kNS stencil slots of
+// [NST][kR][kSW] and kNS point-wise slots of [NPW][kR][kTX] (all 128-byte
+// multiples), plus 128 bytes to align the dynamic base.
 template <int NST, int NPW>
 __host__ __device__ constexpr size_t segment_smem() {
-  return size_t(kBarBytes) + size_t(NST) * kRing * kSW * 4 + size_t(kNS) * NPW * kR * kTX * 4;
+  return size_t(128) + kBarBytes + size_t(kNS) * NST * kR * kSW * 4 +
+         size_t(kNS) * NPW * kR * kTX * 4;
 }
 
-// Reads the stage input from the ring: row (cell row + dz) mod kRing, column c + dx.
+// Reads the stage input from the stencil slots: ring row q = (cell row + dz)
+// mod kRing lives in slot q / kR, row q % kR; column c + dx.
+template <int NST>
 struct RingAcc {
   const float* ring;
   int rr, c;
   __device__ __forceinline__ float at(int f, int dz, int dx) const {
-    return ring[(f * kRing + ((rr + dz) & (kRing - 1))) * kSW + c + dx];
+    const int q = (rr + dz) & (kRing - 1);
+    return ring[(((q / kR) * NST + f) * kR + (q % kR)) * kSW + c + dx];
   }
 };
-struct FluidRing : RingAcc {
+struct FluidRing : RingAcc<3> {
   __device__ __forceinline__ float fvx(int dz, int dx) const { return at(0, dz, dx); }
   __device__ __forceinline__ float fvz(int dz, int dx) const { return at(1, dz, dx); }
   __device__ __forceinline__ float fp(int dz, int dx) const { return at(2, dz, dx); }
 };
-struct SolidRing : RingAcc {
+struct SolidRing : RingAcc<5> {
   __device__ __forceinline__ float svx(int dz, int dx) const { return at(0, dz, dx); }
   __device__ __forceinline__ float svz(int dz, int dx) const { return at(1, dz, dx); }
   __device__ __forceinline__ float ssx(int dz, int dx) const { return at(2, dz, dx); }
@@ -104,45 +114,39 @@ struct Segment {
   int nch;    // computed chunks
 };
 
-// Producer warp: chunk k (k = -1 .. nch, the two ends carry only halo rows)
-// goes to slot (k + 1) % kNS once the slot's previous chunk is released.
-// The byte count announced on the barrier is accumulated from exactly the
-// copies issued below it.
-template <int NST, int NPW>
-__device__ __forceinline__ void produce(const Segment& sg, int P, const float* const* st_src,
-                                        const float* const* pw_src, float* ring, float* slots,
+// Producer (one lane of warp 8): chunk k (k = -1 .. nch; the two ends carry
+// only the halo rows) goes to slot (k + 1) % kNS once the slot's previous
+// chunk is released. Per chunk one 3-D TMA box brings all stencil fields of
+// kR rows (with the column halo), and up to three boxes the point-wise inputs.
+// Tiled TMA always delivers whole boxes (zero-filled outside the arrays), so
+// the byte count announced on the barrier is a compile-time constant.
+template <int NST, int NCOEF, int KIND>
+__device__ __forceinline__ void produce(const Segment& sg, const CUtensorMap* in_map,
+                                        const CUtensorMap* coef_map, const CUtensorMap* un_map,
+                                        const CUtensorMap* acc_map, float* ring, float* slots,
                                         uint64_t* full, uint64_t* empty, int* status) {
-  const int lane = threadIdx.x & 31;
-  const int s0 = max(0, sg.x0 - 4), s1 = min(P, sg.x0 + kTX + 4);  // staged stencil columns
-  const int p0 = sg.x0, p1 = min(P, sg.x0 + kTX);                   // staged point-wise columns
-  const unsigned st_bytes = unsigned(s1 - s0) * 4u, pw_bytes = unsigned(p1 - p0) * 4u;
+  if ((threadIdx.x & 31) != 0) return;
+  constexpr int NPW = PW<NST, NCOEF, KIND>::n;
+  constexpr unsigned kStBytes = NST * kR * kSW * 4, kPwBytes = NPW * kR * kTX * 4;
+  constexpr int kF = kR * kTX;  // floats per point-wise field in a slot
   for (int k = -1; k <= sg.nch; ++k) {
     const int u = k + 1, slot = u % kNS;
     if (u >= kNS && !mbar_wait(&empty[slot], ((u / kNS) - 1) & 1)) {
-      if (lane == 0) atomicOr(status, 2);
+      atomicOr(status, 2);
       return;
     }
     const int r0 = sg.z0 + k * kR;
     const bool pw = k >= 0 && k < sg.nch;
-    unsigned bytes = 0;
-    for (int rr = 0; rr < kR; ++rr) {
-      const int r = r0 + rr;
-      if (r >= 0 && r < sg.rows) bytes += NST * st_bytes;
-      if (pw && r < sg.z1) bytes += NPW * pw_bytes;
-    }
-    if (lane == 0) mbar_arrive_expect_tx(&full[slot], bytes);
-    __syncwarp();
-    for (int q = lane; q < (NST + NPW) * kR; q += 32) {
-      if (q < NST * kR) {
-        const int f = q / kR, r = r0 + q % kR;
-        if (r < 0 || r >= sg.rows) continue;
-        float* dst = ring + (f * kRing + ((r - sg.z0 + kR) & (kRing - 1))) * kSW + (s0 - sg.x0 + 4);
-        bulk_g2s(dst, st_src[f] + (size_t)r * P + s0, st_bytes, &full[slot]);
-      } else {
-        const int qq = q - NST * kR, p = qq / kR, rr = qq % kR, r = r0 + rr;
-        if (!pw || r >= sg.z1) continue;
-        float* dst = slots + ((size_t)(slot * NPW + p) * kR + rr) * kTX;
-        bulk_g2s(dst, pw_src[p] + (size_t)r * P + p0, pw_bytes, &full[slot]);
+    mbar_arrive_expect_tx(&full[slot], kStBytes + (pw ? kPwBytes : 0u));
+    tma_load_3d(ring + slot * NST * kR * kSW, in_map, sg.x0 - 4, r0, 0, &full[slot]);
+    if (pw) {
+      float* d = slots + slot * NPW * kF;
+      tma_load_3d(d, coef_map, sg.x0, r0, 0, &full[slot]);
+      if (KIND == kStageMid) {
+        tma_load_3d(d + NCOEF * kF, un_map, sg.x0, r0, 0, &full[slot]);
+        tma_load_3d(d + (NCOEF + NST) * kF, acc_map, sg.x0, r0, 0, &full[slot]);
+      } else if (KIND == kStageLast) {
+        tma_load_3d(d + NCOEF * kF, acc_map, sg.x0, r0, 0, &full[slot]);
       }
     }
   }
@@ -171,22 +175,16 @@ __device__ __forceinline__ void consume(const Segment& sg, uint64_t* full, uint6
   }
 }
 
-template <int DIR, int KIND>
-__device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, const Fields& out,
-                                              const Fields& un, const Fields& acc, int s, int it,
-                                              int blk, int ntx, char* smem) {
-  constexpr int NST = 3, NPW = FluidPW<KIND>::n;
-  const int P = C.P, nx = C.nx;
-  Segment sg;
-  sg.x0 = (blk % ntx) * kTX;
-  sg.z0 = 3 + (blk / ntx) * kSeg;
-  sg.z1 = min(sg.z0 + kSeg, C.nzf - 1);
-  sg.rows = C.nzf;
-  sg.nch = (sg.z1 - sg.z0 + kR - 1) / kR;
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
-  uint64_t* empty = full + kNS;
-  float* ring = reinterpret_cast<float*>(smem + kBarBytes);
-  float* slots = ring + NST * kRing * kSW;
+// Carves the barriers and the slots out of the dynamic shared memory (base
+// rounded up to 128 bytes) and initialises the barriers.
+template <int NST>
+__device__ __forceinline__ void segment_setup(char* smem_raw, uint64_t*& full, uint64_t*& empty,
+                                              float*& ring, float*& slots) {
+  char* smem = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+  full = reinterpret_cast<uint64_t*>(smem);
+  empty = full + kNS;
+  ring = reinterpret_cast<float*>(smem + kBarBytes);
+  slots = ring + kNS * NST * kR * kSW;
   if (threadIdx.x == 0) {
     for (int i = 0; i < kNS; ++i) {
       mbar_init(&full[i], 1);
@@ -195,13 +193,27 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
     mbar_fence_init();
   }
   __syncthreads();
+}
+
+template <int DIR, int KIND>
+__device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, const Fields& out,
+                                              const Fields& un, const Fields& acc,
+                                              const StageMaps& maps, int s, int it, int blk,
+                                              int ntx, char* smem) {
+  constexpr int NST = 3, NCOEF = 6, NPW = PW<NST, NCOEF, KIND>::n;
+  const int P = C.P, nx = C.nx;
+  Segment sg;
+  sg.x0 = (blk % ntx) * kTX;
+  sg.z0 = 3 + (blk / ntx) * kSeg;
+  sg.z1 = min(sg.z0 + kSeg, C.nzf - 1);
+  sg.rows = C.nzf;
+  sg.nch = (sg.z1 - sg.z0 + kR - 1) / kR;
+  uint64_t *full, *empty;
+  float *ring, *slots;
+  segment_setup<NST>(smem, full, empty, ring, slots);
   if (threadIdx.x >= kConsumers) {
-    const float* st_src[NST] = {in.fvx, in.fvz, in.fp};
-    const float* pw_src[12] = {C.xix, C.xiz, C.zex, C.zez, C.rhof, C.K,
-                               KIND == kStageMid ? un.fvx : acc.fvx,
-                               KIND == kStageMid ? un.fvz : acc.fvz,
-                               KIND == kStageMid ? un.fp : acc.fp, acc.fvx, acc.fvz, acc.fp};
-    produce<NST, NPW>(sg, P, st_src, pw_src, ring, slots, full, empty, C.status);
+    produce<NST, NCOEF, KIND>(sg, &maps.fin, &maps.fcoef, &maps.fun, &maps.facc, ring, slots, full,
+                              empty, C.status);
     return;
   }
   const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
@@ -215,8 +227,8 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
     if (!colok || iz >= sg.z1) return;
     FluidRing A;
     A.ring = ring; A.rr = (iz - sg.z0 + kR) & (kRing - 1); A.c = tx + 4;
-    const float* pw = slots + ((size_t)slot * NPW * kR + ty) * kTX + tx;  // field p at pw[p * kR * kTX]
     constexpr int F = kR * kTX;
+    const float* pw = slots + (size_t)slot * NPW * F + ty * kTX + tx;  // field p at pw[p * F]
     const FluidCoefs cf{pw[0], pw[F], pw[2 * F], pw[3 * F], pw[4 * F], pw[5 * F]};
     float ade[4] = {0.f, 0.f, 0.f, 0.f};
     const size_t si = (size_t)iz * C.Ps + scol;
@@ -237,10 +249,10 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
         outs[f][i] = fmaf(cc, kv[f], u0);
         accs[f][i] = fmaf(w, kv[f], u0);
       } else if (KIND == kStageMid) {
-        outs[f][i] = fmaf(cc, kv[f], pw[(6 + f) * F]);
-        accs[f][i] = fmaf(w, kv[f], pw[(9 + f) * F]);
+        outs[f][i] = fmaf(cc, kv[f], pw[(NCOEF + f) * F]);
+        accs[f][i] = fmaf(w, kv[f], pw[(NCOEF + NST + f) * F]);
       } else {
-        outs[f][i] = fmaf(cc, kv[f], pw[(6 + f) * F]);
+        outs[f][i] = fmaf(cc, kv[f], pw[(NCOEF + f) * F]);
       }
     }
     if (side) {
@@ -256,9 +268,10 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
 
 template <int DIR, int KIND>
 __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, const Fields& out,
-                                              const Fields& un, const Fields& acc, int s, int blk,
-                                              int ntx, char* smem) {
-  constexpr int NST = 5, NPW = SolidPW<KIND>::n;
+                                              const Fields& un, const Fields& acc,
+                                              const StageMaps& maps, int s, int blk, int ntx,
+                                              char* smem) {
+  constexpr int NST = 5, NCOEF = 9, NPW = PW<NST, NCOEF, KIND>::n;
   const int P = C.P, nx = C.nx, npd = C.npd, nzs = C.nzs;
   Segment sg;
   sg.x0 = (blk % ntx) * kTX;
@@ -266,27 +279,12 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
   sg.z1 = min(sg.z0 + kSeg, nzs - 3);
   sg.rows = nzs;
   sg.nch = (sg.z1 - sg.z0 + kR - 1) / kR;
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
-  uint64_t* empty = full + kNS;
-  float* ring = reinterpret_cast<float*>(smem + kBarBytes);
-  float* slots = ring + NST * kRing * kSW;
-  if (threadIdx.x == 0) {
-    for (int i = 0; i < kNS; ++i) {
-      mbar_init(&full[i], 1);
-      mbar_init(&empty[i], kConsumers / 32);
-    }
-    mbar_fence_init();
-  }
-  __syncthreads();
+  uint64_t *full, *empty;
+  float *ring, *slots;
+  segment_setup<NST>(smem, full, empty, ring, slots);
   if (threadIdx.x >= kConsumers) {
-    const size_t goff = (size_t)(C.nzf - 1) * P;  // solid row r -> global metric row r + nz_f - 1
-    const float* st_src[NST] = {in.svx, in.svz, in.ssx, in.ssz, in.ssxz};
-    const Fields& a = KIND == kStageMid ? un : acc;
-    const float* pw_src[19] = {C.xix + goff, C.xiz + goff, C.zex + goff, C.zez + goff, C.rhos,
-                               C.C11, C.C13, C.C33, C.C55,
-                               a.svx, a.svz, a.ssx, a.ssz, a.ssxz,
-                               acc.svx, acc.svz, acc.ssx, acc.ssz, acc.ssxz};
-    produce<NST, NPW>(sg, P, st_src, pw_src, ring, slots, full, empty, C.status);
+    produce<NST, NCOEF, KIND>(sg, &maps.sin, &maps.scoef, &maps.sun, &maps.sacc, ring, slots, full,
+                              empty, C.status);
     return;
   }
   const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
@@ -302,8 +300,8 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
     const bool bottom = iz >= zb0;
     SolidRing A;
     A.ring = ring; A.rr = (iz - sg.z0 + kR) & (kRing - 1); A.c = tx + 4;
-    const float* pw = slots + ((size_t)slot * NPW * kR + ty) * kTX + tx;
     constexpr int F = kR * kTX;
+    const float* pw = slots + (size_t)slot * NPW * F + ty * kTX + tx;
     const SolidCoefs cf{pw[0], pw[F], pw[2 * F], pw[3 * F], pw[4 * F],
                         pw[5 * F], pw[6 * F], pw[7 * F], pw[8 * F]};
     float xade[4] = {0.f, 0.f, 0.f, 0.f}, zade[4] = {0.f, 0.f, 0.f, 0.f};
@@ -329,10 +327,10 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
         outs[f][i] = fmaf(cc, kv[f], u0);
         accs[f][i] = fmaf(w, kv[f], u0);
       } else if (KIND == kStageMid) {
-        outs[f][i] = fmaf(cc, kv[f], pw[(9 + f) * F]);
-        accs[f][i] = fmaf(w, kv[f], pw[(14 + f) * F]);
+        outs[f][i] = fmaf(cc, kv[f], pw[(NCOEF + f) * F]);
+        accs[f][i] = fmaf(w, kv[f], pw[(NCOEF + NST + f) * F]);
       } else {
-        outs[f][i] = fmaf(cc, kv[f], pw[(9 + f) * F]);
+        outs[f][i] = fmaf(cc, kv[f], pw[(NCOEF + f) * F]);
       }
     }
     if (side) {
@@ -453,17 +451,18 @@ __device__ __forceinline__ void interface_strip(const Coef& C, const Fields& in,
 
 template <int DIR, int KIND>
 __global__ void __launch_bounds__(kThreads, 2)
-    stage_kernel(Coef C, Fields in, Fields out, Fields un, Fields acc, int s, int ntx, int nbf,
+    stage_kernel(Coef C, Fields in, Fields out, Fields un, Fields acc,
+                 const __grid_constant__ StageMaps maps, int s, int ntx, int nbi, int nbf,
                  int nbs) {
-  extern __shared__ __align__(128) char smem[];
+  extern __shared__ char smem[];
   const int b = blockIdx.x;
-  if (b < nbf) {
+  if (b < nbi) {  // first, so the short interface blocks overlap the segments
+    interface_strip<DIR, KIND>(C, in, out, un, acc, s, b);
+  } else if (b < nbi + nbf) {
     const int it = __ldg(C.step);
-    fluid_segment<DIR, KIND>(C, in, out, un, acc, s, it, b, ntx, smem);
-  } else if (b < nbf + nbs) {
-    solid_segment<DIR, KIND>(C, in, out, un, acc, s, b - nbf, ntx, smem);
+    fluid_segment<DIR, KIND>(C, in, out, un, acc, maps, s, it, b - nbi, ntx, smem);
   } else {
-    interface_strip<DIR, KIND>(C, in, out, un, acc, s, b - nbf - nbs);
+    solid_segment<DIR, KIND>(C, in, out, un, acc, maps, s, b - nbi - nbf, ntx, smem);
   }
 }
 
@@ -539,7 +538,7 @@ __global__ void set_step_kernel(int* step, unsigned* done, int it) {
 
 template <int KIND>
 static size_t smem_for_kind() {
-  const size_t f = segment_smem<3, FluidPW<KIND>::n>(), so = segment_smem<5, SolidPW<KIND>::n>();
+  const size_t f = segment_smem<3, PW<3, 6, KIND>::n>(), so = segment_smem<5, PW<5, 9, KIND>::n>();
   return f > so ? f : so;
 }
 
@@ -556,11 +555,11 @@ void stage_grid(int nx, int nzf, int nzs, int* ntx, int* nbf, int* nbs, int* nbi
 
 template <int DIR, int KIND>
 static cudaError_t launch_one(const Coef& C, const Fields& in, const Fields& out, const Fields& un,
-                              const Fields& acc, int s, cudaStream_t st) {
+                              const Fields& acc, const StageMaps& maps, int s, cudaStream_t st) {
   int ntx, nbf, nbs, nbi;
   stage_grid(C.nx, C.nzf, C.nzs, &ntx, &nbf, &nbs, &nbi);
-  stage_kernel<DIR, KIND><<<nbf + nbs + nbi, kThreads, smem_for_kind<KIND>(), st>>>(
-      C, in, out, un, acc, s, ntx, nbf, nbs);
+  stage_kernel<DIR, KIND><<<nbi + nbf + nbs, kThreads, smem_for_kind<KIND>(), st>>>(
+      C, in, out, un, acc, maps, s, ntx, nbi, nbf, nbs);
   return cudaGetLastError();
 }
 
@@ -581,16 +580,17 @@ cudaError_t configure_device() {
 }
 
 cudaError_t launch_stage(const Coef& C, const Fields& in, const Fields& out, const Fields& un,
-                         const Fields& acc, int stage, int dir, cudaStream_t st) {
+                         const Fields& acc, const StageMaps& maps, int stage, int dir,
+                         cudaStream_t st) {
   const int kind = stage == 0 ? kStageFirst : (stage == 3 ? kStageLast : kStageMid);
   if (dir == kDirF) {
-    if (kind == kStageFirst) return launch_one<kDirF, kStageFirst>(C, in, out, un, acc, stage, st);
-    if (kind == kStageMid) return launch_one<kDirF, kStageMid>(C, in, out, un, acc, stage, st);
-    return launch_one<kDirF, kStageLast>(C, in, out, un, acc, stage, st);
+    if (kind == kStageFirst) return launch_one<kDirF, kStageFirst>(C, in, out, un, acc, maps, stage, st);
+    if (kind == kStageMid) return launch_one<kDirF, kStageMid>(C, in, out, un, acc, maps, stage, st);
+    return launch_one<kDirF, kStageLast>(C, in, out, un, acc, maps, stage, st);
   }
-  if (kind == kStageFirst) return launch_one<kDirB, kStageFirst>(C, in, out, un, acc, stage, st);
-  if (kind == kStageMid) return launch_one<kDirB, kStageMid>(C, in, out, un, acc, stage, st);
-  return launch_one<kDirB, kStageLast>(C, in, out, un, acc, stage, st);
+  if (kind == kStageFirst) return launch_one<kDirB, kStageFirst>(C, in, out, un, acc, maps, stage, st);
+  if (kind == kStageMid) return launch_one<kDirB, kStageMid>(C, in, out, un, acc, maps, stage, st);
+  return launch_one<kDirB, kStageLast>(C, in, out, un, acc, maps, stage, st);
 }
 
 cudaError_t launch_finish(const Coef& C, const Fields& U, cudaStream_t st) {

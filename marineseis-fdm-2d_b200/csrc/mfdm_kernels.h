@@ -10,8 +10,10 @@ namespace mfdm {
 cudaError_t configure_device();
 // Launches RK stage `stage` (0..3) with operator direction `dir` (0 = F, 1 = B).
 // Stage 0 reads `in` == U^n; stages 1-2 read `in` and U^n (`un`); stage 3 writes U.
+// `maps` holds the TMA descriptors of this stage's input, U^n, accumulator and coefficients.
 cudaError_t launch_stage(const Coef& C, const Fields& in, const Fields& out, const Fields& un,
-                         const Fields& acc, int stage, int dir, cudaStream_t st);
+                         const Fields& acc, const StageMaps& maps, int stage, int dir,
+                         cudaStream_t st);
 // Interface filter, receiver sampling and step-counter advance.
 cudaError_t launch_finish(const Coef& C, const Fields& U, cudaStream_t st);
 // Sets the device step counter to `it`.
