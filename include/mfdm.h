@@ -149,6 +149,59 @@ int mfdm_set_field(mfdm_model* m, int field, const float* host);
  * in the reference layout. Returns MFDM_OK or an error code (the CLI exits 1). */
 int mfdm_run_cli(const char* json_path, const char* out_root, int device);
 
+/* ---- stepping without allocating ------------------------------------------
+ * No counterpart in the reference. For callers that cannot allocate device
+ * memory (a fixed device-memory budget set at start-up, a framework pool that
+ * owns the GPU, code where cudaMalloc must not run) but already hold the model
+ * and the wavefield on the current device. All arrays below are device
+ * pointers, row-major [rows][nx] float32 with row pitch nx; the model arrays
+ * are read, the eight state arrays are read and overwritten.
+ */
+typedef struct mfdm_device_model {
+  int nx, nz_f, nz_s;
+  float fpeak, dt;
+  int npd, npow;
+  float thickness, vp_max, rc, beta0;
+  int src_x, src_z;               /* source column / fluid row (src_x < 0: none) */
+  const float* K;                 /* [nz_f][nx] */
+  const float* rho_f;
+  const float* C11;               /* [nz_s][nx] */
+  const float* C13;
+  const float* C33;
+  const float* C55;
+  const float* rho_s;
+  const float* J;                 /* [nz_f+nz_s-1][nx] */
+  const float* xi_x;
+  const float* xi_z;
+  const float* ze_x;
+  const float* ze_z;
+  float* vx_f;                    /* [nz_f][nx] state, in and out */
+  float* vz_f;
+  float* p_f;
+  float* vx_s;                    /* [nz_s][nx] state, in and out */
+  float* vz_s;
+  float* sx_s;
+  float* sz_s;
+  float* sxz_s;
+} mfdm_device_model;
+
+/* Size of the library's static device array used by mfdm_step_noalloc; every
+ * GPU that loads the library holds it until the process exits. */
+#define MFDM_NOALLOC_MAX_BYTES (32u << 20)
+
+/* Steps time indices it .. it + nsteps - 1 of `dm` on `stream` (a cudaStream_t,
+ * NULL = legacy default stream) and returns after the stream has finished.
+ * Allocates nothing: the coefficient blocks, RK stage buffers, accumulator,
+ * ADE memory and tables live in one static device array of
+ * MFDM_NOALLOC_MAX_BYTES; models that need more are rejected with
+ * MFDM_ERR_ARG. The first call on a device resolves that array's address and
+ * configures the kernels there, so make it before any stream capture. Calls
+ * share the array and it keeps the last call's contents: the ADE memory
+ * carries from one call to the next, so start a run with it == 0 (which
+ * clears it) and continue one model with consecutive time indices; calls that
+ * overlap on the GPU race. No receiver buffer: read the state arrays. */
+int mfdm_step_noalloc(const mfdm_device_model* dm, int it, int nsteps, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,7 +33,7 @@ FIELDS = {"fluid_vx": 0, "fluid_vz": 1, "fluid_p": 2, "solid_vx": 3, "solid_vz":
 EXPORTS = ("mfdm_last_error", "mfdm_open_json", "mfdm_open_desc", "mfdm_load_desc", "mfdm_close",
            "mfdm_get_info", "mfdm_set_shot", "mfdm_update_rk4", "mfdm_step", "mfdm_time_steps",
            "mfdm_synchronize", "mfdm_get_records", "mfdm_get_field", "mfdm_set_field",
-           "mfdm_run_cli")
+           "mfdm_run_cli", "mfdm_step_noalloc")
 
 
 class MfdmError(RuntimeError):
@@ -67,6 +67,19 @@ class Info(ctypes.Structure):
                 ("cells", ctypes.c_longlong), ("device_bytes", ctypes.c_longlong)]
 
 
+class DeviceModel(ctypes.Structure):
+    """mfdm_device_model: device pointers for mfdm_step_noalloc (no allocation)."""
+    _fields_ = [("nx", ctypes.c_int), ("nz_f", ctypes.c_int), ("nz_s", ctypes.c_int),
+                ("fpeak", ctypes.c_float), ("dt", ctypes.c_float),
+                ("npd", ctypes.c_int), ("npow", ctypes.c_int),
+                ("thickness", ctypes.c_float), ("vp_max", ctypes.c_float),
+                ("rc", ctypes.c_float), ("beta0", ctypes.c_float),
+                ("src_x", ctypes.c_int), ("src_z", ctypes.c_int)] + [
+        (n, ctypes.c_void_p) for n in ("K", "rho_f", "C11", "C13", "C33", "C55", "rho_s", "J",
+                                       "xi_x", "xi_z", "ze_x", "ze_z", "vx_f", "vz_f", "p_f",
+                                       "vx_s", "vz_s", "sx_s", "sz_s", "sxz_s")]
+
+
 _lib = None
 
 
@@ -95,6 +108,8 @@ def load_library(path: str = LIB_PATH):
         "mfdm_get_field": (ctypes.c_int, [vp, ctypes.c_int, _fp]),
         "mfdm_set_field": (ctypes.c_int, [vp, ctypes.c_int, _fp]),
         "mfdm_run_cli": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]),
+        "mfdm_step_noalloc": (ctypes.c_int, [ctypes.POINTER(DeviceModel), ctypes.c_int,
+                                             ctypes.c_int, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -240,6 +255,12 @@ class Solver:
     def set_field(self, name: str, values: np.ndarray):
         a = _f32(values)
         _check(self._lib.mfdm_set_field(self._h, FIELDS[name], a.ctypes.data_as(_fp)))
+
+
+def step_noalloc(dm: DeviceModel, it: int, nsteps: int, stream: Optional[int] = None):
+    """mfdm_step_noalloc: steps device-resident arrays without any allocation."""
+    _check(load_library().mfdm_step_noalloc(ctypes.byref(dm), int(it), int(nsteps),
+                                            ctypes.c_void_p(stream or 0)))
 
 
 def run_cli(json_path: str, out_root: str, device: int = 0):

@@ -573,6 +573,14 @@ int field_ptr(mfdm_model* m, int field, float** p, int* rows) {
 
 }  // namespace
 
+namespace mfdm {
+// Shared with other translation units of the library.
+int set_error(int code, const char* msg) { return fail(code, msg); }
+int encode_block_map(CUtensorMap* map, const float* base, int P, int rows, int nf, int box_x) {
+  return encode_block(map, base, P, rows, nf, box_x);
+}
+}  // namespace mfdm
+
 extern "C" {
 
 const char* mfdm_last_error(void) { return g_err.c_str(); }
