@@ -37,8 +37,23 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
+#ifndef MFDM_WAIT_HINT_NS
+#define MFDM_WAIT_HINT_NS 20000  // suspend hint of mbarrier.try_wait (0: none)
+#endif
+
+// try_wait suspends the thread in hardware until the phase completes or the
+// hint (ns) elapses, instead of spinning on issue slots.
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   uint32_t ok;
+#if MFDM_WAIT_HINT_NS > 0
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity), "r"(unsigned(MFDM_WAIT_HINT_NS))
+      : "memory");
+#else
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -46,6 +61,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
       : "=r"(ok)
       : "r"(smem_addr(bar)), "r"(parity)
       : "memory");
+#endif
   return ok != 0;
 }
 
@@ -60,7 +76,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   for (;;) {
-    for (int i = 0; i < 64; ++i)
+    for (int i = 0; i < 8; ++i)
       if (mbar_try_wait(bar, parity)) return true;
     if (global_ns() - t0 > kWaitNs) return false;
   }

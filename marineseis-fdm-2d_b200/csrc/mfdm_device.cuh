@@ -137,6 +137,21 @@ __device__ __forceinline__ int xstrip_col(int ix, int nx, int npd) {
   return (ix - 3 < npd) ? ix - 3 : npd + ix - (nx - 3 - npd);
 }
 
+// The density slots of the coefficient blocks hold 1/rho (FP64 reciprocal
+// rounded once) and the momentum RHS multiplies by it instead of dividing
+// (reference: `rhodvx_dt / Mf.rho[idx]`, pml_fs_kernels.cuh:432); the two
+// differ by at most one rounding. Build with MFDM_RCP_RHO=0 to divide.
+#ifndef MFDM_RCP_RHO
+#define MFDM_RCP_RHO 1
+#endif
+__device__ __forceinline__ float over_rho(float x, float r) {
+#if MFDM_RCP_RHO
+  return x * r;
+#else
+  return x / r;
+#endif
+}
+
 // Centre-cell coefficients of a fluid / solid cell (metric at the cell's global row).
 struct FluidCoefs { float xix, xiz, zex, zez, rho, K; };
 struct SolidCoefs { float xix, xiz, zex, zez, rho, c11, c13, c33, c55; };
@@ -167,7 +182,9 @@ struct SolidK {
 // Fluid RHS at (iz, ix), iz in [3, nz_f-1] (pml_fs_kernels.cuh:333-507).
 // `A` reads the stage input: A.fp(dz, dx), A.fvx(dz, dx), A.fvz(dz, dx) relative
 // to the cell; `ade` holds the stage-input ADE memory (V0, V1, E0, E1) of the cell.
-template <int DIR, class Acc>
+// INTERIOR = true: the caller guarantees 6 <= iz <= nz_f-4 (no conservative
+// rows, full-order zeta stencils), so those branches compile away.
+template <int DIR, bool INTERIOR = false, class Acc>
 __device__ __forceinline__ FluidK fluid_rhs(const Coef& C, const Acc& A, int iz, int ix,
                                             bool side, const float* ade, const FluidCoefs& cf) {
   FluidK o;
@@ -182,7 +199,7 @@ __device__ __forceinline__ FluidK fluid_rhs(const Coef& C, const Acc& A, int iz,
   // ---- momentum: rho dv/dt = -grad p ----
   {
     float rvx, rvz, divx = 0.f, divz = 0.f;
-    if (d_if < 3 || d_fs < 3) {
+    if (!INTERIOR && (d_if < 3 || d_fs < 3)) {
       // conservative flux form with mirrored ghosts (pml_fs_kernels.cuh:356-415)
       auto Ff = [&](int r) -> float2 {
         const size_t k = (size_t)r * P + ix;
@@ -227,19 +244,19 @@ __device__ __forceinline__ FluidK fluid_rhs(const Coef& C, const Acc& A, int iz,
       }
     }
     const float rho = cf.rho;
-    o.vx = rvx / rho;
-    o.vz = rvz / rho;
+    o.vx = over_rho(rvx, rho);
+    o.vz = over_rho(rvz, rho);
     if (side) {
       const float dpb = pml.x, apdpb = pml.y, invb = pml.z;
       o.V0 = -apdpb * ade[0] + dpb * divx;
       o.V1 = -apdpb * ade[1] + dpb * divz;
-      o.vx += ((invb - 1.0f) * divx - invb * ade[0]) / rho;
-      o.vz += ((invb - 1.0f) * divz - invb * ade[1]) / rho;
+      o.vx += over_rho((invb - 1.0f) * divx - invb * ade[0], rho);
+      o.vz += over_rho((invb - 1.0f) * divz - invb * ade[1], rho);
     }
   }
   // ---- pressure: dp/dt = -K div v ----
-  o.has_E = (iz != 3);
-  if (iz == 3) {
+  o.has_E = INTERIOR || (iz != 3);
+  if (!INTERIOR && iz == 3) {
     o.p = 0.0f;  // pressure-free surface row
   } else {
     auto vxc = [&](int j) { return A.fvx(j, 0); };
@@ -248,7 +265,7 @@ __device__ __forceinline__ FluidK fluid_rhs(const Coef& C, const Acc& A, int iz,
                                 A.fvx(0, 1), A.fvx(0, 2), A.fvx(0, 3));
     const float dvzdx = d5<DIR>(A.fvz(0, -3), A.fvz(0, -2), A.fvz(0, -1), A.fvz(0, 0),
                                 A.fvz(0, 1), A.fvz(0, 2), A.fvz(0, 3));
-    const int dn = min(iz - 3, nzf - 1 - iz);
+    const int dn = INTERIOR ? 3 : min(iz - 3, nzf - 1 - iz);
     const float dvxdz = dz_near<DIR>(vxc, dn, false);
     const float dvzdz = dz_near<DIR>(vzc, dn, false);
     const float Kc = cf.K;
@@ -269,7 +286,8 @@ __device__ __forceinline__ FluidK fluid_rhs(const Coef& C, const Acc& A, int iz,
 // Solid RHS at (iz, ix), iz in [0, nz_s-4] (pml_fs_kernels.cuh:509-752).
 // `A` reads the stage input: A.svx, A.svz, A.ssx, A.ssz, A.ssxz (dz, dx);
 // `xade` / `zade` are the stage-input xi / zeta ADE memory of the cell.
-template <int DIR, class Acc>
+// INTERIOR = true: the caller guarantees 3 <= iz <= nz_s-4.
+template <int DIR, bool INTERIOR = false, class Acc>
 __device__ __forceinline__ SolidK solid_rhs(const Coef& C, const Acc& A, int iz, int ix, bool side,
                                             bool bottom, const float* xade, const float* zade,
                                             const SolidCoefs& cf) {
@@ -285,7 +303,7 @@ __device__ __forceinline__ SolidK solid_rhs(const Coef& C, const Acc& A, int iz,
   // ---- momentum: rho dv/dt = div sigma ----
   {
     float rvx, rvz, dxx = 0.f, dxz = 0.f, dzx = 0.f, dzz = 0.f;
-    if (iz < 3) {
+    if (!INTERIOR && iz < 3) {
       // conservative flux form with the interface ghost G = 2F0 - Fn (pml_fs_kernels.cuh:654-680)
       auto Fs = [&](int r) -> float2 {
         const size_t k = (size_t)(r + nzf - 1) * P + ix;
@@ -350,21 +368,21 @@ __device__ __forceinline__ SolidK solid_rhs(const Coef& C, const Acc& A, int iz,
       }
     }
     const float rho = cf.rho;
-    o.vx = rvx / rho;
-    o.vz = rvz / rho;
+    o.vx = over_rho(rvx, rho);
+    o.vz = over_rho(rvz, rho);
     if (side) {
       const float dpb = px.x, apdpb = px.y, invb = px.z;
       o.XV0 = -apdpb * xade[0] + dpb * dxx;
       o.XV1 = -apdpb * xade[1] + dpb * dxz;
-      o.vx += ((invb - 1.0f) * dxx - invb * xade[0]) / rho;
-      o.vz += ((invb - 1.0f) * dxz - invb * xade[1]) / rho;
+      o.vx += over_rho((invb - 1.0f) * dxx - invb * xade[0], rho);
+      o.vz += over_rho((invb - 1.0f) * dxz - invb * xade[1], rho);
     }
     if (bottom) {
       const float dpb = pz.x, apdpb = pz.y, invb = pz.z;
       o.ZV0 = -apdpb * zade[0] + dpb * dzx;
       o.ZV1 = -apdpb * zade[1] + dpb * dzz;
-      o.vx += ((invb - 1.0f) * dzx - invb * zade[0]) / rho;
-      o.vz += ((invb - 1.0f) * dzz - invb * zade[1]) / rho;
+      o.vx += over_rho((invb - 1.0f) * dzx - invb * zade[0], rho);
+      o.vz += over_rho((invb - 1.0f) * dzz - invb * zade[1], rho);
     }
   }
   // ---- stress: VTI constitutive law ----
@@ -375,8 +393,8 @@ __device__ __forceinline__ SolidK solid_rhs(const Coef& C, const Acc& A, int iz,
                                 A.svx(0, 1), A.svx(0, 2), A.svx(0, 3));
     const float dvzdx = d5<DIR>(A.svz(0, -3), A.svz(0, -2), A.svz(0, -1), A.svz(0, 0),
                                 A.svz(0, 1), A.svz(0, 2), A.svz(0, 3));
-    const float dvxdz = dz_near<DIR>(vxc, iz, true);
-    const float dvzdz = dz_near<DIR>(vzc, iz, true);
+    const float dvxdz = dz_near<DIR>(vxc, INTERIOR ? 3 : iz, true);
+    const float dvzdz = dz_near<DIR>(vzc, INTERIOR ? 3 : iz, true);
     const float c11 = cf.c11, c13 = cf.c13, c33 = cf.c33, c55 = cf.c55;
     o.sx = c11 * (xix * dvxdx + zex * dvxdz) + c13 * (xiz * dvzdx + zez * dvzdz);
     o.sz = c13 * (xix * dvxdx + zex * dvxdz) + c33 * (xiz * dvzdx + zez * dvzdz);

@@ -385,9 +385,20 @@ int upload_model(mfdm_model* m, const HostModel& h) {
     return MFDM_OK;
   };
   int rc;
-  if ((rc = up(C.K, h.K, nzf)) || (rc = up(C.rhof, h.rhof, nzf)) || (rc = up(C.C11, h.C11, nzs)) ||
+#if MFDM_RCP_RHO
+  // density slots hold 1/rho (reciprocal in FP64, rounded once)
+  std::vector<float> rf(h.rhof.size()), rs(h.rhos.size());
+  for (size_t i = 0; i < rf.size(); ++i) rf[i] = float(1.0 / double(h.rhof[i]));
+  for (size_t i = 0; i < rs.size(); ++i) rs[i] = float(1.0 / double(h.rhos[i]));
+  const std::vector<float>& rho_f_dev = rf;
+  const std::vector<float>& rho_s_dev = rs;
+#else
+  const std::vector<float>& rho_f_dev = h.rhof;
+  const std::vector<float>& rho_s_dev = h.rhos;
+#endif
+  if ((rc = up(C.K, h.K, nzf)) || (rc = up(C.rhof, rho_f_dev, nzf)) || (rc = up(C.C11, h.C11, nzs)) ||
       (rc = up(C.C13, h.C13, nzs)) || (rc = up(C.C33, h.C33, nzs)) ||
-      (rc = up(C.C55, h.C55, nzs)) || (rc = up(C.rhos, h.rhos, nzs)) || (rc = up(C.J, h.J, nz)) ||
+      (rc = up(C.C55, h.C55, nzs)) || (rc = up(C.rhos, rho_s_dev, nzs)) || (rc = up(C.J, h.J, nz)) ||
       (rc = up(C.xix, h.xix, nz)) || (rc = up(C.xiz, h.xiz, nz)) || (rc = up(C.zex, h.zex, nz)) ||
       (rc = up(C.zez, h.zez, nz)))
     return rc;

@@ -10,7 +10,7 @@
 // device step counter. Reference: src/pml_fs_kernels.cu:533-868.
 //
 // Block roles inside one stage launch (blockIdx.x ranges):
-//   [0, nbf)          fluid segments: a 64-column strip of up to kSeg fluid rows
+//   [0, nbf)          fluid segments: a 64-column strip of up to kSeg (24) fluid rows
 //                     (rows 3..nz_f-2)
 //   [nbf, nbf+nbs)    solid segments: the same over solid rows 1..nz_s-4
 //   [nbf+nbs, ...)    interface strip: one thread per column, fluid row nz_f-1
@@ -39,7 +39,10 @@ constexpr int kNS = 4;                   // chunk slots in flight
 constexpr int kRing = kR * kNS;          // ring rows (power of two)
 constexpr int kConsumers = 256;          // warps 0-7
 constexpr int kThreads = kConsumers + 32;  // + producer warp
-constexpr int kSeg = 64;                 // rows per segment block
+#ifndef MFDM_SEG_ROWS
+#define MFDM_SEG_ROWS 24
+#endif
+constexpr int kSeg = MFDM_SEG_ROWS;      // rows per segment block
 constexpr int kBarBytes = 128;           // full[kNS] + empty[kNS], padded
 constexpr int kFinishThreads = 256;      // filter / receiver kernel
 
@@ -236,7 +239,9 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
 #pragma unroll
       for (int q = 0; q < 4; ++q) ade[q] = __ldg(in.fx[q] + si);
     }
-    FluidK k = fluid_rhs<DIR>(C, A, iz, ix, side, ade, cf);
+    // rows 6 .. nz_f-4 take the specialised interior body (no conservative rows)
+    FluidK k = (iz >= 6 && iz <= C.nzf - 4) ? fluid_rhs<DIR, true>(C, A, iz, ix, side, ade, cf)
+                                            : fluid_rhs<DIR, false>(C, A, iz, ix, side, ade, cf);
     k.p += source_term(C, iz, ix, it, s);
     const size_t i = (size_t)iz * P + ix;
     const float kv[3] = {k.vx, k.vz, k.p};
@@ -315,7 +320,8 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
 #pragma unroll
       for (int q = 0; q < 4; ++q) zade[q] = __ldg(in.sz[q] + szi);
     }
-    SolidK k = solid_rhs<DIR>(C, A, iz, ix, side, bottom, xade, zade, cf);
+    SolidK k = iz >= 3 ? solid_rhs<DIR, true>(C, A, iz, ix, side, bottom, xade, zade, cf)
+                       : solid_rhs<DIR, false>(C, A, iz, ix, side, bottom, xade, zade, cf);
     const size_t i = (size_t)iz * P + ix;
     const float kv[5] = {k.vx, k.vz, k.sx, k.sz, k.sxz};
     float* const outs[5] = {out.svx, out.svz, out.ssx, out.ssz, out.ssxz};

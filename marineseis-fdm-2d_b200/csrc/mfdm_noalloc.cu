@@ -129,6 +129,12 @@ __global__ void tables_kernel(Tables t, float4* pmlx, float4* pmlz, float2* nrm,
   }
 }
 
+// Density slots hold 1/rho in the kernels' coefficient blocks (see mfdm_device.cuh).
+__global__ void reciprocal_kernel(float* a, size_t n) {
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = float(1.0 / double(a[i]));
+}
+
 int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
 }  // namespace
@@ -213,6 +219,12 @@ extern "C" int mfdm_step_noalloc(const mfdm_device_model* dm, int it, int nsteps
       (rc = copy_rows(sco + 6 * ns, dm->C13, 0, nzs)) || (rc = copy_rows(sco + 7 * ns, dm->C33, 0, nzs)) ||
       (rc = copy_rows(sco + 8 * ns, dm->C55, 0, nzs)))
     return rc;
+#if MFDM_RCP_RHO
+  // rows x pitch of each density slot; the padding columns become 1/0 = inf and are never read
+  reciprocal_kernel<<<unsigned((nf + 255) / 256), 256, 0, st>>>(fco + 4 * nf, nf);
+  reciprocal_kernel<<<unsigned((ns + 255) / 256), 256, 0, st>>>(sco + 4 * ns, ns);
+  NA_CU(cudaGetLastError());
+#endif
   const float* gmet[5] = {dm->J, dm->xi_x, dm->xi_z, dm->ze_x, dm->ze_z};
   for (int q = 0; q < 5; ++q)
     if ((rc = copy_rows(F(o_met[q]), gmet[q], 0, nz)) != MFDM_OK) return rc;
