@@ -28,8 +28,9 @@ constexpr int kStageR = 4;               // rows per chunk
 // one RK set (fluid: vx, vz, p; solid: vx, vz, sx, sz, sxz) or of the
 // coefficients (fluid: xi_x, xi_z, ze_x, ze_z, rho, K; solid: xi_x, xi_z,
 // ze_x, ze_z, rho, C11, C13, C33, C55); one box = all fields of kStageR rows.
+// Stage-input boxes land as [row][field][col], the others as [field][row][col].
 struct StageMaps {
-  CUtensorMap fin, sin;    // stage input, box {kStageSW, kStageR, nfield}
+  CUtensorMap fin, sin;    // stage input, box {kStageSW, nfield, kStageR}
   CUtensorMap fun, sun;    // U^n, box {kStageTX, kStageR, nfield}
   CUtensorMap facc, sacc;  // accumulator, box {kStageTX, kStageR, nfield}
   CUtensorMap fcoef, scoef;  // coefficients, box {kStageTX, kStageR, 6 | 9}

@@ -241,8 +241,13 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-// Map of a block [nf][rows][P] of floats read in boxes {box_x, kStageR, nf}.
-int encode_block(CUtensorMap* map, const float* base, int P, int rows, int nf, int box_x) {
+// Map of a block [nf][rows][P] of floats read in boxes of box_x columns, kStageR
+// rows and all nf fields. Point-wise maps land as [field][row][col] (dimensions
+// column, row, field); stencil maps (rows_outer) land as [row][field][col]
+// (dimensions column, field, row), so consecutive chunks stack into one
+// row-contiguous ring.
+int encode_block(CUtensorMap* map, const float* base, int P, int rows, int nf, int box_x,
+                 bool rows_outer) {
   static EncodeTiledFn fn = nullptr;
   if (!fn) {
     void* p = nullptr;
@@ -252,9 +257,13 @@ int encode_block(CUtensorMap* map, const float* base, int P, int rows, int nf, i
       return fail(MFDM_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
     fn = reinterpret_cast<EncodeTiledFn>(p);
   }
-  const cuuint64_t dims[3] = {cuuint64_t(P), cuuint64_t(rows), cuuint64_t(nf)};
-  const cuuint64_t strides[2] = {cuuint64_t(P) * 4, cuuint64_t(rows) * P * 4};
-  const cuuint32_t box[3] = {cuuint32_t(box_x), cuuint32_t(mfdm::kStageR), cuuint32_t(nf)};
+  const cuuint64_t row_stride = cuuint64_t(P) * 4, field_stride = cuuint64_t(rows) * P * 4;
+  const cuuint64_t dims[3] = {cuuint64_t(P), cuuint64_t(rows_outer ? nf : rows),
+                              cuuint64_t(rows_outer ? rows : nf)};
+  const cuuint64_t strides[2] = {rows_outer ? field_stride : row_stride,
+                                 rows_outer ? row_stride : field_stride};
+  const cuuint32_t box[3] = {cuuint32_t(box_x), cuuint32_t(rows_outer ? nf : mfdm::kStageR),
+                             cuuint32_t(rows_outer ? mfdm::kStageR : nf)};
   const cuuint32_t es[3] = {1, 1, 1};
   const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims,
                         strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -528,14 +537,14 @@ int build(mfdm_model* m, HostModel&& h, int device) {
   C.done = reinterpret_cast<unsigned*>(misc + 1);
   C.status = misc + 2;
   for (int s = 0; s < 4; ++s) {
-    if ((rc = encode_block(&m->fst[s], F(o_fb[s]), P, nzf, 3, mfdm::kStageSW)) ||
-        (rc = encode_block(&m->sst[s], F(o_sb[s]), P, nzs, 5, mfdm::kStageSW)) ||
-        (rc = encode_block(&m->fpw[s], F(o_fb[s]), P, nzf, 3, mfdm::kStageTX)) ||
-        (rc = encode_block(&m->spw[s], F(o_sb[s]), P, nzs, 5, mfdm::kStageTX)))
+    if ((rc = encode_block(&m->fst[s], F(o_fb[s]), P, nzf, 3, mfdm::kStageSW, true)) ||
+        (rc = encode_block(&m->sst[s], F(o_sb[s]), P, nzs, 5, mfdm::kStageSW, true)) ||
+        (rc = encode_block(&m->fpw[s], F(o_fb[s]), P, nzf, 3, mfdm::kStageTX, false)) ||
+        (rc = encode_block(&m->spw[s], F(o_sb[s]), P, nzs, 5, mfdm::kStageTX, false)))
       return rc;
   }
-  if ((rc = encode_block(&m->fco, m->fcoef, P, nzf, 6, mfdm::kStageTX)) ||
-      (rc = encode_block(&m->sco, m->scoef, P, nzs, 9, mfdm::kStageTX)))
+  if ((rc = encode_block(&m->fco, m->fcoef, P, nzf, 6, mfdm::kStageTX, false)) ||
+      (rc = encode_block(&m->sco, m->scoef, P, nzs, 9, mfdm::kStageTX, false)))
     return rc;
   if ((rc = upload_model(m, h)) != MFDM_OK) return rc;
   MFDM_CU(mfdm::launch_set_step(m->C, 0, m->stream));
@@ -587,8 +596,9 @@ int field_ptr(mfdm_model* m, int field, float** p, int* rows) {
 namespace mfdm {
 // Shared with other translation units of the library.
 int set_error(int code, const char* msg) { return fail(code, msg); }
-int encode_block_map(CUtensorMap* map, const float* base, int P, int rows, int nf, int box_x) {
-  return encode_block(map, base, P, rows, nf, box_x);
+int encode_block_map(CUtensorMap* map, const float* base, int P, int rows, int nf, int box_x,
+                     bool rows_outer) {
+  return encode_block(map, base, P, rows, nf, box_x, rows_outer);
 }
 }  // namespace mfdm
 

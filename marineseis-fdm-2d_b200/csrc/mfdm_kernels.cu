@@ -17,11 +17,12 @@
 //                     and solid row 0 together, so the normal/tangential
 //                     coupling happens in registers.
 //
-// A segment block is a producer/consumer pipeline. Warp 8 streams the segment
-// down in chunks of kR rows with bulk asynchronous copies (cp.async.bulk, one
-// per field row, completing on an mbarrier): the stencil fields of the stage
-// input with a 4-column halo into a 16-row ring (kNS chunk slots), and the
-// point-wise inputs (coefficients, U^n, accumulator) into per-slot buffers.
+// A segment block is a producer/consumer pipeline. Lane 0 of warp 8 streams the
+// segment down in chunks of kR rows with 3-D TMA boxes (cp.async.bulk.tensor)
+// completing on the chunk slot's mbarrier: all stencil fields of the stage
+// input with a 4-column halo into a row-contiguous 16-row ring (kNS chunk
+// slots), and the point-wise inputs (coefficients, U^n, accumulator) into the
+// slot's point-wise buffer.
 // Warps 0-7 compute one cell each per chunk purely from shared memory and
 // store the stage output and accumulator straight to HBM, coalesced along x.
 // Each field row thus crosses HBM once per stage; only the 3-row halo above
@@ -47,6 +48,11 @@ constexpr int kBarBytes = 128;           // full[kNS] + empty[kNS], padded
 constexpr int kFinishThreads = 256;      // filter / receiver kernel
 
 static_assert(kTX * kR == kConsumers, "one cell per consumer thread per chunk");
+// The stencil ring is row-contiguous ([ring row][field][col]) with kR extra rows
+// on each side: the chunk in the last slot is also copied above the first slot
+// and the chunk in the first slot below the last one, so the rows dz = -3..3
+// around any ring row are contiguous and no read wraps around.
+constexpr int kRingRows = kRing + 2 * kR;
 static_assert((kRing & (kRing - 1)) == 0, "ring rows must be a power of two");
 
 // Point-wise inputs staged per chunk, by stage kind: coefficients, then U^n
@@ -56,24 +62,26 @@ struct PW {
   static constexpr int n = NCOEF + (KIND == kStageMid ? 2 * NST : (KIND == kStageLast ? NST : 0));
 };
 
-// Shared memory of one segment block: barriers, kNS stencil slots of
-// [NST][kR][kSW] and kNS point-wise slots of [NPW][kR][kTX] (all 128-byte
+// Shared memory of one segment block: barriers, the stencil ring of kRingRows
+// rows [NST][kSW], kNS point-wise slots of [NPW][kR][kTX] (all 128-byte
 // multiples), plus 128 bytes to align the dynamic base.
 template <int NST, int NPW>
 __host__ __device__ constexpr size_t segment_smem() {
-  return size_t(128) + kBarBytes + size_t(kNS) * NST * kR * kSW * 4 +
+  return size_t(128) + kBarBytes + size_t(kRingRows) * NST * kSW * 4 +
          size_t(kNS) * NPW * kR * kTX * 4;
 }
 
-// Reads the stage input from the stencil slots: ring row q = (cell row + dz)
-// mod kRing lives in slot q / kR, row q % kR; column c + dx.
+// Reads the stage input from the stencil ring: the cell's ring row rr and the
+// rows dz = -3..3 around it are contiguous, so every read is the cell's base
+// plus a compile-time offset.
 template <int NST>
 struct RingAcc {
-  const float* ring;
-  int rr, c;
+  const float* base;  // ring row (rr) of the cell, its column (with the halo)
+  __device__ __forceinline__ void init(const float* ring, int rr, int c) {
+    base = ring + (kR + rr) * (NST * kSW) + c;
+  }
   __device__ __forceinline__ float at(int f, int dz, int dx) const {
-    const int q = (rr + dz) & (kRing - 1);
-    return ring[(((q / kR) * NST + f) * kR + (q % kR)) * kSW + c + dx];
+    return base[dz * (NST * kSW) + f * kSW + dx];
   }
 };
 struct FluidRing : RingAcc<3> {
@@ -120,7 +128,8 @@ struct Segment {
 // Producer (one lane of warp 8): chunk k (k = -1 .. nch; the two ends carry
 // only the halo rows) goes to slot (k + 1) % kNS once the slot's previous
 // chunk is released. Per chunk one 3-D TMA box brings all stencil fields of
-// kR rows (with the column halo), and up to three boxes the point-wise inputs.
+// kR rows (with the column halo; chunks of the first and last slot a second
+// time, past the ring's other end), and up to three boxes the point-wise inputs.
 // Tiled TMA always delivers whole boxes (zero-filled outside the arrays), so
 // the byte count announced on the barrier is a compile-time constant.
 template <int NST, int NCOEF, int KIND>
@@ -131,6 +140,7 @@ __device__ __forceinline__ void produce(const Segment& sg, const CUtensorMap* in
   if ((threadIdx.x & 31) != 0) return;
   constexpr int NPW = PW<NST, NCOEF, KIND>::n;
   constexpr unsigned kStBytes = NST * kR * kSW * 4, kPwBytes = NPW * kR * kTX * 4;
+  constexpr int kRowF = NST * kSW;  // floats per ring row
   constexpr int kF = kR * kTX;  // floats per point-wise field in a slot
   for (int k = -1; k <= sg.nch; ++k) {
     const int u = k + 1, slot = u % kNS;
@@ -140,8 +150,12 @@ __device__ __forceinline__ void produce(const Segment& sg, const CUtensorMap* in
     }
     const int r0 = sg.z0 + k * kR;
     const bool pw = k >= 0 && k < sg.nch;
-    mbar_arrive_expect_tx(&full[slot], kStBytes + (pw ? kPwBytes : 0u));
-    tma_load_3d(ring + slot * NST * kR * kSW, in_map, sg.x0 - 4, r0, 0, &full[slot]);
+    const bool dup = slot == 0 || slot == kNS - 1;  // also copied past the ring's other end
+    mbar_arrive_expect_tx(&full[slot], kStBytes * (dup ? 2u : 1u) + (pw ? kPwBytes : 0u));
+    tma_load_3d(ring + (kR + slot * kR) * kRowF, in_map, sg.x0 - 4, 0, r0, &full[slot]);
+    if (dup)
+      tma_load_3d(ring + (slot == 0 ? kR + kRing : 0) * kRowF, in_map, sg.x0 - 4, 0, r0,
+                  &full[slot]);
     if (pw) {
       float* d = slots + slot * NPW * kF;
       tma_load_3d(d, coef_map, sg.x0, r0, 0, &full[slot]);
@@ -187,7 +201,7 @@ __device__ __forceinline__ void segment_setup(char* smem_raw, uint64_t*& full, u
   full = reinterpret_cast<uint64_t*>(smem);
   empty = full + kNS;
   ring = reinterpret_cast<float*>(smem + kBarBytes);
-  slots = ring + kNS * NST * kR * kSW;
+  slots = ring + kRingRows * NST * kSW;
   if (threadIdx.x == 0) {
     for (int i = 0; i < kNS; ++i) {
       mbar_init(&full[i], 1);
@@ -229,7 +243,7 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
     const int iz = sg.z0 + c * kR + ty;
     if (!colok || iz >= sg.z1) return;
     FluidRing A;
-    A.ring = ring; A.rr = (iz - sg.z0 + kR) & (kRing - 1); A.c = tx + 4;
+    A.init(ring, (iz - sg.z0 + kR) & (kRing - 1), tx + 4);
     constexpr int F = kR * kTX;
     const float* pw = slots + (size_t)slot * NPW * F + ty * kTX + tx;  // field p at pw[p * F]
     const FluidCoefs cf{pw[0], pw[F], pw[2 * F], pw[3 * F], pw[4 * F], pw[5 * F]};
@@ -304,7 +318,7 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
     if (!colok || iz >= sg.z1) return;
     const bool bottom = iz >= zb0;
     SolidRing A;
-    A.ring = ring; A.rr = (iz - sg.z0 + kR) & (kRing - 1); A.c = tx + 4;
+    A.init(ring, (iz - sg.z0 + kR) & (kRing - 1), tx + 4);
     constexpr int F = kR * kTX;
     const float* pw = slots + (size_t)slot * NPW * F + ty * kTX + tx;
     const SolidCoefs cf{pw[0], pw[F], pw[2 * F], pw[3 * F], pw[4 * F],

@@ -26,8 +26,10 @@ void stage_grid(int nx, int nzf, int nzs, int* ntx, int* nbf, int* nbs, int* nbi
 cudaError_t upload_constants(const float* srcw25, const float* w7);
 
 // Library-internal host helpers (mfdm_host.cu): record a failure for
-// mfdm_last_error() and return `code`; encode a TMA map of a [nf][rows][P] block.
+// mfdm_last_error() and return `code`; encode a TMA map of a [nf][rows][P] block
+// (rows_outer: boxes land as [row][field][col], the stencil-ring layout).
 int set_error(int code, const char* msg);
-int encode_block_map(CUtensorMap* map, const float* base, int P, int rows, int nf, int box_x);
+int encode_block_map(CUtensorMap* map, const float* base, int P, int rows, int nf, int box_x,
+                     bool rows_outer);
 
 }  // namespace mfdm
