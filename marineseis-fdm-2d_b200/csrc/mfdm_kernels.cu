@@ -27,6 +27,8 @@
 // store the stage output and accumulator straight to HBM, coalesced along x.
 // Each field row thus crosses HBM once per stage; only the 3-row halo above
 // and below a segment and the 4-column halo of a strip are read twice.
+#include <type_traits>
+
 #include "mfdm_async.cuh"
 #include "mfdm_device.cuh"
 #include "mfdm_kernels.h"
@@ -36,7 +38,8 @@ namespace mfdm {
 constexpr int kTX = kStageTX;            // computed columns per strip
 constexpr int kSW = kStageSW;            // staged row width (4-column halo each side)
 constexpr int kR = kStageR;              // rows per chunk
-constexpr int kNS = 4;                   // chunk slots in flight
+constexpr int kNS = 4;                   // stencil chunk slots
+constexpr int kNP = 4;                   // point-wise chunk slots
 constexpr int kRing = kR * kNS;          // ring rows (power of two)
 constexpr int kConsumers = 256;          // warps 0-7
 constexpr int kThreads = kConsumers + 32;  // + producer warp
@@ -44,7 +47,7 @@ constexpr int kThreads = kConsumers + 32;  // + producer warp
 #define MFDM_SEG_ROWS 24
 #endif
 constexpr int kSeg = MFDM_SEG_ROWS;      // rows per segment block
-constexpr int kBarBytes = 128;           // full[kNS] + empty[kNS], padded
+constexpr int kBarBytes = 128;           // full/empty barriers of both rings
 constexpr int kFinishThreads = 256;      // filter / receiver kernel
 
 static_assert(kTX * kR == kConsumers, "one cell per consumer thread per chunk");
@@ -54,6 +57,7 @@ static_assert(kTX * kR == kConsumers, "one cell per consumer thread per chunk");
 // around any ring row are contiguous and no read wraps around.
 constexpr int kRingRows = kRing + 2 * kR;
 static_assert((kRing & (kRing - 1)) == 0, "ring rows must be a power of two");
+static_assert(2 * (kNS + kNP) * 8 <= kBarBytes, "barrier region too small");
 
 // Point-wise inputs staged per chunk, by stage kind: coefficients, then U^n
 // (middle stages), then the accumulator (middle and last stages).
@@ -63,12 +67,12 @@ struct PW {
 };
 
 // Shared memory of one segment block: barriers, the stencil ring of kRingRows
-// rows [NST][kSW], kNS point-wise slots of [NPW][kR][kTX] (all 128-byte
+// rows [NST][kSW], kNP point-wise slots of [NPW][kR][kTX] (all 128-byte
 // multiples), plus 128 bytes to align the dynamic base.
 template <int NST, int NPW>
 __host__ __device__ constexpr size_t segment_smem() {
   return size_t(128) + kBarBytes + size_t(kRingRows) * NST * kSW * 4 +
-         size_t(kNS) * NPW * kR * kTX * 4;
+         size_t(kNP) * NPW * kR * kTX * 4;
 }
 
 // Reads the stage input from the stencil ring: the cell's ring row rr and the
@@ -125,87 +129,115 @@ struct Segment {
   int nch;    // computed chunks
 };
 
-// Producer (one lane of warp 8): chunk k (k = -1 .. nch; the two ends carry
-// only the halo rows) goes to slot (k + 1) % kNS once the slot's previous
-// chunk is released. Per chunk one 3-D TMA box brings all stencil fields of
-// kR rows (with the column halo; chunks of the first and last slot a second
-// time, past the ring's other end), and up to three boxes the point-wise inputs.
+// The mbarriers of a segment block: the stencil ring's full/empty pair per
+// slot and the point-wise ring's.
+struct Bars {
+  uint64_t *full, *empty, *pfull, *pempty;
+};
+
+// Producer (one lane of warp 8). Stencil chunk k (k = -1 .. nch; the two ends
+// carry only the halo rows) goes to ring slot (k + 1) % kNS once the slot's
+// previous chunk is released: one 3-D TMA box with all stencil fields of kR
+// rows and the column halo (chunks of the first and last slot a second time,
+// past the ring's other end). The point-wise inputs of chunk k (k = 0 .. nch-1:
+// coefficients, U^n, accumulator, up to three boxes) go to point-wise slot
+// k % kNP once chunk k - kNP is computed, and are issued right after stencil
+// chunk k - 1: both then wait for the same chunk, and the point-wise block,
+// the bulk of the bytes, is in flight kNP - 1 chunks ahead of its use.
 // Tiled TMA always delivers whole boxes (zero-filled outside the arrays), so
-// the byte count announced on the barrier is a compile-time constant.
+// every byte count announced on a barrier is a compile-time constant.
 template <int NST, int NCOEF, int KIND>
 __device__ __forceinline__ void produce(const Segment& sg, const CUtensorMap* in_map,
                                         const CUtensorMap* coef_map, const CUtensorMap* un_map,
                                         const CUtensorMap* acc_map, float* ring, float* slots,
-                                        uint64_t* full, uint64_t* empty, int* status) {
+                                        const Bars& B, int* status) {
   if ((threadIdx.x & 31) != 0) return;
   constexpr int NPW = PW<NST, NCOEF, KIND>::n;
   constexpr unsigned kStBytes = NST * kR * kSW * 4, kPwBytes = NPW * kR * kTX * 4;
   constexpr int kRowF = NST * kSW;  // floats per ring row
-  constexpr int kF = kR * kTX;  // floats per point-wise field in a slot
+  constexpr int kF = kR * kTX;      // floats per point-wise field in a slot
+  static_assert(kNP == kNS, "issue order assumes equal ring depths");
   for (int k = -1; k <= sg.nch; ++k) {
     const int u = k + 1, slot = u % kNS;
-    if (u >= kNS && !mbar_wait(&empty[slot], ((u / kNS) - 1) & 1)) {
+    if (u >= kNS && !mbar_wait(&B.empty[slot], ((u / kNS) - 1) & 1)) {
       atomicOr(status, 2);
       return;
     }
     const int r0 = sg.z0 + k * kR;
-    const bool pw = k >= 0 && k < sg.nch;
     const bool dup = slot == 0 || slot == kNS - 1;  // also copied past the ring's other end
-    mbar_arrive_expect_tx(&full[slot], kStBytes * (dup ? 2u : 1u) + (pw ? kPwBytes : 0u));
-    tma_load_3d(ring + (kR + slot * kR) * kRowF, in_map, sg.x0 - 4, 0, r0, &full[slot]);
+    mbar_arrive_expect_tx(&B.full[slot], kStBytes * (dup ? 2u : 1u));
+    tma_load_3d(ring + (kR + slot * kR) * kRowF, in_map, sg.x0 - 4, 0, r0, &B.full[slot]);
     if (dup)
       tma_load_3d(ring + (slot == 0 ? kR + kRing : 0) * kRowF, in_map, sg.x0 - 4, 0, r0,
-                  &full[slot]);
-    if (pw) {
-      float* d = slots + slot * NPW * kF;
-      tma_load_3d(d, coef_map, sg.x0, r0, 0, &full[slot]);
+                  &B.full[slot]);
+    const int j = k + 1;  // point-wise chunk issued after stencil chunk j - 1
+    if (j < sg.nch) {
+      const int ps = j % kNP;
+      if (j >= kNP && !mbar_wait(&B.pempty[ps], ((j / kNP) - 1) & 1)) {
+        atomicOr(status, 2);
+        return;
+      }
+      const int q0 = sg.z0 + j * kR;
+      float* d = slots + ps * NPW * kF;
+      mbar_arrive_expect_tx(&B.pfull[ps], kPwBytes);
+      tma_load_3d(d, coef_map, sg.x0, q0, 0, &B.pfull[ps]);
       if (KIND == kStageMid) {
-        tma_load_3d(d + NCOEF * kF, un_map, sg.x0, r0, 0, &full[slot]);
-        tma_load_3d(d + (NCOEF + NST) * kF, acc_map, sg.x0, r0, 0, &full[slot]);
+        tma_load_3d(d + NCOEF * kF, un_map, sg.x0, q0, 0, &B.pfull[ps]);
+        tma_load_3d(d + (NCOEF + NST) * kF, acc_map, sg.x0, q0, 0, &B.pfull[ps]);
       } else if (KIND == kStageLast) {
-        tma_load_3d(d + NCOEF * kF, acc_map, sg.x0, r0, 0, &full[slot]);
+        tma_load_3d(d + NCOEF * kF, acc_map, sg.x0, q0, 0, &B.pfull[ps]);
       }
     }
   }
 }
 
-// Consumer side of the pipeline: waits for chunk c+1 (the halo below chunk c),
-// hands each thread its cell, then releases chunk c-1.
+// Consumer side of the pipeline: per chunk c waits for stencil chunk c+1 (the
+// halo below chunk c) and point-wise chunk c, hands each thread its cell, then
+// releases stencil chunk c-1 and point-wise chunk c.
 template <class Body>
-__device__ __forceinline__ void consume(const Segment& sg, uint64_t* full, uint64_t* empty,
-                                        int* status, const Body& body) {
+__device__ __forceinline__ void consume(const Segment& sg, const Bars& B, int* status,
+                                        const Body& body) {
   const int lane = threadIdx.x & 31;
-  // chunks -1 and 0 (slots 0 and 1, first use)
-  if (!mbar_wait(&full[0], 0) || !mbar_wait(&full[1], 0)) {
+  // stencil chunks -1 and 0 (slots 0 and 1, first use)
+  if (!mbar_wait(&B.full[0], 0) || !mbar_wait(&B.full[1], 0)) {
     if (lane == 0) atomicOr(status, 2);
     return;
   }
   for (int c = 0; c < sg.nch; ++c) {
-    const int un = c + 2;  // use index of chunk c+1
-    if (!mbar_wait(&full[un % kNS], (un / kNS) & 1)) {
+    const int un = c + 2;  // stencil use of chunk c+1
+    if (!mbar_wait(&B.full[un % kNS], (un / kNS) & 1) ||
+        !mbar_wait(&B.pfull[c % kNP], (c / kNP) & 1)) {
       if (lane == 0) atomicOr(status, 2);
       return;
     }
-    body(c, (c + 1) % kNS);
+    body(c, c % kNP);
     __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[c % kNS]);  // chunk c-1 is no longer needed
+    if (lane == 0) {
+      mbar_arrive(&B.empty[c % kNS]);  // stencil chunk c-1 is no longer needed
+      mbar_arrive(&B.pempty[c % kNP]);
+    }
   }
 }
 
 // Carves the barriers and the slots out of the dynamic shared memory (base
 // rounded up to 128 bytes) and initialises the barriers.
 template <int NST>
-__device__ __forceinline__ void segment_setup(char* smem_raw, uint64_t*& full, uint64_t*& empty,
-                                              float*& ring, float*& slots) {
+__device__ __forceinline__ void segment_setup(char* smem_raw, Bars& B, float*& ring, float*& slots) {
   char* smem = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
-  full = reinterpret_cast<uint64_t*>(smem);
-  empty = full + kNS;
+  B.full = reinterpret_cast<uint64_t*>(smem);
+  B.empty = B.full + kNS;
+  B.pfull = B.empty + kNS;
+  B.pempty = B.pfull + kNP;
   ring = reinterpret_cast<float*>(smem + kBarBytes);
   slots = ring + kRingRows * NST * kSW;
   if (threadIdx.x == 0) {
     for (int i = 0; i < kNS; ++i) {
-      mbar_init(&full[i], 1);
-      mbar_init(&empty[i], kConsumers / 32);
+      mbar_init(&B.full[i], 1);
+      mbar_init(&B.empty[i], kConsumers / 32);
+    }
+    for (int i = 0; i < kNP; ++i) {
+      mbar_init(&B.pfull[i], 1);
+      mbar_init(&B.pempty[i], kConsumers / 32);
     }
     mbar_fence_init();
   }
@@ -225,12 +257,12 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
   sg.z1 = min(sg.z0 + kSeg, C.nzf - 1);
   sg.rows = C.nzf;
   sg.nch = (sg.z1 - sg.z0 + kR - 1) / kR;
-  uint64_t *full, *empty;
+  Bars B;
   float *ring, *slots;
-  segment_setup<NST>(smem, full, empty, ring, slots);
+  segment_setup<NST>(smem, B, ring, slots);
   if (threadIdx.x >= kConsumers) {
-    produce<NST, NCOEF, KIND>(sg, &maps.fin, &maps.fcoef, &maps.fun, &maps.facc, ring, slots, full,
-                              empty, C.status);
+    produce<NST, NCOEF, KIND>(sg, &maps.fin, &maps.fcoef, &maps.fun, &maps.facc, ring, slots, B,
+                              C.status);
     return;
   }
   const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
@@ -239,9 +271,16 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
   const bool side = colok && min(ix - 3, nx - 4 - ix) < C.npd;
   const int scol = side ? xstrip_col(ix, nx, C.npd) : 0;
   const float cc = C.rk_c[s], w = (KIND == kStageLast) ? 0.f : C.rk_w[s];
-  consume(sg, full, empty, C.status, [&](int c, int slot) {
+  // Segments with no side-strip cell, no edge column and no source cell take a
+  // body without those branches.
+  const bool general = sg.x0 < 3 + C.npd || sg.x0 + kTX > nx - 3 - C.npd ||
+                       (C.srcx >= 0 && C.srcx >= sg.x0 - 2 && C.srcx < sg.x0 + kTX + 2 &&
+                        C.srcz >= sg.z0 - 2 && C.srcz < sg.z1 + 2);
+  auto cell = [&](auto gen_tag, int c, int slot) {
+    constexpr bool GEN = decltype(gen_tag)::value;
     const int iz = sg.z0 + c * kR + ty;
-    if (!colok || iz >= sg.z1) return;
+    if ((GEN && !colok) || iz >= sg.z1) return;
+    const bool sd = GEN && side;  // a side-strip cell
     FluidRing A;
     A.init(ring, (iz - sg.z0 + kR) & (kRing - 1), tx + 4);
     constexpr int F = kR * kTX;
@@ -249,14 +288,14 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
     const FluidCoefs cf{pw[0], pw[F], pw[2 * F], pw[3 * F], pw[4 * F], pw[5 * F]};
     float ade[4] = {0.f, 0.f, 0.f, 0.f};
     const size_t si = (size_t)iz * C.Ps + scol;
-    if (side) {
+    if (sd) {
 #pragma unroll
       for (int q = 0; q < 4; ++q) ade[q] = __ldg(in.fx[q] + si);
     }
     // rows 6 .. nz_f-4 take the specialised interior body (no conservative rows)
-    FluidK k = (iz >= 6 && iz <= C.nzf - 4) ? fluid_rhs<DIR, true>(C, A, iz, ix, side, ade, cf)
-                                            : fluid_rhs<DIR, false>(C, A, iz, ix, side, ade, cf);
-    k.p += source_term(C, iz, ix, it, s);
+    FluidK k = (iz >= 6 && iz <= C.nzf - 4) ? fluid_rhs<DIR, true>(C, A, iz, ix, sd, ade, cf)
+                                            : fluid_rhs<DIR, false>(C, A, iz, ix, sd, ade, cf);
+    if (GEN) k.p += source_term(C, iz, ix, it, s);
     const size_t i = (size_t)iz * P + ix;
     const float kv[3] = {k.vx, k.vz, k.p};
     float* const outs[3] = {out.fvx, out.fvz, out.fp};
@@ -274,7 +313,7 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
         outs[f][i] = fmaf(cc, kv[f], pw[(NCOEF + f) * F]);
       }
     }
-    if (side) {
+    if (sd) {
       rk_update<KIND>(k.V0, ade[0], un.fx[0], out.fx[0], acc.fx[0], si, cc, w);
       rk_update<KIND>(k.V1, ade[1], un.fx[1], out.fx[1], acc.fx[1], si, cc, w);
       if (k.has_E) {
@@ -282,7 +321,11 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
         rk_update<KIND>(k.E1, ade[3], un.fx[3], out.fx[3], acc.fx[3], si, cc, w);
       }
     }
-  });
+  };
+  if (general)
+    consume(sg, B, C.status, [&](int c, int slot) { cell(std::true_type{}, c, slot); });
+  else
+    consume(sg, B, C.status, [&](int c, int slot) { cell(std::false_type{}, c, slot); });
 }
 
 template <int DIR, int KIND>
@@ -298,12 +341,12 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
   sg.z1 = min(sg.z0 + kSeg, nzs - 3);
   sg.rows = nzs;
   sg.nch = (sg.z1 - sg.z0 + kR - 1) / kR;
-  uint64_t *full, *empty;
+  Bars B;
   float *ring, *slots;
-  segment_setup<NST>(smem, full, empty, ring, slots);
+  segment_setup<NST>(smem, B, ring, slots);
   if (threadIdx.x >= kConsumers) {
-    produce<NST, NCOEF, KIND>(sg, &maps.sin, &maps.scoef, &maps.sun, &maps.sacc, ring, slots, full,
-                              empty, C.status);
+    produce<NST, NCOEF, KIND>(sg, &maps.sin, &maps.scoef, &maps.sun, &maps.sacc, ring, slots, B,
+                              C.status);
     return;
   }
   const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
@@ -313,10 +356,15 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
   const int scol = side ? xstrip_col(ix, nx, npd) : 0;
   const int zb0 = nzs - 3 - npd;  // first row of the bottom strip
   const float cc = C.rk_c[s], w = (KIND == kStageLast) ? 0.f : C.rk_w[s];
-  consume(sg, full, empty, C.status, [&](int c, int slot) {
+  // Segments with no PML cell and no edge column take a body without those
+  // branches (every cell of such a segment is an interior column).
+  const bool general = sg.x0 < 3 + npd || sg.x0 + kTX > nx - 3 - npd || sg.z1 > zb0;
+  auto cell = [&](auto gen_tag, int c, int slot) {
+    constexpr bool GEN = decltype(gen_tag)::value;
     const int iz = sg.z0 + c * kR + ty;
-    if (!colok || iz >= sg.z1) return;
-    const bool bottom = iz >= zb0;
+    if ((GEN && !colok) || iz >= sg.z1) return;
+    const bool sd = GEN && side;  // a side-strip cell
+    const bool bottom = GEN && iz >= zb0;
     SolidRing A;
     A.init(ring, (iz - sg.z0 + kR) & (kRing - 1), tx + 4);
     constexpr int F = kR * kTX;
@@ -326,7 +374,7 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
     float xade[4] = {0.f, 0.f, 0.f, 0.f}, zade[4] = {0.f, 0.f, 0.f, 0.f};
     const size_t sxi = (size_t)iz * C.Ps + scol;
     const size_t szi = (size_t)(iz - zb0) * P + ix;
-    if (side) {
+    if (sd) {
 #pragma unroll
       for (int q = 0; q < 4; ++q) xade[q] = __ldg(in.sx[q] + sxi);
     }
@@ -334,8 +382,8 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
 #pragma unroll
       for (int q = 0; q < 4; ++q) zade[q] = __ldg(in.sz[q] + szi);
     }
-    SolidK k = iz >= 3 ? solid_rhs<DIR, true>(C, A, iz, ix, side, bottom, xade, zade, cf)
-                       : solid_rhs<DIR, false>(C, A, iz, ix, side, bottom, xade, zade, cf);
+    SolidK k = iz >= 3 ? solid_rhs<DIR, true>(C, A, iz, ix, sd, bottom, xade, zade, cf)
+                       : solid_rhs<DIR, false>(C, A, iz, ix, sd, bottom, xade, zade, cf);
     const size_t i = (size_t)iz * P + ix;
     const float kv[5] = {k.vx, k.vz, k.sx, k.sz, k.sxz};
     float* const outs[5] = {out.svx, out.svz, out.ssx, out.ssz, out.ssxz};
@@ -353,7 +401,7 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
         outs[f][i] = fmaf(cc, kv[f], pw[(NCOEF + f) * F]);
       }
     }
-    if (side) {
+    if (sd) {
       rk_update<KIND>(k.XV0, xade[0], un.sx[0], out.sx[0], acc.sx[0], sxi, cc, w);
       rk_update<KIND>(k.XV1, xade[1], un.sx[1], out.sx[1], acc.sx[1], sxi, cc, w);
       rk_update<KIND>(k.XE0, xade[2], un.sx[2], out.sx[2], acc.sx[2], sxi, cc, w);
@@ -365,7 +413,11 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
       rk_update<KIND>(k.ZE0, zade[2], un.sz[2], out.sz[2], acc.sz[2], szi, cc, w);
       rk_update<KIND>(k.ZE1, zade[3], un.sz[3], out.sz[3], acc.sz[3], szi, cc, w);
     }
-  });
+  };
+  if (general)
+    consume(sg, B, C.status, [&](int c, int slot) { cell(std::true_type{}, c, slot); });
+  else
+    consume(sg, B, C.status, [&](int c, int slot) { cell(std::false_type{}, c, slot); });
 }
 
 // Interface strip: fluid row nz_f-1 and solid row 0 of one column, their RHS,
