@@ -247,8 +247,8 @@ __device__ __forceinline__ void segment_setup(char* smem_raw, Bars& B, float*& r
 template <int DIR, int KIND>
 __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, const Fields& out,
                                               const Fields& un, const Fields& acc,
-                                              const StageMaps& maps, int s, int it, int blk,
-                                              int ntx, char* smem) {
+                                              const StageMaps& maps, int s, float cc, float w,
+                                              int it, int blk, int ntx, char* smem) {
   constexpr int NST = 3, NCOEF = 6, NPW = PW<NST, NCOEF, KIND>::n;
   const int P = C.P, nx = C.nx;
   Segment sg;
@@ -270,10 +270,11 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
   const bool colok = ix >= 3 && ix <= nx - 4;
   const bool side = colok && min(ix - 3, nx - 4 - ix) < C.npd;
   const int scol = side ? xstrip_col(ix, nx, C.npd) : 0;
-  const float cc = C.rk_c[s], w = (KIND == kStageLast) ? 0.f : C.rk_w[s];
-  // Segments with no side-strip cell, no edge column and no source cell take a
-  // body without those branches.
+  // Segments with no side-strip cell, no edge column, no source cell and no
+  // conservative or one-sided row (rows 6 .. nz_f-4 only) take a body without
+  // those branches.
   const bool general = sg.x0 < 3 + C.npd || sg.x0 + kTX > nx - 3 - C.npd ||
+                       sg.z0 < 6 || sg.z1 - 1 > C.nzf - 4 ||
                        (C.srcx >= 0 && C.srcx >= sg.x0 - 2 && C.srcx < sg.x0 + kTX + 2 &&
                         C.srcz >= sg.z0 - 2 && C.srcz < sg.z1 + 2);
   auto cell = [&](auto gen_tag, int c, int slot) {
@@ -293,8 +294,9 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
       for (int q = 0; q < 4; ++q) ade[q] = __ldg(in.fx[q] + si);
     }
     // rows 6 .. nz_f-4 take the specialised interior body (no conservative rows)
-    FluidK k = (iz >= 6 && iz <= C.nzf - 4) ? fluid_rhs<DIR, true>(C, A, iz, ix, sd, ade, cf)
-                                            : fluid_rhs<DIR, false>(C, A, iz, ix, sd, ade, cf);
+    FluidK k = (!GEN || (iz >= 6 && iz <= C.nzf - 4))
+                   ? fluid_rhs<DIR, true>(C, A, iz, ix, sd, ade, cf)
+                   : fluid_rhs<DIR, false>(C, A, iz, ix, sd, ade, cf);
     if (GEN) k.p += source_term(C, iz, ix, it, s);
     const size_t i = (size_t)iz * P + ix;
     const float kv[3] = {k.vx, k.vz, k.p};
@@ -331,8 +333,8 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
 template <int DIR, int KIND>
 __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, const Fields& out,
                                               const Fields& un, const Fields& acc,
-                                              const StageMaps& maps, int s, int blk, int ntx,
-                                              char* smem) {
+                                              const StageMaps& maps, float cc, float w, int blk,
+                                              int ntx, char* smem) {
   constexpr int NST = 5, NCOEF = 9, NPW = PW<NST, NCOEF, KIND>::n;
   const int P = C.P, nx = C.nx, npd = C.npd, nzs = C.nzs;
   Segment sg;
@@ -355,10 +357,9 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
   const bool side = colok && min(ix - 3, nx - 4 - ix) < npd;
   const int scol = side ? xstrip_col(ix, nx, npd) : 0;
   const int zb0 = nzs - 3 - npd;  // first row of the bottom strip
-  const float cc = C.rk_c[s], w = (KIND == kStageLast) ? 0.f : C.rk_w[s];
-  // Segments with no PML cell and no edge column take a body without those
-  // branches (every cell of such a segment is an interior column).
-  const bool general = sg.x0 < 3 + npd || sg.x0 + kTX > nx - 3 - npd || sg.z1 > zb0;
+  // Segments with no PML cell, no edge column and no flux-form row (rows >= 3
+  // only) take a body without those branches.
+  const bool general = sg.x0 < 3 + npd || sg.x0 + kTX > nx - 3 - npd || sg.z1 > zb0 || sg.z0 < 3;
   auto cell = [&](auto gen_tag, int c, int slot) {
     constexpr bool GEN = decltype(gen_tag)::value;
     const int iz = sg.z0 + c * kR + ty;
@@ -382,8 +383,9 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
 #pragma unroll
       for (int q = 0; q < 4; ++q) zade[q] = __ldg(in.sz[q] + szi);
     }
-    SolidK k = iz >= 3 ? solid_rhs<DIR, true>(C, A, iz, ix, sd, bottom, xade, zade, cf)
-                       : solid_rhs<DIR, false>(C, A, iz, ix, sd, bottom, xade, zade, cf);
+    SolidK k = (!GEN || iz >= 3)
+                   ? solid_rhs<DIR, true>(C, A, iz, ix, sd, bottom, xade, zade, cf)
+                   : solid_rhs<DIR, false>(C, A, iz, ix, sd, bottom, xade, zade, cf);
     const size_t i = (size_t)iz * P + ix;
     const float kv[5] = {k.vx, k.vz, k.sx, k.sz, k.sxz};
     float* const outs[5] = {out.svx, out.svz, out.ssx, out.ssz, out.ssxz};
@@ -425,8 +427,8 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
 // In the last stage the eight coupled state values go to C.ipre, the filter's input.
 template <int DIR, int KIND>
 __device__ __forceinline__ void interface_strip(const Coef& C, const Fields& in, const Fields& out,
-                                                const Fields& un, const Fields& acc, int s,
-                                                int blk) {
+                                                const Fields& un, const Fields& acc, float c,
+                                                float w, int blk) {
   const int nx = C.nx, P = C.P, nzf = C.nzf, nzs = C.nzs, npd = C.npd;
   if (threadIdx.x >= kConsumers) return;
   const int ix = blk * kConsumers + threadIdx.x;
@@ -435,7 +437,6 @@ __device__ __forceinline__ void interface_strip(const Coef& C, const Fields& in,
   const int scol = side ? xstrip_col(ix, nx, npd) : 0;
   const int zb0 = nzs - 3 - npd;
   const bool bottom = 0 >= zb0;
-  const float c = C.rk_c[s], w = (KIND == kStageLast) ? 0.f : C.rk_w[s];
 
   const size_t fi = (size_t)(nzf - 1) * P + ix;  // fluid interface cell
   const size_t si = ix;                          // solid interface cell
@@ -521,20 +522,22 @@ __device__ __forceinline__ void interface_strip(const Coef& C, const Fields& in,
   }
 }
 
+// One RK stage: `s` indexes the Ricker table; cc and w are the stage's RK
+// weights (out = base + cc k, accumulator += w k).
 template <int DIR, int KIND>
 __global__ void __launch_bounds__(kThreads, 2)
     stage_kernel(Coef C, Fields in, Fields out, Fields un, Fields acc,
-                 const __grid_constant__ StageMaps maps, int s, int ntx, int nbi, int nbf,
-                 int nbs) {
+                 const __grid_constant__ StageMaps maps, int s, float cc, float w, int ntx,
+                 int nbi, int nbf, int nbs) {
   extern __shared__ char smem[];
   const int b = blockIdx.x;
   if (b < nbi) {  // first, so the short interface blocks overlap the segments
-    interface_strip<DIR, KIND>(C, in, out, un, acc, s, b);
+    interface_strip<DIR, KIND>(C, in, out, un, acc, cc, w, b);
   } else if (b < nbi + nbf) {
     const int it = __ldg(C.step);
-    fluid_segment<DIR, KIND>(C, in, out, un, acc, maps, s, it, b - nbi, ntx, smem);
+    fluid_segment<DIR, KIND>(C, in, out, un, acc, maps, s, cc, w, it, b - nbi, ntx, smem);
   } else {
-    solid_segment<DIR, KIND>(C, in, out, un, acc, maps, s, b - nbi - nbf, ntx, smem);
+    solid_segment<DIR, KIND>(C, in, out, un, acc, maps, cc, w, b - nbi - nbf, ntx, smem);
   }
 }
 
@@ -630,8 +633,9 @@ static cudaError_t launch_one(const Coef& C, const Fields& in, const Fields& out
                               const Fields& acc, const StageMaps& maps, int s, cudaStream_t st) {
   int ntx, nbf, nbs, nbi;
   stage_grid(C.nx, C.nzf, C.nzs, &ntx, &nbf, &nbs, &nbi);
+  const float cc = C.rk_c[s], w = (KIND == kStageLast) ? 0.f : C.rk_w[s];
   stage_kernel<DIR, KIND><<<nbi + nbf + nbs, kThreads, smem_for_kind<KIND>(), st>>>(
-      C, in, out, un, acc, maps, s, ntx, nbi, nbf, nbs);
+      C, in, out, un, acc, maps, s, cc, w, ntx, nbi, nbf, nbs);
   return cudaGetLastError();
 }
 
