@@ -63,8 +63,17 @@ struct HostModel {
   int npd = 0, npow = 2;
   float thickness = 0.f, vp_max = 0.f, rc = 0.f, beta0 = 1.f;
   std::vector<int> srcx, srcz;
-  // host arrays, [rows][nx]
+  // host arrays, [rows][nx], when the model was read from files
   std::vector<float> K, rhof, C11, C13, C33, C55, rhos, J, xix, xiz, zex, zez;
+  // The arrays the upload reads: the vectors above, or the caller's own memory
+  // (mfdm_desc), which is then copied to the device directly, without a host copy.
+  struct View {
+    const float *K, *rhof, *C11, *C13, *C33, *C55, *rhos, *J, *xix, *xiz, *zex, *zez;
+  } v{};
+  void view_own() {
+    v = {K.data(), rhof.data(), C11.data(), C13.data(), C33.data(), C55.data(),
+         rhos.data(), J.data(), xix.data(), xiz.data(), zex.data(), zez.data()};
+  }
 };
 
 int round_up(int v, int m) { return (v + m - 1) / m * m; }
@@ -127,12 +136,10 @@ int validate(const HostModel& h) {
   if (h.nt < 0) return fail(MFDM_ERR_ARG, "nt must be >= 0");
   if (h.snapshot <= 0) return fail(MFDM_ERR_ARG, "snapshot interval must be > 0");
   if (h.srcx.size() != h.srcz.size()) return fail(MFDM_ERR_ARG, "posx/posz length mismatch");
-  const size_t nf = size_t(h.nx) * h.nzf, ns = size_t(h.nx) * h.nzs,
-               ng = size_t(h.nx) * (h.nzf + h.nzs - 1);
-  if (h.K.size() != nf || h.rhof.size() != nf || h.C11.size() != ns || h.C13.size() != ns ||
-      h.C33.size() != ns || h.C55.size() != ns || h.rhos.size() != ns || h.J.size() != ng ||
-      h.xix.size() != ng || h.xiz.size() != ng || h.zex.size() != ng || h.zez.size() != ng)
-    return fail(MFDM_ERR_ARG, "array sizes do not match the grid");
+  const HostModel::View& v = h.v;
+  if (!v.K || !v.rhof || !v.C11 || !v.C13 || !v.C33 || !v.C55 || !v.rhos || !v.J || !v.xix ||
+      !v.xiz || !v.zex || !v.zez)
+    return fail(MFDM_ERR_ARG, "null model array");
   return MFDM_OK;
 }
 
@@ -216,6 +223,7 @@ int load_json(const char* path, HostModel& h) {
       const int rc = read_bin(J.get_string(it.key), it.n, *it.dst);
       if (rc != MFDM_OK) return rc;
     }
+    h.view_own();
   } catch (const std::exception& e) {
     return fail(MFDM_ERR_CONFIG, e.what());
   }
@@ -378,46 +386,38 @@ int check_status(mfdm_model* m) {
 // scalars of `h` into the buffers of `m` (shape already checked).
 int upload_model(mfdm_model* m, const HostModel& h) {
   const int nx = h.nx, nzf = h.nzf, nzs = h.nzs, nz = nzf + nzs - 1, P = m->P;
+  const HostModel::View& v = h.v;
   Coef& C = m->C;
-  auto up = [&](const float* dst_c, const std::vector<float>& v, int rows) -> int {
-    float* dst = const_cast<float*>(dst_c);
-    MFDM_CU(cudaMemcpy2DAsync(dst, size_t(P) * sizeof(float), v.data(), size_t(nx) * sizeof(float),
-                              size_t(nx) * sizeof(float), size_t(rows), cudaMemcpyHostToDevice,
-                              m->stream));
-    return MFDM_OK;
-  };
-  auto up_rows = [&](const float* dst_c, const std::vector<float>& v, int row0, int rows) -> int {
-    float* dst = const_cast<float*>(dst_c);
-    MFDM_CU(cudaMemcpy2DAsync(dst, size_t(P) * sizeof(float), v.data() + size_t(row0) * nx,
+  // Host [rows][nx] -> device [rows][P], straight from the caller's memory
+  // (full PCIe rate when the caller's buffers are pinned).
+  auto up = [&](const float* dst_c, const float* src, int rows) -> int {
+    MFDM_CU(cudaMemcpy2DAsync(const_cast<float*>(dst_c), size_t(P) * sizeof(float), src,
                               size_t(nx) * sizeof(float), size_t(nx) * sizeof(float), size_t(rows),
                               cudaMemcpyHostToDevice, m->stream));
     return MFDM_OK;
   };
   int rc;
-#if MFDM_RCP_RHO
-  // density slots hold 1/rho (reciprocal in FP64, rounded once)
-  std::vector<float> rf(h.rhof.size()), rs(h.rhos.size());
-  for (size_t i = 0; i < rf.size(); ++i) rf[i] = float(1.0 / double(h.rhof[i]));
-  for (size_t i = 0; i < rs.size(); ++i) rs[i] = float(1.0 / double(h.rhos[i]));
-  const std::vector<float>& rho_f_dev = rf;
-  const std::vector<float>& rho_s_dev = rs;
-#else
-  const std::vector<float>& rho_f_dev = h.rhof;
-  const std::vector<float>& rho_s_dev = h.rhos;
-#endif
-  if ((rc = up(C.K, h.K, nzf)) || (rc = up(C.rhof, rho_f_dev, nzf)) || (rc = up(C.C11, h.C11, nzs)) ||
-      (rc = up(C.C13, h.C13, nzs)) || (rc = up(C.C33, h.C33, nzs)) ||
-      (rc = up(C.C55, h.C55, nzs)) || (rc = up(C.rhos, rho_s_dev, nzs)) || (rc = up(C.J, h.J, nz)) ||
-      (rc = up(C.xix, h.xix, nz)) || (rc = up(C.xiz, h.xiz, nz)) || (rc = up(C.zex, h.zex, nz)) ||
-      (rc = up(C.zez, h.zez, nz)))
+  if ((rc = up(C.K, v.K, nzf)) || (rc = up(C.rhof, v.rhof, nzf)) || (rc = up(C.C11, v.C11, nzs)) ||
+      (rc = up(C.C13, v.C13, nzs)) || (rc = up(C.C33, v.C33, nzs)) ||
+      (rc = up(C.C55, v.C55, nzs)) || (rc = up(C.rhos, v.rhos, nzs)) || (rc = up(C.J, v.J, nz)) ||
+      (rc = up(C.xix, v.xix, nz)) || (rc = up(C.xiz, v.xiz, nz)) || (rc = up(C.zex, v.zex, nz)) ||
+      (rc = up(C.zez, v.zez, nz)))
     return rc;
+#if MFDM_RCP_RHO
+  // density slots hold 1/rho (reciprocal in FP64, rounded once), formed on the device
+  MFDM_CU(mfdm::launch_reciprocal(const_cast<float*>(C.rhof), nzf, nx, P, m->stream));
+  MFDM_CU(mfdm::launch_reciprocal(const_cast<float*>(C.rhos), nzs, nx, P, m->stream));
+#endif
   // Per-medium copies of the metric for the streamed coefficient blocks: fluid
-  // rows are global rows 0..nz_f-1, solid rows are global rows nz_f-1..nz-1.
-  const size_t nfe = size_t(nzf) * P, nse = size_t(nzs) * P;
-  const std::vector<float>* met[4] = {&h.xix, &h.xiz, &h.zex, &h.zez};
+  // rows are global rows 0..nz_f-1, solid rows are global rows nz_f-1..nz-1
+  // (device to device, from the global-row metric just uploaded).
+  const size_t nfe = size_t(nzf) * P, nse = size_t(nzs) * P, pitch = size_t(P) * sizeof(float);
+  const float* met[4] = {C.xix, C.xiz, C.zex, C.zez};
   for (int q = 0; q < 4; ++q) {
-    if ((rc = up_rows(m->fcoef + q * nfe, *met[q], 0, nzf)) != MFDM_OK) return rc;
-    if ((rc = up_rows(m->scoef + q * nse, *met[q], nzf - 1, nzs)) != MFDM_OK) return rc;
+    MFDM_CU(cudaMemcpy2DAsync(m->fcoef + q * nfe, pitch, met[q], pitch, pitch, size_t(nzf),
+                              cudaMemcpyDeviceToDevice, m->stream));
+    MFDM_CU(cudaMemcpy2DAsync(m->scoef + q * nse, pitch, met[q] + size_t(nzf - 1) * P, pitch, pitch,
+                              size_t(nzs), cudaMemcpyDeviceToDevice, m->stream));
   }
   std::vector<float4> px, pz;
   pml_profile(h, nx, true, true, px);
@@ -426,7 +426,7 @@ int upload_model(mfdm_model* m, const HostModel& h) {
   std::vector<float2> nrm(static_cast<size_t>(nx));
   for (int ix = 0; ix < nx; ++ix) {
     const size_t i = size_t(nzf - 1) * nx + ix;
-    const double a = h.zex[i], b = h.zez[i], s = std::sqrt(a * a + b * b);
+    const double a = v.zex[i], b = v.zez[i], s = std::sqrt(a * a + b * b);
     nrm[size_t(ix)] = s > 0 ? make_float2(float(a / s), float(b / s)) : make_float2(0.f, 1.f);
   }
   MFDM_CU(cudaMemcpyAsync(const_cast<float4*>(C.pmlx), px.data(), px.size() * sizeof(float4),
@@ -629,16 +629,9 @@ int desc_to_host(const mfdm_desc* d, HostModel& h) {
     h.srcx.push_back(d->src_x[i]);
     h.srcz.push_back(d->src_z[i]);
   }
-  const size_t nf = size_t(h.nx) * h.nzf, ns = size_t(h.nx) * h.nzs,
-               ng = size_t(h.nx) * (h.nzf + h.nzs - 1);
-  struct Item { const float* src; std::vector<float>* dst; size_t n; } items[] = {
-      {d->K, &h.K, nf}, {d->rho_f, &h.rhof, nf}, {d->C11, &h.C11, ns}, {d->C13, &h.C13, ns},
-      {d->C33, &h.C33, ns}, {d->C55, &h.C55, ns}, {d->rho_s, &h.rhos, ns}, {d->J, &h.J, ng},
-      {d->xi_x, &h.xix, ng}, {d->xi_z, &h.xiz, ng}, {d->ze_x, &h.zex, ng}, {d->ze_z, &h.zez, ng}};
-  for (const Item& it : items) {
-    if (!it.src) return fail(MFDM_ERR_ARG, "null model array");
-    it.dst->assign(it.src, it.src + it.n);
-  }
+  // the caller's arrays are read in place by the upload (no host copy)
+  h.v = {d->K, d->rho_f, d->C11, d->C13, d->C33, d->C55, d->rho_s,
+         d->J, d->xi_x, d->xi_z, d->ze_x, d->ze_z};
   return MFDM_OK;
 }
 

@@ -604,6 +604,14 @@ __global__ void __launch_bounds__(kFinishThreads) finish_kernel(Coef C, Fields U
   }
 }
 
+__global__ void reciprocal_rows_kernel(float* a, int rows, int nx, int P) {
+  const int ix = blockIdx.x * blockDim.x + threadIdx.x, iz = blockIdx.y;
+  if (ix < nx && iz < rows) {
+    float* p = a + (size_t)iz * P + ix;
+    *p = float(1.0 / double(*p));
+  }
+}
+
 __global__ void set_step_kernel(int* step, unsigned* done, int it) {
   *step = it;
   *done = 0u;
@@ -672,6 +680,12 @@ cudaError_t launch_stage(const Coef& C, const Fields& in, const Fields& out, con
 cudaError_t launch_finish(const Coef& C, const Fields& U, cudaStream_t st) {
   const int nb = (C.nx + kFinishThreads - 1) / kFinishThreads;
   finish_kernel<<<nb, kFinishThreads, 0, st>>>(C, U);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reciprocal(float* a, int rows, int nx, int P, cudaStream_t st) {
+  if (rows <= 0 || nx <= 0) return cudaSuccess;
+  reciprocal_rows_kernel<<<dim3((nx + 255) / 256, rows), 256, 0, st>>>(a, rows, nx, P);
   return cudaGetLastError();
 }
 

@@ -16,6 +16,9 @@ cudaError_t launch_stage(const Coef& C, const Fields& in, const Fields& out, con
                          cudaStream_t st);
 // Interface filter, receiver sampling and step-counter advance.
 cudaError_t launch_finish(const Coef& C, const Fields& U, cudaStream_t st);
+// Replaces each of rows x nx floats (row pitch P) by its reciprocal, computed in
+// FP64 and rounded once.
+cudaError_t launch_reciprocal(float* a, int rows, int nx, int P, cudaStream_t st);
 // Sets the device step counter to `it`.
 cudaError_t launch_set_step(const Coef& C, int it, cudaStream_t st);
 // Dynamic shared memory of one stage block.
