@@ -20,7 +20,7 @@
 // A segment block is a producer/consumer pipeline. Lane 0 of warp 8 streams the
 // segment down in chunks of kR rows with 3-D TMA boxes (cp.async.bulk.tensor)
 // completing on the chunk slot's mbarrier: all stencil fields of the stage
-// input with a 4-column halo into a row-contiguous 16-row ring (kNS chunk
+// input with a 4-column halo into a row-contiguous ring (kNS chunk
 // slots), and the point-wise inputs (coefficients, U^n, accumulator) into the
 // slot's point-wise buffer.
 // Warps 0-7 compute one cell each per chunk purely from shared memory and
@@ -38,16 +38,22 @@ namespace mfdm {
 constexpr int kTX = kStageTX;            // computed columns per strip
 constexpr int kSW = kStageSW;            // staged row width (4-column halo each side)
 constexpr int kR = kStageR;              // rows per chunk
-constexpr int kNS = 4;                   // stencil chunk slots
-constexpr int kNP = 4;                   // point-wise chunk slots
-constexpr int kRing = kR * kNS;          // ring rows (power of two)
+#ifndef MFDM_STENCIL_SLOTS
+#define MFDM_STENCIL_SLOTS 5
+#endif
+#ifndef MFDM_PW_SLOTS
+#define MFDM_PW_SLOTS 3
+#endif
+constexpr int kNS = MFDM_STENCIL_SLOTS;   // stencil chunk slots
+constexpr int kNP = MFDM_PW_SLOTS;        // point-wise chunk slots
+constexpr int kRing = kR * kNS;          // ring rows
 constexpr int kConsumers = 256;          // warps 0-7
 constexpr int kThreads = kConsumers + 32;  // + producer warp
 #ifndef MFDM_SEG_ROWS
 #define MFDM_SEG_ROWS 24
 #endif
 constexpr int kSeg = MFDM_SEG_ROWS;      // rows per segment block
-constexpr int kBarBytes = 128;           // full/empty barriers of both rings
+constexpr int kBarBytes = 256;           // full/empty barriers of both rings
 constexpr int kFinishThreads = 256;      // filter / receiver kernel
 
 static_assert(kTX * kR == kConsumers, "one cell per consumer thread per chunk");
@@ -56,7 +62,7 @@ static_assert(kTX * kR == kConsumers, "one cell per consumer thread per chunk");
 // and the chunk in the first slot below the last one, so the rows dz = -3..3
 // around any ring row are contiguous and no read wraps around.
 constexpr int kRingRows = kRing + 2 * kR;
-static_assert((kRing & (kRing - 1)) == 0, "ring rows must be a power of two");
+static_assert(kNS >= 3 && kNP >= 1, "ring depths");
 static_assert(2 * (kNS + kNP) * 8 <= kBarBytes, "barrier region too small");
 
 // Point-wise inputs staged per chunk, by stage kind: coefficients, then U^n
@@ -139,11 +145,11 @@ struct Bars {
 // carry only the halo rows) goes to ring slot (k + 1) % kNS once the slot's
 // previous chunk is released: one 3-D TMA box with all stencil fields of kR
 // rows and the column halo (chunks of the first and last slot a second time,
-// past the ring's other end). The point-wise inputs of chunk k (k = 0 .. nch-1:
+// past the ring's other end). The point-wise inputs of chunk j (j = 0 .. nch-1:
 // coefficients, U^n, accumulator, up to three boxes) go to point-wise slot
-// k % kNP once chunk k - kNP is computed, and are issued right after stencil
-// chunk k - 1: both then wait for the same chunk, and the point-wise block,
-// the bulk of the bytes, is in flight kNP - 1 chunks ahead of its use.
+// j % kNP once chunk j - kNP is computed, and are issued right after stencil
+// chunk j + D, D = kNS - 1 - kNP: the two waits then become due together, so
+// neither ring holds up the other.
 // Tiled TMA always delivers whole boxes (zero-filled outside the arrays), so
 // every byte count announced on a barrier is a compile-time constant.
 template <int NST, int NCOEF, int KIND>
@@ -156,7 +162,22 @@ __device__ __forceinline__ void produce(const Segment& sg, const CUtensorMap* in
   constexpr unsigned kStBytes = NST * kR * kSW * 4, kPwBytes = NPW * kR * kTX * 4;
   constexpr int kRowF = NST * kSW;  // floats per ring row
   constexpr int kF = kR * kTX;      // floats per point-wise field in a slot
-  static_assert(kNP == kNS, "issue order assumes equal ring depths");
+  constexpr int D = kNS - 1 - kNP;
+  auto issue_pw = [&](int j) -> bool {
+    const int ps = j % kNP;
+    if (j >= kNP && !mbar_wait(&B.pempty[ps], ((j / kNP) - 1) & 1)) return false;
+    const int q0 = sg.z0 + j * kR;
+    float* d = slots + ps * NPW * kF;
+    mbar_arrive_expect_tx(&B.pfull[ps], kPwBytes);
+    tma_load_3d(d, coef_map, sg.x0, q0, 0, &B.pfull[ps]);
+    if (KIND == kStageMid) {
+      tma_load_3d(d + NCOEF * kF, un_map, sg.x0, q0, 0, &B.pfull[ps]);
+      tma_load_3d(d + (NCOEF + NST) * kF, acc_map, sg.x0, q0, 0, &B.pfull[ps]);
+    } else if (KIND == kStageLast) {
+      tma_load_3d(d + NCOEF * kF, acc_map, sg.x0, q0, 0, &B.pfull[ps]);
+    }
+    return true;
+  };
   for (int k = -1; k <= sg.nch; ++k) {
     const int u = k + 1, slot = u % kNS;
     if (u >= kNS && !mbar_wait(&B.empty[slot], ((u / kNS) - 1) & 1)) {
@@ -170,23 +191,16 @@ __device__ __forceinline__ void produce(const Segment& sg, const CUtensorMap* in
     if (dup)
       tma_load_3d(ring + (slot == 0 ? kR + kRing : 0) * kRowF, in_map, sg.x0 - 4, 0, r0,
                   &B.full[slot]);
-    const int j = k + 1;  // point-wise chunk issued after stencil chunk j - 1
-    if (j < sg.nch) {
-      const int ps = j % kNP;
-      if (j >= kNP && !mbar_wait(&B.pempty[ps], ((j / kNP) - 1) & 1)) {
-        atomicOr(status, 2);
-        return;
-      }
-      const int q0 = sg.z0 + j * kR;
-      float* d = slots + ps * NPW * kF;
-      mbar_arrive_expect_tx(&B.pfull[ps], kPwBytes);
-      tma_load_3d(d, coef_map, sg.x0, q0, 0, &B.pfull[ps]);
-      if (KIND == kStageMid) {
-        tma_load_3d(d + NCOEF * kF, un_map, sg.x0, q0, 0, &B.pfull[ps]);
-        tma_load_3d(d + (NCOEF + NST) * kF, acc_map, sg.x0, q0, 0, &B.pfull[ps]);
-      } else if (KIND == kStageLast) {
-        tma_load_3d(d + NCOEF * kF, acc_map, sg.x0, q0, 0, &B.pfull[ps]);
-      }
+    const int j = k - D;  // point-wise chunk due with stencil chunk k
+    if (j >= 0 && j < sg.nch && !issue_pw(j)) {
+      atomicOr(status, 2);
+      return;
+    }
+  }
+  for (int j = (sg.nch + 1 - D > 0 ? sg.nch + 1 - D : 0); j < sg.nch; ++j) {
+    if (!issue_pw(j)) {
+      atomicOr(status, 2);
+      return;
     }
   }
 }
@@ -283,7 +297,7 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
     if ((GEN && !colok) || iz >= sg.z1) return;
     const bool sd = GEN && side;  // a side-strip cell
     FluidRing A;
-    A.init(ring, (iz - sg.z0 + kR) & (kRing - 1), tx + 4);
+    A.init(ring, ((c + 1) % kNS) * kR + ty, tx + 4);
     constexpr int F = kR * kTX;
     const float* pw = slots + (size_t)slot * NPW * F + ty * kTX + tx;  // field p at pw[p * F]
     const FluidCoefs cf{pw[0], pw[F], pw[2 * F], pw[3 * F], pw[4 * F], pw[5 * F]};
@@ -367,7 +381,7 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
     const bool sd = GEN && side;  // a side-strip cell
     const bool bottom = GEN && iz >= zb0;
     SolidRing A;
-    A.init(ring, (iz - sg.z0 + kR) & (kRing - 1), tx + 4);
+    A.init(ring, ((c + 1) % kNS) * kR + ty, tx + 4);
     constexpr int F = kR * kTX;
     const float* pw = slots + (size_t)slot * NPW * F + ty * kTX + tx;
     const SolidCoefs cf{pw[0], pw[F], pw[2 * F], pw[3 * F], pw[4 * F],
