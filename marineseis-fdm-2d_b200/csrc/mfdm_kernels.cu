@@ -56,6 +56,7 @@ constexpr int kSeg = MFDM_SEG_ROWS;      // rows per segment block
 constexpr int kBarBytes = 256;           // full/empty barriers of both rings
 constexpr int kFinishThreads = 256;      // filter / receiver kernel
 
+
 static_assert(kTX * kR == kConsumers, "one cell per consumer thread per chunk");
 // The stencil ring is row-contiguous ([ring row][field][col]) with kR extra rows
 // on each side: the chunk in the last slot is also copied above the first slot
@@ -262,7 +263,7 @@ template <int DIR, int KIND>
 __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, const Fields& out,
                                               const Fields& un, const Fields& acc,
                                               const StageMaps& maps, int s, float cc, float w,
-                                              int it, int blk, int ntx, char* smem) {
+                                              int blk, int ntx, char* smem) {
   constexpr int NST = 3, NCOEF = 6, NPW = PW<NST, NCOEF, KIND>::n;
   const int P = C.P, nx = C.nx;
   Segment sg;
@@ -274,6 +275,7 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
   Bars B;
   float *ring, *slots;
   segment_setup<NST>(smem, B, ring, slots);
+  const int it = __ldg(C.step);
   if (threadIdx.x >= kConsumers) {
     produce<NST, NCOEF, KIND>(sg, &maps.fin, &maps.fcoef, &maps.fun, &maps.facc, ring, slots, B,
                               C.status);
@@ -548,8 +550,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   if (b < nbi) {  // first, so the short interface blocks overlap the segments
     interface_strip<DIR, KIND>(C, in, out, un, acc, cc, w, b);
   } else if (b < nbi + nbf) {
-    const int it = __ldg(C.step);
-    fluid_segment<DIR, KIND>(C, in, out, un, acc, maps, s, cc, w, it, b - nbi, ntx, smem);
+    fluid_segment<DIR, KIND>(C, in, out, un, acc, maps, s, cc, w, b - nbi, ntx, smem);
   } else {
     solid_segment<DIR, KIND>(C, in, out, un, acc, maps, cc, w, b - nbi - nbf, ntx, smem);
   }
@@ -567,13 +568,23 @@ __global__ void __launch_bounds__(kFinishThreads) finish_kernel(Coef C, Fields U
   float r0 = 0.f, r1 = 0.f, r2 = 0.f;
   if (ix >= 3 && ix <= nx - 4) {
     const int klo = max(-3, 3 - ix), khi = min(3, nx - 4 - ix);
+    // taps k = klo..khi in ascending order (the reference's summation order);
+    // fully unrolled and predicated, so all loads are in flight together
     float wsum = 0.0f;
-    for (int k = klo; k <= khi; ++k) wsum += c_w7[k + 3];
+#pragma unroll
+    for (int k = -3; k <= 3; ++k)
+      if (k >= klo && k <= khi) wsum += c_w7[k + 3];
     float v[8];
 #pragma unroll
     for (int f = 0; f < 8; ++f) {
+      float t[7];
+#pragma unroll
+      for (int k = -3; k <= 3; ++k)
+        t[k + 3] = (k >= klo && k <= khi) ? __ldg(C.ipre + (size_t)f * P + ix + k) : 0.f;
       float sum = 0.0f;
-      for (int k = klo; k <= khi; ++k) sum += c_w7[k + 3] * C.ipre[(size_t)f * P + ix + k];
+#pragma unroll
+      for (int k = -3; k <= 3; ++k)
+        if (k >= klo && k <= khi) sum += c_w7[k + 3] * t[k + 3];
       v[f] = sum / wsum;
     }
     const float2 n = __ldg(C.nrm + ix);
@@ -632,6 +643,7 @@ __global__ void set_step_kernel(int* step, unsigned* done, int it) {
 }
 
 // ---- host-side launchers ----------------------------------------------------
+
 
 template <int KIND>
 static size_t smem_for_kind() {
