@@ -66,6 +66,7 @@ typedef struct mfdm_info {
   int nsamples;                   /* receiver samples recorded so far */
   long long cells;                /* nx * (nz_f + nz_s): cells updated per step */
   long long device_bytes;         /* device memory held by the handle */
+  int nshots;                     /* shots stepped together (1 unless opened with mfdm_open_batch) */
 } mfdm_info;
 
 /* Field ids for mfdm_get_field / mfdm_set_field. */
@@ -141,6 +142,33 @@ int mfdm_get_records(mfdm_model* m, int first, int count, float* solid_vx, float
  * (MemManager::U_cp_d2h, src/elements.cu:335-343, for the snapshot writer). */
 int mfdm_get_field(mfdm_model* m, int field, float* host);
 int mfdm_set_field(mfdm_model* m, int field, const float* host);
+
+/* ---- batched shots ------------------------------------------------------
+ * Several shots of one model stepped together: one launch per RK stage covers
+ * every shot (the model's coefficients are shared, each shot has its own
+ * wavefield). The reference runs shots one after another from one JSON
+ * (src/main.cu:94-136) without clearing the wavefield between them and with
+ * one frequency for all; here every shot starts from rest and carries its own
+ * source cell and Ricker frequency, with the CFS-PML alpha0 = 2 pi fpeak and
+ * beta0 that go with it (elements.cu:121-124, 824-873). */
+typedef struct mfdm_shot {
+  int src_x, src_z;  /* source column and fluid row (src_x < 0: no source) */
+  float fpeak;       /* Ricker peak frequency, Hz                           */
+  float beta0;       /* CFS-PML beta0 for this shot (>= 1)                  */
+} mfdm_shot;
+
+/* Opens `nshots` shots on the model of `d` (d->src_* and d->fpeak / d->beta0
+ * are not used). mfdm_step / mfdm_time_steps / mfdm_synchronize / mfdm_close
+ * act on all shots; mfdm_get_records / mfdm_get_field read shot 0;
+ * mfdm_set_shot is rejected (MFDM_ERR_ARG). */
+int mfdm_open_batch(const mfdm_desc* d, int nshots, const mfdm_shot* shots, int device,
+                    mfdm_model** out);
+/* Every shot back to rest, step counter to 0, records cleared. */
+int mfdm_batch_reset(mfdm_model* m);
+/* Receiver rows / state field of one shot (as mfdm_get_records / mfdm_get_field). */
+int mfdm_batch_get_records(mfdm_model* m, int shot, int first, int count, float* svx, float* svz,
+                           float* fp);
+int mfdm_batch_get_field(mfdm_model* m, int shot, int field, float* host);
 
 /* The drop-in command line: `main_debug <model.json> <out_root>`
  * (src/main.cu:58-216). Clears out_root, runs every shot and writes

@@ -33,7 +33,8 @@ FIELDS = {"fluid_vx": 0, "fluid_vz": 1, "fluid_p": 2, "solid_vx": 3, "solid_vz":
 EXPORTS = ("mfdm_last_error", "mfdm_open_json", "mfdm_open_desc", "mfdm_load_desc", "mfdm_close",
            "mfdm_get_info", "mfdm_set_shot", "mfdm_update_rk4", "mfdm_step", "mfdm_time_steps",
            "mfdm_synchronize", "mfdm_get_records", "mfdm_get_field", "mfdm_set_field",
-           "mfdm_run_cli", "mfdm_step_noalloc")
+           "mfdm_run_cli", "mfdm_step_noalloc", "mfdm_open_batch", "mfdm_batch_reset",
+           "mfdm_batch_get_records", "mfdm_batch_get_field")
 
 
 class MfdmError(RuntimeError):
@@ -64,7 +65,14 @@ class Info(ctypes.Structure):
                 ("pitch", ctypes.c_int), ("nt", ctypes.c_int), ("snapshot", ctypes.c_int),
                 ("gap", ctypes.c_int), ("nsrc", ctypes.c_int), ("shot", ctypes.c_int),
                 ("step", ctypes.c_int), ("nsamples", ctypes.c_int),
-                ("cells", ctypes.c_longlong), ("device_bytes", ctypes.c_longlong)]
+                ("cells", ctypes.c_longlong), ("device_bytes", ctypes.c_longlong),
+                ("nshots", ctypes.c_int)]
+
+
+class Shot(ctypes.Structure):
+    """mfdm_shot: one shot of a batch (source cell, Ricker peak frequency, PML beta0)."""
+    _fields_ = [("src_x", ctypes.c_int), ("src_z", ctypes.c_int), ("fpeak", ctypes.c_float),
+                ("beta0", ctypes.c_float)]
 
 
 class DeviceModel(ctypes.Structure):
@@ -110,6 +118,12 @@ def load_library(path: str = LIB_PATH):
         "mfdm_run_cli": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]),
         "mfdm_step_noalloc": (ctypes.c_int, [ctypes.POINTER(DeviceModel), ctypes.c_int,
                                              ctypes.c_int, vp]),
+        "mfdm_open_batch": (ctypes.c_int, [ctypes.POINTER(Desc), ctypes.c_int,
+                                           ctypes.POINTER(Shot), ctypes.c_int, ctypes.POINTER(vp)]),
+        "mfdm_batch_reset": (ctypes.c_int, [vp]),
+        "mfdm_batch_get_records": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                  _fp, _fp, _fp]),
+        "mfdm_batch_get_field": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, _fp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -255,6 +269,50 @@ class Solver:
     def set_field(self, name: str, values: np.ndarray):
         a = _f32(values)
         _check(self._lib.mfdm_set_field(self._h, FIELDS[name], a.ctypes.data_as(_fp)))
+
+
+class Batch(Solver):
+    """Shots of one model stepped together (mfdm_open_batch): one launch per RK
+    stage covers every shot. ``shots`` is a sequence of (src_x, src_z, fpeak,
+    beta0); every shot starts from rest."""
+
+    @classmethod
+    def from_model(cls, model, shots, device: int = 0) -> "Batch":
+        d, keep = make_desc(model)
+        arr = (Shot * len(shots))(*[Shot(int(x), int(z), float(f), float(b))
+                                    for x, z, f, b in shots])
+        h = ctypes.c_void_p()
+        _check(load_library().mfdm_open_batch(ctypes.byref(d), len(shots), arr, device,
+                                              ctypes.byref(h)))
+        del keep
+        return cls(h)
+
+    def reset(self):
+        _check(self._lib.mfdm_batch_reset(self._h))
+
+    def set_shot(self, isrc: int = 0, reset: bool = True):
+        raise MfdmError(-1, "a batch runs its own shots: use reset()")
+
+    def records(self, first: int = 0, count: Optional[int] = None,
+                shot: int = 0) -> Dict[str, np.ndarray]:
+        info = self.info()
+        if count is None:
+            count = info["nsamples"] - first
+        nx = info["nx"]
+        out = {k: np.zeros((count, nx), dtype=np.float32) for k in ("svx", "svz", "fp")}
+        _check(self._lib.mfdm_batch_get_records(self._h, int(shot), int(first), int(count),
+                                                out["svx"].ctypes.data_as(_fp),
+                                                out["svz"].ctypes.data_as(_fp),
+                                                out["fp"].ctypes.data_as(_fp)))
+        return out
+
+    def field(self, name: str, shot: int = 0) -> np.ndarray:
+        info = self.info()
+        fid = FIELDS[name]
+        rows = info["nz_f"] if fid < 3 else info["nz_s"]
+        out = np.zeros((rows, info["nx"]), dtype=np.float32)
+        _check(self._lib.mfdm_batch_get_field(self._h, int(shot), fid, out.ctypes.data_as(_fp)))
+        return out
 
 
 def step_noalloc(dm: DeviceModel, it: int, nsteps: int, stream: Optional[int] = None):

@@ -29,6 +29,7 @@ constexpr int kStageR = 4;               // rows per chunk
 // coefficients (fluid: xi_x, xi_z, ze_x, ze_z, rho, K; solid: xi_x, xi_z,
 // ze_x, ze_z, rho, C11, C13, C33, C55); one box = all fields of kStageR rows.
 // Stage-input boxes land as [row][field][col], the others as [field][row][col].
+// The state maps have a fourth dimension, the shot; the coefficient maps none.
 struct StageMaps {
   CUtensorMap fin, sin;    // stage input, box {kStageSW, nfield, kStageR}
   CUtensorMap fun, sun;    // U^n, box {kStageTX, kStageR, nfield}
@@ -81,6 +82,13 @@ struct Coef {
   unsigned* done;                   // block arrival counter of the finish kernel
   float* ipre;                      // interface rows before the filter [8][P]
   int* status;                      // sticky error word (non-finite detector)
+  // Shots stepped together (blockIdx.y of the step kernels). Every per-shot
+  // buffer of shot b sits b strides after shot 0's: the RK sets, ADE strips,
+  // PML tables and interface rows (shot_stride), the Ricker table (src_stride)
+  // and the receiver rows (rec_stride), all in floats.
+  int nshots;
+  size_t shot_stride, src_stride, rec_stride;
+  const int2* __restrict__ src_pos;  // per-shot source (x, z); nullptr: srcx, srcz
 };
 
 // One RK4 state set (state, stage ping/pong or accumulator).
@@ -91,6 +99,41 @@ struct Fields {
   float* sx[4];  // solid xi ADE
   float* sz[4];  // solid zeta ADE
 };
+
+// The set of one shot: every pointer `so` floats further.
+__device__ __forceinline__ Fields shot_fields(const Fields& f, size_t so) {
+  Fields g;
+  g.fvx = f.fvx + so; g.fvz = f.fvz + so; g.fp = f.fp + so;
+  g.svx = f.svx + so; g.svz = f.svz + so; g.ssx = f.ssx + so; g.ssz = f.ssz + so;
+  g.ssxz = f.ssxz + so;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    g.fx[q] = f.fx[q] + so;
+    g.sx[q] = f.sx[q] + so;
+    g.sz[q] = f.sz[q] + so;
+  }
+  return g;
+}
+
+// The coefficients as seen by one shot: its PML tables, interface rows,
+// Ricker table, receiver rows and source position.
+__device__ __forceinline__ Coef shot_coef(const Coef& C, int shot) {
+  Coef c = C;
+  if (shot > 0) {
+    const size_t so = size_t(shot) * C.shot_stride;
+    c.pmlx = reinterpret_cast<const float4*>(reinterpret_cast<const float*>(C.pmlx) + so);
+    c.pmlz = reinterpret_cast<const float4*>(reinterpret_cast<const float*>(C.pmlz) + so);
+    c.ipre = C.ipre + so;
+    c.src_amp = C.src_amp + size_t(shot) * C.src_stride;
+    if (C.rec) c.rec = C.rec + size_t(shot) * C.rec_stride;
+  }
+  if (C.src_pos) {
+    const int2 p = __ldg(C.src_pos + shot);
+    c.srcx = p.x;
+    c.srcz = p.y;
+  }
+  return c;
+}
 
 __constant__ float c_srcw[25];  // 5x5 source spreading weights (src/elements.cu:34-40)
 __constant__ float c_w7[7];     // interface filter weights (src/elements.cu:30-33)

@@ -89,10 +89,22 @@ float ricker_ref(float fpeak, float time) {
   return (1 - 2 * temp) * expf(-temp);
 }
 
+// One shot of a handle: source cell and Ricker peak frequency, and the PML
+// beta0 that goes with it (alpha0 = 2 pi fpeak follows the frequency).
+struct ShotCfg {
+  int x = -1, z = 0;
+  float fpeak = 0.f, beta0 = 1.f;
+};
+
 }  // namespace
 
 struct mfdm_model {
   int device = 0;
+  int nshots = 1;              // shots stepped together (1 for a plain handle)
+  std::vector<ShotCfg> shots;  // per-shot source, frequency and PML beta0
+  bool batch = false;          // opened with mfdm_open_batch
+  size_t region = 0;           // bytes of one shot's state region
+  int* d_srcpos = nullptr;     // per-shot source cells (batch handles)
   cudaStream_t stream = nullptr;
   HostModel cfg;  // scalars (arrays released after upload)
   int P = 0, Ps = 0, nz = 0, gap = 1;
@@ -148,8 +160,9 @@ int validate(const HostModel& h) {
 // k counted from the inner edge of the band of npd cells inside 3 frozen cells.
 // Stored per cell as (d/beta, alpha + d/beta, 1/beta), the factors the
 // reference derives inside every kernel.
-void pml_profile(const HostModel& h, int n, bool lo, bool hi, std::vector<float4>& out) {
-  const double alpha0 = 2.0 * M_PI * double(h.fpeak);
+void pml_profile(const HostModel& h, int n, bool lo, bool hi, float fpeak, float beta0,
+                 std::vector<float4>& out) {
+  const double alpha0 = 2.0 * M_PI * double(fpeak);
   const double d0 = -(h.npow + 1) * double(h.vp_max) * std::log(double(h.rc)) /
                     (2.0 * double(h.thickness));
   out.assign(size_t(n), make_float4(0.f, 1.f, 1.f, 0.f));
@@ -161,7 +174,7 @@ void pml_profile(const HostModel& h, int n, bool lo, bool hi, std::vector<float4
     if (k > 0) {
       const double r = double(k) / double(h.npd);
       d = d0 * std::pow(r, double(h.npow));
-      be = 1.0 + (double(h.beta0) - 1.0) * r * r;
+      be = 1.0 + (double(beta0) - 1.0) * r * r;
       al = alpha0 * (1.0 - r);
     }
     const double dpb = d / be;
@@ -230,16 +243,15 @@ int load_json(const char* path, HostModel& h) {
   return MFDM_OK;
 }
 
-void fill_src_table(const HostModel& h, int steps, std::vector<float>& amp) {
-  amp.assign(size_t(steps) * 4, 0.f);
+void fill_src_table(const HostModel& h, float fpeak, int steps, float* amp) {
   const float dt = h.dt;
   const float half = float(double(dt) * 0.5);
   for (int it = 0; it < steps; ++it) {
     const float t = float(it) * dt;  // `const float time = it * mem.dt` (src/pml_fs_kernels.cu:770)
-    amp[size_t(it) * 4 + 0] = ricker_ref(h.fpeak, t);
-    amp[size_t(it) * 4 + 1] = ricker_ref(h.fpeak, t + half);
-    amp[size_t(it) * 4 + 2] = ricker_ref(h.fpeak, t + half);
-    amp[size_t(it) * 4 + 3] = ricker_ref(h.fpeak, t + dt);
+    amp[size_t(it) * 4 + 0] = ricker_ref(fpeak, t);
+    amp[size_t(it) * 4 + 1] = ricker_ref(fpeak, t + half);
+    amp[size_t(it) * 4 + 2] = ricker_ref(fpeak, t + half);
+    amp[size_t(it) * 4 + 3] = ricker_ref(fpeak, t + dt);
   }
 }
 
@@ -254,8 +266,9 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
 // column, row, field); stencil maps (rows_outer) land as [row][field][col]
 // (dimensions column, field, row), so consecutive chunks stack into one
 // row-contiguous ring.
+// With nshots > 0 the map has a fourth dimension, the shot, of stride shot_bytes.
 int encode_block(CUtensorMap* map, const float* base, int P, int rows, int nf, int box_x,
-                 bool rows_outer) {
+                 bool rows_outer, int nshots = 0, size_t shot_bytes = 0) {
   static EncodeTiledFn fn = nullptr;
   if (!fn) {
     void* p = nullptr;
@@ -266,14 +279,15 @@ int encode_block(CUtensorMap* map, const float* base, int P, int rows, int nf, i
     fn = reinterpret_cast<EncodeTiledFn>(p);
   }
   const cuuint64_t row_stride = cuuint64_t(P) * 4, field_stride = cuuint64_t(rows) * P * 4;
-  const cuuint64_t dims[3] = {cuuint64_t(P), cuuint64_t(rows_outer ? nf : rows),
-                              cuuint64_t(rows_outer ? rows : nf)};
-  const cuuint64_t strides[2] = {rows_outer ? field_stride : row_stride,
-                                 rows_outer ? row_stride : field_stride};
-  const cuuint32_t box[3] = {cuuint32_t(box_x), cuuint32_t(rows_outer ? nf : mfdm::kStageR),
-                             cuuint32_t(rows_outer ? mfdm::kStageR : nf)};
-  const cuuint32_t es[3] = {1, 1, 1};
-  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims,
+  const cuuint64_t dims[4] = {cuuint64_t(P), cuuint64_t(rows_outer ? nf : rows),
+                              cuuint64_t(rows_outer ? rows : nf), cuuint64_t(nshots > 0 ? nshots : 1)};
+  const cuuint64_t strides[3] = {rows_outer ? field_stride : row_stride,
+                                 rows_outer ? row_stride : field_stride, cuuint64_t(shot_bytes)};
+  const cuuint32_t box[4] = {cuuint32_t(box_x), cuuint32_t(rows_outer ? nf : mfdm::kStageR),
+                             cuuint32_t(rows_outer ? mfdm::kStageR : nf), 1};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, nshots > 0 ? 4 : 3,
+                        const_cast<float*>(base), dims,
                         strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(MFDM_ERR_CUDA, "tensor map encoding failed (" + std::to_string(int(r)) + ")");
@@ -291,31 +305,35 @@ void release_graph(mfdm_model* m) {
 int ensure_capacity(mfdm_model* m, int steps) {
   if (steps > m->src_steps) {
     const int cap = std::max(steps, m->src_steps * 2);
-    std::vector<float> amp;
-    fill_src_table(m->cfg, cap, amp);
+    std::vector<float> amp(size_t(m->nshots) * cap * 4, 0.f);  // [shot][step][stage]
+    for (int b = 0; b < m->nshots; ++b)
+      fill_src_table(m->cfg, m->shots[size_t(b)].fpeak, cap, amp.data() + size_t(b) * cap * 4);
     float* d = nullptr;
     MFDM_CU(cudaMalloc(&d, amp.size() * sizeof(float)));
     MFDM_CU(cudaMemcpy(d, amp.data(), amp.size() * sizeof(float), cudaMemcpyHostToDevice));
     if (m->d_src) cudaFree(m->d_src);
     m->d_src = d;
     m->src_steps = cap;
+    m->C.src_stride = size_t(cap) * 4;
     release_graph(m);
   }
   const int need = (steps + m->gap - 1) / m->gap;
   if (need > m->rec_cap) {
     const int cap = std::max(need, m->rec_cap * 2);
-    const size_t row = size_t(3) * m->cfg.nx * sizeof(float);
+    const size_t row = size_t(3) * m->cfg.nx * sizeof(float);  // [shot][sample][3][nx]
     float* d = nullptr;
-    MFDM_CU(cudaMalloc(&d, size_t(cap) * row));
-    MFDM_CU(cudaMemsetAsync(d, 0, size_t(cap) * row, m->stream));
+    MFDM_CU(cudaMalloc(&d, size_t(m->nshots) * cap * row));
+    MFDM_CU(cudaMemsetAsync(d, 0, size_t(m->nshots) * cap * row, m->stream));
     if (m->d_rec) {
-      MFDM_CU(cudaMemcpyAsync(d, m->d_rec, size_t(m->rec_cap) * row, cudaMemcpyDeviceToDevice,
-                              m->stream));
+      MFDM_CU(cudaMemcpy2DAsync(d, size_t(cap) * row, m->d_rec, size_t(m->rec_cap) * row,
+                                size_t(m->rec_cap) * row, size_t(m->nshots),
+                                cudaMemcpyDeviceToDevice, m->stream));
       MFDM_CU(cudaStreamSynchronize(m->stream));
       cudaFree(m->d_rec);
     }
     m->d_rec = d;
     m->rec_cap = cap;
+    m->C.rec_stride = size_t(cap) * 3 * m->cfg.nx;
     release_graph(m);
   }
   m->C.src_amp = m->d_src;
@@ -419,9 +437,11 @@ int upload_model(mfdm_model* m, const HostModel& h) {
     MFDM_CU(cudaMemcpy2DAsync(m->scoef + q * nse, pitch, met[q] + size_t(nzf - 1) * P, pitch, pitch,
                               size_t(nzs), cudaMemcpyDeviceToDevice, m->stream));
   }
-  std::vector<float4> px, pz;
-  pml_profile(h, nx, true, true, px);
-  pml_profile(h, nzs, false, true, pz);
+  if (!m->batch) {  // a plain handle's single shot follows the model's frequency
+    m->shots.resize(1);
+    m->shots[0].fpeak = h.fpeak;
+    m->shots[0].beta0 = h.beta0;
+  }
   // Interface unit normal n = grad(zeta)/|grad(zeta)| in FP64 (src/elements.cu:892-905).
   std::vector<float2> nrm(static_cast<size_t>(nx));
   for (int ix = 0; ix < nx; ++ix) {
@@ -429,12 +449,20 @@ int upload_model(mfdm_model* m, const HostModel& h) {
     const double a = v.zex[i], b = v.zez[i], s = std::sqrt(a * a + b * b);
     nrm[size_t(ix)] = s > 0 ? make_float2(float(a / s), float(b / s)) : make_float2(0.f, 1.f);
   }
-  MFDM_CU(cudaMemcpyAsync(const_cast<float4*>(C.pmlx), px.data(), px.size() * sizeof(float4),
-                          cudaMemcpyHostToDevice, m->stream));
-  MFDM_CU(cudaMemcpyAsync(const_cast<float4*>(C.pmlz), pz.data(), pz.size() * sizeof(float4),
-                          cudaMemcpyHostToDevice, m->stream));
   MFDM_CU(cudaMemcpyAsync(const_cast<float2*>(C.nrm), nrm.data(), nrm.size() * sizeof(float2),
                           cudaMemcpyHostToDevice, m->stream));
+  // CFS-PML factors per shot (alpha0 and beta0 follow the shot's frequency)
+  for (int b = 0; b < m->nshots; ++b) {
+    std::vector<float4> px, pz;
+    const ShotCfg& sh = m->shots[size_t(b)];
+    pml_profile(h, nx, true, true, sh.fpeak, sh.beta0, px);
+    pml_profile(h, nzs, false, true, sh.fpeak, sh.beta0, pz);
+    const size_t so = size_t(b) * C.shot_stride;
+    MFDM_CU(cudaMemcpyAsync(const_cast<float*>(reinterpret_cast<const float*>(C.pmlx)) + so, px.data(),
+                            px.size() * sizeof(float4), cudaMemcpyHostToDevice, m->stream));
+    MFDM_CU(cudaMemcpyAsync(const_cast<float*>(reinterpret_cast<const float*>(C.pmlz)) + so, pz.data(),
+                            pz.size() * sizeof(float4), cudaMemcpyHostToDevice, m->stream));
+  }
   MFDM_CU(cudaStreamSynchronize(m->stream));
 
   const float dt = h.dt;
@@ -462,9 +490,25 @@ int upload_model(mfdm_model* m, const HostModel& h) {
 }
 
 // Carves every fixed-size device buffer out of one allocation and uploads the model.
-int build(mfdm_model* m, HostModel&& h, int device) {
+// `shots` (batch handles): the shots stepped together; nullptr for a plain handle.
+int build(mfdm_model* m, HostModel&& h, int device, const std::vector<ShotCfg>* shots = nullptr) {
   int rc = validate(h);
   if (rc != MFDM_OK) return rc;
+  if (shots) {
+    if (shots->empty()) return fail(MFDM_ERR_ARG, "a batch needs at least one shot");
+    for (const ShotCfg& sh : *shots) {
+      if (!(sh.fpeak > 0.f) || !(sh.beta0 >= 1.f))
+        return fail(MFDM_ERR_ARG, "each shot needs fpeak > 0 and beta0 >= 1");
+      if (sh.x >= 0 && (sh.x >= h.nx || sh.z < 0 || sh.z >= h.nzf))
+        return fail(MFDM_ERR_ARG, "shot source outside the fluid grid");
+    }
+    m->batch = true;
+    m->shots = *shots;
+  } else {
+    m->batch = false;
+    m->shots.assign(1, ShotCfg{});
+  }
+  m->nshots = int(m->shots.size());
   m->device = device;
   int ndev = 0;
   MFDM_CU(cudaGetDeviceCount(&ndev));
@@ -491,33 +535,47 @@ int build(mfdm_model* m, HostModel&& h, int device) {
   const size_t o_fco = take(6 * nf), o_sco = take(9 * ns);
   const size_t o_J = take(ng), o_xix = take(ng), o_xiz = take(ng), o_zex = take(ng),
                o_zez = take(ng);
-  const size_t o_pmlx = take(size_t(nx) * 4), o_pmlz = take(size_t(nzs) * 4),
-               o_nrm = take(size_t(nx) * 2), o_ipre = take(size_t(8) * P), o_misc = take(64);
-  // Each RK set: one fluid block [3][nz_f][P] and one solid block [5][nz_s][P]
-  // (the TMA boxes span the fields), then the ADE strips.
+  const size_t o_nrm = take(size_t(nx) * 2), o_misc = take(64),
+               o_srcpos = take(size_t(2) * m->nshots);
+  const size_t shared = off;
+  // One region per shot (equal sizes, so shot b's buffers are b regions after
+  // shot 0's): each RK set's fluid block [3][nz_f][P] and solid block
+  // [5][nz_s][P] (the TMA boxes span the fields), the ADE strips, the PML
+  // factors and the interface rows.
+  size_t roff = 0;
+  auto rtake = [&](size_t nfloats) {
+    const size_t o = roff;
+    roff += (nfloats * sizeof(float) + 255) / 256 * 256;
+    return o;
+  };
   size_t o_fb[4], o_sb[4], o_ade[4][12];
   for (int s = 0; s < 4; ++s) {
-    o_fb[s] = take(3 * nf);
-    o_sb[s] = take(5 * ns);
-    for (int q = 0; q < 4; ++q) o_ade[s][q] = take(size_t(nzf) * Ps);
-    for (int q = 0; q < 4; ++q) o_ade[s][4 + q] = take(size_t(nzs) * Ps);
-    for (int q = 0; q < 4; ++q) o_ade[s][8 + q] = take(size_t(npdr) * P);
+    o_fb[s] = rtake(3 * nf);
+    o_sb[s] = rtake(5 * ns);
+    for (int q = 0; q < 4; ++q) o_ade[s][q] = rtake(size_t(nzf) * Ps);
+    for (int q = 0; q < 4; ++q) o_ade[s][4 + q] = rtake(size_t(nzs) * Ps);
+    for (int q = 0; q < 4; ++q) o_ade[s][8 + q] = rtake(size_t(npdr) * P);
   }
+  const size_t o_pmlx = rtake(size_t(nx) * 4), o_pmlz = rtake(size_t(nzs) * 4),
+               o_ipre = rtake(size_t(8) * P);
+  m->region = roff;
+  off = shared + roff * size_t(m->nshots);
   m->dbytes = off;
   MFDM_CU(cudaMalloc(&m->dmem, off));
   MFDM_CU(cudaMemsetAsync(m->dmem, 0, off, m->stream));
   char* base = m->dmem;
   auto F = [&](size_t o) { return reinterpret_cast<float*>(base + o); };
+  auto R = [&](size_t o) { return reinterpret_cast<float*>(base + shared + o); };  // shot 0
   for (int s = 0; s < 4; ++s) {
     Fields& S = m->S[s];
-    float* fb = F(o_fb[s]);
-    float* sb = F(o_sb[s]);
+    float* fb = R(o_fb[s]);
+    float* sb = R(o_sb[s]);
     S.fvx = fb; S.fvz = fb + nf; S.fp = fb + 2 * nf;
     S.svx = sb; S.svz = sb + ns; S.ssx = sb + 2 * ns; S.ssz = sb + 3 * ns; S.ssxz = sb + 4 * ns;
     for (int q = 0; q < 4; ++q) {
-      S.fx[q] = F(o_ade[s][q]);
-      S.sx[q] = F(o_ade[s][4 + q]);
-      S.sz[q] = F(o_ade[s][8 + q]);
+      S.fx[q] = R(o_ade[s][q]);
+      S.sx[q] = R(o_ade[s][4 + q]);
+      S.sz[q] = R(o_ade[s][8 + q]);
     }
   }
   m->fcoef = F(o_fco);
@@ -528,19 +586,35 @@ int build(mfdm_model* m, HostModel&& h, int device) {
   C.rhos = m->scoef + 4 * ns; C.C11 = m->scoef + 5 * ns; C.C13 = m->scoef + 6 * ns;
   C.C33 = m->scoef + 7 * ns; C.C55 = m->scoef + 8 * ns;
   C.J = F(o_J); C.xix = F(o_xix); C.xiz = F(o_xiz); C.zex = F(o_zex); C.zez = F(o_zez);
-  C.pmlx = reinterpret_cast<const float4*>(F(o_pmlx));
-  C.pmlz = reinterpret_cast<const float4*>(F(o_pmlz));
+  C.pmlx = reinterpret_cast<const float4*>(R(o_pmlx));
+  C.pmlz = reinterpret_cast<const float4*>(R(o_pmlz));
   C.nrm = reinterpret_cast<const float2*>(F(o_nrm));
-  C.ipre = F(o_ipre);
+  C.ipre = R(o_ipre);
   int* misc = reinterpret_cast<int*>(F(o_misc));
   C.step = misc;
   C.done = reinterpret_cast<unsigned*>(misc + 1);
   C.status = misc + 2;
+  C.nshots = m->nshots;
+  C.shot_stride = roff / sizeof(float);
+  C.src_stride = 0;
+  C.rec_stride = 0;
+  C.src_pos = nullptr;
+  if (m->batch) {
+    m->d_srcpos = reinterpret_cast<int*>(F(o_srcpos));
+    std::vector<int> pos(size_t(2) * m->nshots);
+    for (int b = 0; b < m->nshots; ++b) {
+      pos[size_t(2 * b)] = m->shots[size_t(b)].x;
+      pos[size_t(2 * b + 1)] = m->shots[size_t(b)].z;
+    }
+    MFDM_CU(cudaMemcpyAsync(m->d_srcpos, pos.data(), pos.size() * sizeof(int),
+                            cudaMemcpyHostToDevice, m->stream));
+    C.src_pos = reinterpret_cast<const int2*>(m->d_srcpos);
+  }
   for (int s = 0; s < 4; ++s) {
-    if ((rc = encode_block(&m->fst[s], F(o_fb[s]), P, nzf, 3, mfdm::kStageSW, true)) ||
-        (rc = encode_block(&m->sst[s], F(o_sb[s]), P, nzs, 5, mfdm::kStageSW, true)) ||
-        (rc = encode_block(&m->fpw[s], F(o_fb[s]), P, nzf, 3, mfdm::kStageTX, false)) ||
-        (rc = encode_block(&m->spw[s], F(o_sb[s]), P, nzs, 5, mfdm::kStageTX, false)))
+    if ((rc = encode_block(&m->fst[s], R(o_fb[s]), P, nzf, 3, mfdm::kStageSW, true, m->nshots, roff)) ||
+        (rc = encode_block(&m->sst[s], R(o_sb[s]), P, nzs, 5, mfdm::kStageSW, true, m->nshots, roff)) ||
+        (rc = encode_block(&m->fpw[s], R(o_fb[s]), P, nzf, 3, mfdm::kStageTX, false, m->nshots, roff)) ||
+        (rc = encode_block(&m->spw[s], R(o_sb[s]), P, nzs, 5, mfdm::kStageTX, false, m->nshots, roff)))
       return rc;
   }
   if ((rc = encode_block(&m->fco, m->fcoef, P, nzf, 6, mfdm::kStageTX, false)) ||
@@ -564,13 +638,14 @@ void destroy(mfdm_model* m) {
   delete m;
 }
 
-int open_common(HostModel&& h, int device, mfdm_model** out) {
+int open_common(HostModel&& h, int device, mfdm_model** out,
+                const std::vector<ShotCfg>* shots = nullptr) {
   if (!out) return fail(MFDM_ERR_ARG, "null output handle");
   *out = nullptr;
   int prev = -1;
   cudaGetDevice(&prev);
   mfdm_model* m = new mfdm_model();
-  const int rc = build(m, std::move(h), device);
+  const int rc = build(m, std::move(h), device, shots);
   if (prev >= 0) cudaSetDevice(prev);
   if (rc != MFDM_OK) {
     const std::string msg = g_err;
@@ -582,11 +657,82 @@ int open_common(HostModel&& h, int device, mfdm_model** out) {
   return MFDM_OK;
 }
 
-int field_ptr(mfdm_model* m, int field, float** p, int* rows) {
+int field_ptr(mfdm_model* m, int field, float** p, int* rows, int shot = 0);
+
+// Zeroes every shot's RK sets (state, stage buffers, accumulator), ADE strips
+// and interface rows; the coefficients and the PML tables stay.
+int clear_state(mfdm_model* m) {
+  const size_t pitch = m->region, h = size_t(m->nshots);
+  const size_t nf = size_t(m->cfg.nzf) * m->P, ns = size_t(m->cfg.nzs) * m->P;
+  for (int s = 0; s < 4; ++s) {
+    const Fields& S = m->S[s];
+    MFDM_CU(cudaMemset2DAsync(S.fvx, pitch, 0, 3 * nf * sizeof(float), h, m->stream));
+    MFDM_CU(cudaMemset2DAsync(S.svx, pitch, 0, 5 * ns * sizeof(float), h, m->stream));
+    for (int q = 0; q < 4; ++q) {
+      MFDM_CU(cudaMemset2DAsync(S.fx[q], pitch, 0, size_t(m->cfg.nzf) * m->Ps * sizeof(float), h,
+                                m->stream));
+      MFDM_CU(cudaMemset2DAsync(S.sx[q], pitch, 0, size_t(m->cfg.nzs) * m->Ps * sizeof(float), h,
+                                m->stream));
+      MFDM_CU(cudaMemset2DAsync(S.sz[q], pitch, 0,
+                                size_t(std::max(m->cfg.npd, 1)) * m->P * sizeof(float), h, m->stream));
+    }
+  }
+  MFDM_CU(cudaMemset2DAsync(m->C.ipre, pitch, 0, size_t(8) * m->P * sizeof(float), h, m->stream));
+  return MFDM_OK;
+}
+
+// Clears the receiver rows and the error word and rewinds the step counter.
+int rewind(mfdm_model* m) {
+  MFDM_CU(cudaMemsetAsync(m->d_rec, 0,
+                          size_t(m->nshots) * m->rec_cap * 3 * m->cfg.nx * sizeof(float), m->stream));
+  MFDM_CU(cudaMemsetAsync(m->C.status, 0, sizeof(int), m->stream));
+  m->host_step = 0;
+  MFDM_CU(mfdm::launch_set_step(m->C, 0, m->stream));
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  return MFDM_OK;
+}
+
+int get_records(mfdm_model* m, int shot, int first, int count, float* svx, float* svz, float* fp) {
+  if (shot < 0 || shot >= m->nshots) return fail(MFDM_ERR_ARG, "shot index out of range");
+  const int avail = (m->host_step + m->gap - 1) / m->gap;
+  if (first < 0 || count < 0 || first + count > avail || first + count > m->rec_cap)
+    return fail(MFDM_ERR_ARG, "record range out of bounds");
+  if (count == 0) return MFDM_OK;
+  DeviceGuard g(m->device);
+  const int nx = m->cfg.nx;
+  const float* rec = m->d_rec + size_t(shot) * m->C.rec_stride;
+  float* outs[3] = {svx, svz, fp};
+  for (int q = 0; q < 3; ++q) {
+    if (!outs[q]) continue;
+    MFDM_CU(cudaMemcpy2DAsync(outs[q], size_t(nx) * sizeof(float),
+                              rec + (size_t(first) * 3 + q) * nx, size_t(3) * nx * sizeof(float),
+                              size_t(nx) * sizeof(float), size_t(count), cudaMemcpyDeviceToHost,
+                              m->stream));
+  }
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  return MFDM_OK;
+}
+
+int get_field(mfdm_model* m, int shot, int field, float* host) {
+  if (!host) return fail(MFDM_ERR_ARG, "null argument");
+  float* p = nullptr;
+  int rows = 0;
+  int rc = field_ptr(m, field, &p, &rows, shot);
+  if (rc != MFDM_OK) return rc;
+  DeviceGuard g(m->device);
+  MFDM_CU(cudaMemcpy2DAsync(host, size_t(m->cfg.nx) * sizeof(float), p, size_t(m->P) * sizeof(float),
+                            size_t(m->cfg.nx) * sizeof(float), size_t(rows), cudaMemcpyDeviceToHost,
+                            m->stream));
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  return MFDM_OK;
+}
+
+int field_ptr(mfdm_model* m, int field, float** p, int* rows, int shot) {
   const Fields& U = m->S[0];
   float* const ptrs[8] = {U.fvx, U.fvz, U.fp, U.svx, U.svz, U.ssx, U.ssz, U.ssxz};
   if (field < 0 || field > 7) return fail(MFDM_ERR_ARG, "bad field id");
-  *p = ptrs[field];
+  if (shot < 0 || shot >= m->nshots) return fail(MFDM_ERR_ARG, "shot index out of range");
+  *p = ptrs[field] + size_t(shot) * m->C.shot_stride;
   *rows = field < 3 ? m->cfg.nzf : m->cfg.nzs;
   return MFDM_OK;
 }
@@ -597,8 +743,8 @@ namespace mfdm {
 // Shared with other translation units of the library.
 int set_error(int code, const char* msg) { return fail(code, msg); }
 int encode_block_map(CUtensorMap* map, const float* base, int P, int rows, int nf, int box_x,
-                     bool rows_outer) {
-  return encode_block(map, base, P, rows, nf, box_x, rows_outer);
+                     bool rows_outer, int nshots, size_t shot_bytes) {
+  return encode_block(map, base, P, rows, nf, box_x, rows_outer, nshots, shot_bytes);
 }
 }  // namespace mfdm
 
@@ -687,13 +833,15 @@ int mfdm_get_info(const mfdm_model* m, mfdm_info* info) {
   info->nsrc = int(m->cfg.srcx.size()); info->shot = m->isrc; info->step = m->host_step;
   info->nsamples = (m->host_step + m->gap - 1) / m->gap;
   info->cells = (long long)m->cfg.nx * (m->cfg.nzf + m->cfg.nzs);
-  info->device_bytes = (long long)m->dbytes + (long long)m->src_steps * 16 +
-                       (long long)m->rec_cap * 12 * m->cfg.nx;
+  info->device_bytes = (long long)m->dbytes + (long long)m->nshots * m->src_steps * 16 +
+                       (long long)m->nshots * m->rec_cap * 12 * m->cfg.nx;
+  info->nshots = m->nshots;
   return MFDM_OK;
 }
 
 int mfdm_set_shot(mfdm_model* m, int isrc, int reset_state) {
   if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  if (m->batch) return fail(MFDM_ERR_ARG, "a batch handle runs its own shots: use mfdm_batch_reset");
   if (isrc < 0 || (isrc >= int(m->cfg.srcx.size()) && !m->cfg.srcx.empty()))
     return fail(MFDM_ERR_ARG, "shot index out of range");
   DeviceGuard g(m->device);
@@ -701,29 +849,10 @@ int mfdm_set_shot(mfdm_model* m, int isrc, int reset_state) {
   m->C.srcx = m->cfg.srcx.empty() ? -1 : m->cfg.srcx[size_t(isrc)];
   m->C.srcz = m->cfg.srcx.empty() ? 0 : m->cfg.srcz[size_t(isrc)];
   release_graph(m);  // the source position is baked into the kernel arguments
-  if (reset_state) {
-    // every state set, the stage buffers and the accumulator (the coefficient block is untouched)
-    for (int s = 0; s < 4; ++s) {
-      const Fields& S = m->S[s];
-      const size_t nf = size_t(m->cfg.nzf) * m->P, ns = size_t(m->cfg.nzs) * m->P;
-      float* fl[3] = {S.fvx, S.fvz, S.fp};
-      float* so[5] = {S.svx, S.svz, S.ssx, S.ssz, S.ssxz};
-      for (float* p : fl) MFDM_CU(cudaMemsetAsync(p, 0, nf * sizeof(float), m->stream));
-      for (float* p : so) MFDM_CU(cudaMemsetAsync(p, 0, ns * sizeof(float), m->stream));
-      for (int q = 0; q < 4; ++q) {
-        MFDM_CU(cudaMemsetAsync(S.fx[q], 0, size_t(m->cfg.nzf) * m->Ps * sizeof(float), m->stream));
-        MFDM_CU(cudaMemsetAsync(S.sx[q], 0, size_t(m->cfg.nzs) * m->Ps * sizeof(float), m->stream));
-        MFDM_CU(cudaMemsetAsync(S.sz[q], 0, size_t(std::max(m->cfg.npd, 1)) * m->P * sizeof(float), m->stream));
-      }
-    }
-    MFDM_CU(cudaMemsetAsync(m->C.ipre, 0, size_t(8) * m->P * sizeof(float), m->stream));
-  }
-  MFDM_CU(cudaMemsetAsync(m->d_rec, 0, size_t(m->rec_cap) * 3 * m->cfg.nx * sizeof(float), m->stream));
-  MFDM_CU(cudaMemsetAsync(m->C.status, 0, sizeof(int), m->stream));
-  m->host_step = 0;
-  MFDM_CU(mfdm::launch_set_step(m->C, 0, m->stream));
-  MFDM_CU(cudaStreamSynchronize(m->stream));
-  return MFDM_OK;
+  int rc;
+  // every state set, the stage buffers and the accumulator (the coefficient block is untouched)
+  if (reset_state && (rc = clear_state(m)) != MFDM_OK) return rc;
+  return rewind(m);
 }
 
 int mfdm_update_rk4(mfdm_model* m, int it, void* stream) {
@@ -797,36 +926,47 @@ int mfdm_synchronize(mfdm_model* m) {
 
 int mfdm_get_records(mfdm_model* m, int first, int count, float* svx, float* svz, float* fp) {
   if (!m) return fail(MFDM_ERR_ARG, "null handle");
-  const int avail = (m->host_step + m->gap - 1) / m->gap;
-  if (first < 0 || count < 0 || first + count > avail || first + count > m->rec_cap)
-    return fail(MFDM_ERR_ARG, "record range out of bounds");
-  if (count == 0) return MFDM_OK;
-  DeviceGuard g(m->device);
-  const int nx = m->cfg.nx;
-  float* outs[3] = {svx, svz, fp};
-  for (int q = 0; q < 3; ++q) {
-    if (!outs[q]) continue;
-    MFDM_CU(cudaMemcpy2DAsync(outs[q], size_t(nx) * sizeof(float),
-                              m->d_rec + (size_t(first) * 3 + q) * nx, size_t(3) * nx * sizeof(float),
-                              size_t(nx) * sizeof(float), size_t(count), cudaMemcpyDeviceToHost,
-                              m->stream));
-  }
-  MFDM_CU(cudaStreamSynchronize(m->stream));
-  return MFDM_OK;
+  return get_records(m, 0, first, count, svx, svz, fp);
 }
 
 int mfdm_get_field(mfdm_model* m, int field, float* host) {
-  if (!m || !host) return fail(MFDM_ERR_ARG, "null argument");
-  float* p = nullptr;
-  int rows = 0;
-  int rc = field_ptr(m, field, &p, &rows);
+  if (!m) return fail(MFDM_ERR_ARG, "null argument");
+  return get_field(m, 0, field, host);
+}
+
+int mfdm_open_batch(const mfdm_desc* d, int nshots, const mfdm_shot* shots, int device,
+                    mfdm_model** out) {
+  if (nshots <= 0 || !shots) return fail(MFDM_ERR_ARG, "a batch needs at least one shot");
+  HostModel h;
+  const int rc = desc_to_host(d, h);
   if (rc != MFDM_OK) return rc;
+  std::vector<ShotCfg> sv(static_cast<size_t>(nshots));
+  for (int b = 0; b < nshots; ++b) {
+    sv[size_t(b)].x = shots[b].src_x;
+    sv[size_t(b)].z = shots[b].src_z;
+    sv[size_t(b)].fpeak = shots[b].fpeak;
+    sv[size_t(b)].beta0 = shots[b].beta0;
+  }
+  return open_common(std::move(h), device, out, &sv);
+}
+
+int mfdm_batch_reset(mfdm_model* m) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
   DeviceGuard g(m->device);
-  MFDM_CU(cudaMemcpy2DAsync(host, size_t(m->cfg.nx) * sizeof(float), p, size_t(m->P) * sizeof(float),
-                            size_t(m->cfg.nx) * sizeof(float), size_t(rows), cudaMemcpyDeviceToHost,
-                            m->stream));
-  MFDM_CU(cudaStreamSynchronize(m->stream));
-  return MFDM_OK;
+  int rc;
+  if ((rc = clear_state(m)) != MFDM_OK) return rc;
+  return rewind(m);
+}
+
+int mfdm_batch_get_records(mfdm_model* m, int shot, int first, int count, float* svx, float* svz,
+                           float* fp) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  return get_records(m, shot, first, count, svx, svz, fp);
+}
+
+int mfdm_batch_get_field(mfdm_model* m, int shot, int field, float* host) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  return get_field(m, shot, field, host);
 }
 
 int mfdm_set_field(mfdm_model* m, int field, const float* host) {

@@ -157,7 +157,7 @@ template <int NST, int NCOEF, int KIND>
 __device__ __forceinline__ void produce(const Segment& sg, const CUtensorMap* in_map,
                                         const CUtensorMap* coef_map, const CUtensorMap* un_map,
                                         const CUtensorMap* acc_map, float* ring, float* slots,
-                                        const Bars& B, int* status) {
+                                        const Bars& B, int* status, int shot) {
   if ((threadIdx.x & 31) != 0) return;
   constexpr int NPW = PW<NST, NCOEF, KIND>::n;
   constexpr unsigned kStBytes = NST * kR * kSW * 4, kPwBytes = NPW * kR * kTX * 4;
@@ -172,10 +172,10 @@ __device__ __forceinline__ void produce(const Segment& sg, const CUtensorMap* in
     mbar_arrive_expect_tx(&B.pfull[ps], kPwBytes);
     tma_load_3d(d, coef_map, sg.x0, q0, 0, &B.pfull[ps]);
     if (KIND == kStageMid) {
-      tma_load_3d(d + NCOEF * kF, un_map, sg.x0, q0, 0, &B.pfull[ps]);
-      tma_load_3d(d + (NCOEF + NST) * kF, acc_map, sg.x0, q0, 0, &B.pfull[ps]);
+      tma_load_4d(d + NCOEF * kF, un_map, sg.x0, q0, 0, shot, &B.pfull[ps]);
+      tma_load_4d(d + (NCOEF + NST) * kF, acc_map, sg.x0, q0, 0, shot, &B.pfull[ps]);
     } else if (KIND == kStageLast) {
-      tma_load_3d(d + NCOEF * kF, acc_map, sg.x0, q0, 0, &B.pfull[ps]);
+      tma_load_4d(d + NCOEF * kF, acc_map, sg.x0, q0, 0, shot, &B.pfull[ps]);
     }
     return true;
   };
@@ -188,9 +188,9 @@ __device__ __forceinline__ void produce(const Segment& sg, const CUtensorMap* in
     const int r0 = sg.z0 + k * kR;
     const bool dup = slot == 0 || slot == kNS - 1;  // also copied past the ring's other end
     mbar_arrive_expect_tx(&B.full[slot], kStBytes * (dup ? 2u : 1u));
-    tma_load_3d(ring + (kR + slot * kR) * kRowF, in_map, sg.x0 - 4, 0, r0, &B.full[slot]);
+    tma_load_4d(ring + (kR + slot * kR) * kRowF, in_map, sg.x0 - 4, 0, r0, shot, &B.full[slot]);
     if (dup)
-      tma_load_3d(ring + (slot == 0 ? kR + kRing : 0) * kRowF, in_map, sg.x0 - 4, 0, r0,
+      tma_load_4d(ring + (slot == 0 ? kR + kRing : 0) * kRowF, in_map, sg.x0 - 4, 0, r0, shot,
                   &B.full[slot]);
     const int j = k - D;  // point-wise chunk due with stencil chunk k
     if (j >= 0 && j < sg.nch && !issue_pw(j)) {
@@ -278,7 +278,7 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
   const int it = __ldg(C.step);
   if (threadIdx.x >= kConsumers) {
     produce<NST, NCOEF, KIND>(sg, &maps.fin, &maps.fcoef, &maps.fun, &maps.facc, ring, slots, B,
-                              C.status);
+                              C.status, blockIdx.y);
     return;
   }
   const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
@@ -364,7 +364,7 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
   segment_setup<NST>(smem, B, ring, slots);
   if (threadIdx.x >= kConsumers) {
     produce<NST, NCOEF, KIND>(sg, &maps.sin, &maps.scoef, &maps.sun, &maps.sacc, ring, slots, B,
-                              C.status);
+                              C.status, blockIdx.y);
     return;
   }
   const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
@@ -542,10 +542,15 @@ __device__ __forceinline__ void interface_strip(const Coef& C, const Fields& in,
 // weights (out = base + cc k, accumulator += w k).
 template <int DIR, int KIND>
 __global__ void __launch_bounds__(kThreads, 2)
-    stage_kernel(Coef C, Fields in, Fields out, Fields un, Fields acc,
+    stage_kernel(Coef C0, Fields in0, Fields out0, Fields un0, Fields acc0,
                  const __grid_constant__ StageMaps maps, int s, float cc, float w, int ntx,
                  int nbi, int nbf, int nbs) {
   extern __shared__ char smem[];
+  // this block's shot (blockIdx.y): its own state, tables and buffers
+  const size_t so = size_t(blockIdx.y) * C0.shot_stride;
+  const Coef C = shot_coef(C0, blockIdx.y);
+  const Fields in = shot_fields(in0, so), out = shot_fields(out0, so), un = shot_fields(un0, so),
+               acc = shot_fields(acc0, so);
   const int b = blockIdx.x;
   if (b < nbi) {  // first, so the short interface blocks overlap the segments
     interface_strip<DIR, KIND>(C, in, out, un, acc, cc, w, b);
@@ -561,7 +566,9 @@ __global__ void __launch_bounds__(kThreads, 2)
 // evaluated out of place from C.ipre, so no block reads values another block
 // already filtered. Then the receiver rows are sampled (src/main.cu:195-211)
 // and the last block to finish advances the device step counter.
-__global__ void __launch_bounds__(kFinishThreads) finish_kernel(Coef C, Fields U) {
+__global__ void __launch_bounds__(kFinishThreads) finish_kernel(Coef C0, Fields U0) {
+  const Coef C = shot_coef(C0, blockIdx.y);
+  const Fields U = shot_fields(U0, size_t(blockIdx.y) * C0.shot_stride);
   const int nx = C.nx, P = C.P, nzf = C.nzf;
   const int ix = blockIdx.x * kFinishThreads + threadIdx.x;
   const int it = *C.step;
@@ -621,7 +628,7 @@ __global__ void __launch_bounds__(kFinishThreads) finish_kernel(Coef C, Fields U
   if (threadIdx.x == 0) {
     __threadfence();
     const unsigned prev = atomicAdd(C.done, 1u);
-    if (prev == gridDim.x - 1) {
+    if (prev == gridDim.x * gridDim.y - 1) {
       *C.done = 0u;
       *C.step = it + 1;
       __threadfence();
@@ -668,7 +675,8 @@ static cudaError_t launch_one(const Coef& C, const Fields& in, const Fields& out
   int ntx, nbf, nbs, nbi;
   stage_grid(C.nx, C.nzf, C.nzs, &ntx, &nbf, &nbs, &nbi);
   const float cc = C.rk_c[s], w = (KIND == kStageLast) ? 0.f : C.rk_w[s];
-  stage_kernel<DIR, KIND><<<nbi + nbf + nbs, kThreads, smem_for_kind<KIND>(), st>>>(
+  const dim3 grid(unsigned(nbi + nbf + nbs), unsigned(C.nshots > 0 ? C.nshots : 1));
+  stage_kernel<DIR, KIND><<<grid, kThreads, smem_for_kind<KIND>(), st>>>(
       C, in, out, un, acc, maps, s, cc, w, ntx, nbi, nbf, nbs);
   return cudaGetLastError();
 }
@@ -705,7 +713,7 @@ cudaError_t launch_stage(const Coef& C, const Fields& in, const Fields& out, con
 
 cudaError_t launch_finish(const Coef& C, const Fields& U, cudaStream_t st) {
   const int nb = (C.nx + kFinishThreads - 1) / kFinishThreads;
-  finish_kernel<<<nb, kFinishThreads, 0, st>>>(C, U);
+  finish_kernel<<<dim3(unsigned(nb), unsigned(C.nshots > 0 ? C.nshots : 1)), kFinishThreads, 0, st>>>(C, U);
   return cudaGetLastError();
 }
 

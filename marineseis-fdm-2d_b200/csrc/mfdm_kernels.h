@@ -30,9 +30,10 @@ cudaError_t upload_constants(const float* srcw25, const float* w7);
 
 // Library-internal host helpers (mfdm_host.cu): record a failure for
 // mfdm_last_error() and return `code`; encode a TMA map of a [nf][rows][P] block
-// (rows_outer: boxes land as [row][field][col], the stencil-ring layout).
+// (rows_outer: boxes land as [row][field][col], the stencil-ring layout; with
+// nshots > 0 a fourth dimension, the shot, of stride shot_bytes).
 int set_error(int code, const char* msg);
 int encode_block_map(CUtensorMap* map, const float* base, int P, int rows, int nf, int box_x,
-                     bool rows_outer);
+                     bool rows_outer, int nshots = 0, size_t shot_bytes = 0);
 
 }  // namespace mfdm

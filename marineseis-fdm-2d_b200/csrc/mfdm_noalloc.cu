@@ -286,10 +286,11 @@ extern "C" int mfdm_step_noalloc(const mfdm_device_model* dm, int it, int nsteps
 
   CUtensorMap fst[4], sst[4], fpw[4], spw[4], fcm, scm;
   for (int s = 0; s < 4; ++s) {
-    if ((rc = mfdm::encode_block_map(&fst[s], F(o_fb[s]), P, nzf, 3, mfdm::kStageSW, true)) ||
-        (rc = mfdm::encode_block_map(&sst[s], F(o_sb[s]), P, nzs, 5, mfdm::kStageSW, true)) ||
-        (rc = mfdm::encode_block_map(&fpw[s], F(o_fb[s]), P, nzf, 3, mfdm::kStageTX, false)) ||
-        (rc = mfdm::encode_block_map(&spw[s], F(o_sb[s]), P, nzs, 5, mfdm::kStageTX, false)))
+    // state maps: one shot (the kernels address the shot as a fourth coordinate)
+    if ((rc = mfdm::encode_block_map(&fst[s], F(o_fb[s]), P, nzf, 3, mfdm::kStageSW, true, 1, 256)) ||
+        (rc = mfdm::encode_block_map(&sst[s], F(o_sb[s]), P, nzs, 5, mfdm::kStageSW, true, 1, 256)) ||
+        (rc = mfdm::encode_block_map(&fpw[s], F(o_fb[s]), P, nzf, 3, mfdm::kStageTX, false, 1, 256)) ||
+        (rc = mfdm::encode_block_map(&spw[s], F(o_sb[s]), P, nzs, 5, mfdm::kStageTX, false, 1, 256)))
       return rc;
   }
   if ((rc = mfdm::encode_block_map(&fcm, fco, P, nzf, 6, mfdm::kStageTX, false)) ||
