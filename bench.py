@@ -200,6 +200,44 @@ def run_reference(args, model, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def batched_shots(model, n: int, seed: int = 2):
+    """n shots spread along the source row, Ricker f in U[10, 25] Hz (seeded),
+    PML beta0 by the generators' rule for that frequency."""
+    rng = np.random.default_rng(seed)
+    lo, hi = model.npd + 10, model.nx - model.npd - 10
+    xs = np.linspace(lo, hi, n).round().astype(int)
+    fs = rng.uniform(10.0, 25.0, n)
+    z = int(model.src_z[0])
+    return [(int(x), z, float(f), float(modelgen.beta0_rule(model, f))) for x, f in zip(xs, fs)]
+
+
+def batched_rate(mfdm, model, device: int, warmup: int, nshots: int = 64, steps: int = 300):
+    """Shot-steps/s of one batch (one launch per RK stage for all shots) against
+    the same shots run one after another through single-shot handles, device
+    time (CUDA events) over `steps` steps each."""
+    import copy
+    shots = batched_shots(model, nshots)
+    with mfdm.Batch.from_model(model, shots, device=device) as b:
+        b.step(warmup)
+        tb, _ = b.time_steps(steps)
+    loop_ms = 0.0
+    m1 = copy.deepcopy(model)
+    with mfdm.Solver.from_model(m1, device=device) as s1:
+        for x, z, f, be in shots:
+            m1.src_x, m1.src_z, m1.fpeak, m1.beta0 = [x], [z], f, be
+            s1.load_model(m1)
+            s1.set_shot(0, reset=True)
+            s1.step(warmup)
+            t1, _ = s1.time_steps(steps)
+            loop_ms += t1
+    cells = model.cells * nshots * steps
+    return {"shots": nshots, "steps": steps, "ricker_hz": "U[10, 25], seed 2",
+            "value": round(cells / (tb / 1e3) / 1e9, 3), "unit": "Gcell/s",
+            "shot_steps_per_s": round(nshots * steps / (tb / 1e3), 1),
+            "per_shot_loop_gcells": round(cells / (loop_ms / 1e3) / 1e9, 3),
+            "speedup_vs_per_shot_loop": round(loop_ms / tb, 3)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -303,6 +341,7 @@ def main():
             other["curvilinear_1200x800"] = {
                 "value": round(small.cells * n2 / (t2 / 1e3) / 1e9, 3), "unit": "Gcell/s",
                 "ms_per_step": round(t2 / n2, 4)}
+        other["batched_1200x800_64_shots"] = batched_rate(mfdm, small, local, args.warmup)
 
     clocks = clk.summary()
     solver.close()

@@ -209,6 +209,15 @@ def make_model(nx: int, nz_f: int, nz_s: int, *, h: float = 5.0, npd: int = 20,
                  fluid=fluid, solid=solid, metric=metric)
 
 
+def beta0_rule(model: Model, fpeak: float, ppw: float = 8.0) -> float:
+    """CFS-PML beta0 of the generators for a given Ricker frequency:
+    min(vs, vp_fluid) / (0.5 ppw h fpeak) (``model_FANDS_PANDF_wavy.py:174-177``),
+    never below 1."""
+    vs_min = float(np.sqrt(np.min(model.solid["C55"] / model.solid["rho"])))
+    vp_f = float(np.sqrt(np.min(model.fluid["K"] / model.fluid["rho"])))
+    return max(1.0, round(min(vs_min, vp_f) / (0.5 * ppw * model.h * fpeak), 4))
+
+
 # --- named workloads ---------------------------------------------------------
 
 def flat_400x400(nt: int = 2000) -> Model:
