@@ -57,6 +57,9 @@ typedef struct mfdm_desc {
   const float* xi_z;
   const float* ze_x;
   const float* ze_z;
+  int boundary_type;              /* 2 (or 0): free surface on top, CFS-PML on the other
+                                     sides; 1: CFS-PML on all four sides (the reference's
+                                     grid.boundary_type, Cpml::FluidSolid)              */
 } mfdm_desc;
 
 typedef struct mfdm_info {

@@ -57,7 +57,7 @@ class Desc(ctypes.Structure):
                 ("nsrc", ctypes.c_int), ("src_x", _ip), ("src_z", _ip),
                 ("K", _fp), ("rho_f", _fp), ("C11", _fp), ("C13", _fp), ("C33", _fp),
                 ("C55", _fp), ("rho_s", _fp), ("J", _fp), ("xi_x", _fp), ("xi_z", _fp),
-                ("ze_x", _fp), ("ze_z", _fp)]
+                ("ze_x", _fp), ("ze_z", _fp), ("boundary_type", ctypes.c_int)]
 
 
 class Info(ctypes.Structure):
@@ -166,6 +166,7 @@ def make_desc(model):
     d.C33, d.C55, d.rho_s = ptr(model.solid["C33"]), ptr(model.solid["C55"]), ptr(model.solid["rho"])
     d.J, d.xi_x, d.xi_z = ptr(model.metric["J"]), ptr(model.metric["xi_x"]), ptr(model.metric["xi_z"])
     d.ze_x, d.ze_z = ptr(model.metric["ze_x"]), ptr(model.metric["ze_z"])
+    d.boundary_type = int(getattr(model, "boundary_type", 2))
     return d, keep
 
 

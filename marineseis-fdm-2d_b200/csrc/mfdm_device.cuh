@@ -69,6 +69,9 @@ struct Coef {
   const float* __restrict__ zez;
   const float4* __restrict__ pmlx;  // per column: d/beta, alpha + d/beta, 1/beta
   const float4* __restrict__ pmlz;  // per solid row (zeta strip)
+  const float4* __restrict__ pmlzf; // per fluid row (top zeta band, four-side CPML only)
+  int cpml;                         // 1: CFS-PML on all four sides (Cpml::FluidSolid, the
+                                    // CPML kernel instantiations), 0: free surface on top
   const float2* __restrict__ nrm;   // interface unit normal per column
   const float* __restrict__ src_amp;  // Ricker value per (step, stage): [steps][4]
   int src_steps;
@@ -98,6 +101,7 @@ struct Fields {
   float* fx[4];  // fluid xi ADE: Vx, Vz, Ex, Ez
   float* sx[4];  // solid xi ADE
   float* sz[4];  // solid zeta ADE
+  float* fz[4];  // fluid zeta ADE, top band rows 3..npd+2 [npd][P] (four-side CPML only)
 };
 
 // The set of one shot: every pointer `so` floats further.
@@ -111,6 +115,7 @@ __device__ __forceinline__ Fields shot_fields(const Fields& f, size_t so) {
     g.fx[q] = f.fx[q] + so;
     g.sx[q] = f.sx[q] + so;
     g.sz[q] = f.sz[q] + so;
+    g.fz[q] = f.fz[q] + so;
   }
   return g;
 }
@@ -123,6 +128,7 @@ __device__ __forceinline__ Coef shot_coef(const Coef& C, int shot) {
     const size_t so = size_t(shot) * C.shot_stride;
     c.pmlx = reinterpret_cast<const float4*>(reinterpret_cast<const float*>(C.pmlx) + so);
     c.pmlz = reinterpret_cast<const float4*>(reinterpret_cast<const float*>(C.pmlz) + so);
+    c.pmlzf = reinterpret_cast<const float4*>(reinterpret_cast<const float*>(C.pmlzf) + so);
     c.ipre = C.ipre + so;
     c.src_amp = C.src_amp + size_t(shot) * C.src_stride;
     if (C.rec) c.rec = C.rec + size_t(shot) * C.rec_stride;
@@ -212,8 +218,9 @@ __device__ __forceinline__ SolidCoefs solid_coefs_global(const Coef& C, size_t m
 // Output of the right-hand side at one fluid cell.
 struct FluidK {
   float vx, vz, p;
-  float V0, V1, E0, E1;  // xi-ADE RHS (valid only in the side strips)
-  bool has_E;            // false on the free-surface row (p fixed)
+  float V0, V1, E0, E1;      // xi-ADE RHS (valid only in the side strips)
+  float ZV0, ZV1, ZE0, ZE1;  // zeta-ADE RHS (top band, four-side CPML only)
+  bool has_E;                // false on the free-surface row (p fixed)
 };
 
 // Output of the right-hand side at one solid cell.
@@ -228,21 +235,28 @@ struct SolidK {
 // to the cell; `ade` holds the stage-input ADE memory (V0, V1, E0, E1) of the cell.
 // INTERIOR = true: the caller guarantees 6 <= iz <= nz_f-4 (no conservative
 // rows, full-order zeta stencils), so those branches compile away.
-template <int DIR, bool INTERIOR = false, class Acc>
+// With CPML (CFS-PML on all four sides, cpml_kernels.cuh:240-415) the top is
+// not a free surface: only the interface rows take the conservative form,
+// row 3 is an ordinary row, and `top` cells (rows 3..npd+2) carry a zeta PML
+// whose stage-input ADE memory is `zade`.
+template <int DIR, bool INTERIOR = false, bool CPML = false, class Acc>
 __device__ __forceinline__ FluidK fluid_rhs(const Coef& C, const Acc& A, int iz, int ix,
-                                            bool side, const float* ade, const FluidCoefs& cf) {
+                                            bool side, const float* ade, const FluidCoefs& cf,
+                                            bool top = false, const float* zade = nullptr) {
   FluidK o;
   const int P = C.P, nzf = C.nzf;
+  const bool cpml = !INTERIOR && CPML;
   const size_t g = (size_t)iz * P + ix;
   const float xix = cf.xix, xiz = cf.xiz, zex = cf.zex, zez = cf.zez;
   const float gxx = xix * xix + xiz * xiz;
-  const int d_if = nzf - 1 - iz, d_fs = iz - 3;
-  float4 pml = make_float4(0.f, 0.f, 0.f, 0.f);
+  const int d_if = nzf - 1 - iz, d_fs = cpml ? 3 : iz - 3;
+  float4 pml = make_float4(0.f, 0.f, 0.f, 0.f), pmz = pml;
   if (side) pml = ldg(C.pmlx + ix);
+  if (top) pmz = ldg(C.pmlzf + iz);
 
   // ---- momentum: rho dv/dt = -grad p ----
   {
-    float rvx, rvz, divx = 0.f, divz = 0.f;
+    float rvx, rvz, divx = 0.f, divz = 0.f, divzx = 0.f, divzz = 0.f;
     if (!INTERIOR && (d_if < 3 || d_fs < 3)) {
       // conservative flux form with mirrored ghosts (pml_fs_kernels.cuh:356-415)
       auto Ff = [&](int r) -> float2 {
@@ -274,6 +288,11 @@ __device__ __forceinline__ FluidK fluid_rhs(const Coef& C, const Acc& A, int iz,
         divx = xix * (xix * Sx + xiz * Sz) / (gxx * Jc);
         divz = xiz * (xix * Sx + xiz * Sz) / (gxx * Jc);
       }
+      if (top) {
+        const float gzz = zex * zex + zez * zez;
+        divzx = zex * (zex * Sx + zez * Sz) / (gzz * Jc);
+        divzz = zez * (zex * Sx + zez * Sz) / (gzz * Jc);
+      }
     } else {
       const float dpdx = d5<DIR>(A.fp(0, -3), A.fp(0, -2), A.fp(0, -1), A.fp(0, 0), A.fp(0, 1),
                                  A.fp(0, 2), A.fp(0, 3));
@@ -286,6 +305,11 @@ __device__ __forceinline__ FluidK fluid_rhs(const Coef& C, const Acc& A, int iz,
         divx = -xix * (gxx * dpdx + gxz * dpdz) / gxx;
         divz = -xiz * (gxx * dpdx + gxz * dpdz) / gxx;
       }
+      if (top) {
+        const float gxz = xix * zex + xiz * zez, gzz = zex * zex + zez * zez;
+        divzx = -zex * (gxz * dpdx + gzz * dpdz) / gzz;
+        divzz = -zez * (gxz * dpdx + gzz * dpdz) / gzz;
+      }
     }
     const float rho = cf.rho;
     o.vx = over_rho(rvx, rho);
@@ -297,10 +321,17 @@ __device__ __forceinline__ FluidK fluid_rhs(const Coef& C, const Acc& A, int iz,
       o.vx += over_rho((invb - 1.0f) * divx - invb * ade[0], rho);
       o.vz += over_rho((invb - 1.0f) * divz - invb * ade[1], rho);
     }
+    if (top) {
+      const float dpb = pmz.x, apdpb = pmz.y, invb = pmz.z;
+      o.ZV0 = -apdpb * zade[0] + dpb * divzx;
+      o.ZV1 = -apdpb * zade[1] + dpb * divzz;
+      o.vx += over_rho((invb - 1.0f) * divzx - invb * zade[0], rho);
+      o.vz += over_rho((invb - 1.0f) * divzz - invb * zade[1], rho);
+    }
   }
   // ---- pressure: dp/dt = -K div v ----
-  o.has_E = INTERIOR || (iz != 3);
-  if (!INTERIOR && iz == 3) {
+  o.has_E = INTERIOR || cpml || (iz != 3);
+  if (!INTERIOR && !cpml && iz == 3) {
     o.p = 0.0f;  // pressure-free surface row
   } else {
     auto vxc = [&](int j) { return A.fvx(j, 0); };
@@ -309,7 +340,7 @@ __device__ __forceinline__ FluidK fluid_rhs(const Coef& C, const Acc& A, int iz,
                                 A.fvx(0, 1), A.fvx(0, 2), A.fvx(0, 3));
     const float dvzdx = d5<DIR>(A.fvz(0, -3), A.fvz(0, -2), A.fvz(0, -1), A.fvz(0, 0),
                                 A.fvz(0, 1), A.fvz(0, 2), A.fvz(0, 3));
-    const int dn = INTERIOR ? 3 : min(iz - 3, nzf - 1 - iz);
+    const int dn = INTERIOR ? 3 : (cpml ? nzf - 1 - iz : min(iz - 3, nzf - 1 - iz));
     const float dvxdz = dz_near<DIR>(vxc, dn, false);
     const float dvzdz = dz_near<DIR>(vzc, dn, false);
     const float Kc = cf.K;
@@ -320,8 +351,20 @@ __device__ __forceinline__ FluidK fluid_rhs(const Coef& C, const Acc& A, int iz,
       const float dpb = pml.x, apdpb = pml.y, invb = pml.z;
       o.E0 = -apdpb * ade[2] + dpb * Dvx;
       o.E1 = -apdpb * ade[3] + dpb * Dvz;
-      o.p += Kc * (-(invb - 1.0f) * xix * Dvx - (invb - 1.0f) * xiz * Dvz + invb * xix * ade[2] +
-                   invb * xiz * ade[3]);
+      if (CPML)  // the four-side variant multiplies K into each term (cpml_kernels.cuh:390-395)
+        o.p += -Kc * (invb - 1.0f) * xix * Dvx - Kc * (invb - 1.0f) * xiz * Dvz +
+               invb * Kc * xix * ade[2] + invb * Kc * xiz * ade[3];
+      else
+        o.p += Kc * (-(invb - 1.0f) * xix * Dvx - (invb - 1.0f) * xiz * Dvz +
+                     invb * xix * ade[2] + invb * xiz * ade[3]);
+    }
+    if (top) {
+      const float gxz = xix * zex + xiz * zez, gzz = zex * zex + zez * zez;
+      const float Dzx = dvxdz + (gxz / gzz) * dvxdx, Dzz = dvzdz + (gxz / gzz) * dvzdx;
+      const float dpb = pmz.x, apdpb = pmz.y, invb = pmz.z;
+      o.ZE0 = -apdpb * zade[2] + dpb * Dzx;
+      o.ZE1 = -apdpb * zade[3] + dpb * Dzz;
+      o.p += Kc * (-(invb - 1.0f) * (zex * Dzx + zez * Dzz) + invb * (zex * zade[2] + zez * zade[3]));
     }
   }
   return o;
@@ -331,7 +374,7 @@ __device__ __forceinline__ FluidK fluid_rhs(const Coef& C, const Acc& A, int iz,
 // `A` reads the stage input: A.svx, A.svz, A.ssx, A.ssz, A.ssxz (dz, dx);
 // `xade` / `zade` are the stage-input xi / zeta ADE memory of the cell.
 // INTERIOR = true: the caller guarantees 3 <= iz <= nz_s-4.
-template <int DIR, bool INTERIOR = false, class Acc>
+template <int DIR, bool INTERIOR = false, bool CPML = false, class Acc>
 __device__ __forceinline__ SolidK solid_rhs(const Coef& C, const Acc& A, int iz, int ix, bool side,
                                             bool bottom, const float* xade, const float* zade,
                                             const SolidCoefs& cf) {
@@ -442,7 +485,15 @@ __device__ __forceinline__ SolidK solid_rhs(const Coef& C, const Acc& A, int iz,
     const float c11 = cf.c11, c13 = cf.c13, c33 = cf.c33, c55 = cf.c55;
     o.sx = c11 * (xix * dvxdx + zex * dvxdz) + c13 * (xiz * dvzdx + zez * dvzdz);
     o.sz = c13 * (xix * dvxdx + zex * dvxdz) + c33 * (xiz * dvzdx + zez * dvzdz);
-    o.sxz = c55 * (xiz * dvxdx + zez * dvxdz + xix * dvzdx + zex * dvzdz);
+    if (CPML) {
+      // The four-side variant reads this line's metric with the solid-local
+      // index, i.e. at global row iz (cpml_kernels.cuh:448-455); kept for parity.
+      const size_t b = (size_t)iz * C.P + ix;
+      o.sxz = c55 * (ldg(C.xiz + b) * dvxdx + ldg(C.zez + b) * dvxdz + ldg(C.xix + b) * dvzdx +
+                     ldg(C.zex + b) * dvzdz);
+    } else {
+      o.sxz = c55 * (xiz * dvxdx + zez * dvxdz + xix * dvzdx + zex * dvzdz);
+    }
     if (side || bottom) {
       const float gxz = xix * zex + xiz * zez;
       if (side) {

@@ -62,6 +62,7 @@ struct HostModel {
   int nt = 0, snapshot = 1;
   int npd = 0, npow = 2;
   float thickness = 0.f, vp_max = 0.f, rc = 0.f, beta0 = 1.f;
+  int bdy = 2;  // boundary type: 2 free surface on top (PANDF), 1 CFS-PML on all sides (CPML)
   std::vector<int> srcx, srcz;
   // host arrays, [rows][nx], when the model was read from files
   std::vector<float> K, rhof, C11, C13, C33, C55, rhos, J, xix, xiz, zex, zez;
@@ -144,6 +145,8 @@ int validate(const HostModel& h) {
     return fail(MFDM_ERR_ARG, "grid too small: need nx, nz_f, nz_s >= 8");
   if (h.npd < 0 || 2 * h.npd > h.nx - 6 || h.npd > h.nzs)
     return fail(MFDM_ERR_ARG, "PML width npd does not fit the grid");
+  if (h.bdy == 1 && h.npd + 3 > h.nzf)
+    return fail(MFDM_ERR_ARG, "the top PML band (rows 3..npd+2) does not fit the fluid rows");
   if (!(h.dt > 0.f) || !(h.fpeak > 0.f)) return fail(MFDM_ERR_ARG, "dt and fpeak must be > 0");
   if (h.nt < 0) return fail(MFDM_ERR_ARG, "nt must be >= 0");
   if (h.snapshot <= 0) return fail(MFDM_ERR_ARG, "snapshot interval must be > 0");
@@ -202,10 +205,12 @@ int load_json(const char* path, HostModel& h) {
     h.snapshot = J.get_int("base.snapshot");
     const int calc_type = J.get_int("grid.calc_type");
     const int bdy = J.get_int("grid.boundary_type");
-    if (calc_type != 1 || bdy != 2)
+    if (calc_type != 1 || (bdy != 1 && bdy != 2))
       return fail(MFDM_ERR_ARG,
                   "unsupported configuration: only calc_type 1 (fluid over solid) with "
-                  "boundary_type 2 (CFS-PML sides and bottom, free surface on top)");
+                  "boundary_type 2 (CFS-PML sides and bottom, free surface on top) or 1 "
+                  "(CFS-PML on all four sides)");
+    h.bdy = bdy;
     const size_t nsrc = J.size("grid.src_pos.posx");
     for (size_t i = 0; i < nsrc; ++i) {
       h.srcx.push_back(J.get_int("grid.src_pos.posx", i));
@@ -457,7 +462,11 @@ int upload_model(mfdm_model* m, const HostModel& h) {
     const ShotCfg& sh = m->shots[size_t(b)];
     pml_profile(h, nx, true, true, sh.fpeak, sh.beta0, px);
     pml_profile(h, nzs, false, true, sh.fpeak, sh.beta0, pz);
+    std::vector<float4> pzf;  // fluid rows: a top band with four-side CPML (elements.cu:866-869)
+    pml_profile(h, nzf, h.bdy == 1, false, sh.fpeak, sh.beta0, pzf);
     const size_t so = size_t(b) * C.shot_stride;
+    MFDM_CU(cudaMemcpyAsync(const_cast<float*>(reinterpret_cast<const float*>(C.pmlzf)) + so, pzf.data(),
+                            pzf.size() * sizeof(float4), cudaMemcpyHostToDevice, m->stream));
     MFDM_CU(cudaMemcpyAsync(const_cast<float*>(reinterpret_cast<const float*>(C.pmlx)) + so, px.data(),
                             px.size() * sizeof(float4), cudaMemcpyHostToDevice, m->stream));
     MFDM_CU(cudaMemcpyAsync(const_cast<float*>(reinterpret_cast<const float*>(C.pmlz)) + so, pz.data(),
@@ -476,7 +485,7 @@ int upload_model(mfdm_model* m, const HostModel& h) {
   c.nx = h.nx; c.nzf = h.nzf; c.nzs = h.nzs;
   c.fpeak = h.fpeak; c.dt = h.dt; c.nt = h.nt; c.snapshot = h.snapshot;
   c.npd = h.npd; c.npow = h.npow; c.thickness = h.thickness;
-  c.vp_max = h.vp_max; c.rc = h.rc; c.beta0 = h.beta0;
+  c.vp_max = h.vp_max; c.rc = h.rc; c.beta0 = h.beta0; c.bdy = h.bdy;
   c.srcx = h.srcx; c.srcz = h.srcz;
   if (m->isrc >= int(c.srcx.size())) m->isrc = 0;
   C.srcx = c.srcx.empty() ? -1 : c.srcx[size_t(m->isrc)];
@@ -548,16 +557,17 @@ int build(mfdm_model* m, HostModel&& h, int device, const std::vector<ShotCfg>* 
     roff += (nfloats * sizeof(float) + 255) / 256 * 256;
     return o;
   };
-  size_t o_fb[4], o_sb[4], o_ade[4][12];
+  size_t o_fb[4], o_sb[4], o_ade[4][12], o_fza[4][4];
   for (int s = 0; s < 4; ++s) {
     o_fb[s] = rtake(3 * nf);
     o_sb[s] = rtake(5 * ns);
     for (int q = 0; q < 4; ++q) o_ade[s][q] = rtake(size_t(nzf) * Ps);
     for (int q = 0; q < 4; ++q) o_ade[s][4 + q] = rtake(size_t(nzs) * Ps);
     for (int q = 0; q < 4; ++q) o_ade[s][8 + q] = rtake(size_t(npdr) * P);
+    for (int q = 0; q < 4; ++q) o_fza[s][q] = rtake(h.bdy == 1 ? size_t(npdr) * P : 1);
   }
   const size_t o_pmlx = rtake(size_t(nx) * 4), o_pmlz = rtake(size_t(nzs) * 4),
-               o_ipre = rtake(size_t(8) * P);
+               o_pmlzf = rtake(size_t(nzf) * 4), o_ipre = rtake(size_t(8) * P);
   m->region = roff;
   off = shared + roff * size_t(m->nshots);
   m->dbytes = off;
@@ -576,6 +586,7 @@ int build(mfdm_model* m, HostModel&& h, int device, const std::vector<ShotCfg>* 
       S.fx[q] = R(o_ade[s][q]);
       S.sx[q] = R(o_ade[s][4 + q]);
       S.sz[q] = R(o_ade[s][8 + q]);
+      S.fz[q] = R(o_fza[s][q]);
     }
   }
   m->fcoef = F(o_fco);
@@ -588,6 +599,8 @@ int build(mfdm_model* m, HostModel&& h, int device, const std::vector<ShotCfg>* 
   C.J = F(o_J); C.xix = F(o_xix); C.xiz = F(o_xiz); C.zex = F(o_zex); C.zez = F(o_zez);
   C.pmlx = reinterpret_cast<const float4*>(R(o_pmlx));
   C.pmlz = reinterpret_cast<const float4*>(R(o_pmlz));
+  C.pmlzf = reinterpret_cast<const float4*>(R(o_pmlzf));
+  C.cpml = h.bdy == 1 ? 1 : 0;
   C.nrm = reinterpret_cast<const float2*>(F(o_nrm));
   C.ipre = R(o_ipre);
   int* misc = reinterpret_cast<int*>(F(o_misc));
@@ -675,6 +688,10 @@ int clear_state(mfdm_model* m) {
                                 m->stream));
       MFDM_CU(cudaMemset2DAsync(S.sz[q], pitch, 0,
                                 size_t(std::max(m->cfg.npd, 1)) * m->P * sizeof(float), h, m->stream));
+      if (m->C.cpml)
+        MFDM_CU(cudaMemset2DAsync(S.fz[q], pitch, 0,
+                                  size_t(std::max(m->cfg.npd, 1)) * m->P * sizeof(float), h,
+                                  m->stream));
     }
   }
   MFDM_CU(cudaMemset2DAsync(m->C.ipre, pitch, 0, size_t(8) * m->P * sizeof(float), h, m->stream));
@@ -769,6 +786,7 @@ int desc_to_host(const mfdm_desc* d, HostModel& h) {
   h.fpeak = d->fpeak; h.dt = d->dt; h.nt = d->nt; h.snapshot = d->snapshot;
   h.npd = d->npd; h.npow = d->npow; h.thickness = d->thickness; h.vp_max = d->vp_max;
   h.rc = d->rc; h.beta0 = d->beta0;
+  h.bdy = d->boundary_type == 1 ? 1 : 2;
   if (h.nx <= 0 || h.nzf <= 0 || h.nzs <= 0) return fail(MFDM_ERR_ARG, "bad grid size");
   for (int i = 0; i < d->nsrc; ++i) {
     if (!d->src_x || !d->src_z) return fail(MFDM_ERR_ARG, "null source arrays");
@@ -814,8 +832,9 @@ int mfdm_load_desc(mfdm_model* m, const mfdm_desc* d) {
   int rc = desc_to_host(d, h);
   if (rc != MFDM_OK) return rc;
   if ((rc = validate(h)) != MFDM_OK) return rc;
-  if (h.nx != m->cfg.nx || h.nzf != m->cfg.nzf || h.nzs != m->cfg.nzs || h.npd != m->cfg.npd)
-    return fail(MFDM_ERR_ARG, "model shape differs from the open handle");
+  if (h.nx != m->cfg.nx || h.nzf != m->cfg.nzf || h.nzs != m->cfg.nzs || h.npd != m->cfg.npd ||
+      h.bdy != m->cfg.bdy)
+    return fail(MFDM_ERR_ARG, "model shape or boundary type differs from the open handle");
   DeviceGuard g(m->device);
   MFDM_CU(cudaStreamSynchronize(m->stream));
   return upload_model(m, h);

@@ -259,7 +259,7 @@ __device__ __forceinline__ void segment_setup(char* smem_raw, Bars& B, float*& r
   __syncthreads();
 }
 
-template <int DIR, int KIND>
+template <int DIR, int KIND, bool CPML>
 __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, const Fields& out,
                                               const Fields& un, const Fields& acc,
                                               const StageMaps& maps, int s, float cc, float w,
@@ -290,7 +290,7 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
   // conservative or one-sided row (rows 6 .. nz_f-4 only) take a body without
   // those branches.
   const bool general = sg.x0 < 3 + C.npd || sg.x0 + kTX > nx - 3 - C.npd ||
-                       sg.z0 < 6 || sg.z1 - 1 > C.nzf - 4 ||
+                       sg.z0 < 6 || sg.z1 - 1 > C.nzf - 4 || (CPML && sg.z0 <= C.npd + 2) ||
                        (C.srcx >= 0 && C.srcx >= sg.x0 - 2 && C.srcx < sg.x0 + kTX + 2 &&
                         C.srcz >= sg.z0 - 2 && C.srcz < sg.z1 + 2);
   auto cell = [&](auto gen_tag, int c, int slot) {
@@ -303,16 +303,23 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
     constexpr int F = kR * kTX;
     const float* pw = slots + (size_t)slot * NPW * F + ty * kTX + tx;  // field p at pw[p * F]
     const FluidCoefs cf{pw[0], pw[F], pw[2 * F], pw[3 * F], pw[4 * F], pw[5 * F]};
-    float ade[4] = {0.f, 0.f, 0.f, 0.f};
+    float ade[4] = {0.f, 0.f, 0.f, 0.f}, zade[4] = {0.f, 0.f, 0.f, 0.f};
     const size_t si = (size_t)iz * C.Ps + scol;
     if (sd) {
 #pragma unroll
       for (int q = 0; q < 4; ++q) ade[q] = __ldg(in.fx[q] + si);
     }
+    // four-side CPML: the top zeta band, rows 3..npd+2, strip row iz - 3
+    const bool tp = GEN && CPML && iz <= C.npd + 2;
+    const size_t zi = (size_t)(iz - 3) * P + ix;
+    if (tp) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) zade[q] = __ldg(in.fz[q] + zi);
+    }
     // rows 6 .. nz_f-4 take the specialised interior body (no conservative rows)
     FluidK k = (!GEN || (iz >= 6 && iz <= C.nzf - 4))
-                   ? fluid_rhs<DIR, true>(C, A, iz, ix, sd, ade, cf)
-                   : fluid_rhs<DIR, false>(C, A, iz, ix, sd, ade, cf);
+                   ? fluid_rhs<DIR, true, CPML>(C, A, iz, ix, sd, ade, cf, tp, zade)
+                   : fluid_rhs<DIR, false, CPML>(C, A, iz, ix, sd, ade, cf, tp, zade);
     if (GEN) k.p += source_term(C, iz, ix, it, s);
     const size_t i = (size_t)iz * P + ix;
     const float kv[3] = {k.vx, k.vz, k.p};
@@ -339,6 +346,12 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
         rk_update<KIND>(k.E1, ade[3], un.fx[3], out.fx[3], acc.fx[3], si, cc, w);
       }
     }
+    if (tp) {
+      rk_update<KIND>(k.ZV0, zade[0], un.fz[0], out.fz[0], acc.fz[0], zi, cc, w);
+      rk_update<KIND>(k.ZV1, zade[1], un.fz[1], out.fz[1], acc.fz[1], zi, cc, w);
+      rk_update<KIND>(k.ZE0, zade[2], un.fz[2], out.fz[2], acc.fz[2], zi, cc, w);
+      rk_update<KIND>(k.ZE1, zade[3], un.fz[3], out.fz[3], acc.fz[3], zi, cc, w);
+    }
   };
   if (general)
     consume(sg, B, C.status, [&](int c, int slot) { cell(std::true_type{}, c, slot); });
@@ -346,7 +359,7 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
     consume(sg, B, C.status, [&](int c, int slot) { cell(std::false_type{}, c, slot); });
 }
 
-template <int DIR, int KIND>
+template <int DIR, int KIND, bool CPML>
 __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, const Fields& out,
                                               const Fields& un, const Fields& acc,
                                               const StageMaps& maps, float cc, float w, int blk,
@@ -400,8 +413,8 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
       for (int q = 0; q < 4; ++q) zade[q] = __ldg(in.sz[q] + szi);
     }
     SolidK k = (!GEN || iz >= 3)
-                   ? solid_rhs<DIR, true>(C, A, iz, ix, sd, bottom, xade, zade, cf)
-                   : solid_rhs<DIR, false>(C, A, iz, ix, sd, bottom, xade, zade, cf);
+                   ? solid_rhs<DIR, true, CPML>(C, A, iz, ix, sd, bottom, xade, zade, cf)
+                   : solid_rhs<DIR, false, CPML>(C, A, iz, ix, sd, bottom, xade, zade, cf);
     const size_t i = (size_t)iz * P + ix;
     const float kv[5] = {k.vx, k.vz, k.sx, k.sz, k.sxz};
     float* const outs[5] = {out.svx, out.svz, out.ssx, out.ssz, out.ssxz};
@@ -441,7 +454,7 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
 // Interface strip: fluid row nz_f-1 and solid row 0 of one column, their RHS,
 // the normal/tangential coupling (pml_fs_kernels.cuh:754-827) and the RK update.
 // In the last stage the eight coupled state values go to C.ipre, the filter's input.
-template <int DIR, int KIND>
+template <int DIR, int KIND, bool CPML>
 __device__ __forceinline__ void interface_strip(const Coef& C, const Fields& in, const Fields& out,
                                                 const Fields& un, const Fields& acc, float c,
                                                 float w, int blk) {
@@ -473,8 +486,17 @@ __device__ __forceinline__ void interface_strip(const Coef& C, const Fields& in,
 #pragma unroll
     for (int q = 0; q < 4; ++q) zade[q] = __ldg(in.sz[q] + szi);
   }
-  FluidK kf = fluid_rhs<DIR>(C, Af, nzf - 1, ix, side, fade, fluid_coefs_global(C, fi));
-  SolidK ks = solid_rhs<DIR>(C, As, 0, ix, side, bottom, xade, zade,
+  // four-side CPML on a grid whose top band reaches the interface row
+  const bool ftop = CPML && nzf - 1 <= npd + 2;
+  float ztop[4] = {0.f, 0.f, 0.f, 0.f};
+  const size_t zti = (size_t)(nzf - 1 - 3) * P + ix;
+  if (ftop) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) ztop[q] = __ldg(in.fz[q] + zti);
+  }
+  FluidK kf = fluid_rhs<DIR, false, CPML>(C, Af, nzf - 1, ix, side, fade, fluid_coefs_global(C, fi),
+                                          ftop, ztop);
+  SolidK ks = solid_rhs<DIR, false, CPML>(C, As, 0, ix, side, bottom, xade, zade,
                              solid_coefs_global(C, si, si + (size_t)(nzf - 1) * P));
 
   // ---- coupling of the stage RHS on the interface ----
@@ -536,11 +558,17 @@ __device__ __forceinline__ void interface_strip(const Coef& C, const Fields& in,
     rk_update<KIND>(ks.ZE0, zade[2], un.sz[2], out.sz[2], acc.sz[2], szi, c, w);
     rk_update<KIND>(ks.ZE1, zade[3], un.sz[3], out.sz[3], acc.sz[3], szi, c, w);
   }
+  if (ftop) {
+    rk_update<KIND>(kf.ZV0, ztop[0], un.fz[0], out.fz[0], acc.fz[0], zti, c, w);
+    rk_update<KIND>(kf.ZV1, ztop[1], un.fz[1], out.fz[1], acc.fz[1], zti, c, w);
+    rk_update<KIND>(kf.ZE0, ztop[2], un.fz[2], out.fz[2], acc.fz[2], zti, c, w);
+    rk_update<KIND>(kf.ZE1, ztop[3], un.fz[3], out.fz[3], acc.fz[3], zti, c, w);
+  }
 }
 
 // One RK stage: `s` indexes the Ricker table; cc and w are the stage's RK
 // weights (out = base + cc k, accumulator += w k).
-template <int DIR, int KIND>
+template <int DIR, int KIND, bool CPML>
 __global__ void __launch_bounds__(kThreads, 2)
     stage_kernel(Coef C0, Fields in0, Fields out0, Fields un0, Fields acc0,
                  const __grid_constant__ StageMaps maps, int s, float cc, float w, int ntx,
@@ -553,11 +581,11 @@ __global__ void __launch_bounds__(kThreads, 2)
                acc = shot_fields(acc0, so);
   const int b = blockIdx.x;
   if (b < nbi) {  // first, so the short interface blocks overlap the segments
-    interface_strip<DIR, KIND>(C, in, out, un, acc, cc, w, b);
+    interface_strip<DIR, KIND, CPML>(C, in, out, un, acc, cc, w, b);
   } else if (b < nbi + nbf) {
-    fluid_segment<DIR, KIND>(C, in, out, un, acc, maps, s, cc, w, b - nbi, ntx, smem);
+    fluid_segment<DIR, KIND, CPML>(C, in, out, un, acc, maps, s, cc, w, b - nbi, ntx, smem);
   } else {
-    solid_segment<DIR, KIND>(C, in, out, un, acc, maps, cc, w, b - nbi - nbf, ntx, smem);
+    solid_segment<DIR, KIND, CPML>(C, in, out, un, acc, maps, cc, w, b - nbi - nbf, ntx, smem);
   }
 }
 
@@ -669,22 +697,26 @@ void stage_grid(int nx, int nzf, int nzs, int* ntx, int* nbf, int* nbs, int* nbi
   *nbi = (nx + kConsumers - 1) / kConsumers;
 }
 
-template <int DIR, int KIND>
+template <int DIR, int KIND, bool CPML>
 static cudaError_t launch_one(const Coef& C, const Fields& in, const Fields& out, const Fields& un,
                               const Fields& acc, const StageMaps& maps, int s, cudaStream_t st) {
   int ntx, nbf, nbs, nbi;
   stage_grid(C.nx, C.nzf, C.nzs, &ntx, &nbf, &nbs, &nbi);
   const float cc = C.rk_c[s], w = (KIND == kStageLast) ? 0.f : C.rk_w[s];
   const dim3 grid(unsigned(nbi + nbf + nbs), unsigned(C.nshots > 0 ? C.nshots : 1));
-  stage_kernel<DIR, KIND><<<grid, kThreads, smem_for_kind<KIND>(), st>>>(
+  stage_kernel<DIR, KIND, CPML><<<grid, kThreads, smem_for_kind<KIND>(), st>>>(
       C, in, out, un, acc, maps, s, cc, w, ntx, nbi, nbf, nbs);
   return cudaGetLastError();
 }
 
 template <int DIR, int KIND>
 static cudaError_t configure_one() {
-  return cudaFuncSetAttribute(stage_kernel<DIR, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)smem_for_kind<KIND>());
+  cudaError_t e = cudaFuncSetAttribute(stage_kernel<DIR, KIND, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem_for_kind<KIND>());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(stage_kernel<DIR, KIND, true>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_for_kind<KIND>());
 }
 
 cudaError_t configure_device() {
@@ -697,18 +729,27 @@ cudaError_t configure_device() {
   return configure_one<kDirB, kStageLast>();
 }
 
+template <bool CPML>
+static cudaError_t launch_stage_bc(const Coef& C, const Fields& in, const Fields& out,
+                                  const Fields& un, const Fields& acc, const StageMaps& maps,
+                                  int stage, int dir, cudaStream_t st) {
+  const int kind = stage == 0 ? kStageFirst : (stage == 3 ? kStageLast : kStageMid);
+  if (dir == kDirF) {
+    if (kind == kStageFirst) return launch_one<kDirF, kStageFirst, CPML>(C, in, out, un, acc, maps, stage, st);
+    if (kind == kStageMid) return launch_one<kDirF, kStageMid, CPML>(C, in, out, un, acc, maps, stage, st);
+    return launch_one<kDirF, kStageLast, CPML>(C, in, out, un, acc, maps, stage, st);
+  }
+  if (kind == kStageFirst) return launch_one<kDirB, kStageFirst, CPML>(C, in, out, un, acc, maps, stage, st);
+  if (kind == kStageMid) return launch_one<kDirB, kStageMid, CPML>(C, in, out, un, acc, maps, stage, st);
+  return launch_one<kDirB, kStageLast, CPML>(C, in, out, un, acc, maps, stage, st);
+}
+
 cudaError_t launch_stage(const Coef& C, const Fields& in, const Fields& out, const Fields& un,
                          const Fields& acc, const StageMaps& maps, int stage, int dir,
                          cudaStream_t st) {
-  const int kind = stage == 0 ? kStageFirst : (stage == 3 ? kStageLast : kStageMid);
-  if (dir == kDirF) {
-    if (kind == kStageFirst) return launch_one<kDirF, kStageFirst>(C, in, out, un, acc, maps, stage, st);
-    if (kind == kStageMid) return launch_one<kDirF, kStageMid>(C, in, out, un, acc, maps, stage, st);
-    return launch_one<kDirF, kStageLast>(C, in, out, un, acc, maps, stage, st);
-  }
-  if (kind == kStageFirst) return launch_one<kDirB, kStageFirst>(C, in, out, un, acc, maps, stage, st);
-  if (kind == kStageMid) return launch_one<kDirB, kStageMid>(C, in, out, un, acc, maps, stage, st);
-  return launch_one<kDirB, kStageLast>(C, in, out, un, acc, maps, stage, st);
+  // the four-side CPML variant runs its own kernel instantiations
+  return C.cpml ? launch_stage_bc<true>(C, in, out, un, acc, maps, stage, dir, st)
+                : launch_stage_bc<false>(C, in, out, un, acc, maps, stage, dir, st);
 }
 
 cudaError_t launch_finish(const Coef& C, const Fields& U, cudaStream_t st) {

@@ -230,7 +230,7 @@ extern "C" int mfdm_step_noalloc(const mfdm_device_model* dm, int it, int nsteps
     if ((rc = copy_rows(F(o_met[q]), gmet[q], 0, nz)) != MFDM_OK) return rc;
 
   // The wavefield in: the caller's arrays become set U.
-  mfdm::Fields S[4];
+  mfdm::Fields S[4] = {};
   for (int s = 0; s < 4; ++s) {
     float* fb = F(o_fb[s]);
     float* sb = F(o_sb[s]);

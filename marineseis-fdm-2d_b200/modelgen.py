@@ -37,7 +37,9 @@ METRIC_FIELDS = ("J", "xi_x", "xi_z", "ze_x", "ze_z")
 
 @dataclass
 class Model:
-    """A fluid-over-solid model on a curvilinear grid (calc_type 1, boundary_type 2)."""
+    """A fluid-over-solid model on a curvilinear grid (calc_type 1). boundary_type 2:
+    free surface on top, CFS-PML left, right and bottom; 1: CFS-PML on all four
+    sides (a top PML band in the fluid instead of the free surface)."""
 
     nx: int
     nz_f: int
@@ -58,6 +60,7 @@ class Model:
     fluid: Dict[str, np.ndarray] = field(default_factory=dict)   # [nz_f][nx]
     solid: Dict[str, np.ndarray] = field(default_factory=dict)   # [nz_s][nx]
     metric: Dict[str, np.ndarray] = field(default_factory=dict)  # [nz_f+nz_s-1][nx]
+    boundary_type: int = 2
 
     @property
     def nz(self) -> int:
@@ -75,7 +78,7 @@ class Model:
                      "snapshot": int(self.snapshot)},
             "grid": {
                 "calc_type": 1,
-                "boundary_type": 2,
+                "boundary_type": int(self.boundary_type),
                 "src_pos": {"posx": [int(v) for v in self.src_x],
                             "posz": [int(v) for v in self.src_z]},
                 "solid": {"nx": self.nx, "nz": self.nz_s,

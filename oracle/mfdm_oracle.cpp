@@ -1,4 +1,5 @@
-// CPU oracle for the MarineSeis-FDM-2D fluid-solid time step (PANDF + FANDS).
+// CPU oracle for the MarineSeis-FDM-2D fluid-solid time step (FANDS with
+// boundary type PANDF, and with CPML: CFS-PML on all four sides).
 //
 // TEST INFRASTRUCTURE ONLY. This file restates, on the CPU, the reference
 // algorithm of `PmlFs::FluidSolid::update_RK4` so that the CUDA library can be
@@ -19,6 +20,9 @@
 //   src/pml_fs_kernels.cu:385-531, 624-868                 ghosts, filter, source, RK4 driver
 //   src/elements.cu:18-40, 121-124, 385-392, 824-905       constants, CFS shape, Ricker, PML tables, normals
 //   src/main.cu:92, 136-213, 245-295                       step loop and record sampling
+//   include/cpml_kernels.cuh:237-662                       the CPML variant (Cpml::FluidSolid):
+//       fluid without a free surface, a top zeta-PML band in the fluid, and the
+//       solid sxz read with the solid-local index into the global metric (:448-455)
 //
 // One deliberate difference: the interface filter (src/pml_fs_kernels.cu:428-525)
 // runs in place in the reference, so a block may read a neighbour's halo after
@@ -70,9 +74,10 @@ enum Field {
   FXVX, FXVZ, FXEX, FXEZ,      // fluid xi-ADE memory
   SXVX, SXVZ, SXEX, SXEZ,      // solid xi-ADE memory
   SZVX, SZVZ, SZEX, SZEZ,      // solid zeta-ADE memory
+  FZVX, FZVZ, FZEX, FZEZ,      // fluid zeta-ADE memory (top band, CPML only)
   NFIELD
 };
-inline bool is_fluid(int f) { return f <= FP || (f >= FXVX && f <= FXEZ); }
+inline bool is_fluid(int f) { return f <= FP || (f >= FXVX && f <= FXEZ) || f >= FZVX; }
 
 template <class R> struct P2 { R x, y; };
 
@@ -129,6 +134,7 @@ struct orc_model {
   const double *K, *rho_f;                          // [nz_f][nx]
   const double *C11, *C13, *C33, *C55, *rho_s;      // [nz_s][nx]
   const double *J, *xi_x, *xi_z, *ze_x, *ze_z;      // [nz_f + nz_s - 1][nx]
+  int cpml;            // 1: CFS-PML on all four sides (boundary type CPML), 0: PANDF
 };
 }
 
@@ -137,10 +143,12 @@ namespace {
 template <class R>
 struct Oracle {
   int nx, nzf, nzs, npd;
+  bool cpml;
   float fpeak_f, dt_f;
   int srcx, srcz;
   std::vector<R> K, rf, C11, C13, C33, C55, rs, J, xx, xz, zx, zz;
   std::vector<R> alx, bex, dpx, alz, bez, dpz;  // xi tables [nx], solid zeta tables [nzs]
+  std::vector<R> alzf, bezf, dpzf;              // fluid zeta tables [nzf] (top band, CPML)
   std::vector<R> nfx, nfz;                      // interface normal [nx]
   using Set = std::vector<std::vector<R>>;
   Set U, Ub, Ut, Kk;
@@ -162,6 +170,7 @@ struct Oracle {
 
   explicit Oracle(const orc_model& m) {
     nx = m.nx; nzf = m.nz_f; nzs = m.nz_s; npd = m.npd;
+    cpml = m.cpml != 0;
     fpeak_f = float(m.fpeak); dt_f = float(m.dt);
     srcx = m.src_x; srcz = m.src_z;
     const size_t nf = size_t(nzf) * nx, ns = size_t(nzs) * nx, ng = size_t(nzf + nzs - 1) * nx;
@@ -183,6 +192,7 @@ struct Oracle {
   void pml_tables(const orc_model& m) {
     alx.assign(nx, 0); bex.assign(nx, 0); dpx.assign(nx, 0);
     alz.assign(nzs, 0); bez.assign(nzs, 0); dpz.assign(nzs, 0);
+    alzf.assign(nzf, 0); bezf.assign(nzf, 0); dpzf.assign(nzf, 0);
     const float vpmax = float(m.vp_max), rc = float(m.rc), thick = float(m.thickness);
     const float beta0 = float(m.beta0);
     const int npow = m.npow;
@@ -216,6 +226,8 @@ struct Oracle {
     };
     profile(alx.data(), bex.data(), dpx.data(), nx, true, true);
     profile(alz.data(), bez.data(), dpz.data(), nzs, false, true);
+    // fluid zeta axis: a top band for CPML only (src/elements.cu:866-869)
+    profile(alzf.data(), bezf.data(), dpzf.data(), nzf, cpml, false);
   }
 
   // Unit normal of the interface from the zeta gradient (src/elements.cu:892-905).
@@ -282,7 +294,8 @@ struct Oracle {
     }
   }
 
-  // Fluid momentum RHS (include/pml_fs_kernels.cuh:333-450).
+  // Fluid momentum RHS (include/pml_fs_kernels.cuh:333-450; CPML:
+  // include/cpml_kernels.cuh:240-342 - no free-surface rows, a top zeta band).
   void fluid_velocity(int dir, const Set& S) {
 #pragma omp parallel for schedule(static)
     for (int iz = 3; iz < nzf; ++iz) {
@@ -290,8 +303,10 @@ struct Oracle {
         const size_t i = size_t(iz) * nx + ix;
         const R xix = xx[i], xiz = xz[i], zex = zx[i], zez = zz[i];
         const R gxx = xix * xix + xiz * xiz;
-        R rvx, rvz, divx, divz;
-        const int d_if = nzf - 1 - iz, d_fs = iz - 3;
+        const R gzz = zex * zex + zez * zez;
+        const bool top = cpml && iz <= npd + 2;
+        R rvx, rvz, divx, divz, divzx = 0, divzz = 0;
+        const int d_if = nzf - 1 - iz, d_fs = cpml ? 3 : iz - 3;
         if (d_if < 3 || d_fs < 3) {
           auto Fxi = [&](int j) { return flux_xi_f(S, i + j); };
           auto Fze = [&](int j) -> P2<R> {
@@ -309,6 +324,10 @@ struct Oracle {
           rvz = Sz / Jc;
           divx = xix * (xix * Sx + xiz * Sz) / (gxx * Jc);
           divz = xiz * (xix * Sx + xiz * Sz) / (gxx * Jc);
+          if (top) {
+            divzx = zex * (zex * Sx + zez * Sz) / (gzz * Jc);
+            divzz = zez * (zex * Sx + zez * Sz) / (gzz * Jc);
+          }
         } else {
           const R dpdx = dmac(dir, &S[FP][i], 1), dpdz = dmac(dir, &S[FP][i], nx);
           rvx = -(xix * dpdx + zex * dpdz);
@@ -316,6 +335,10 @@ struct Oracle {
           const R gxz = xix * zex + xiz * zez;
           divx = -xix * (gxx * dpdx + gxz * dpdz) / gxx;
           divz = -xiz * (gxx * dpdx + gxz * dpdz) / gxx;
+          if (top) {
+            divzx = -zex * (gxz * dpdx + gzz * dpdz) / gzz;
+            divzz = -zez * (gxz * dpdx + gzz * dpdz) / gzz;
+          }
         }
         const R rho = rf[i];
         R kvx = rvx / rho, kvz = rvz / rho;
@@ -328,22 +351,31 @@ struct Oracle {
           kvx += ((invb - R(1)) * divx - invb * V0) / rho;
           kvz += ((invb - R(1)) * divz - invb * V1) / rho;
         }
+        if (top) {
+          const R dpb = dpzf[iz] / bezf[iz], apdpb = alzf[iz] + dpb, invb = R(1) / bezf[iz];
+          const R V0 = S[FZVX][i], V1 = S[FZVZ][i];
+          Kk[FZVX][i] = -apdpb * V0 + dpb * divzx;
+          Kk[FZVZ][i] = -apdpb * V1 + dpb * divzz;
+          kvx += ((invb - R(1)) * divzx - invb * V0) / rho;
+          kvz += ((invb - R(1)) * divzz - invb * V1) / rho;
+        }
         Kk[FVX][i] = kvx;
         Kk[FVZ][i] = kvz;
       }
     }
   }
 
-  // Fluid pressure RHS (include/pml_fs_kernels.cuh:452-507).
+  // Fluid pressure RHS (include/pml_fs_kernels.cuh:452-507; CPML:
+  // include/cpml_kernels.cuh:345-415 - row 3 is an ordinary row, a top zeta band).
   void fluid_stress(int dir, const Set& S) {
 #pragma omp parallel for schedule(static)
     for (int iz = 3; iz < nzf; ++iz) {
       for (int ix = 3; ix <= nx - 4; ++ix) {
         const size_t i = size_t(iz) * nx + ix;
-        if (iz == 3) { Kk[FP][i] = 0; continue; }
+        if (!cpml && iz == 3) { Kk[FP][i] = 0; continue; }
         const R xix = xx[i], xiz = xz[i], zex = zx[i], zez = zz[i];
         const R dvxdx = dmac(dir, &S[FVX][i], 1), dvzdx = dmac(dir, &S[FVZ][i], 1);
-        const int dn = std::min(iz - 3, nzf - 1 - iz);
+        const int dn = cpml ? nzf - 1 - iz : std::min(iz - 3, nzf - 1 - iz);
         const R dvxdz = dz_near(dir, &S[FVX][i], nx, dn, false);
         const R dvzdz = dz_near(dir, &S[FVZ][i], nx, dn, false);
         const R Kc = K[i];
@@ -356,8 +388,21 @@ struct Oracle {
           const R E0 = S[FXEX][i], E1 = S[FXEZ][i];
           Kk[FXEX][i] = -apdpb * E0 + dpb * Dvx;
           Kk[FXEZ][i] = -apdpb * E1 + dpb * Dvz;
-          kp += Kc * (-(invb - R(1)) * xix * Dvx - (invb - R(1)) * xiz * Dvz +
-                      invb * xix * E0 + invb * xiz * E1);
+          if (cpml)
+            kp += -Kc * (invb - R(1)) * xix * Dvx - Kc * (invb - R(1)) * xiz * Dvz +
+                  invb * Kc * xix * E0 + invb * Kc * xiz * E1;
+          else
+            kp += Kc * (-(invb - R(1)) * xix * Dvx - (invb - R(1)) * xiz * Dvz +
+                        invb * xix * E0 + invb * xiz * E1);
+        }
+        if (cpml && iz <= npd + 2) {
+          const R gxz = xix * zex + xiz * zez, gzz = zex * zex + zez * zez;
+          const R Dzx = dvxdz + (gxz / gzz) * dvxdx, Dzz = dvzdz + (gxz / gzz) * dvzdx;
+          const R dpb = dpzf[iz] / bezf[iz], apdpb = alzf[iz] + dpb, invb = R(1) / bezf[iz];
+          const R E0 = S[FZEX][i], E1 = S[FZEZ][i];
+          Kk[FZEX][i] = -apdpb * E0 + dpb * Dzx;
+          Kk[FZEZ][i] = -apdpb * E1 + dpb * Dzz;
+          kp += Kc * (-(invb - R(1)) * (zex * Dzx + zez * Dzz) + invb * (zex * E0 + zez * E1));
         }
         Kk[FP][i] = kp;
       }
@@ -378,7 +423,10 @@ struct Oracle {
         const R c11 = C11[i], c13 = C13[i], c33 = C33[i], c55 = C55[i];
         R ksx = c11 * (xix * dvxdx + zex * dvxdz) + c13 * (xiz * dvzdx + zez * dvzdz);
         R ksz = c13 * (xix * dvxdx + zex * dvxdz) + c33 * (xiz * dvzdx + zez * dvzdz);
-        R ksxz = c55 * (xiz * dvxdx + zez * dvxdz + xix * dvzdx + zex * dvzdz);
+        // CPML reads this line's metric with the solid-local index i, i.e. at
+        // global row iz (include/cpml_kernels.cuh:448-455); kept for parity.
+        R ksxz = cpml ? c55 * (xz[i] * dvxdx + zz[i] * dvxdz + xx[i] * dvzdx + zx[i] * dvzdz)
+                      : c55 * (xiz * dvxdx + zez * dvxdz + xix * dvzdx + zex * dvzdz);
         const int distx = std::min(ix - 3, nx - 4 - ix);
         const bool side = distx < npd, bottom = iz >= nzs - 3 - npd;
         if (side || bottom) {
@@ -564,9 +612,11 @@ struct Oracle {
     jobs.clear();
     for (int f = 0; f < NFIELD; ++f) {
       const int rows = is_fluid(f) ? nzf : nzs;
-      const bool xstrip = (f >= FXVX && f <= SXEZ), zstrip = f >= SZVX;
+      const bool xstrip = (f >= FXVX && f <= SXEZ), zstrip = (f >= SZVX && f <= SZEZ);
+      const bool fzstrip = f >= FZVX;
       for (int r = 0; r < rows; ++r) {
         if (zstrip && r < nzs - 3 - npd) continue;
+        if (fzstrip && (!cpml || r < 3 || r > npd + 2)) continue;
         if (xstrip) jobs.push_back({f, r, 3, std::min(nx, 3 + npd), std::max(0, nx - 3 - npd), nx - 3});
         else jobs.push_back({f, r, 0, nx, 0, 0});
       }

@@ -28,7 +28,8 @@ class _Model(ctypes.Structure):
                 ("src_x", ctypes.c_int), ("src_z", ctypes.c_int),
                 ("K", _dp), ("rho_f", _dp),
                 ("C11", _dp), ("C13", _dp), ("C33", _dp), ("C55", _dp), ("rho_s", _dp),
-                ("J", _dp), ("xi_x", _dp), ("xi_z", _dp), ("ze_x", _dp), ("ze_z", _dp)]
+                ("J", _dp), ("xi_x", _dp), ("xi_z", _dp), ("ze_x", _dp), ("ze_z", _dp),
+                ("cpml", ctypes.c_int)]
 
 
 def build() -> str:
@@ -109,6 +110,7 @@ def _model_struct(model, shot=0, round_inputs=True):
     m.rho_s = arr(model.solid["rho"])
     m.J, m.xi_x, m.xi_z = arr(model.metric["J"]), arr(model.metric["xi_x"]), arr(model.metric["xi_z"])
     m.ze_x, m.ze_z = arr(model.metric["ze_x"]), arr(model.metric["ze_z"])
+    m.cpml = 1 if getattr(model, "boundary_type", 2) == 1 else 0
     return m, keep
 
 

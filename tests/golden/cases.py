@@ -47,6 +47,23 @@ def curvilinear_1200x800():
     return modelgen.curvilinear_1200x800(nt=6000)
 
 
+def cpml_flat_small():
+    """flat_small with CFS-PML on all four sides (boundary_type 1): a top PML band
+    in the fluid instead of the free surface (Cpml::FluidSolid); 400 steps, while
+    the wave is still in the grid (later the absorbed field is FP32 noise)."""
+    m = flat_small()
+    m.boundary_type = 1
+    m.nt = 400
+    return m
+
+
+def cpml_curv_small():
+    """curv_small with CFS-PML on all four sides (boundary_type 1)."""
+    m = curv_small()
+    m.boundary_type = 1
+    return m
+
+
 # name -> (builder, receiver stride kept in the fixture, keep final snapshot)
 CASES = {
     "flat_small": (flat_small, 1, True),
@@ -54,6 +71,8 @@ CASES = {
     "shallow_src": (shallow_src, 1, True),
     "flat_400x400": (flat_400x400, 8, False),
     "curvilinear_1200x800": (curvilinear_1200x800, 40, False),
+    "cpml_flat_small": (cpml_flat_small, 1, True),
+    "cpml_curv_small": (cpml_curv_small, 1, True),
 }
 
 

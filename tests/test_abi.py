@@ -106,7 +106,8 @@ def test_type_mismatch(lib, mfdm, small_model):
 
 def test_unsupported_configuration(lib, mfdm, small_model):
     _, j = small_model
-    _edit(j, lambda c: c["grid"].__setitem__("boundary_type", 1))
+    # Dirichlet boundaries (boundary_type 0) are not built; 1 and 2 are
+    _edit(j, lambda c: c["grid"].__setitem__("boundary_type", 0))
     rc, msg = _open(mfdm, j)
     assert rc == ERR["ARG"] and "unsupported" in msg
 

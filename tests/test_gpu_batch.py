@@ -36,8 +36,9 @@ def single_shot(lib, model, shot, nt):
         return s.records(), {n: s.field(n) for n in lib.FIELDS}
 
 
-def test_batch_matches_single_shots(lib, cases):
-    model = cases.curv_small()
+@pytest.mark.parametrize("case", ["curv_small", "cpml_curv_small"])
+def test_batch_matches_single_shots(lib, cases, case):
+    model = getattr(cases, case)()
     nt = 200
     with lib.Batch.from_model(model, SHOTS) as b:
         assert b.info()["nshots"] == len(SHOTS)

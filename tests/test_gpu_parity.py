@@ -5,7 +5,9 @@
 * against the CPU oracle (FP32 and FP64) on whole wavefields;
 * through size-independent properties at the 4096 x 2048 size (linearity,
   oracle agreement over a bounded number of steps);
-* the drop-in CLI's output tree and the multi-shot and error behaviour.
+* the drop-in CLI's output tree and the multi-shot and error behaviour;
+* the four-side CFS-PML variant (boundary_type 1, Cpml::FluidSolid) on its
+  own reference-build fixtures.
 
 Tolerance: relative L2 <= 1e-5 in FP32 (per record trace set / per field).
 """
@@ -20,7 +22,8 @@ from conftest import rel_l2
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-5
-ALL_CASES = ["flat_small", "curv_small", "shallow_src", "flat_400x400", "curvilinear_1200x800"]
+ALL_CASES = ["flat_small", "curv_small", "shallow_src", "flat_400x400", "curvilinear_1200x800",
+             "cpml_flat_small", "cpml_curv_small"]
 
 
 @pytest.fixture(scope="module")
@@ -80,7 +83,8 @@ def test_records_match_reference_build(lib, cases, name):
             assert e_ref <= TOL, (name, k, e_ref)
 
 
-@pytest.mark.parametrize("name", ["flat_small", "curv_small", "shallow_src"])
+@pytest.mark.parametrize("name", ["flat_small", "curv_small", "shallow_src", "cpml_flat_small",
+                                  "cpml_curv_small"])
 def test_all_fields_match_oracle(lib, oracle, cases, name):
     model = cases.CASES[name][0]()
     nt = model.nt

@@ -29,7 +29,8 @@ def _check_case(oracle, cases, name, nsteps=None, precision=32):
     return errs, out, g
 
 
-@pytest.mark.parametrize("name", ["flat_small", "curv_small", "shallow_src"])
+@pytest.mark.parametrize("name", ["flat_small", "curv_small", "shallow_src", "cpml_flat_small",
+                                  "cpml_curv_small"])
 def test_oracle_matches_reference_small(oracle, cases, name):
     errs, _, g = _check_case(oracle, cases, name)
     assert float(g["run_to_run_rel_l2"]) == 0.0
