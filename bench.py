@@ -214,15 +214,18 @@ def batched_shots(model, n: int, seed: int = 2):
 def batched_rate(mfdm, model, device: int, warmup: int, nshots: int = 64, steps: int = 300):
     """Shot-steps/s of one batch (one launch per RK stage for all shots) against
     the same shots run one after another through single-shot handles, device
-    time (CUDA events) over `steps` steps each."""
+    time (CUDA events) over `steps` steps each. Both arms pick their segment
+    height with the autotuner first."""
     import copy
     shots = batched_shots(model, nshots)
     with mfdm.Batch.from_model(model, shots, device=device) as b:
+        tile_b = b.autotune()
         b.step(warmup)
         tb, _ = b.time_steps(steps)
     loop_ms = 0.0
     m1 = copy.deepcopy(model)
     with mfdm.Solver.from_model(m1, device=device) as s1:
+        tile_1 = s1.autotune()
         for x, z, f, be in shots:
             m1.src_x, m1.src_z, m1.fpeak, m1.beta0 = [x], [z], f, be
             s1.load_model(m1)
@@ -235,7 +238,40 @@ def batched_rate(mfdm, model, device: int, warmup: int, nshots: int = 64, steps:
             "value": round(cells / (tb / 1e3) / 1e9, 3), "unit": "Gcell/s",
             "shot_steps_per_s": round(nshots * steps / (tb / 1e3), 1),
             "per_shot_loop_gcells": round(cells / (loop_ms / 1e3) / 1e9, 3),
-            "speedup_vs_per_shot_loop": round(loop_ms / tb, 3)}
+            "speedup_vs_per_shot_loop": round(loop_ms / tb, 3),
+            "seg_rows": {"batch": tile_b, "per_shot": tile_1}}
+
+
+def uneven_rate(mfdm, device: int, nmodels: int = 32, steps: int = 128):
+    """Cell-steps/s of `nmodels` layered models of seeded uneven sizes (nx
+    400..2000, nz 300..1000, seed 3) stepped together as one group (one
+    captured graph, the models on parallel branches) against the same models
+    stepped one after another, each through its own captured graph. Every model
+    gets its segment height from the autotuner first; device time (CUDA events)."""
+    models = modelgen.uneven_models(nmodels, seed=3, nt=10)
+    solvers = [mfdm.Solver.from_model(m, device=device) for m in models]
+    try:
+        tiles = [s.autotune() for s in solvers]
+        loop_ms = 0.0
+        for s in solvers:
+            s.set_shot(0, reset=True)
+            s.step(32)  # warm-up, graph capture
+            t, _ = s.time_steps(steps)
+            loop_ms += t
+        for s in solvers:
+            s.set_shot(0, reset=True)
+        with mfdm.Group(solvers) as g:
+            g.step(32)
+            tg = g.time_steps(steps)
+    finally:
+        for s in solvers:
+            s.close()
+    cells = sum(m.cells for m in models) * steps
+    return {"models": nmodels, "steps": steps, "cells": sum(m.cells for m in models),
+            "value": round(cells / (tg / 1e3) / 1e9, 3), "unit": "Gcell/s",
+            "model_loop_gcells": round(cells / (loop_ms / 1e3) / 1e9, 3),
+            "speedup_vs_model_loop": round(loop_ms / tg, 3),
+            "seg_rows": {str(r): tiles.count(r) for r in sorted(set(tiles))}}
 
 
 def main():
@@ -342,6 +378,7 @@ def main():
                 "value": round(small.cells * n2 / (t2 / 1e3) / 1e9, 3), "unit": "Gcell/s",
                 "ms_per_step": round(t2 / n2, 4)}
         other["batched_1200x800_64_shots"] = batched_rate(mfdm, small, local, args.warmup)
+        other["uneven_32_models"] = uneven_rate(mfdm, local)
 
     clocks = clk.summary()
     solver.close()

@@ -70,6 +70,7 @@ typedef struct mfdm_info {
   long long cells;                /* nx * (nz_f + nz_s): cells updated per step */
   long long device_bytes;         /* device memory held by the handle */
   int nshots;                     /* shots stepped together (1 unless opened with mfdm_open_batch) */
+  int seg_rows;                   /* rows per segment block of the stage launches */
 } mfdm_info;
 
 /* Field ids for mfdm_get_field / mfdm_set_field. */
@@ -172,6 +173,41 @@ int mfdm_batch_reset(mfdm_model* m);
 int mfdm_batch_get_records(mfdm_model* m, int shot, int first, int count, float* svx, float* svz,
                            float* fp);
 int mfdm_batch_get_field(mfdm_model* m, int shot, int field, float* host);
+
+/* ---- tile shape ---------------------------------------------------------
+ * A stage launch covers each medium with segment blocks of 64 columns by
+ * `seg_rows` rows. Small grids want short segments (more blocks than SMs),
+ * large ones long segments (fewer halo re-reads). The reference launches
+ * fixed 16x16 blocks (src/pml_fs_kernels.cu:533-622) and has no tuner. */
+
+/* Sets the segment height: a multiple of 4 in [4, 128], or 0 for the default
+ * (24). Results do not depend on it beyond FP32 rounding of the last bit. */
+int mfdm_set_tile(mfdm_model* m, int seg_rows);
+
+/* Times every candidate segment height on this handle's model and shots
+ * (a few steps each, CUDA events on the handle's stream), keeps the fastest and
+ * writes it to *seg_rows (may be NULL). The choice is cached per device, grid
+ * shape, PML width, boundary type and shot count, so a second handle of the
+ * same shape is not timed again. The timing steps change the state: on return
+ * every shot is back at rest at step 0 with its records cleared, as after
+ * mfdm_set_shot(m, shot, 1) or mfdm_batch_reset. */
+int mfdm_autotune(mfdm_model* m, int* seg_rows);
+
+/* ---- groups of models ---------------------------------------------------
+ * Models of different grid sizes (plain or batched handles, one device)
+ * stepped together: every step of every model is one node of one captured
+ * CUDA graph, the models on parallel branches, so small models fill the GPU
+ * together and the host issues one graph launch per 32 steps of all of them.
+ * The reference runs one model per process. */
+typedef struct mfdm_group mfdm_group;
+/* Groups `n` open handles (not owned; they must outlive the group). */
+int mfdm_group_open(mfdm_model* const* models, int n, mfdm_group** out);
+/* Advances every model by `nsteps` (all must be at the same time index), then
+ * synchronises and checks each model's non-finite flag. */
+int mfdm_group_step(mfdm_group* g, int nsteps);
+/* As mfdm_group_step, reporting the device time of the whole run (ms). */
+int mfdm_group_time_steps(mfdm_group* g, int nsteps, float* total_ms);
+int mfdm_group_close(mfdm_group* g);
 
 /* The drop-in command line: `main_debug <model.json> <out_root>`
  * (src/main.cu:58-216). Clears out_root, runs every shot and writes

@@ -34,7 +34,8 @@ EXPORTS = ("mfdm_last_error", "mfdm_open_json", "mfdm_open_desc", "mfdm_load_des
            "mfdm_get_info", "mfdm_set_shot", "mfdm_update_rk4", "mfdm_step", "mfdm_time_steps",
            "mfdm_synchronize", "mfdm_get_records", "mfdm_get_field", "mfdm_set_field",
            "mfdm_run_cli", "mfdm_step_noalloc", "mfdm_open_batch", "mfdm_batch_reset",
-           "mfdm_batch_get_records", "mfdm_batch_get_field")
+           "mfdm_batch_get_records", "mfdm_batch_get_field", "mfdm_set_tile", "mfdm_autotune",
+           "mfdm_group_open", "mfdm_group_step", "mfdm_group_time_steps", "mfdm_group_close")
 
 
 class MfdmError(RuntimeError):
@@ -66,7 +67,7 @@ class Info(ctypes.Structure):
                 ("gap", ctypes.c_int), ("nsrc", ctypes.c_int), ("shot", ctypes.c_int),
                 ("step", ctypes.c_int), ("nsamples", ctypes.c_int),
                 ("cells", ctypes.c_longlong), ("device_bytes", ctypes.c_longlong),
-                ("nshots", ctypes.c_int)]
+                ("nshots", ctypes.c_int), ("seg_rows", ctypes.c_int)]
 
 
 class Shot(ctypes.Structure):
@@ -124,6 +125,12 @@ def load_library(path: str = LIB_PATH):
         "mfdm_batch_get_records": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                   _fp, _fp, _fp]),
         "mfdm_batch_get_field": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, _fp]),
+        "mfdm_set_tile": (ctypes.c_int, [vp, ctypes.c_int]),
+        "mfdm_autotune": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int)]),
+        "mfdm_group_open": (ctypes.c_int, [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]),
+        "mfdm_group_step": (ctypes.c_int, [vp, ctypes.c_int]),
+        "mfdm_group_time_steps": (ctypes.c_int, [vp, ctypes.c_int, _fp]),
+        "mfdm_group_close": (ctypes.c_int, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -246,6 +253,18 @@ class Solver:
     def synchronize(self):
         _check(self._lib.mfdm_synchronize(self._h))
 
+    # -- tile shape -----------------------------------------------------------
+    def set_tile(self, seg_rows: int):
+        """Rows per segment block of the stage launches (multiple of 4 in [4, 128]; 0: 24)."""
+        _check(self._lib.mfdm_set_tile(self._h, int(seg_rows)))
+
+    def autotune(self) -> int:
+        """Times the candidate segment heights, keeps the fastest and returns it.
+        Leaves every shot at rest at step 0 (mfdm_autotune)."""
+        seg = ctypes.c_int()
+        _check(self._lib.mfdm_autotune(self._h, ctypes.byref(seg)))
+        return seg.value
+
     # -- data out -----------------------------------------------------------
     def records(self, first: int = 0, count: Optional[int] = None) -> Dict[str, np.ndarray]:
         info = self.info()
@@ -314,6 +333,45 @@ class Batch(Solver):
         out = np.zeros((rows, info["nx"]), dtype=np.float32)
         _check(self._lib.mfdm_batch_get_field(self._h, int(shot), fid, out.ctypes.data_as(_fp)))
         return out
+
+
+class Group:
+    """Models of different sizes stepped together through one captured graph
+    (mfdm_group_*). The solvers stay owned by the caller and must stay open."""
+
+    def __init__(self, solvers):
+        self._lib = load_library()
+        self._solvers = list(solvers)
+        arr = (ctypes.c_void_p * len(self._solvers))(*[s._h for s in self._solvers])
+        h = ctypes.c_void_p()
+        _check(self._lib.mfdm_group_open(arr, len(self._solvers), ctypes.byref(h)))
+        self._h = h
+
+    def step(self, nsteps: int):
+        _check(self._lib.mfdm_group_step(self._h, int(nsteps)))
+
+    def time_steps(self, nsteps: int) -> float:
+        """Steps every model and returns the device time of the whole run (ms)."""
+        total = ctypes.c_float()
+        _check(self._lib.mfdm_group_time_steps(self._h, int(nsteps), ctypes.byref(total)))
+        return total.value
+
+    def close(self):
+        if self._h:
+            self._lib.mfdm_group_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def step_noalloc(dm: DeviceModel, it: int, nsteps: int, stream: Optional[int] = None):

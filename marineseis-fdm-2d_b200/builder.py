@@ -62,7 +62,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
         subprocess.run(cmd, check=True)
     os.makedirs(os.path.dirname(CLI), exist_ok=True)
     if force or _stale(CLI, [LIB, os.path.join(CSRC, "main_debug.cpp")]):
-        cmd = [nvcc, "-O2", "-std=c++17", os.path.join(CSRC, "main_debug.cpp"), "-L" + HERE,
+        cmd = [nvcc] + ARCH + ["-O2", "-std=c++17", os.path.join(CSRC, "main_debug.cpp"), "-L" + HERE,
                "-lmfdm", "-Xlinker", "-rpath=$ORIGIN/..", "-o", CLI]
         if verbose:
             print(" ".join(cmd))

@@ -85,7 +85,9 @@ struct Coef {
   unsigned* done;                   // block arrival counter of the finish kernel
   float* ipre;                      // interface rows before the filter [8][P]
   int* status;                      // sticky error word (non-finite detector)
-  // Shots stepped together (blockIdx.y of the step kernels). Every per-shot
+  int seg;                          // rows per segment block of the stage launches (0: 24)
+  // Shots stepped together (the stage launch's fastest block index, blockIdx.y
+  // of the finish kernel). Every per-shot
   // buffer of shot b sits b strides after shot 0's: the RK sets, ADE strips,
   // PML tables and interface rows (shot_stride), the Ricker table (src_stride)
   // and the receiver rows (rec_stride), all in floats.

@@ -18,6 +18,8 @@
 #include <fstream>
 #include <iomanip>
 #include <iostream>
+#include <map>
+#include <mutex>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -120,6 +122,7 @@ struct mfdm_model {
   float* d_rec = nullptr;
   int rec_cap = 0;
   cudaGraphExec_t graph = nullptr;
+  unsigned gen = 0;  // bumped whenever captured launches go stale (groups recapture)
   // TMA descriptors: per RK set (U, A, B, acc) the stencil box and the
   // point-wise box of the fluid and solid blocks, and the coefficient blocks.
   CUtensorMap fst[4], sst[4], fpw[4], spw[4], fco, sco;
@@ -300,6 +303,7 @@ int encode_block(CUtensorMap* map, const float* base, int P, int rows, int nf, i
 }
 
 void release_graph(mfdm_model* m) {
+  ++m->gen;
   if (m->graph) {
     cudaGraphExecDestroy(m->graph);
     m->graph = nullptr;
@@ -855,6 +859,7 @@ int mfdm_get_info(const mfdm_model* m, mfdm_info* info) {
   info->device_bytes = (long long)m->dbytes + (long long)m->nshots * m->src_steps * 16 +
                        (long long)m->nshots * m->rec_cap * 12 * m->cfg.nx;
   info->nshots = m->nshots;
+  info->seg_rows = mfdm::stage_seg_rows(m->C);
   return MFDM_OK;
 }
 
@@ -986,6 +991,272 @@ int mfdm_batch_get_records(mfdm_model* m, int shot, int first, int count, float*
 int mfdm_batch_get_field(mfdm_model* m, int shot, int field, float* host) {
   if (!m) return fail(MFDM_ERR_ARG, "null handle");
   return get_field(m, shot, field, host);
+}
+
+int mfdm_set_tile(mfdm_model* m, int seg_rows) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  if (seg_rows != 0 && (seg_rows < 4 || seg_rows > 128 || seg_rows % 4 != 0))
+    return fail(MFDM_ERR_ARG, "segment rows must be a multiple of 4 in [4, 128] (0: default)");
+  DeviceGuard g(m->device);
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  m->C.seg = seg_rows;
+  release_graph(m);  // the segment height is baked into the captured launches
+  return MFDM_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+const int kSegCandidates[] = {8, 12, 16, 24, 32, 48};
+
+std::mutex g_tune_mu;
+std::map<std::vector<int>, int> g_tune;  // (device, nx, nz_f, nz_s, npd, bdy, nshots) -> rows
+
+// Device time of one captured kGraphSteps-step replay with `seg` rows per segment
+// (after one untimed replay that also captures the graph).
+int time_segment_rows(mfdm_model* m, int seg, float* ms) {
+  m->C.seg = seg;
+  release_graph(m);
+  int rc;
+  if ((rc = enqueue_steps(m, kGraphSteps)) != MFDM_OK) return rc;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  MFDM_CU(cudaEventCreate(&e0));
+  struct Free { cudaEvent_t *a, *b; ~Free() { cudaEventDestroy(*a); if (*b) cudaEventDestroy(*b); } } fr{&e0, &e1};
+  MFDM_CU(cudaEventCreate(&e1));
+  MFDM_CU(cudaEventRecord(e0, m->stream));
+  if ((rc = enqueue_steps(m, kGraphSteps)) != MFDM_OK) return rc;
+  MFDM_CU(cudaEventRecord(e1, m->stream));
+  MFDM_CU(cudaEventSynchronize(e1));
+  MFDM_CU(cudaEventElapsedTime(ms, e0, e1));
+  return check_status(m);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mfdm_autotune(mfdm_model* m, int* seg_rows) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  DeviceGuard g(m->device);
+  const HostModel& h = m->cfg;
+  const std::vector<int> key = {m->device, h.nx, h.nzf, h.nzs, h.npd, h.bdy, m->nshots};
+  int best = 0;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) best = it->second;
+  }
+  int rc;
+  if (best == 0) {
+    // from rest at step 0, so no state of the caller's is stepped
+    if ((rc = clear_state(m)) != MFDM_OK) return rc;
+    if ((rc = rewind(m)) != MFDM_OK) return rc;
+    const int n = int(sizeof(kSegCandidates) / sizeof(int));
+    if ((rc = ensure_capacity(m, 2 * kGraphSteps * n)) != MFDM_OK) return rc;
+    float best_ms = 0.f;
+    for (int i = 0; i < n; ++i) {
+      float ms = 0.f;
+      if ((rc = time_segment_rows(m, kSegCandidates[i], &ms)) != MFDM_OK) return rc;
+      if (best == 0 || ms < best_ms) {
+        best = kSegCandidates[i];
+        best_ms = ms;
+      }
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[key] = best;
+  }
+  m->C.seg = best;
+  release_graph(m);
+  if ((rc = clear_state(m)) != MFDM_OK) return rc;
+  if ((rc = rewind(m)) != MFDM_OK) return rc;
+  if (seg_rows) *seg_rows = best;
+  return MFDM_OK;
+}
+
+}  // extern "C"
+
+// ---- groups of models ---------------------------------------------------------
+
+struct mfdm_group {
+  int device = 0;
+  std::vector<mfdm_model*> ms;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t graph = nullptr;
+  std::vector<unsigned> gens;  // model generations the graph was captured from
+};
+
+namespace {
+
+void group_destroy(mfdm_group* g) {
+  if (!g) return;
+  DeviceGuard d(g->device);
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  if (g->graph) cudaGraphExecDestroy(g->graph);
+  for (cudaEvent_t e : g->join)
+    if (e) cudaEventDestroy(e);
+  if (g->fork) cudaEventDestroy(g->fork);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  delete g;
+}
+
+// Enqueues `k` steps of every model on the model's own stream, forked from and
+// joined back into the group stream (the models run concurrently). `graph`:
+// graph-step indices 0..k-1 (captured), else the models' own time indices.
+int group_enqueue(mfdm_group* g, int k, bool graph) {
+  MFDM_CU(cudaEventRecord(g->fork, g->stream));
+  for (size_t i = 0; i < g->ms.size(); ++i) {
+    mfdm_model* m = g->ms[i];
+    MFDM_CU(cudaStreamWaitEvent(m->stream, g->fork, 0));
+    for (int j = 0; j < k; ++j) {
+      const int rc = enqueue_step(m, graph ? j : m->host_step + j, m->stream);
+      if (rc != MFDM_OK) return rc;
+    }
+    MFDM_CU(cudaEventRecord(g->join[i], m->stream));
+    MFDM_CU(cudaStreamWaitEvent(g->stream, g->join[i], 0));
+  }
+  return MFDM_OK;
+}
+
+int group_capture(mfdm_group* g) {
+  if (g->graph) {
+    cudaGraphExecDestroy(g->graph);
+    g->graph = nullptr;
+  }
+  cudaGraph_t gr = nullptr;
+  MFDM_CU(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+  const int rc = group_enqueue(g, kGraphSteps, true);
+  cudaError_t e = cudaStreamEndCapture(g->stream, &gr);
+  if (rc != MFDM_OK) {
+    if (gr) cudaGraphDestroy(gr);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(MFDM_ERR_CUDA, std::string("group capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&g->graph, gr, 0);
+  cudaGraphDestroy(gr);
+  if (e != cudaSuccess)
+    return fail(MFDM_ERR_CUDA, std::string("group instantiate: ") + cudaGetErrorString(e));
+  g->gens.clear();
+  for (mfdm_model* m : g->ms) g->gens.push_back(m->gen);
+  return MFDM_OK;
+}
+
+int group_run(mfdm_group* g, int nsteps) {
+  if (nsteps < 0) return fail(MFDM_ERR_ARG, "negative step count");
+  const int t0 = g->ms[0]->host_step;
+  int rc;
+  for (mfdm_model* m : g->ms)
+    if (m->host_step != t0) return fail(MFDM_ERR_ARG, "grouped models are at different time indices");
+  // buffer growth enqueues on the model streams; a graph launched on the
+  // group stream would not wait for it
+  for (mfdm_model* m : g->ms) {
+    if ((rc = ensure_capacity(m, t0 + nsteps)) != MFDM_OK) return rc;
+    MFDM_CU(cudaStreamSynchronize(m->stream));
+  }
+  while (nsteps > 0) {
+    const int step = g->ms[0]->host_step;
+    int k = 1;
+    if ((step & 1) == 0 && nsteps >= kGraphSteps) {
+      bool stale = !g->graph;
+      for (size_t i = 0; i < g->ms.size() && !stale; ++i) stale = g->gens[i] != g->ms[i]->gen;
+      if (stale && (rc = group_capture(g)) != MFDM_OK) return rc;
+      MFDM_CU(cudaGraphLaunch(g->graph, g->stream));
+      k = kGraphSteps;
+    } else if ((rc = group_enqueue(g, 1, false)) != MFDM_OK) {
+      return rc;
+    }
+    for (mfdm_model* m : g->ms) m->host_step += k;
+    nsteps -= k;
+  }
+  return MFDM_OK;
+}
+
+int group_check(mfdm_group* g) {
+  MFDM_CU(cudaStreamSynchronize(g->stream));
+  for (mfdm_model* m : g->ms) {
+    const int rc = check_status(m);
+    if (rc != MFDM_OK) return rc;
+  }
+  return MFDM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mfdm_group_open(mfdm_model* const* models, int n, mfdm_group** out) {
+  if (!out) return fail(MFDM_ERR_ARG, "null output handle");
+  *out = nullptr;
+  if (!models || n <= 0) return fail(MFDM_ERR_ARG, "a group needs at least one model");
+  mfdm_group* g = new mfdm_group();
+  g->device = models[0] ? models[0]->device : 0;
+  for (int i = 0; i < n; ++i) {
+    if (!models[i]) {
+      delete g;
+      return fail(MFDM_ERR_ARG, "null model handle in group");
+    }
+    if (models[i]->device != g->device) {
+      delete g;
+      return fail(MFDM_ERR_ARG, "grouped models must be on one device");
+    }
+    for (int j = 0; j < i; ++j)
+      if (models[j] == models[i]) {
+        delete g;
+        return fail(MFDM_ERR_ARG, "a model appears twice in the group");
+      }
+    g->ms.push_back(models[i]);
+  }
+  DeviceGuard d(g->device);
+  auto cu = [&](cudaError_t e) {
+    if (e == cudaSuccess) return true;
+    fail(MFDM_ERR_CUDA, std::string("group setup: ") + cudaGetErrorString(e));
+    return false;
+  };
+  bool ok = cu(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking)) &&
+            cu(cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming));
+  g->join.assign(size_t(n), nullptr);
+  for (int i = 0; ok && i < n; ++i) ok = cu(cudaEventCreateWithFlags(&g->join[size_t(i)], cudaEventDisableTiming));
+  if (!ok) {
+    const std::string msg = g_err;
+    group_destroy(g);
+    g_err = msg;
+    return MFDM_ERR_CUDA;
+  }
+  *out = g;
+  return MFDM_OK;
+}
+
+int mfdm_group_step(mfdm_group* g, int nsteps) {
+  if (!g) return fail(MFDM_ERR_ARG, "null group");
+  DeviceGuard d(g->device);
+  const int rc = group_run(g, nsteps);
+  if (rc != MFDM_OK) return rc;
+  return group_check(g);
+}
+
+int mfdm_group_time_steps(mfdm_group* g, int nsteps, float* total_ms) {
+  if (!g || !total_ms) return fail(MFDM_ERR_ARG, "null argument");
+  DeviceGuard d(g->device);
+  cudaEvent_t e[2] = {};
+  MFDM_CU(cudaEventCreate(&e[0]));
+  struct Free { cudaEvent_t* e; ~Free() { for (int i = 0; i < 2; ++i) if (e[i]) cudaEventDestroy(e[i]); } } fr{e};
+  MFDM_CU(cudaEventCreate(&e[1]));
+  // every model's earlier work first, so the timed region holds only these steps
+  for (mfdm_model* m : g->ms) MFDM_CU(cudaStreamSynchronize(m->stream));
+  MFDM_CU(cudaEventRecord(e[0], g->stream));
+  const int rc = group_run(g, nsteps);
+  if (rc != MFDM_OK) return rc;
+  MFDM_CU(cudaEventRecord(e[1], g->stream));
+  MFDM_CU(cudaEventSynchronize(e[1]));
+  MFDM_CU(cudaEventElapsedTime(total_ms, e[0], e[1]));
+  return group_check(g);
+}
+
+int mfdm_group_close(mfdm_group* g) {
+  group_destroy(g);
+  return MFDM_OK;
 }
 
 int mfdm_set_field(mfdm_model* m, int field, const float* host) {

@@ -10,12 +10,15 @@
 // device step counter. Reference: src/pml_fs_kernels.cu:533-868.
 //
 // Block roles inside one stage launch (blockIdx.x ranges):
-//   [0, nbf)          fluid segments: a 64-column strip of up to kSeg (24) fluid rows
-//                     (rows 3..nz_f-2)
-//   [nbf, nbf+nbs)    solid segments: the same over solid rows 1..nz_s-4
-//   [nbf+nbs, ...)    interface strip: one thread per column, fluid row nz_f-1
+//   [0, nbi)          interface strip: one thread per column, fluid row nz_f-1
 //                     and solid row 0 together, so the normal/tangential
 //                     coupling happens in registers.
+//   [nbi, nbi+nbf)    fluid segments: a 64-column strip of up to `seg` fluid rows
+//                     (rows 3..nz_f-2; seg is 24 unless tuned per model)
+//   [nbi+nbf, ...)    solid segments: the same over solid rows 1..nz_s-4
+// With several shots the launch is one-dimensional with the shot fastest
+// (blockIdx.x = block * nshots + shot), so the shots of one segment run side
+// by side and all but the first read the segment's coefficients from L2.
 //
 // A segment block is a producer/consumer pipeline. Lane 0 of warp 8 streams the
 // segment down in chunks of kR rows with 3-D TMA boxes (cp.async.bulk.tensor)
@@ -49,10 +52,7 @@ constexpr int kNP = MFDM_PW_SLOTS;        // point-wise chunk slots
 constexpr int kRing = kR * kNS;          // ring rows
 constexpr int kConsumers = 256;          // warps 0-7
 constexpr int kThreads = kConsumers + 32;  // + producer warp
-#ifndef MFDM_SEG_ROWS
-#define MFDM_SEG_ROWS 24
-#endif
-constexpr int kSeg = MFDM_SEG_ROWS;      // rows per segment block
+constexpr int kSeg = 24;                 // default rows per segment block
 constexpr int kBarBytes = 256;           // full/empty barriers of both rings
 constexpr int kFinishThreads = 256;      // filter / receiver kernel
 
@@ -263,13 +263,13 @@ template <int DIR, int KIND, bool CPML>
 __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, const Fields& out,
                                               const Fields& un, const Fields& acc,
                                               const StageMaps& maps, int s, float cc, float w,
-                                              int blk, int ntx, char* smem) {
+                                              int blk, int ntx, int seg, int shot, char* smem) {
   constexpr int NST = 3, NCOEF = 6, NPW = PW<NST, NCOEF, KIND>::n;
   const int P = C.P, nx = C.nx;
   Segment sg;
   sg.x0 = (blk % ntx) * kTX;
-  sg.z0 = 3 + (blk / ntx) * kSeg;
-  sg.z1 = min(sg.z0 + kSeg, C.nzf - 1);
+  sg.z0 = 3 + (blk / ntx) * seg;
+  sg.z1 = min(sg.z0 + seg, C.nzf - 1);
   sg.rows = C.nzf;
   sg.nch = (sg.z1 - sg.z0 + kR - 1) / kR;
   Bars B;
@@ -278,7 +278,7 @@ __device__ __forceinline__ void fluid_segment(const Coef& C, const Fields& in, c
   const int it = __ldg(C.step);
   if (threadIdx.x >= kConsumers) {
     produce<NST, NCOEF, KIND>(sg, &maps.fin, &maps.fcoef, &maps.fun, &maps.facc, ring, slots, B,
-                              C.status, blockIdx.y);
+                              C.status, shot);
     return;
   }
   const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
@@ -363,13 +363,13 @@ template <int DIR, int KIND, bool CPML>
 __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, const Fields& out,
                                               const Fields& un, const Fields& acc,
                                               const StageMaps& maps, float cc, float w, int blk,
-                                              int ntx, char* smem) {
+                                              int ntx, int seg, int shot, char* smem) {
   constexpr int NST = 5, NCOEF = 9, NPW = PW<NST, NCOEF, KIND>::n;
   const int P = C.P, nx = C.nx, npd = C.npd, nzs = C.nzs;
   Segment sg;
   sg.x0 = (blk % ntx) * kTX;
-  sg.z0 = 1 + (blk / ntx) * kSeg;
-  sg.z1 = min(sg.z0 + kSeg, nzs - 3);
+  sg.z0 = 1 + (blk / ntx) * seg;
+  sg.z1 = min(sg.z0 + seg, nzs - 3);
   sg.rows = nzs;
   sg.nch = (sg.z1 - sg.z0 + kR - 1) / kR;
   Bars B;
@@ -377,7 +377,7 @@ __device__ __forceinline__ void solid_segment(const Coef& C, const Fields& in, c
   segment_setup<NST>(smem, B, ring, slots);
   if (threadIdx.x >= kConsumers) {
     produce<NST, NCOEF, KIND>(sg, &maps.sin, &maps.scoef, &maps.sun, &maps.sacc, ring, slots, B,
-                              C.status, blockIdx.y);
+                              C.status, shot);
     return;
   }
   const int tx = threadIdx.x % kTX, ty = threadIdx.x / kTX;
@@ -572,20 +572,23 @@ template <int DIR, int KIND, bool CPML>
 __global__ void __launch_bounds__(kThreads, 2)
     stage_kernel(Coef C0, Fields in0, Fields out0, Fields un0, Fields acc0,
                  const __grid_constant__ StageMaps maps, int s, float cc, float w, int ntx,
-                 int nbi, int nbf, int nbs) {
+                 int nbi, int nbf, int nbs, int seg, int nshots) {
   extern __shared__ char smem[];
-  // this block's shot (blockIdx.y): its own state, tables and buffers
-  const size_t so = size_t(blockIdx.y) * C0.shot_stride;
-  const Coef C = shot_coef(C0, blockIdx.y);
+  // this block's shot (the fastest index): its own state, tables and buffers
+  const int shot = int(blockIdx.x % unsigned(nshots));
+  const int b = int(blockIdx.x / unsigned(nshots));
+  const size_t so = size_t(shot) * C0.shot_stride;
+  const Coef C = shot_coef(C0, shot);
   const Fields in = shot_fields(in0, so), out = shot_fields(out0, so), un = shot_fields(un0, so),
                acc = shot_fields(acc0, so);
-  const int b = blockIdx.x;
   if (b < nbi) {  // first, so the short interface blocks overlap the segments
     interface_strip<DIR, KIND, CPML>(C, in, out, un, acc, cc, w, b);
   } else if (b < nbi + nbf) {
-    fluid_segment<DIR, KIND, CPML>(C, in, out, un, acc, maps, s, cc, w, b - nbi, ntx, smem);
+    fluid_segment<DIR, KIND, CPML>(C, in, out, un, acc, maps, s, cc, w, b - nbi, ntx, seg, shot,
+                                   smem);
   } else {
-    solid_segment<DIR, KIND, CPML>(C, in, out, un, acc, maps, cc, w, b - nbi - nbf, ntx, smem);
+    solid_segment<DIR, KIND, CPML>(C, in, out, un, acc, maps, cc, w, b - nbi - nbf, ntx, seg, shot,
+                                   smem);
   }
 }
 
@@ -688,12 +691,14 @@ static size_t smem_for_kind() {
 
 size_t stage_smem_bytes() { return smem_for_kind<kStageMid>(); }
 
-void stage_grid(int nx, int nzf, int nzs, int* ntx, int* nbf, int* nbs, int* nbi) {
+int stage_seg_rows(const Coef& C) { return C.seg > 0 ? C.seg : kSeg; }
+
+void stage_grid(int nx, int nzf, int nzs, int seg, int* ntx, int* nbf, int* nbs, int* nbi) {
   *ntx = (nx + kTX - 1) / kTX;
   const int frows = nzf - 1 - 3;  // fluid rows 3..nz_f-2
   const int srows = nzs - 4;      // solid rows 1..nz_s-4
-  *nbf = frows > 0 ? *ntx * ((frows + kSeg - 1) / kSeg) : 0;
-  *nbs = srows > 0 ? *ntx * ((srows + kSeg - 1) / kSeg) : 0;
+  *nbf = frows > 0 ? *ntx * ((frows + seg - 1) / seg) : 0;
+  *nbs = srows > 0 ? *ntx * ((srows + seg - 1) / seg) : 0;
   *nbi = (nx + kConsumers - 1) / kConsumers;
 }
 
@@ -701,11 +706,12 @@ template <int DIR, int KIND, bool CPML>
 static cudaError_t launch_one(const Coef& C, const Fields& in, const Fields& out, const Fields& un,
                               const Fields& acc, const StageMaps& maps, int s, cudaStream_t st) {
   int ntx, nbf, nbs, nbi;
-  stage_grid(C.nx, C.nzf, C.nzs, &ntx, &nbf, &nbs, &nbi);
+  const int seg = stage_seg_rows(C), nshots = C.nshots > 0 ? C.nshots : 1;
+  stage_grid(C.nx, C.nzf, C.nzs, seg, &ntx, &nbf, &nbs, &nbi);
   const float cc = C.rk_c[s], w = (KIND == kStageLast) ? 0.f : C.rk_w[s];
-  const dim3 grid(unsigned(nbi + nbf + nbs), unsigned(C.nshots > 0 ? C.nshots : 1));
+  const unsigned grid = unsigned(nbi + nbf + nbs) * unsigned(nshots);
   stage_kernel<DIR, KIND, CPML><<<grid, kThreads, smem_for_kind<KIND>(), st>>>(
-      C, in, out, un, acc, maps, s, cc, w, ntx, nbi, nbf, nbs);
+      C, in, out, un, acc, maps, s, cc, w, ntx, nbi, nbf, nbs, seg, nshots);
   return cudaGetLastError();
 }
 

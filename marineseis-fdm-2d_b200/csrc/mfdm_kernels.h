@@ -23,8 +23,11 @@ cudaError_t launch_reciprocal(float* a, int rows, int nx, int P, cudaStream_t st
 cudaError_t launch_set_step(const Coef& C, int it, cudaStream_t st);
 // Dynamic shared memory of one stage block.
 size_t stage_smem_bytes();
-// Block counts of one stage launch: column tiles, fluid tiles, solid tiles, interface blocks.
-void stage_grid(int nx, int nzf, int nzs, int* ntx, int* nbf, int* nbs, int* nbi);
+// Rows per segment block of a stage launch (C.seg, or the default 24 when unset).
+int stage_seg_rows(const Coef& C);
+// Block counts of one stage launch (per shot) with `seg` rows per segment:
+// column tiles, fluid tiles, solid tiles, interface blocks.
+void stage_grid(int nx, int nzf, int nzs, int seg, int* ntx, int* nbf, int* nbs, int* nbi);
 // Uploads the 5x5 source weights and the 7-point interface filter weights.
 cudaError_t upload_constants(const float* srcw25, const float* w7);
 

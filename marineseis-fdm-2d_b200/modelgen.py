@@ -246,6 +246,51 @@ def curvilinear(nx: int, nz: int, *, zeta0: Optional[int] = None, nt: int = 6000
                       perturb=perturb, corr_len=50.0, seed=seed)
 
 
+def layered(nx: int, nz: int, *, seed: int, nt: int = 2000, dt: float = 3e-4,
+            vp_range=(1500.0, 4500.0), max_layers: int = 6) -> Model:
+    """Water over a seeded stack of flat-lying solid layers (2..max_layers), vp
+    rising with depth inside ``vp_range``, vs = vp / sqrt(3), Gardner density
+    rho = 310 vp^0.25 (kg/m^3, vp in m/s), on a gently undulating seafloor
+    (0..30 m amplitude) between 30% and 60% of the depth. dt = 0.3 ms keeps
+    vp dt / h <= 0.27 at vp = 4500 m/s and h = 5 m."""
+    rng = np.random.default_rng(seed)
+    zeta0 = int(rng.integers(int(0.3 * nz), int(0.6 * nz) + 1))
+    nz_f = zeta0 + 1
+    nz_s = nz - nz_f + 1
+    amp = float(rng.uniform(0.0, 30.0))
+    m = make_model(nx, nz_f, nz_s, h=5.0, npd=20, fpeak=15.0, dt=dt, nt=nt,
+                   src_x=[int(rng.integers(nx // 4, 3 * nx // 4))], src_z=[zeta0 - 10],
+                   amp=amp, wavelength=600.0)
+    nl = int(rng.integers(2, max_layers + 1))
+    tops = np.sort(rng.choice(np.arange(1, nz_s - 1), size=nl - 1, replace=False))
+    vps = np.sort(rng.uniform(max(vp_range[0], 1800.0), vp_range[1], size=nl))
+    vp = np.empty((nz_s, nx))
+    for k, v in enumerate(vps):
+        lo = 0 if k == 0 else tops[k - 1]
+        hi = nz_s if k == nl - 1 else tops[k]
+        vp[lo:hi] = v
+    vs = vp / math.sqrt(3.0)
+    rho = 310.0 * vp ** 0.25
+    mu = rho * vs ** 2
+    lam = rho * (vp ** 2 - 2.0 * vs ** 2)
+    m.solid = {"C11": lam + 2.0 * mu, "C13": lam, "C33": lam + 2.0 * mu, "C55": mu, "rho": rho}
+    m.vp_max = float(max(vps.max(), vp_range[0]))
+    m.beta0 = beta0_rule(m, m.fpeak)
+    return m
+
+
+def uneven_models(n: int = 32, seed: int = 3, nt: int = 2000) -> List[Model]:
+    """``n`` layered models of seeded uneven sizes, nx in [400, 2000] and nz in
+    [300, 1000] (multiples of 8)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        nx = int(rng.integers(50, 251)) * 8
+        nz = int(rng.integers(38, 126)) * 8
+        out.append(layered(nx, nz, seed=seed * 1000 + k, nt=nt))
+    return out
+
+
 def curvilinear_1200x800(nt: int = 6000) -> Model:
     return curvilinear(1200, 800, nt=nt)
 
