@@ -634,14 +634,30 @@ struct Oracle {
   }
 
   // Stage input `S`: the state itself for the first stage, U_tmp afterwards.
+  bool src_on = true;  // false: the stage RHS without the source (the linear operator alone)
   void stage(int dir, R t, const Set& S) {
     build_ghosts(S);
     fluid_velocity(dir, S);
     fluid_stress(dir, S);
     solid_velocity(dir, S);
     solid_stress(dir, S);
-    add_source(ricker(t));
+    if (src_on) add_source(ricker(t));
     couple(dir);
+  }
+
+  // Flat packing of a set: the NFIELD arrays [rows][nx] one after another.
+  size_t set_len() const {
+    size_t n = 0;
+    for (int f = 0; f < NFIELD; ++f) n += size_t(is_fluid(f) ? nzf : nzs) * nx;
+    return n;
+  }
+  void pack(const Set& S, double* out) const {
+    for (int f = 0; f < NFIELD; ++f)
+      for (size_t k = 0; k < S[f].size(); ++k) *out++ = double(S[f][k]);
+  }
+  void unpack(const double* in, Set& S) const {
+    for (int f = 0; f < NFIELD; ++f)
+      for (size_t k = 0; k < S[f].size(); ++k) S[f][k] = R(*in++);
   }
 
   // One RK4 step with direction order FBFB (even it) or BFBF (odd it)
@@ -650,7 +666,10 @@ struct Oracle {
   // C = 1*A + c*B (matrix_add) and A += c*B (matrix_self_add,
   // src/common_kernels.cu:4-31); the same per-value arithmetic is applied here
   // without the copies: U_b = U + w1 k1 is exactly U_b += w1 k1 on a copy.
-  void step(int it) {
+  // `save` (optional): the four stage inputs U, U_tmp, U_tmp, U_tmp, packed.
+  void step(int it, double* save = nullptr) {
+    const size_t sl = save ? set_len() : 0;
+    if (save) pack(U, save);
     const int d0 = (it & 1) ? kB : kF, d1 = 1 - d0;
     R time, half, dt;
     if constexpr (std::is_same<R, float>::value) {
@@ -668,16 +687,19 @@ struct Oracle {
       Ut[f][k] = R(1) * U[f][k] + c_half * Kk[f][k];
       Ub[f][k] = U[f][k] + w6 * Kk[f][k];
     });
+    if (save) pack(Ut, save + sl);
     stage(d1, time + half, Ut);
     for_cells([&](int f, size_t k) {
       Ut[f][k] = R(1) * U[f][k] + c_half * Kk[f][k];
       Ub[f][k] += w3 * Kk[f][k];
     });
+    if (save) pack(Ut, save + 2 * sl);
     stage(d0, time + half, Ut);
     for_cells([&](int f, size_t k) {
       Ut[f][k] = R(1) * U[f][k] + c_full * Kk[f][k];
       Ub[f][k] += w3 * Kk[f][k];
     });
+    if (save) pack(Ut, save + 3 * sl);
     stage(d1, time + dt, Ut);
     for_cells([&](int f, size_t k) { U[f][k] = R(1) * Ub[f][k] + w_last * Kk[f][k]; });
     filter();
@@ -794,6 +816,88 @@ void orc_destroy(orc_handle* h) {
   if (h->precision == 64) delete static_cast<Oracle<double>*>(h->impl);
   else delete static_cast<Oracle<float>*>(h->impl);
   delete h;
+}
+
+// ---- linearised pieces for the FP64 adjoint oracle ----------------------------
+// A set is packed as the NFIELD arrays in Field order, fluid-sized fields
+// [nz_f][nx], solid-sized [nz_s][nx].
+
+long long orc_set_len(orc_handle* h) {
+  if (!h) return -1;
+  return h->precision == 64 ? (long long)static_cast<Oracle<double>*>(h->impl)->set_len()
+                            : (long long)static_cast<Oracle<float>*>(h->impl)->set_len();
+}
+
+extern "C++" template <class R>
+int rhs_impl(Oracle<R>* o, int dir, const double* in, double* out) {
+  typename Oracle<R>::Set S;
+  o->alloc(S);
+  o->unpack(in, S);
+  for (auto& f : o->Kk) std::fill(f.begin(), f.end(), R(0));
+  const bool src = o->src_on;
+  o->src_on = false;
+  o->stage(dir, R(0), S);
+  o->src_on = src;
+  o->pack(o->Kk, out);
+  return 0;
+}
+
+// out = the stage right-hand side of the packed set `in` with operator
+// direction `dir` (0 F, 1 B), without the source: the linear operator L_dir,
+// interface coupling included.
+int orc_rhs(orc_handle* h, int dir, const double* in, double* out) {
+  if (!h || !in || !out || (dir != 0 && dir != 1)) return -1;
+  return h->precision == 64 ? rhs_impl(static_cast<Oracle<double>*>(h->impl), dir, in, out)
+                            : rhs_impl(static_cast<Oracle<float>*>(h->impl), dir, in, out);
+}
+
+extern "C++" template <class R>
+int filter_impl(Oracle<R>* o, double* set) {
+  typename Oracle<R>::Set keep = o->U;
+  o->unpack(set, o->U);
+  o->filter();
+  o->pack(o->U, set);
+  o->U = keep;
+  return 0;
+}
+
+// Applies the post-step interface filter to the packed set in place.
+int orc_filter(orc_handle* h, double* set) {
+  if (!h || !set) return -1;
+  return h->precision == 64 ? filter_impl(static_cast<Oracle<double>*>(h->impl), set)
+                            : filter_impl(static_cast<Oracle<float>*>(h->impl), set);
+}
+
+// Reads / replaces the state (and sets the step index of the next step).
+int orc_get_state(orc_handle* h, double* set) {
+  if (!h || !set) return -1;
+  if (h->precision == 64) { auto* o = static_cast<Oracle<double>*>(h->impl); o->pack(o->U, set); }
+  else { auto* o = static_cast<Oracle<float>*>(h->impl); o->pack(o->U, set); }
+  return 0;
+}
+int orc_set_state(orc_handle* h, const double* set, int it) {
+  if (!h || !set || it < 0) return -1;
+  if (h->precision == 64) { auto* o = static_cast<Oracle<double>*>(h->impl); o->unpack(set, o->U); }
+  else { auto* o = static_cast<Oracle<float>*>(h->impl); o->unpack(set, o->U); }
+  h->it = it;
+  return 0;
+}
+
+// One step at the handle's step index, the four stage inputs packed into
+// `save` (4 sets), then the index advances.
+int orc_step_save(orc_handle* h, double* save) {
+  if (!h || !save) return -1;
+  unsigned saved = _mm_getcsr();
+#pragma omp parallel
+  { _mm_setcsr(_mm_getcsr() | 0x8040u); }
+  _mm_setcsr(saved | 0x8040u);
+  if (h->precision == 64) static_cast<Oracle<double>*>(h->impl)->step(h->it, save);
+  else static_cast<Oracle<float>*>(h->impl)->step(h->it, save);
+#pragma omp parallel
+  { _mm_setcsr(saved); }
+  _mm_setcsr(saved);
+  ++h->it;
+  return 0;
 }
 
 int orc_max_threads(void) {
