@@ -209,6 +209,40 @@ int mfdm_group_step(mfdm_group* g, int nsteps);
 int mfdm_group_time_steps(mfdm_group* g, int nsteps, float* total_ms);
 int mfdm_group_close(mfdm_group* g);
 
+/* ---- adjoint-state gradients ---------------------------------------------
+ * The reference has no adjoint. These return the exact gradient of
+ * J = sum over receiver samples of residual . record, for a plain handle's
+ * current shot started from rest, with respect to the seven coefficient
+ * arrays of the model: the discrete adjoint of this library's own RK4 step
+ * (transposed stage operators, interface filter and RK4 bookkeeping), with
+ * checkpoint-and-recompute time stepping. For an L2 misfit the residual is
+ * record - observed. Gradients with respect to vp, vs and rho follow by the
+ * chain rule (C11 = C33 = rho vp^2, C13 = rho (vp^2 - 2 vs^2), C55 = rho vs^2). */
+typedef struct mfdm_coef_grad {
+  double* K;          /* d J / d K                     [nz_f][nx] (any pointer may be NULL) */
+  double* rcp_rho_f;  /* d J / d (1 / rho), fluid      [nz_f][nx] */
+  double* C11;        /* d J / d C11                   [nz_s][nx] */
+  double* C13;
+  double* C33;
+  double* C55;
+  double* rcp_rho_s;  /* d J / d (1 / rho), solid      [nz_s][nx] */
+} mfdm_coef_grad;
+
+/* Runs `nsteps` steps of the current shot from rest, storing the state every
+ * `ckpt_every` steps (ceil(nsteps / ckpt_every) state copies on the device).
+ * The records are read with mfdm_get_records as after mfdm_step. The first
+ * call on a handle also assembles the transposed stage operators (lattice
+ * probes of the stage kernel; about 2 x 49 stage launches per state array). */
+int mfdm_adjoint_forward(mfdm_model* m, int nsteps, int ckpt_every);
+
+/* Back-propagates receiver residuals through the run of the preceding
+ * mfdm_adjoint_forward (no other step in between): res_* are
+ * [ceil(nsteps / gap)][nx] (NULL = 0), in the mfdm_get_records layout.
+ * Recomputes each checkpoint segment once, keeping its stage inputs
+ * (4 * ckpt_every state copies). On return the handle is back at rest at step 0. */
+int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_svz,
+                          const float* res_fp, mfdm_coef_grad* grad);
+
 /* The drop-in command line: `main_debug <model.json> <out_root>`
  * (src/main.cu:58-216). Clears out_root, runs every shot and writes
  * <out_root>/<shot>/record/{solid_vx,solid_vz,fluid_p}.bin and

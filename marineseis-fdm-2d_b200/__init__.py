@@ -35,7 +35,11 @@ EXPORTS = ("mfdm_last_error", "mfdm_open_json", "mfdm_open_desc", "mfdm_load_des
            "mfdm_synchronize", "mfdm_get_records", "mfdm_get_field", "mfdm_set_field",
            "mfdm_run_cli", "mfdm_step_noalloc", "mfdm_open_batch", "mfdm_batch_reset",
            "mfdm_batch_get_records", "mfdm_batch_get_field", "mfdm_set_tile", "mfdm_autotune",
-           "mfdm_group_open", "mfdm_group_step", "mfdm_group_time_steps", "mfdm_group_close")
+           "mfdm_group_open", "mfdm_group_step", "mfdm_group_time_steps", "mfdm_group_close",
+           "mfdm_adjoint_forward", "mfdm_adjoint_backward")
+
+# Coefficient arrays the adjoint differentiates (mfdm_coef_grad order).
+GRAD_COEFS = ("K", "rcp_rho_f", "C11", "C13", "C33", "C55", "rcp_rho_s")
 
 
 class MfdmError(RuntimeError):
@@ -68,6 +72,11 @@ class Info(ctypes.Structure):
                 ("step", ctypes.c_int), ("nsamples", ctypes.c_int),
                 ("cells", ctypes.c_longlong), ("device_bytes", ctypes.c_longlong),
                 ("nshots", ctypes.c_int), ("seg_rows", ctypes.c_int)]
+
+
+class CoefGrad(ctypes.Structure):
+    """mfdm_coef_grad: host [rows][nx] float64 arrays (NULL: not wanted)."""
+    _fields_ = [(k, ctypes.POINTER(ctypes.c_double)) for k in GRAD_COEFS]
 
 
 class Shot(ctypes.Structure):
@@ -131,6 +140,8 @@ def load_library(path: str = LIB_PATH):
         "mfdm_group_step": (ctypes.c_int, [vp, ctypes.c_int]),
         "mfdm_group_time_steps": (ctypes.c_int, [vp, ctypes.c_int, _fp]),
         "mfdm_group_close": (ctypes.c_int, [vp]),
+        "mfdm_adjoint_forward": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+        "mfdm_adjoint_backward": (ctypes.c_int, [vp, _fp, _fp, _fp, ctypes.POINTER(CoefGrad)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -252,6 +263,38 @@ class Solver:
 
     def synchronize(self):
         _check(self._lib.mfdm_synchronize(self._h))
+
+    # -- adjoint ----------------------------------------------------------------
+    def adjoint_forward(self, nsteps: int, ckpt_every: int = 50) -> Dict[str, np.ndarray]:
+        """Runs the current shot from rest with checkpoints (mfdm_adjoint_forward)
+        and returns its records {'svx', 'svz', 'fp'}: [samples][nx]."""
+        _check(self._lib.mfdm_adjoint_forward(self._h, int(nsteps), int(ckpt_every)))
+        return self.records()
+
+    def adjoint_backward(self, residual: Dict[str, np.ndarray]) -> Dict[str, np.ndarray]:
+        """Gradients of sum(residual . records) with respect to the coefficient
+        arrays (mfdm_adjoint_backward): {'K', 'rcp_rho_f'}: [nz_f][nx] and
+        {'C11', 'C13', 'C33', 'C55', 'rcp_rho_s'}: [nz_s][nx], float64."""
+        info = self.info()
+        nx = info["nx"]
+        keep = []
+
+        def res(name):
+            a = residual.get(name)
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=np.float32)
+            if a.ndim != 2 or a.shape[1] != nx:
+                raise ValueError(f"residual {name} must be [samples][{nx}]")
+            keep.append(a)
+            return a.ctypes.data_as(_fp)
+
+        out = {k: np.zeros((info["nz_f"] if k in ("K", "rcp_rho_f") else info["nz_s"], nx))
+               for k in GRAD_COEFS}
+        g = CoefGrad(*[out[k].ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for k in GRAD_COEFS])
+        _check(self._lib.mfdm_adjoint_backward(self._h, res("svx"), res("svz"), res("fp"),
+                                               ctypes.byref(g)))
+        return out
 
     # -- tile shape -----------------------------------------------------------
     def set_tile(self, seg_rows: int):

@@ -1,0 +1,101 @@
+// Adjoint-state backward of the RK4 time step (library-internal).
+//
+// The reference has no adjoint. This is the exact discrete adjoint of the
+// library's own forward step: every piece of the step is linear in the state,
+// so its transpose is assembled or derived from the forward kernels rather than
+// written out by hand for every boundary case.
+//
+// * The stage operators L_F and L_B (the stage right-hand side without the
+//   source, interface coupling included) are assembled once per model as CSR
+//   matrices of L^T by probing the forward stage kernel: every output of the
+//   stencil depends on inputs at most 3 cells away in x and in the global row,
+//   so one stage launch on an input field that is 1 on a 7 x 7 lattice and 0
+//   elsewhere yields 1/49 of that field's columns, each output attributable to
+//   exactly one input.
+// * The interface filter's transpose and the RK4 bookkeeping are written out
+//   (they are short); the coupling uses the same device functions as the
+//   forward kernels.
+// * The derivative of a stage RHS with respect to one material coefficient of
+//   a cell is the RHS of that cell evaluated with the coefficient set to 1 and
+//   the others to 0, the forward's own RHS functions with another coefficient
+//   set.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mfdm_device.cuh"
+
+namespace mfdm {
+
+constexpr int kSetArrays = 24;  // state arrays of one RK set (fluid, solid, ADE strips)
+
+// Where every array of one RK set sits inside the set's contiguous range, and
+// how its cells map to global (row, column): fluid rows are global rows,
+// solid row r is global row nz_f - 1 + r, xi-strip slots are the columns
+// 3..npd+2 and nx-3-npd..nx-4, the solid zeta strip starts at solid row
+// nz_s - 3 - npd and the fluid top band at fluid row 3.
+struct SetLayout {
+  long long len;                    // floats per set
+  long long off[kSetArrays];        // first float of each array
+  int rows[kSetArrays];             // rows of each array (0: absent)
+  int pitch[kSetArrays];            // floats per row
+  int ncols[kSetArrays];            // valid columns per row
+  int kind[kSetArrays];             // 0 fluid, 1 solid, 2 fluid xi strip, 3 solid xi strip,
+                                    // 4 solid zeta strip, 5 fluid zeta band
+  int nx, nzf, nzs, npd;
+};
+
+// Transposed stage operator of one direction: row j of L^T (an input value of
+// the stage) lists the outputs that read it.
+struct CsrT {
+  long long* rowptr = nullptr;  // len + 1
+  int* col = nullptr;
+  float* val = nullptr;
+  long long nnz = 0;
+};
+
+namespace adj {
+
+// Sets `v` at the cells of array `a` on lattice point (cz, cx) (global row mod 7, column mod 7).
+cudaError_t set_lattice(float* set, const SetLayout& L, int a, int cz, int cx, float v, cudaStream_t st);
+// Fills the whole set with v.
+cudaError_t fill(float* set, long long n, float v, cudaStream_t st);
+// mask[i] = out[i] != 0.
+cudaError_t make_mask(const float* out, uint8_t* mask, long long n, cudaStream_t st);
+// Attributes every non-zero output of a lattice probe of array `a` to its
+// input. Pass 1 (rowptr == nullptr): count[j]++; pass 2: writes col / val
+// (value / scale) at rowptr[j] + cursor[j]++. Unattributable outputs raise *err.
+cudaError_t extract(const float* out, const SetLayout& L, int a, int cz, int cx, float scale,
+                    unsigned long long* count, const long long* rowptr, int* cursor, int* col,
+                    float* val, int* err, cudaStream_t st);
+// rowptr = exclusive prefix sum of count (len + 1 entries); scratch from *tmp.
+cudaError_t scan(const unsigned long long* count, long long* rowptr, long long len, void** tmp,
+                 size_t* tmp_bytes, cudaStream_t st);
+// Sorts every row of the CSR by column (deterministic sums).
+cudaError_t sort_rows(const CsrT& A, long long len, cudaStream_t st);
+
+// One reverse stage: y = L^T kb, lam += (mask_lam ? M : 1) y and, when kbn is
+// given, kbn = M (w mu + c y).
+cudaError_t reverse_stage(const CsrT& A, long long len, const float* kb, float* lam,
+                          const uint8_t* mask, bool mask_lam, float* kbn, const float* mu, float w,
+                          float c, cudaStream_t st);
+// y = L^T x (tests and diagnostics).
+cudaError_t apply_t(const CsrT& A, long long len, const float* x, float* y, cudaStream_t st);
+
+// Adds one receiver sample's residuals (svx, svz, fp rows of nx) to lam.
+cudaError_t inject(float* lam, const SetLayout& L, const float* res, cudaStream_t st);
+// lam <- F^T lam on the interface rows (the transposed post-step filter);
+// tmp holds 8 * nx floats.
+cudaError_t filter_t(float* lam, const SetLayout& L, const Coef& C, float* tmp, cudaStream_t st);
+// mu = lam, kb = c M lam.
+cudaError_t start(const float* lam, float* mu, float* kb, const uint8_t* mask, long long n, float c,
+                  cudaStream_t st);
+
+// Material gradients of one stage: g[m][cell] += kb . dL_dir/dm (Y) over the
+// cell's main fields (and the coupled interface column). Y and KB are sets.
+// g: K, 1/rho_f ([nz_f][P]) then C11, C13, C33, C55, 1/rho_s ([nz_s][P]).
+cudaError_t gradient(const Coef& C, const Fields& Y, const Fields& KB, double* const* g, int dir,
+                     cudaStream_t st);
+
+}  // namespace adj
+}  // namespace mfdm

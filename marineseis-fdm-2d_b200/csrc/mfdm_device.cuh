@@ -204,6 +204,26 @@ __device__ __forceinline__ float over_rho(float x, float r) {
 #endif
 }
 
+// Direct reads of the stage input (the interface strip and the gradient kernels).
+struct FluidGlobal {
+  const float *vx, *vz, *p;
+  size_t base;
+  int P;
+  __device__ __forceinline__ float fvx(int dz, int dx) const { return __ldg(vx + base + (ptrdiff_t)dz * P + dx); }
+  __device__ __forceinline__ float fvz(int dz, int dx) const { return __ldg(vz + base + (ptrdiff_t)dz * P + dx); }
+  __device__ __forceinline__ float fp(int dz, int dx) const { return __ldg(p + base + (ptrdiff_t)dz * P + dx); }
+};
+struct SolidGlobal {
+  const float *vx, *vz, *sx, *sz, *sxz;
+  size_t base;
+  int P;
+  __device__ __forceinline__ float svx(int dz, int dx) const { return __ldg(vx + base + (ptrdiff_t)dz * P + dx); }
+  __device__ __forceinline__ float svz(int dz, int dx) const { return __ldg(vz + base + (ptrdiff_t)dz * P + dx); }
+  __device__ __forceinline__ float ssx(int dz, int dx) const { return __ldg(sx + base + (ptrdiff_t)dz * P + dx); }
+  __device__ __forceinline__ float ssz(int dz, int dx) const { return __ldg(sz + base + (ptrdiff_t)dz * P + dx); }
+  __device__ __forceinline__ float ssxz(int dz, int dx) const { return __ldg(sxz + base + (ptrdiff_t)dz * P + dx); }
+};
+
 // Centre-cell coefficients of a fluid / solid cell (metric at the cell's global row).
 struct FluidCoefs { float xix, xiz, zex, zez, rho, K; };
 struct SolidCoefs { float xix, xiz, zex, zez, rho, c11, c13, c33, c55; };
@@ -529,6 +549,62 @@ __device__ __forceinline__ SolidK solid_rhs(const Coef& C, const Acc& A, int iz,
     }
   }
   return o;
+}
+
+// Normal/tangential coupling of the stage RHS on the interface
+// (pml_fs_kernels.cuh:754-827): kf = fluid (vx, vz, p), ks = solid (vx, vz,
+// sx, sz, sxz) RHS of one column, kv = the eight coupled values in that order.
+// Direction F: the fluid takes the solid's normal velocity and traction;
+// B: the solid takes the fluid's.
+template <int DIR>
+__device__ __forceinline__ void couple_rhs(float2 n, const float* kf, const float* ks, float* kv) {
+  const float vxf = kf[0], vzf = kf[1];
+  float pf = kf[2];
+  const float vxs = ks[0], vzs = ks[1], sxx = ks[2], szz = ks[3], sxz = ks[4];
+  float vnf = n.x * vxf + n.y * vzf;
+  const float vtf = n.y * vxf - n.x * vzf;
+  float vns = n.x * vxs + n.y * vzs;
+  const float vts = n.y * vxs - n.x * vzs;
+  float snn = n.x * n.x * sxx + 2 * n.x * n.y * sxz + n.y * n.y * szz;
+  float snt = n.x * n.y * (sxx - szz) + (n.y * n.y - n.x * n.x) * sxz;
+  const float stt = n.y * n.y * sxx - 2 * n.x * n.y * sxz + n.x * n.x * szz;
+  if (DIR == kDirF) {
+    vnf = vns;
+    pf = -snn;
+    snt = 0.f;
+  } else {
+    vns = vnf;
+    snn = -pf;
+    snt = 0.f;
+  }
+  kv[0] = n.x * vnf + n.y * vtf;
+  kv[1] = n.y * vnf - n.x * vtf;
+  kv[2] = pf;
+  kv[3] = n.x * vns + n.y * vts;
+  kv[4] = n.y * vns - n.x * vts;
+  kv[5] = n.x * n.x * snn + 2 * n.x * n.y * snt + n.y * n.y * stt;
+  kv[6] = n.y * n.y * snn - 2 * n.x * n.y * snt + n.x * n.x * stt;
+  kv[7] = -n.x * n.y * stt + (n.y * n.y - n.x * n.x) * snt;
+}
+
+// Continuity average of the filtered interface values (src/pml_fs_kernels.cu:
+// 470-520): v = filtered (fluid vx, vz, p, solid vx, vz, sx, sz, sxz) of one
+// column, u = the new interface state in the same order.
+__device__ __forceinline__ void interface_average(float2 n, const float* v, float* u) {
+  const float vnf = n.x * v[0] + n.y * v[1], vtf = n.y * v[0] - n.x * v[1];
+  const float vns = n.x * v[3] + n.y * v[4], vts = n.y * v[3] - n.x * v[4];
+  const float snn = n.x * n.x * v[5] + 2.0f * n.x * n.y * v[7] + n.y * n.y * v[6];
+  const float stt = n.y * n.y * v[5] - 2.0f * n.x * n.y * v[7] + n.x * n.x * v[6];
+  const float vn = 0.5f * (vnf + vns);
+  const float sn = 0.5f * (snn - v[2]);
+  u[0] = n.x * vn + n.y * vtf;
+  u[1] = n.y * vn - n.x * vtf;
+  u[2] = -sn;
+  u[3] = n.x * vn + n.y * vts;
+  u[4] = n.y * vn - n.x * vts;
+  u[5] = n.x * n.x * sn + n.y * n.y * stt;
+  u[6] = n.y * n.y * sn + n.x * n.x * stt;
+  u[7] = n.x * n.y * (sn - stt);
 }
 
 // Source term of stage `s` at fluid cell (iz, ix): 5x5 Gaussian spreading of the

@@ -10,6 +10,8 @@
 
 #include <algorithm>
 #include <cerrno>
+#include <chrono>
+#include <cstdint>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -26,6 +28,7 @@
 
 #include "../../include/mfdm.h"
 #include "json_config.h"
+#include "mfdm_adjoint.h"
 #include "mfdm_kernels.h"
 
 namespace fs = std::filesystem;
@@ -101,6 +104,8 @@ struct ShotCfg {
 
 }  // namespace
 
+struct AdjointState;
+
 struct mfdm_model {
   int device = 0;
   int nshots = 1;              // shots stepped together (1 for a plain handle)
@@ -128,6 +133,40 @@ struct mfdm_model {
   CUtensorMap fst[4], sst[4], fpw[4], spw[4], fco, sco;
   float* fcoef = nullptr;  // [6][nz_f][P]: xi_x, xi_z, ze_x, ze_z, rho, K
   float* scoef = nullptr;  // [9][nz_s][P]: xi_x, xi_z, ze_x, ze_z, rho, C11, C13, C33, C55
+  AdjointState* adj = nullptr;  // adjoint operators and buffers (mfdm_adjoint_*)
+};
+
+// Device buffers of the adjoint (one plain handle): the transposed stage
+// operators of both directions, the updated-cell mask, the adjoint sets, the
+// material gradients, the checkpoints of the forward run and the stage inputs
+// of one checkpoint segment.
+struct AdjointState {
+  mfdm::SetLayout L{};
+  mfdm::CsrT A[2];
+  uint8_t* mask = nullptr;
+  float *lam = nullptr, *mu = nullptr, *kb[2] = {nullptr, nullptr}, *tmp = nullptr;
+  double* grad = nullptr;  // K, 1/rho_f [nz_f][P]; C11, C13, C33, C55, 1/rho_s [nz_s][P]
+  float* ckpt = nullptr;   // checkpoint sets
+  size_t ckpt_sets = 0;
+  float* seg = nullptr;    // 4 stage-input sets per step of one segment
+  size_t seg_steps = 0;
+  float* res = nullptr;    // residual samples [ns][3][nx]
+  size_t res_floats = 0;
+  void* scan_tmp = nullptr;
+  size_t scan_bytes = 0;
+  bool built = false;
+  int nsteps = -1, every = 0;  // the forward run a backward pass may follow
+  double build_ms = 0.0;       // operator assembly time (host clock)
+  ~AdjointState() {
+    for (auto& a : A) {
+      cudaFree(a.rowptr);
+      cudaFree(a.col);
+      cudaFree(a.val);
+    }
+    cudaFree(mask); cudaFree(lam); cudaFree(mu); cudaFree(kb[0]); cudaFree(kb[1]);
+    cudaFree(tmp); cudaFree(grad); cudaFree(ckpt); cudaFree(seg); cudaFree(res);
+    cudaFree(scan_tmp);
+  }
 };
 
 namespace {
@@ -354,8 +393,12 @@ int ensure_capacity(mfdm_model* m, int steps) {
 
 // Enqueues the five launches of one step. With `ev` (6 events) an event is
 // recorded before the first launch and after every launch.
-int enqueue_step(mfdm_model* m, int it, cudaStream_t st, cudaEvent_t* ev = nullptr) {
+// With `save` (4 set-sized buffers) the four stage inputs are copied out as the
+// step runs (U, then the outputs of stages 0, 1 and 2), for the adjoint.
+int enqueue_step(mfdm_model* m, int it, cudaStream_t st, cudaEvent_t* ev = nullptr,
+                 float* const* save = nullptr) {
   const int d0 = (it & 1) ? mfdm::kDirB : mfdm::kDirF, d1 = 1 - d0;
+  const size_t set_bytes = size_t(m->S[1].fvx - m->S[0].fvx) * sizeof(float);
   const Fields &U = m->S[0], &A = m->S[1], &B = m->S[2], &Acc = m->S[3];
   const Coef& C = m->C;
   // stage s reads in[s] and writes out[s]: U -> A -> B -> A -> U
@@ -364,6 +407,7 @@ int enqueue_step(mfdm_model* m, int it, cudaStream_t st, cudaEvent_t* ev = nullp
   const int in_set[4] = {0, 1, 2, 1};
   const int dir[4] = {d0, d1, d0, d1};
   if (ev) MFDM_CU(cudaEventRecord(ev[0], st));
+  if (save) MFDM_CU(cudaMemcpyAsync(save[0], U.fvx, set_bytes, cudaMemcpyDeviceToDevice, st));
   for (int s = 0; s < 4; ++s) {
     mfdm::StageMaps maps;
     maps.fin = m->fst[in_set[s]];
@@ -376,6 +420,8 @@ int enqueue_step(mfdm_model* m, int it, cudaStream_t st, cudaEvent_t* ev = nullp
     maps.scoef = m->sco;
     MFDM_CU(mfdm::launch_stage(C, *in[s], *out[s], U, Acc, maps, s, dir[s], st));
     if (ev) MFDM_CU(cudaEventRecord(ev[s + 1], st));
+    if (save && s < 3)
+      MFDM_CU(cudaMemcpyAsync(save[s + 1], out[s]->fvx, set_bytes, cudaMemcpyDeviceToDevice, st));
   }
   MFDM_CU(mfdm::launch_finish(C, U, st));
   if (ev) MFDM_CU(cudaEventRecord(ev[5], st));
@@ -651,6 +697,7 @@ void destroy(mfdm_model* m) {
   if (m->d_src) cudaFree(m->d_src);
   if (m->d_rec) cudaFree(m->d_rec);
   if (m->dmem) cudaFree(m->dmem);
+  delete m->adj;
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
 }
@@ -841,6 +888,10 @@ int mfdm_load_desc(mfdm_model* m, const mfdm_desc* d) {
     return fail(MFDM_ERR_ARG, "model shape or boundary type differs from the open handle");
   DeviceGuard g(m->device);
   MFDM_CU(cudaStreamSynchronize(m->stream));
+  if (m->adj) {  // the transposed operators hold the old coefficients
+    m->adj->built = false;
+    m->adj->nsteps = -1;
+  }
   return upload_model(m, h);
 }
 
@@ -1271,6 +1322,298 @@ int mfdm_set_field(mfdm_model* m, int field, const float* host) {
                             m->stream));
   MFDM_CU(cudaStreamSynchronize(m->stream));
   return MFDM_OK;
+}
+
+}  // extern "C"
+
+// ---- adjoint-state gradients ---------------------------------------------------
+
+namespace {
+
+// Layout of one RK set, read off the handle's own buffers (set 0; the other
+// sets are the same at a fixed stride).
+mfdm::SetLayout set_layout(const mfdm_model* m) {
+  mfdm::SetLayout L{};
+  const Fields& S = m->S[0];
+  const float* base = S.fvx;
+  L.len = m->S[1].fvx - m->S[0].fvx;
+  const float* arr[mfdm::kSetArrays] = {
+      S.fvx, S.fvz, S.fp, S.svx, S.svz, S.ssx, S.ssz, S.ssxz,
+      S.fx[0], S.fx[1], S.fx[2], S.fx[3], S.sx[0], S.sx[1], S.sx[2], S.sx[3],
+      S.sz[0], S.sz[1], S.sz[2], S.sz[3], S.fz[0], S.fz[1], S.fz[2], S.fz[3]};
+  const HostModel& h = m->cfg;
+  const int npd = h.npd;
+  for (int a = 0; a < mfdm::kSetArrays; ++a) {
+    L.off[a] = arr[a] - base;
+    if (a < 3) { L.rows[a] = h.nzf; L.pitch[a] = m->P; L.ncols[a] = h.nx; L.kind[a] = 0; }
+    else if (a < 8) { L.rows[a] = h.nzs; L.pitch[a] = m->P; L.ncols[a] = h.nx; L.kind[a] = 1; }
+    else if (a < 12) { L.rows[a] = npd > 0 ? h.nzf : 0; L.pitch[a] = m->Ps; L.ncols[a] = 2 * npd; L.kind[a] = 2; }
+    else if (a < 16) { L.rows[a] = npd > 0 ? h.nzs : 0; L.pitch[a] = m->Ps; L.ncols[a] = 2 * npd; L.kind[a] = 3; }
+    else if (a < 20) { L.rows[a] = npd; L.pitch[a] = m->P; L.ncols[a] = h.nx; L.kind[a] = 4; }
+    else { L.rows[a] = m->C.cpml ? npd : 0; L.pitch[a] = m->P; L.ncols[a] = h.nx; L.kind[a] = 5; }
+  }
+  L.nx = h.nx; L.nzf = h.nzf; L.nzs = h.nzs; L.npd = npd;
+  return L;
+}
+
+// The Fields view of a set-sized buffer.
+Fields fields_at(const mfdm::SetLayout& L, float* base) {
+  Fields F;
+  float* p[mfdm::kSetArrays];
+  for (int a = 0; a < mfdm::kSetArrays; ++a) p[a] = base + L.off[a];
+  F.fvx = p[0]; F.fvz = p[1]; F.fp = p[2];
+  F.svx = p[3]; F.svz = p[4]; F.ssx = p[5]; F.ssz = p[6]; F.ssxz = p[7];
+  for (int q = 0; q < 4; ++q) {
+    F.fx[q] = p[8 + q]; F.sx[q] = p[12 + q]; F.sz[q] = p[16 + q]; F.fz[q] = p[20 + q];
+  }
+  return F;
+}
+
+template <class T>
+int dalloc(T** p, size_t n) {
+  MFDM_CU(cudaMalloc(reinterpret_cast<void**>(p), std::max<size_t>(n, 1) * sizeof(T)));
+  return MFDM_OK;
+}
+
+// Assembles L_F^T and L_B^T by lattice probes of the stage kernel on the
+// handle's own sets: input A (1 on the lattice points of one array), U^n = B
+// (0), accumulator = Acc (scratch), output U = c k. Leaves the state at rest.
+int adjoint_build(mfdm_model* m) {
+  AdjointState* a = m->adj;
+  const auto t0 = std::chrono::steady_clock::now();
+  const mfdm::SetLayout& L = a->L;
+  const long long n = L.len;
+  cudaStream_t st = m->stream;
+  int rc;
+  if ((rc = clear_state(m)) != MFDM_OK) return rc;
+  Coef C = m->C;
+  C.srcx = -1;  // the operator without the source
+  C.src_pos = nullptr;
+  const int stage = 1;  // a middle stage: out = U^n + c k, with U^n = 0
+  const float cc = C.rk_c[stage], scale = 1.0f / cc;
+  mfdm::StageMaps maps;
+  maps.fin = m->fst[1]; maps.sin = m->sst[1];
+  maps.fun = m->fpw[2]; maps.sun = m->spw[2];
+  maps.facc = m->fpw[3]; maps.sacc = m->spw[3];
+  maps.fcoef = m->fco; maps.scoef = m->sco;
+  const Fields &Out = m->S[0], &In = m->S[1], &Un = m->S[2], &Acc = m->S[3];
+  // cells a stage updates: with input 0 and U^n = 1 the output is 1 exactly there
+  MFDM_CU(mfdm::adj::fill(Un.fvx, n, 1.0f, st));
+  MFDM_CU(mfdm::launch_stage(C, In, Out, Un, Acc, maps, stage, mfdm::kDirF, st));
+  MFDM_CU(mfdm::adj::make_mask(Out.fvx, a->mask, n, st));
+  MFDM_CU(cudaMemsetAsync(Un.fvx, 0, size_t(n) * sizeof(float), st));
+  MFDM_CU(cudaMemsetAsync(Out.fvx, 0, size_t(n) * sizeof(float), st));
+  unsigned long long* count = nullptr;
+  int *cursor = nullptr, *err = nullptr;
+  if ((rc = dalloc(&count, size_t(n) + 1)) != MFDM_OK) return rc;
+  struct Free { void* p[3]; ~Free() { for (void* q : p) cudaFree(q); } } fr{{count, nullptr, nullptr}};
+  if ((rc = dalloc(&cursor, size_t(n))) != MFDM_OK) return rc;
+  fr.p[1] = cursor;
+  if ((rc = dalloc(&err, 1)) != MFDM_OK) return rc;
+  fr.p[2] = err;
+  MFDM_CU(cudaMemsetAsync(err, 0, sizeof(int), st));
+  for (int d = 0; d < 2; ++d) {
+    mfdm::CsrT& A = a->A[d];
+    MFDM_CU(cudaMemsetAsync(count, 0, (size_t(n) + 1) * sizeof(unsigned long long), st));
+    for (int pass = 0; pass < 2; ++pass) {
+      if (pass == 1) {
+        if ((rc = dalloc(&A.rowptr, size_t(n) + 1)) != MFDM_OK) return rc;
+        MFDM_CU(mfdm::adj::scan(count, A.rowptr, n, &a->scan_tmp, &a->scan_bytes, st));
+        MFDM_CU(cudaMemcpyAsync(&A.nnz, A.rowptr + n, sizeof(long long), cudaMemcpyDeviceToHost, st));
+        MFDM_CU(cudaStreamSynchronize(st));
+        if (A.nnz >= (1LL << 31) || n >= (1LL << 31))
+          return fail(MFDM_ERR_ARG, "model too large for the adjoint operators");
+        if ((rc = dalloc(&A.col, size_t(A.nnz))) != MFDM_OK) return rc;
+        if ((rc = dalloc(&A.val, size_t(A.nnz))) != MFDM_OK) return rc;
+        MFDM_CU(cudaMemsetAsync(cursor, 0, size_t(n) * sizeof(int), st));
+      }
+      for (int arr = 0; arr < mfdm::kSetArrays; ++arr) {
+        if (L.rows[arr] <= 0) continue;
+        for (int cz = 0; cz < 7; ++cz)
+          for (int cx = 0; cx < 7; ++cx) {
+            MFDM_CU(mfdm::adj::set_lattice(In.fvx, L, arr, cz, cx, 1.0f, st));
+            MFDM_CU(mfdm::launch_stage(C, In, Out, Un, Acc, maps, stage, d, st));
+            MFDM_CU(mfdm::adj::extract(Out.fvx, L, arr, cz, cx, scale, count,
+                                       pass ? A.rowptr : nullptr, cursor, A.col, A.val, err, st));
+            MFDM_CU(mfdm::adj::set_lattice(In.fvx, L, arr, cz, cx, 0.0f, st));
+          }
+      }
+    }
+    MFDM_CU(mfdm::adj::sort_rows(A, n, st));
+  }
+  int nerr = 0;
+  MFDM_CU(cudaMemcpyAsync(&nerr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MFDM_CU(cudaStreamSynchronize(st));
+  if (nerr) return fail(MFDM_ERR_CUDA, "adjoint operator assembly: " + std::to_string(nerr) +
+                                           " outputs outside the 3-cell stencil radius");
+  if ((rc = clear_state(m)) != MFDM_OK) return rc;
+  if ((rc = rewind(m)) != MFDM_OK) return rc;
+  a->built = true;
+  a->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return MFDM_OK;
+}
+
+int adjoint_prepare(mfdm_model* m) {
+  if (m->batch || m->nshots != 1)
+    return fail(MFDM_ERR_ARG, "the adjoint runs on plain (single-shot) handles");
+  if (!m->adj) {
+    m->adj = new AdjointState();
+    AdjointState* a = m->adj;
+    a->L = set_layout(m);
+    const size_t n = size_t(a->L.len);
+    int rc;
+    if ((rc = dalloc(&a->mask, n)) || (rc = dalloc(&a->lam, n)) || (rc = dalloc(&a->mu, n)) ||
+        (rc = dalloc(&a->kb[0], n)) || (rc = dalloc(&a->kb[1], n)) ||
+        (rc = dalloc(&a->tmp, size_t(8) * m->cfg.nx)) ||
+        (rc = dalloc(&a->grad, size_t(2) * m->cfg.nzf * m->P + size_t(5) * m->cfg.nzs * m->P)))
+      return rc;
+  }
+  if (!m->adj->built) return adjoint_build(m);
+  return MFDM_OK;
+}
+
+double* grad_array(mfdm_model* m, int k) {
+  const size_t nf = size_t(m->cfg.nzf) * m->P, ns = size_t(m->cfg.nzs) * m->P;
+  return m->adj->grad + (k < 2 ? size_t(k) * nf : 2 * nf + size_t(k - 2) * ns);
+}
+
+// Transposed step n: lam holds lambda^{n+1} on entry and lambda^n on return;
+// `slot` holds the step's four stage inputs.
+int reverse_step(mfdm_model* m, int n, float* slot) {
+  AdjointState* a = m->adj;
+  const mfdm::SetLayout& L = a->L;
+  const long long len = L.len;
+  cudaStream_t st = m->stream;
+  const Coef& C = m->C;
+  const int d0 = (n & 1) ? mfdm::kDirB : mfdm::kDirF, d1 = 1 - d0;
+  Fields Y[4];
+  for (int s = 0; s < 4; ++s) Y[s] = fields_at(L, slot + size_t(s) * size_t(len));
+  const Fields K0 = fields_at(L, a->kb[0]), K1 = fields_at(L, a->kb[1]);
+  double* g[7];
+  for (int k = 0; k < 7; ++k) g[k] = grad_array(m, k);
+  const float *c = C.rk_c, *w = C.rk_w;
+  if (n % m->gap == 0)
+    MFDM_CU(mfdm::adj::inject(a->lam, L, a->res + size_t(n / m->gap) * 3 * m->cfg.nx, st));
+  MFDM_CU(mfdm::adj::filter_t(a->lam, L, C, a->tmp, st));
+  MFDM_CU(mfdm::adj::start(a->lam, a->mu, a->kb[0], a->mask, len, c[3], st));
+  MFDM_CU(mfdm::adj::gradient(C, Y[3], K0, g, d1, st));
+  MFDM_CU(mfdm::adj::reverse_stage(a->A[d1], len, a->kb[0], a->lam, a->mask, true, a->kb[1], a->mu, w[2], c[2], st));
+  MFDM_CU(mfdm::adj::gradient(C, Y[2], K1, g, d0, st));
+  MFDM_CU(mfdm::adj::reverse_stage(a->A[d0], len, a->kb[1], a->lam, a->mask, true, a->kb[0], a->mu, w[1], c[1], st));
+  MFDM_CU(mfdm::adj::gradient(C, Y[1], K0, g, d1, st));
+  MFDM_CU(mfdm::adj::reverse_stage(a->A[d1], len, a->kb[0], a->lam, a->mask, true, a->kb[1], a->mu, w[0], c[0], st));
+  MFDM_CU(mfdm::adj::gradient(C, Y[0], K1, g, d0, st));
+  MFDM_CU(mfdm::adj::reverse_stage(a->A[d0], len, a->kb[1], a->lam, a->mask, false, nullptr, a->mu, 0.f, 0.f, st));
+  return MFDM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mfdm_adjoint_forward(mfdm_model* m, int nsteps, int ckpt_every) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  if (nsteps < 1 || ckpt_every < 1) return fail(MFDM_ERR_ARG, "need nsteps >= 1 and ckpt_every >= 1");
+  DeviceGuard g(m->device);
+  int rc;
+  if ((rc = adjoint_prepare(m)) != MFDM_OK) return rc;
+  AdjointState* a = m->adj;
+  const size_t len = size_t(a->L.len);
+  const size_t ncp = size_t((nsteps + ckpt_every - 1) / ckpt_every);
+  if (ncp > a->ckpt_sets) {
+    cudaFree(a->ckpt);
+    a->ckpt = nullptr;
+    a->ckpt_sets = 0;
+    if ((rc = dalloc(&a->ckpt, ncp * len)) != MFDM_OK) return rc;
+    a->ckpt_sets = ncp;
+  }
+  a->nsteps = -1;
+  if ((rc = clear_state(m)) != MFDM_OK) return rc;
+  if ((rc = rewind(m)) != MFDM_OK) return rc;
+  if ((rc = ensure_capacity(m, nsteps)) != MFDM_OK) return rc;
+  for (size_t k = 0; k < ncp; ++k) {
+    MFDM_CU(cudaMemcpyAsync(a->ckpt + k * len, m->S[0].fvx, len * sizeof(float),
+                            cudaMemcpyDeviceToDevice, m->stream));
+    const int todo = std::min(ckpt_every, nsteps - int(k) * ckpt_every);
+    if ((rc = enqueue_steps(m, todo)) != MFDM_OK) return rc;
+  }
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  if ((rc = check_status(m)) != MFDM_OK) return rc;
+  a->nsteps = nsteps;
+  a->every = ckpt_every;
+  return MFDM_OK;
+}
+
+int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_svz,
+                          const float* res_fp, mfdm_coef_grad* out) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  AdjointState* a = m->adj;
+  if (!a || a->nsteps < 1 || m->host_step != a->nsteps)
+    return fail(MFDM_ERR_ARG, "mfdm_adjoint_backward needs the mfdm_adjoint_forward run just before it");
+  DeviceGuard g(m->device);
+  int rc;
+  const int nsteps = a->nsteps, every = a->every, nx = m->cfg.nx;
+  const size_t len = size_t(a->L.len);
+  const int ns = (nsteps + m->gap - 1) / m->gap;
+  // residuals, [ns][3][nx] in the receiver-buffer order (svx, svz, fp)
+  const size_t rf = size_t(ns) * 3 * nx;
+  if (rf > a->res_floats) {
+    cudaFree(a->res);
+    a->res = nullptr;
+    a->res_floats = 0;
+    if ((rc = dalloc(&a->res, rf)) != MFDM_OK) return rc;
+    a->res_floats = rf;
+  }
+  {
+    std::vector<float> h(rf, 0.f);
+    const float* src[3] = {res_svx, res_svz, res_fp};
+    for (int j = 0; j < ns; ++j)
+      for (int q = 0; q < 3; ++q)
+        if (src[q]) std::memcpy(&h[(size_t(j) * 3 + q) * nx], src[q] + size_t(j) * nx, nx * sizeof(float));
+    MFDM_CU(cudaMemcpy(a->res, h.data(), rf * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  if (size_t(every) > a->seg_steps) {
+    cudaFree(a->seg);
+    a->seg = nullptr;
+    a->seg_steps = 0;
+    if ((rc = dalloc(&a->seg, size_t(every) * 4 * len)) != MFDM_OK) return rc;
+    a->seg_steps = size_t(every);
+  }
+  cudaStream_t st = m->stream;
+  const size_t gbytes = (size_t(2) * m->cfg.nzf * m->P + size_t(5) * m->cfg.nzs * m->P) * sizeof(double);
+  MFDM_CU(cudaMemsetAsync(a->grad, 0, gbytes, st));
+  MFDM_CU(cudaMemsetAsync(a->lam, 0, len * sizeof(float), st));
+  a->nsteps = -1;
+  const int ncp = (nsteps + every - 1) / every;
+  for (int k = ncp - 1; k >= 0; --k) {
+    const int t0 = k * every, t1 = std::min(nsteps, t0 + every);
+    // recompute the segment from its checkpoint, keeping every stage input
+    MFDM_CU(cudaMemcpyAsync(m->S[0].fvx, a->ckpt + size_t(k) * len, len * sizeof(float),
+                            cudaMemcpyDeviceToDevice, st));
+    MFDM_CU(mfdm::launch_set_step(m->C, t0, st));
+    for (int n = t0; n < t1; ++n) {
+      float* slot = a->seg + size_t(n - t0) * 4 * len;
+      float* save[4] = {slot, slot + len, slot + 2 * len, slot + 3 * len};
+      if ((rc = enqueue_step(m, n, st, nullptr, save)) != MFDM_OK) return rc;
+    }
+    for (int n = t1 - 1; n >= t0; --n)
+      if ((rc = reverse_step(m, n, a->seg + size_t(n - t0) * 4 * len)) != MFDM_OK) return rc;
+  }
+  MFDM_CU(cudaStreamSynchronize(st));
+  if (out) {
+    double* dst[7] = {out->K, out->rcp_rho_f, out->C11, out->C13, out->C33, out->C55, out->rcp_rho_s};
+    for (int k = 0; k < 7; ++k) {
+      if (!dst[k]) continue;
+      const int rows = k < 2 ? m->cfg.nzf : m->cfg.nzs;
+      MFDM_CU(cudaMemcpy2D(dst[k], size_t(nx) * sizeof(double), grad_array(m, k),
+                           size_t(m->P) * sizeof(double), size_t(nx) * sizeof(double), size_t(rows),
+                           cudaMemcpyDeviceToHost));
+    }
+  }
+  // the recomputation left a mid-run state: back to rest
+  if ((rc = clear_state(m)) != MFDM_OK) return rc;
+  if ((rc = rewind(m)) != MFDM_OK) return rc;
+  return check_status(m);
 }
 
 }  // extern "C"

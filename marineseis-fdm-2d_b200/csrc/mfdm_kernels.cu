@@ -107,26 +107,6 @@ struct SolidRing : RingAcc<5> {
   __device__ __forceinline__ float ssz(int dz, int dx) const { return at(3, dz, dx); }
   __device__ __forceinline__ float ssxz(int dz, int dx) const { return at(4, dz, dx); }
 };
-// Direct reads of the stage input (interface strip).
-struct FluidGlobal {
-  const float *vx, *vz, *p;
-  size_t base;
-  int P;
-  __device__ __forceinline__ float fvx(int dz, int dx) const { return __ldg(vx + base + (ptrdiff_t)dz * P + dx); }
-  __device__ __forceinline__ float fvz(int dz, int dx) const { return __ldg(vz + base + (ptrdiff_t)dz * P + dx); }
-  __device__ __forceinline__ float fp(int dz, int dx) const { return __ldg(p + base + (ptrdiff_t)dz * P + dx); }
-};
-struct SolidGlobal {
-  const float *vx, *vz, *sx, *sz, *sxz;
-  size_t base;
-  int P;
-  __device__ __forceinline__ float svx(int dz, int dx) const { return __ldg(vx + base + (ptrdiff_t)dz * P + dx); }
-  __device__ __forceinline__ float svz(int dz, int dx) const { return __ldg(vz + base + (ptrdiff_t)dz * P + dx); }
-  __device__ __forceinline__ float ssx(int dz, int dx) const { return __ldg(sx + base + (ptrdiff_t)dz * P + dx); }
-  __device__ __forceinline__ float ssz(int dz, int dx) const { return __ldg(sz + base + (ptrdiff_t)dz * P + dx); }
-  __device__ __forceinline__ float ssxz(int dz, int dx) const { return __ldg(sxz + base + (ptrdiff_t)dz * P + dx); }
-};
-
 // Geometry of one segment block.
 struct Segment {
   int x0;     // first computed column of the strip
@@ -501,33 +481,9 @@ __device__ __forceinline__ void interface_strip(const Coef& C, const Fields& in,
 
   // ---- coupling of the stage RHS on the interface ----
   const float2 n = __ldg(C.nrm + ix);
-  const float vxf = kf.vx, vzf = kf.vz;
-  float pf = kf.p;
-  const float vxs = ks.vx, vzs = ks.vz, sxx = ks.sx, szz = ks.sz, sxz = ks.sxz;
-  float vnf = n.x * vxf + n.y * vzf;
-  const float vtf = n.y * vxf - n.x * vzf;
-  float vns = n.x * vxs + n.y * vzs;
-  const float vts = n.y * vxs - n.x * vzs;
-  float snn = n.x * n.x * sxx + 2 * n.x * n.y * sxz + n.y * n.y * szz;
-  float snt = n.x * n.y * (sxx - szz) + (n.y * n.y - n.x * n.x) * sxz;
-  const float stt = n.y * n.y * sxx - 2 * n.x * n.y * sxz + n.x * n.x * szz;
-  if (DIR == kDirF) {  // fluid takes the solid's normal velocity and traction
-    vnf = vns;
-    pf = -snn;
-    snt = 0.f;
-  } else {             // solid takes the fluid's
-    vns = vnf;
-    snn = -pf;
-    snt = 0.f;
-  }
-  const float kv[8] = {n.x * vnf + n.y * vtf,
-                       n.y * vnf - n.x * vtf,
-                       pf,
-                       n.x * vns + n.y * vts,
-                       n.y * vns - n.x * vts,
-                       n.x * n.x * snn + 2 * n.x * n.y * snt + n.y * n.y * stt,
-                       n.y * n.y * snn - 2 * n.x * n.y * snt + n.x * n.x * stt,
-                       -n.x * n.y * stt + (n.y * n.y - n.x * n.x) * snt};
+  const float kfv[3] = {kf.vx, kf.vz, kf.p}, ksv[5] = {ks.vx, ks.vz, ks.sx, ks.sz, ks.sxz};
+  float kv[8];
+  couple_rhs<DIR>(n, kfv, ksv, kv);
   const float uin[8] = {Af.fvx(0, 0), Af.fvz(0, 0), Af.fp(0, 0), As.svx(0, 0),
                         As.svz(0, 0), As.ssx(0, 0), As.ssz(0, 0), As.ssxz(0, 0)};
   float* const outs[8] = {out.fvx, out.fvz, out.fp, out.svx, out.svz, out.ssx, out.ssz, out.ssxz};
@@ -625,25 +581,20 @@ __global__ void __launch_bounds__(kFinishThreads) finish_kernel(Coef C0, Fields 
         if (k >= klo && k <= khi) sum += c_w7[k + 3] * t[k + 3];
       v[f] = sum / wsum;
     }
-    const float2 n = __ldg(C.nrm + ix);
-    const float vnf = n.x * v[0] + n.y * v[1], vtf = n.y * v[0] - n.x * v[1];
-    const float vns = n.x * v[3] + n.y * v[4], vts = n.y * v[3] - n.x * v[4];
-    const float snn = n.x * n.x * v[5] + 2.0f * n.x * n.y * v[7] + n.y * n.y * v[6];
-    const float stt = n.y * n.y * v[5] - 2.0f * n.x * n.y * v[7] + n.x * n.x * v[6];
-    const float vn = 0.5f * (vnf + vns);
-    const float sn = 0.5f * (snn - v[2]);
+    float u[8];
+    interface_average(__ldg(C.nrm + ix), v, u);
     const size_t fi = (size_t)(nzf - 1) * P + ix;
-    U.fvx[fi] = n.x * vn + n.y * vtf;
-    U.fvz[fi] = n.y * vn - n.x * vtf;
-    U.fp[fi] = -sn;
-    r0 = n.x * vn + n.y * vts;
-    r1 = n.y * vn - n.x * vts;
-    r2 = -sn;
-    U.svx[ix] = r0;
-    U.svz[ix] = r1;
-    U.ssx[ix] = n.x * n.x * sn + n.y * n.y * stt;
-    U.ssz[ix] = n.y * n.y * sn + n.x * n.x * stt;
-    U.ssxz[ix] = n.x * n.y * (sn - stt);
+    U.fvx[fi] = u[0];
+    U.fvz[fi] = u[1];
+    U.fp[fi] = u[2];
+    r0 = u[3];
+    r1 = u[4];
+    r2 = u[2];
+    U.svx[ix] = u[3];
+    U.svz[ix] = u[4];
+    U.ssx[ix] = u[5];
+    U.ssz[ix] = u[6];
+    U.ssxz[ix] = u[7];
     if (!(isfinite(r0) && isfinite(r1) && isfinite(r2))) atomicOr(C.status, 1);
   }
   if (ix < nx && C.rec != nullptr && C.gap > 0 && it % C.gap == 0) {
