@@ -1,6 +1,8 @@
 // sm_100a kernels of the adjoint-state backward (see mfdm_adjoint.h).
 #include <cub/device/device_scan.cuh>
 
+#include <algorithm>
+
 #include "mfdm_adjoint.h"
 
 namespace mfdm {
@@ -63,6 +65,21 @@ __device__ __forceinline__ bool locate(const SetLayout& L, long long i, int& a, 
   r = int(loc / L.pitch[a]);
   c = int(loc % L.pitch[a]);
   return r < L.rows[a] && c < L.ncols[a];
+}
+
+// Output cells where the forward stage evaluates the plain interior formula:
+// main fields, outside the xi strips, fluid rows 6..nz_f-4 (four-side CPML:
+// below the top band, npd+3..nz_f-4), solid rows 3 .. nz_s-4-npd (above the
+// zeta strip). Everywhere else (strips, conservative and one-sided rows, the
+// interface) the CSR part of the transposed operator applies.
+__device__ __forceinline__ bool interior_cell(const SetLayout& L, int a, int r, int c) {
+  if (a >= 8) return false;
+  if (c < 3 + L.npd || c > L.nx - 4 - L.npd) return false;
+  if (a < 3) {
+    const int lo = L.cpml ? max(3, L.npd + 3) : 6;
+    return r >= lo && r <= L.nzf - 4;
+  }
+  return r >= 3 && r < L.nzs - 3 - L.npd;
 }
 
 __global__ void k_set_lattice(float* set, SetLayout L, int a, int cz, int cx, float v) {
@@ -143,22 +160,6 @@ __device__ __forceinline__ float row_dot(const long long* __restrict__ rowptr,
 #pragma unroll
   for (int o = kLanes / 2; o > 0; o >>= 1) s += __shfl_xor_sync(grp, s, o);
   return s;
-}
-
-template <bool MASK_LAM, bool NEXT>
-__global__ void k_reverse(const long long* __restrict__ rowptr, const int* __restrict__ col,
-                          const float* __restrict__ val, const float* __restrict__ kb, float* lam,
-                          const uint8_t* __restrict__ mask, float* kbn, const float* __restrict__ mu,
-                          float w, float c, long long len) {
-  const long long row = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / kLanes;
-  const int lane = threadIdx.x % kLanes;
-  if (row >= len) return;  // whole groups leave together
-  const float y = row_dot(rowptr, col, val, kb, row, lane);
-  if (lane == 0) {
-    const float m = mask[row] ? 1.0f : 0.0f;
-    lam[row] += MASK_LAM ? m * y : y;
-    if (NEXT) kbn[row] = m * fmaf(c, y, w * mu[row]);
-  }
 }
 
 __global__ void k_apply_t(const long long* __restrict__ rowptr, const int* __restrict__ col,
@@ -242,22 +243,144 @@ __global__ void k_start(const float* __restrict__ lam, float* mu, float* kb,
   }
 }
 
+__global__ void k_drop_count(const long long* __restrict__ rowptr, const int* __restrict__ col,
+                             SetLayout L, unsigned long long* count) {
+  const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (j >= L.len) return;
+  unsigned long long n = 0;
+  for (long long k = rowptr[j]; k < rowptr[j + 1]; ++k) {
+    int a, r, c;
+    if (!(locate(L, col[k], a, r, c) && interior_cell(L, a, r, c))) ++n;
+  }
+  count[j] = n;
+}
+
+__global__ void k_drop_fill(const long long* __restrict__ rowptr, const int* __restrict__ col,
+                            const float* __restrict__ val, SetLayout L,
+                            const long long* __restrict__ rp2, int* col2, float* val2) {
+  const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (j >= L.len) return;
+  long long o = rp2[j];
+  for (long long k = rowptr[j]; k < rowptr[j + 1]; ++k) {
+    int a, r, c;
+    if (!(locate(L, col[k], a, r, c) && interior_cell(L, a, r, c))) {
+      col2[o] = col[k];
+      val2[o] = val[k];
+      ++o;
+    }
+  }
+}
+
+// Q fields of the transposed interior formulas at every main-field cell (0
+// outside the interior set). For an interior output cell i the forward stage is
+// (pml_fs_kernels.cuh:333-752, interior branches)
+//   fluid  k_vx = -r (xix Dx p + zex Dz p),  k_vz = -r (xiz Dx p + zez Dz p),
+//          k_p  = -K (xix Dx vx + zex Dz vx + xiz Dx vz + zez Dz vz)
+//   solid  k_vx = r (xix Dx sx + zex Dz sx + xiz Dx sxz + zez Dz sxz),
+//          k_vz = r (xix Dx sxz + zex Dz sxz + xiz Dx sz + zez Dz sz),
+//          k_sx = c11 (xix Dx vx + zex Dz vx) + c13 (xiz Dx vz + zez Dz vz),
+//          k_sz = c13 (xix Dx vx + zex Dz vx) + c33 (xiz Dx vz + zez Dz vz),
+//          k_sxz = c55 (xiz' Dx vx + zez' Dz vx + xix' Dx vz + zex' Dz vz)
+// (r = 1/rho; the primed metric is read at global row iz in the four-side CPML
+// variant, cpml_kernels.cuh:448-455), so the Dx / Dz coefficient of every
+// (output, input) pair times x at i, summed per input field, gives qx / qz.
+// Q fields of fluid cell (r, c); only interior cells are non-zero.
+__device__ __forceinline__ void q_fluid(const Coef& C, const SetLayout& L, const float* __restrict__ x,
+                                        float* qx, float* qz, int r, int c, bool write_zero) {
+  const size_t g = (size_t)r * C.P + c;
+  const long long i0 = L.off[0] + g, i1 = L.off[1] + g, i2 = L.off[2] + g;
+  if (!interior_cell(L, 0, r, c)) {
+    if (write_zero) {
+      qx[i0] = 0.f; qz[i0] = 0.f; qx[i1] = 0.f; qz[i1] = 0.f; qx[i2] = 0.f; qz[i2] = 0.f;
+    }
+    return;
+  }
+  const float xix = __ldg(C.xix + g), xiz = __ldg(C.xiz + g), zex = __ldg(C.zex + g),
+              zez = __ldg(C.zez + g), rr = __ldg(C.rhof + g), K = __ldg(C.K + g);
+  const float kvx = x[i0], kvz = x[i1], kp = x[i2];
+  qx[i2] = -rr * (xix * kvx + xiz * kvz);
+  qz[i2] = -rr * (zex * kvx + zez * kvz);
+  qx[i0] = -K * xix * kp;
+  qz[i0] = -K * zex * kp;
+  qx[i1] = -K * xiz * kp;
+  qz[i1] = -K * zez * kp;
+}
+
+// Q fields of solid cell (r, c); only interior cells are non-zero.
+template <bool CPML>
+__device__ __forceinline__ void q_solid(const Coef& C, const SetLayout& L, const float* __restrict__ x,
+                                        float* qx, float* qz, int r, int c, bool write_zero) {
+  const int P = C.P;
+  const size_t m = (size_t)r * P + c, g = m + (size_t)(L.nzf - 1) * P;
+  float q[10] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // (x, z) for vx, vz, sx, sz, sxz
+  if (interior_cell(L, 3, r, c)) {
+    const float xix = __ldg(C.xix + g), xiz = __ldg(C.xiz + g), zex = __ldg(C.zex + g),
+                zez = __ldg(C.zez + g);
+    const size_t b = CPML ? m : g;
+    const float bxix = __ldg(C.xix + b), bxiz = __ldg(C.xiz + b), bzex = __ldg(C.zex + b),
+                bzez = __ldg(C.zez + b);
+    const float rr = __ldg(C.rhos + m), c11 = __ldg(C.C11 + m), c13 = __ldg(C.C13 + m),
+                c33 = __ldg(C.C33 + m), c55 = __ldg(C.C55 + m);
+    const float kvx = x[L.off[3] + m], kvz = x[L.off[4] + m], ksx = x[L.off[5] + m],
+                ksz = x[L.off[6] + m], ksxz = x[L.off[7] + m];
+    const float a1 = c11 * ksx + c13 * ksz, a2 = c13 * ksx + c33 * ksz;
+    q[0] = xix * a1 + c55 * bxiz * ksxz;   // vx, x
+    q[1] = zex * a1 + c55 * bzez * ksxz;   // vx, z
+    q[2] = xiz * a2 + c55 * bxix * ksxz;   // vz, x
+    q[3] = zez * a2 + c55 * bzex * ksxz;   // vz, z
+    q[4] = rr * xix * kvx;                 // sx
+    q[5] = rr * zex * kvx;
+    q[6] = rr * xiz * kvz;                 // sz
+    q[7] = rr * zez * kvz;
+    q[8] = rr * (xiz * kvx + xix * kvz);   // sxz
+    q[9] = rr * (zez * kvx + zex * kvz);
+  } else if (!write_zero) {
+    return;
+  }
+#pragma unroll
+  for (int f = 0; f < 5; ++f) {
+    qx[L.off[3 + f] + m] = q[2 * f];
+    qz[L.off[3 + f] + m] = q[2 * f + 1];
+  }
+}
+
+template <bool CPML>
+__global__ void k_qfields(Coef C, SetLayout L, const float* __restrict__ x, float* qx, float* qz) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = blockIdx.y;
+  if (c >= L.nx) return;
+  if (row < L.nzf) q_fluid(C, L, x, qx, qz, row, c, true);
+  else q_solid<CPML>(C, L, x, qx, qz, row - L.nzf, c, true);
+}
+
 // ---- material gradients ----------------------------------------------------------
 
 struct Grad {
   double *K, *rf, *c11, *c13, *c33, *c55, *rs;
 };
 
-// Fluid rows 3..nz_f-2 then solid rows 1..nz_s-4 (blockIdx.y), columns 3..nx-4.
 template <int DIR, bool CPML>
-__global__ void __launch_bounds__(128) k_grad_cells(Coef C, Fields Y, Fields KB, Grad G) {
+__device__ __forceinline__ void grad_iface(const Coef& C, const Fields& Y, const Fields& KB,
+                                           const Grad& G, int ix);
+
+// blockIdx.y = 0: the interface columns (first, they take longest); then fluid
+// rows 3..nz_f-2 and solid rows 1..nz_s-4; columns 3..nx-4. Interior cells also
+// write the Q fields of the stage adjoint (kb) for the transposed operator.
+template <int DIR, bool CPML>
+__global__ void __launch_bounds__(128) k_grad_cells(Coef C, SetLayout L, Fields Y, Fields KB,
+                                                    const float* __restrict__ kb, float* qx,
+                                                    float* qz, Grad G) {
   const int ix = blockIdx.x * blockDim.x + threadIdx.x;
   const int nx = C.nx, P = C.P, nzf = C.nzf, nzs = C.nzs, npd = C.npd;
   if (ix < 3 || ix > nx - 4) return;
+  if (blockIdx.y == 0) {
+    grad_iface<DIR, CPML>(C, Y, KB, G, ix);
+    return;
+  }
   const bool side = min(ix - 3, nx - 4 - ix) < npd;
   const int scol = side ? xstrip_col(ix, nx, npd) : 0;
   const int nfr = nzf - 4;
-  const int row = blockIdx.y;
+  const int row = blockIdx.y - 1;
   if (row < nfr) {
     const int iz = 3 + row;
     const size_t g = (size_t)iz * P + ix;
@@ -274,6 +397,7 @@ __global__ void __launch_bounds__(128) k_grad_cells(Coef C, Fields Y, Fields KB,
     // velocity terms carry 1/rho, the pressure term K
     G.rf[g] += double(__ldg(KB.fvx + g)) * o.vx + double(__ldg(KB.fvz + g)) * o.vz;
     G.K[g] += double(__ldg(KB.fp + g)) * o.p;
+    if (qx) q_fluid(C, L, kb, qx, qz, iz, ix, false);
     return;
   }
   const int iz = 1 + row - nfr;
@@ -301,14 +425,14 @@ __global__ void __launch_bounds__(128) k_grad_cells(Coef C, Fields Y, Fields KB,
   G.c55[m] += ksxz * o1.sxz;
   G.rs[m] += kvx * o1.vx + kvz * o1.vz;
   G.c13[m] += ksx * o2.sx + ksz * o2.sz;
+  if (qx) q_solid<CPML>(C, L, kb, qx, qz, iz, ix, false);
 }
 
 // Interface column ix: both media's RHS at the interface row, coupled, per coefficient.
 template <int DIR, bool CPML>
-__global__ void __launch_bounds__(128) k_grad_iface(Coef C, Fields Y, Fields KB, Grad G) {
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void grad_iface(const Coef& C, const Fields& Y, const Fields& KB,
+                                           const Grad& G, int ix) {
   const int nx = C.nx, P = C.P, nzf = C.nzf, nzs = C.nzs, npd = C.npd;
-  if (ix < 3 || ix > nx - 4) return;
   const bool side = min(ix - 3, nx - 4 - ix) < npd;
   const int scol = side ? xstrip_col(ix, nx, npd) : 0;
   const int zb0 = nzs - 3 - npd;
@@ -359,6 +483,73 @@ __global__ void __launch_bounds__(128) k_grad_iface(Coef C, Fields Y, Fields KB,
   G.c33[si] += coupled(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, o1.sz, 0.f);
   G.c55[si] += coupled(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, o1.sxz);
   G.c13[si] += coupled(0.f, 0.f, 0.f, 0.f, 0.f, o2.sx, o2.sz, 0.f);
+}
+
+// Transposed interior stencil at input cell (a, r, c): D_F^T g (j) = sum_t a_t g(j - t),
+// D_B^T g (j) = -sum_t a_t g(j + t), taps t = -1..3 of the DRP pair.
+template <int DIR>
+__device__ __forceinline__ float t_stencil(const SetLayout& L, const float* __restrict__ qx,
+                                           const float* __restrict__ qz, int a, int r, int c) {
+  const float at[5] = {kAm1, kA0, kA1, kA2, kA3};
+  const long long base = L.off[a];
+  const int P = L.pitch[a], rows = L.rows[a], ncols = L.ncols[a];
+  float s = 0.0f;
+#pragma unroll
+  for (int t = -1; t <= 3; ++t) {
+    const int cc = DIR == kDirF ? c - t : c + t, rr = DIR == kDirF ? r - t : r + t;
+    if (cc >= 0 && cc < ncols) s = fmaf(at[t + 1], __ldg(qx + base + (long long)r * P + cc), s);
+    if (rr >= 0 && rr < rows) s = fmaf(at[t + 1], __ldg(qz + base + (long long)rr * P + c), s);
+  }
+  return DIR == kDirF ? s : -s;
+}
+
+// One thread per row of L^T: the sparse rest plus, on main-field cells, the
+// transposed interior stencil; then the RK bookkeeping of the reverse stage.
+template <int DIR, int MODE>  // MODE 0: y only; 1: lam += y; 2: lam += M y, kbn; 3: lam += M y
+__global__ void k_reverse_h(const long long* __restrict__ rowptr, const int* __restrict__ col,
+                            const float* __restrict__ val, const float* __restrict__ kb,
+                            const float* __restrict__ qx, const float* __restrict__ qz, SetLayout L,
+                            float* y_or_lam, const uint8_t* __restrict__ mask, float* kbn,
+                            const float* __restrict__ mu, float w, float cw) {
+  const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (j >= L.len) return;
+  float y = 0.0f;
+  for (long long k = rowptr[j]; k < rowptr[j + 1]; ++k) y = fmaf(val[k], __ldg(kb + col[k]), y);
+  {
+    // the fluid block (3 arrays of nz_f rows) and the solid block (5 of nz_s)
+    // are contiguous at pitch P
+    const long long P = L.pitch[0], nf = (long long)L.nzf * P, ns = (long long)L.nzs * P;
+    long long rel = j - L.off[0];
+    int a = -1;
+    long long loc = 0;
+    if (rel >= 0 && rel < 3 * nf) {
+      a = int(rel / nf);
+      loc = rel - a * nf;
+    } else if ((rel = j - L.off[3]) >= 0 && rel < 5 * ns) {
+      a = 3 + int(rel / ns);
+      loc = rel - (a - 3) * ns;
+    }
+    if (a >= 0) {
+      const int r = int(loc / P), c = int(loc - r * P);
+      if (c < L.nx) y += t_stencil<DIR>(L, qx, qz, a, r, c);
+    }
+  }
+  if (MODE == 0) {
+    y_or_lam[j] = y;
+    return;
+  }
+  const float m = mask[j] ? 1.0f : 0.0f;
+  y_or_lam[j] += MODE == 1 ? y : m * y;
+  if (MODE == 2) kbn[j] = m * fmaf(cw, y, w * mu[j]);
+}
+
+__global__ void k_random(float* x, long long n, unsigned seed) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    unsigned h = unsigned(i) * 2654435761u ^ seed;
+    h ^= h >> 15; h *= 2246822519u; h ^= h >> 13; h *= 3266489917u; h ^= h >> 16;
+    x[i] = float(h) * (2.0f / 4294967296.0f) - 1.0f;
+  }
 }
 
 unsigned grid_for(long long n, int block) {
@@ -414,24 +605,68 @@ cudaError_t sort_rows(const CsrT& A, long long len, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-cudaError_t reverse_stage(const CsrT& A, long long len, const float* kb, float* lam,
-                          const uint8_t* mask, bool mask_lam, float* kbn, const float* mu, float w,
-                          float c, cudaStream_t st) {
-  const unsigned grid = unsigned((len * kLanes + kBlock - 1) / kBlock);
-  if (mask_lam && kbn)
-    k_reverse<true, true><<<grid, kBlock, 0, st>>>(A.rowptr, A.col, A.val, kb, lam, mask, kbn, mu, w, c, len);
-  else if (mask_lam)
-    k_reverse<true, false><<<grid, kBlock, 0, st>>>(A.rowptr, A.col, A.val, kb, lam, mask, kbn, mu, w, c, len);
-  else if (kbn)
-    k_reverse<false, true><<<grid, kBlock, 0, st>>>(A.rowptr, A.col, A.val, kb, lam, mask, kbn, mu, w, c, len);
-  else
-    k_reverse<false, false><<<grid, kBlock, 0, st>>>(A.rowptr, A.col, A.val, kb, lam, mask, kbn, mu, w, c, len);
+cudaError_t drop_interior(const CsrT& full, const SetLayout& L, CsrT* rest,
+                          unsigned long long* count, void** tmp, size_t* tmp_bytes, cudaStream_t st) {
+  const unsigned g = unsigned((L.len + kBlock - 1) / kBlock);
+  k_drop_count<<<g, kBlock, 0, st>>>(full.rowptr, full.col, L, count);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(count + L.len, 0, sizeof(unsigned long long), st)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&rest->rowptr, size_t(L.len + 1) * sizeof(long long))) != cudaSuccess) return e;
+  if ((e = scan(count, rest->rowptr, L.len, tmp, tmp_bytes, st)) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(&rest->nnz, rest->rowptr + L.len, sizeof(long long),
+                           cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return e;
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&rest->col, size_t(std::max<long long>(rest->nnz, 1)) * sizeof(int))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&rest->val, size_t(std::max<long long>(rest->nnz, 1)) * sizeof(float))) != cudaSuccess) return e;
+  k_drop_fill<<<g, kBlock, 0, st>>>(full.rowptr, full.col, full.val, L, rest->rowptr, rest->col, rest->val);
   return cudaGetLastError();
 }
 
-cudaError_t apply_t(const CsrT& A, long long len, const float* x, float* y, cudaStream_t st) {
-  const unsigned grid = unsigned((len * kLanes + kBlock - 1) / kBlock);
-  k_apply_t<<<grid, kBlock, 0, st>>>(A.rowptr, A.col, A.val, x, y, len);
+cudaError_t random_fill(float* x, long long n, unsigned seed, cudaStream_t st) {
+  k_random<<<grid_for(n, kBlock), kBlock, 0, st>>>(x, n, seed);
+  return cudaGetLastError();
+}
+
+template <int DIR, int MODE>
+static cudaError_t hybrid_t(const HybridT& H, const Coef& C, const SetLayout& L, const float* kb,
+                            float* out, const uint8_t* mask, float* kbn, const float* mu, float w,
+                            float c, bool q_ready, cudaStream_t st) {
+  if (!q_ready) {
+    const dim3 gq(unsigned((L.nx + 127) / 128), unsigned(L.nzf + L.nzs));
+    if (L.cpml) k_qfields<true><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz);
+    else k_qfields<false><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  k_reverse_h<DIR, MODE><<<unsigned((L.len + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+      H.rest.rowptr, H.rest.col, H.rest.val, kb, H.qx, H.qz, L, out, mask, kbn, mu, w, c);
+  return cudaGetLastError();
+}
+
+template <int MODE>
+static cudaError_t hybrid_dir(const HybridT& H, const Coef& C, const SetLayout& L, int dir,
+                              const float* kb, float* out, const uint8_t* mask, float* kbn,
+                              const float* mu, float w, float c, bool q_ready, cudaStream_t st) {
+  return dir == kDirF ? hybrid_t<kDirF, MODE>(H, C, L, kb, out, mask, kbn, mu, w, c, q_ready, st)
+                      : hybrid_t<kDirB, MODE>(H, C, L, kb, out, mask, kbn, mu, w, c, q_ready, st);
+}
+
+cudaError_t reverse_stage(const HybridT& H, const Coef& C, const SetLayout& L, int dir,
+                          const float* kb, float* lam, const uint8_t* mask, bool mask_lam,
+                          float* kbn, const float* mu, float w, float c, bool q_ready,
+                          cudaStream_t st) {
+  if (!mask_lam) return hybrid_dir<1>(H, C, L, dir, kb, lam, mask, kbn, mu, w, c, q_ready, st);
+  if (kbn) return hybrid_dir<2>(H, C, L, dir, kb, lam, mask, kbn, mu, w, c, q_ready, st);
+  return hybrid_dir<3>(H, C, L, dir, kb, lam, mask, kbn, mu, w, c, q_ready, st);
+}
+
+cudaError_t apply_t(const HybridT& H, const Coef& C, const SetLayout& L, int dir, const float* x,
+                    float* y, cudaStream_t st) {
+  if (H.qx) return hybrid_dir<0>(H, C, L, dir, x, y, nullptr, nullptr, nullptr, 0.f, 0.f, false, st);
+  const unsigned grid = unsigned((L.len * kLanes + kBlock - 1) / kBlock);
+  k_apply_t<<<grid, kBlock, 0, st>>>(H.rest.rowptr, H.rest.col, H.rest.val, x, y, L.len);
   return cudaGetLastError();
 }
 
@@ -458,23 +693,32 @@ cudaError_t start(const float* lam, float* mu, float* kb, const uint8_t* mask, l
 }
 
 template <int DIR, bool CPML>
-static cudaError_t gradient_t(const Coef& C, const Fields& Y, const Fields& KB, const Grad& G,
-                              cudaStream_t st) {
-  const int rows = (C.nzf - 4) + (C.nzs - 4);
+static cudaError_t gradient_t(const Coef& C, const SetLayout& L, const Fields& Y, const Fields& KB,
+                              const float* kb, float* qx, float* qz, const Grad& G, cudaStream_t st) {
+  const int rows = 1 + (C.nzf - 4) + (C.nzs - 4);
   const unsigned gx = unsigned((C.nx + 127) / 128);
-  k_grad_cells<DIR, CPML><<<dim3(gx, unsigned(rows)), 128, 0, st>>>(C, Y, KB, G);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  k_grad_iface<DIR, CPML><<<gx, 128, 0, st>>>(C, Y, KB, G);
+  k_grad_cells<DIR, CPML><<<dim3(gx, unsigned(rows)), 128, 0, st>>>(C, L, Y, KB, kb, qx, qz, G);
   return cudaGetLastError();
 }
 
-cudaError_t gradient(const Coef& C, const Fields& Y, const Fields& KB, double* const* g, int dir,
-                     cudaStream_t st) {
+cudaError_t gradient(const Coef& C, const SetLayout& L, const Fields& Y, const float* kb,
+                     double* const* g, int dir, HybridT* H, cudaStream_t st) {
   const Grad G{g[0], g[1], g[2], g[3], g[4], g[5], g[6]};
+  Fields KB;
+  float* p[kSetArrays];
+  for (int a = 0; a < kSetArrays; ++a) p[a] = const_cast<float*>(kb) + L.off[a];
+  KB.fvx = p[0]; KB.fvz = p[1]; KB.fp = p[2];
+  KB.svx = p[3]; KB.svz = p[4]; KB.ssx = p[5]; KB.ssz = p[6]; KB.ssxz = p[7];
+  for (int q = 0; q < 4; ++q) {
+    KB.fx[q] = p[8 + q]; KB.sx[q] = p[12 + q]; KB.sz[q] = p[16 + q]; KB.fz[q] = p[20 + q];
+  }
+  float* qx = H ? H->qx : nullptr;
+  float* qz = H ? H->qz : nullptr;
   if (C.cpml)
-    return dir == kDirF ? gradient_t<kDirF, true>(C, Y, KB, G, st) : gradient_t<kDirB, true>(C, Y, KB, G, st);
-  return dir == kDirF ? gradient_t<kDirF, false>(C, Y, KB, G, st) : gradient_t<kDirB, false>(C, Y, KB, G, st);
+    return dir == kDirF ? gradient_t<kDirF, true>(C, L, Y, KB, kb, qx, qz, G, st)
+                        : gradient_t<kDirB, true>(C, L, Y, KB, kb, qx, qz, G, st);
+  return dir == kDirF ? gradient_t<kDirF, false>(C, L, Y, KB, kb, qx, qz, G, st)
+                      : gradient_t<kDirB, false>(C, L, Y, KB, kb, qx, qz, G, st);
 }
 
 }  // namespace adj

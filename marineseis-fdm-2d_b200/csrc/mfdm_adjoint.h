@@ -43,6 +43,7 @@ struct SetLayout {
   int kind[kSetArrays];             // 0 fluid, 1 solid, 2 fluid xi strip, 3 solid xi strip,
                                     // 4 solid zeta strip, 5 fluid zeta band
   int nx, nzf, nzs, npd;
+  int cpml;                         // four-side CFS-PML (fluid top band, no free surface)
 };
 
 // Transposed stage operator of one direction: row j of L^T (an input value of
@@ -52,6 +53,20 @@ struct CsrT {
   int* col = nullptr;
   float* val = nullptr;
   long long nnz = 0;
+};
+
+// The transposed operator in two parts. Output cells where the forward stage
+// takes the plain interior formula (no PML strip, no conservative or
+// one-sided row, not the interface) contribute through the transposed stencil:
+// there L = (material x metric) . D, and the biased DRP pair satisfies
+// D_F^T = -D_B and D_B^T = -D_F, so L^T x is the opposite-bias derivative of the
+// point-wise products of x with the cell's coefficients (the Q fields). All
+// other outputs contribute through the CSR (the probed operator with the
+// interior outputs dropped).
+struct HybridT {
+  CsrT rest;              // CSR of L^T restricted to non-interior outputs
+  float* qx = nullptr;    // set-sized: xi-direction products, by input field
+  float* qz = nullptr;    // set-sized: zeta-direction products
 };
 
 namespace adj {
@@ -74,13 +89,23 @@ cudaError_t scan(const unsigned long long* count, long long* rowptr, long long l
 // Sorts every row of the CSR by column (deterministic sums).
 cudaError_t sort_rows(const CsrT& A, long long len, cudaStream_t st);
 
+// Drops from `full` the entries whose output lies in the interior set, into
+// `rest` (allocated here); count and tmp are scratch.
+cudaError_t drop_interior(const CsrT& full, const SetLayout& L, CsrT* rest,
+                          unsigned long long* count, void** tmp, size_t* tmp_bytes, cudaStream_t st);
+
 // One reverse stage: y = L^T kb, lam += (mask_lam ? M : 1) y and, when kbn is
 // given, kbn = M (w mu + c y).
-cudaError_t reverse_stage(const CsrT& A, long long len, const float* kb, float* lam,
-                          const uint8_t* mask, bool mask_lam, float* kbn, const float* mu, float w,
-                          float c, cudaStream_t st);
-// y = L^T x (tests and diagnostics).
-cudaError_t apply_t(const CsrT& A, long long len, const float* x, float* y, cudaStream_t st);
+// q_ready: the Q fields of kb are already in H (written by gradient()).
+cudaError_t reverse_stage(const HybridT& H, const Coef& C, const SetLayout& L, int dir,
+                          const float* kb, float* lam, const uint8_t* mask, bool mask_lam,
+                          float* kbn, const float* mu, float w, float c, bool q_ready,
+                          cudaStream_t st);
+// x = uniform pseudo-random values in [-1, 1) (self-checks).
+cudaError_t random_fill(float* x, long long n, unsigned seed, cudaStream_t st);
+// y = L^T x through the hybrid (H) or through a plain CSR (H.qx == nullptr).
+cudaError_t apply_t(const HybridT& H, const Coef& C, const SetLayout& L, int dir, const float* x,
+                    float* y, cudaStream_t st);
 
 // Adds one receiver sample's residuals (svx, svz, fp rows of nx) to lam.
 cudaError_t inject(float* lam, const SetLayout& L, const float* res, cudaStream_t st);
@@ -92,10 +117,13 @@ cudaError_t start(const float* lam, float* mu, float* kb, const uint8_t* mask, l
                   cudaStream_t st);
 
 // Material gradients of one stage: g[m][cell] += kb . dL_dir/dm (Y) over the
-// cell's main fields (and the coupled interface column). Y and KB are sets.
-// g: K, 1/rho_f ([nz_f][P]) then C11, C13, C33, C55, 1/rho_s ([nz_s][P]).
-cudaError_t gradient(const Coef& C, const Fields& Y, const Fields& KB, double* const* g, int dir,
-                     cudaStream_t st);
+// cell's main fields (and the coupled interface column); Y is a set, kb a
+// set-sized buffer. g: K, 1/rho_f ([nz_f][P]) then C11, C13, C33, C55,
+// 1/rho_s ([nz_s][P]). With H, the Q fields of kb for H's transposed operator
+// are written on the way (the interior cells; the rest of H's Q buffers must
+// hold 0).
+cudaError_t gradient(const Coef& C, const SetLayout& L, const Fields& Y, const float* kb,
+                     double* const* g, int dir, HybridT* H, cudaStream_t st);
 
 }  // namespace adj
 }  // namespace mfdm

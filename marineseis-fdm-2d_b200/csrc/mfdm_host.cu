@@ -142,7 +142,7 @@ struct mfdm_model {
 // of one checkpoint segment.
 struct AdjointState {
   mfdm::SetLayout L{};
-  mfdm::CsrT A[2];
+  mfdm::HybridT H[2];      // transposed stage operators, F and B (shared Q buffers)
   uint8_t* mask = nullptr;
   float *lam = nullptr, *mu = nullptr, *kb[2] = {nullptr, nullptr}, *tmp = nullptr;
   double* grad = nullptr;  // K, 1/rho_f [nz_f][P]; C11, C13, C33, C55, 1/rho_s [nz_s][P]
@@ -158,11 +158,13 @@ struct AdjointState {
   int nsteps = -1, every = 0;  // the forward run a backward pass may follow
   double build_ms = 0.0;       // operator assembly time (host clock)
   ~AdjointState() {
-    for (auto& a : A) {
-      cudaFree(a.rowptr);
-      cudaFree(a.col);
-      cudaFree(a.val);
+    for (auto& h : H) {
+      cudaFree(h.rest.rowptr);
+      cudaFree(h.rest.col);
+      cudaFree(h.rest.val);
     }
+    cudaFree(H[0].qx);
+    cudaFree(H[0].qz);
     cudaFree(mask); cudaFree(lam); cudaFree(mu); cudaFree(kb[0]); cudaFree(kb[1]);
     cudaFree(tmp); cudaFree(grad); cudaFree(ckpt); cudaFree(seg); cudaFree(res);
     cudaFree(scan_tmp);
@@ -1353,6 +1355,7 @@ mfdm::SetLayout set_layout(const mfdm_model* m) {
     else { L.rows[a] = m->C.cpml ? npd : 0; L.pitch[a] = m->P; L.ncols[a] = h.nx; L.kind[a] = 5; }
   }
   L.nx = h.nx; L.nzf = h.nzf; L.nzs = h.nzs; L.npd = npd;
+  L.cpml = m->C.cpml;
   return L;
 }
 
@@ -1413,7 +1416,7 @@ int adjoint_build(mfdm_model* m) {
   fr.p[2] = err;
   MFDM_CU(cudaMemsetAsync(err, 0, sizeof(int), st));
   for (int d = 0; d < 2; ++d) {
-    mfdm::CsrT& A = a->A[d];
+    mfdm::CsrT A;  // the full probed operator of this direction
     MFDM_CU(cudaMemsetAsync(count, 0, (size_t(n) + 1) * sizeof(unsigned long long), st));
     for (int pass = 0; pass < 2; ++pass) {
       if (pass == 1) {
@@ -1440,6 +1443,36 @@ int adjoint_build(mfdm_model* m) {
       }
     }
     MFDM_CU(mfdm::adj::sort_rows(A, n, st));
+    // keep only the non-interior outputs; the transposed interior stencil
+    // covers the rest. Checked against the full operator on a random vector.
+    mfdm::HybridT full;
+    full.rest = A;
+    mfdm::HybridT& H = a->H[d];
+    H.qx = a->H[0].qx;
+    H.qz = a->H[0].qz;
+    cudaError_t e = mfdm::adj::drop_interior(A, L, &H.rest, count, &a->scan_tmp, &a->scan_bytes, st);
+    float *x = a->mu, *y0 = a->kb[0], *y1 = a->kb[1];
+    if (e == cudaSuccess) e = mfdm::adj::random_fill(x, n, 12345u + unsigned(d), st);
+    if (e == cudaSuccess) e = mfdm::adj::apply_t(full, C, L, d, x, y0, st);
+    if (e == cudaSuccess) e = mfdm::adj::apply_t(H, C, L, d, x, y1, st);
+    cudaFree(A.rowptr);
+    cudaFree(A.col);
+    cudaFree(A.val);
+    MFDM_CU(e);
+    std::vector<float> h0(static_cast<size_t>(n)), h1(static_cast<size_t>(n));
+    MFDM_CU(cudaMemcpyAsync(h0.data(), y0, size_t(n) * sizeof(float), cudaMemcpyDeviceToHost, st));
+    MFDM_CU(cudaMemcpyAsync(h1.data(), y1, size_t(n) * sizeof(float), cudaMemcpyDeviceToHost, st));
+    MFDM_CU(cudaStreamSynchronize(st));
+    double num = 0.0, den = 0.0;
+    for (size_t i = 0; i < h0.size(); ++i) {
+      const double dd = double(h1[i]) - double(h0[i]);
+      num += dd * dd;
+      den += double(h0[i]) * double(h0[i]);
+    }
+    if (!(num <= 1e-8 * den))
+      return fail(MFDM_ERR_CUDA, "adjoint operator assembly: the transposed interior stencil "
+                                 "disagrees with the probed operator (relative L2 " +
+                                     std::to_string(std::sqrt(num / std::max(den, 1e-300))) + ")");
   }
   int nerr = 0;
   MFDM_CU(cudaMemcpyAsync(&nerr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1463,10 +1496,14 @@ int adjoint_prepare(mfdm_model* m) {
     const size_t n = size_t(a->L.len);
     int rc;
     if ((rc = dalloc(&a->mask, n)) || (rc = dalloc(&a->lam, n)) || (rc = dalloc(&a->mu, n)) ||
+        (rc = dalloc(&a->H[0].qx, n)) || (rc = dalloc(&a->H[0].qz, n)) ||
         (rc = dalloc(&a->kb[0], n)) || (rc = dalloc(&a->kb[1], n)) ||
         (rc = dalloc(&a->tmp, size_t(8) * m->cfg.nx)) ||
         (rc = dalloc(&a->grad, size_t(2) * m->cfg.nzf * m->P + size_t(5) * m->cfg.nzs * m->P)))
       return rc;
+    // Q fields off the interior set are never written and must stay 0
+    MFDM_CU(cudaMemset(a->H[0].qx, 0, n * sizeof(float)));
+    MFDM_CU(cudaMemset(a->H[0].qz, 0, n * sizeof(float)));
   }
   if (!m->adj->built) return adjoint_build(m);
   return MFDM_OK;
@@ -1488,7 +1525,6 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
   const int d0 = (n & 1) ? mfdm::kDirB : mfdm::kDirF, d1 = 1 - d0;
   Fields Y[4];
   for (int s = 0; s < 4; ++s) Y[s] = fields_at(L, slot + size_t(s) * size_t(len));
-  const Fields K0 = fields_at(L, a->kb[0]), K1 = fields_at(L, a->kb[1]);
   double* g[7];
   for (int k = 0; k < 7; ++k) g[k] = grad_array(m, k);
   const float *c = C.rk_c, *w = C.rk_w;
@@ -1496,14 +1532,15 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
     MFDM_CU(mfdm::adj::inject(a->lam, L, a->res + size_t(n / m->gap) * 3 * m->cfg.nx, st));
   MFDM_CU(mfdm::adj::filter_t(a->lam, L, C, a->tmp, st));
   MFDM_CU(mfdm::adj::start(a->lam, a->mu, a->kb[0], a->mask, len, c[3], st));
-  MFDM_CU(mfdm::adj::gradient(C, Y[3], K0, g, d1, st));
-  MFDM_CU(mfdm::adj::reverse_stage(a->A[d1], len, a->kb[0], a->lam, a->mask, true, a->kb[1], a->mu, w[2], c[2], st));
-  MFDM_CU(mfdm::adj::gradient(C, Y[2], K1, g, d0, st));
-  MFDM_CU(mfdm::adj::reverse_stage(a->A[d0], len, a->kb[1], a->lam, a->mask, true, a->kb[0], a->mu, w[1], c[1], st));
-  MFDM_CU(mfdm::adj::gradient(C, Y[1], K0, g, d1, st));
-  MFDM_CU(mfdm::adj::reverse_stage(a->A[d1], len, a->kb[0], a->lam, a->mask, true, a->kb[1], a->mu, w[0], c[0], st));
-  MFDM_CU(mfdm::adj::gradient(C, Y[0], K1, g, d0, st));
-  MFDM_CU(mfdm::adj::reverse_stage(a->A[d0], len, a->kb[1], a->lam, a->mask, false, nullptr, a->mu, 0.f, 0.f, st));
+  // each stage: gradient (which also forms the Q fields of kb), then L^T kb
+  MFDM_CU(mfdm::adj::gradient(C, L, Y[3], a->kb[0], g, d1, &a->H[d1], st));
+  MFDM_CU(mfdm::adj::reverse_stage(a->H[d1], C, L, d1, a->kb[0], a->lam, a->mask, true, a->kb[1], a->mu, w[2], c[2], true, st));
+  MFDM_CU(mfdm::adj::gradient(C, L, Y[2], a->kb[1], g, d0, &a->H[d0], st));
+  MFDM_CU(mfdm::adj::reverse_stage(a->H[d0], C, L, d0, a->kb[1], a->lam, a->mask, true, a->kb[0], a->mu, w[1], c[1], true, st));
+  MFDM_CU(mfdm::adj::gradient(C, L, Y[1], a->kb[0], g, d1, &a->H[d1], st));
+  MFDM_CU(mfdm::adj::reverse_stage(a->H[d1], C, L, d1, a->kb[0], a->lam, a->mask, true, a->kb[1], a->mu, w[0], c[0], true, st));
+  MFDM_CU(mfdm::adj::gradient(C, L, Y[0], a->kb[1], g, d0, &a->H[d0], st));
+  MFDM_CU(mfdm::adj::reverse_stage(a->H[d0], C, L, d0, a->kb[1], a->lam, a->mask, false, nullptr, a->mu, 0.f, 0.f, true, st));
   return MFDM_OK;
 }
 
