@@ -274,6 +274,37 @@ def uneven_rate(mfdm, device: int, nmodels: int = 32, steps: int = 128):
             "seg_rows": {str(r): tiles.count(r) for r in sorted(set(tiles))}}
 
 
+def adjoint_rate(mfdm, device: int, nsteps: int = 4000, every: int = 50):
+    """Cost of the adjoint-state gradient against a plain forward run on the
+    800x400 curvilinear model (4000 RK4 steps, checkpoint every 50): host
+    wall time of the synchronous calls. The adjoint's forward pass (with
+    checkpoints) plus its backward pass is compared with mfdm_step over the
+    same steps; the one-time operator assembly is listed separately."""
+    m = modelgen.curvilinear(800, 400, nt=nsteps)
+    with mfdm.Solver.from_model(m, device=device) as s:
+        s.set_shot(0, reset=True)
+        s.step(64)
+        s.set_shot(0, reset=True)
+        t0 = time.perf_counter()
+        s.step(nsteps)
+        fwd = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        s.adjoint_forward(nsteps, every)  # first call also assembles the operators
+        first = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        rec = s.adjoint_forward(nsteps, every)
+        afwd = time.perf_counter() - t0
+        rng = np.random.default_rng(1)
+        res = {k: rng.standard_normal(v.shape).astype(np.float32) for k, v in rec.items()}
+        t0 = time.perf_counter()
+        s.adjoint_backward(res)
+        bwd = time.perf_counter() - t0
+    return {"model": "curvilinear 800x400", "steps": nsteps, "ckpt_every": every,
+            "forward_s": round(fwd, 4), "adjoint_forward_s": round(afwd, 4),
+            "backward_s": round(bwd, 4), "assembly_s": round(first - afwd, 4),
+            "adjoint_over_forward": round((afwd + bwd) / fwd, 3)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -379,6 +410,7 @@ def main():
                 "ms_per_step": round(t2 / n2, 4)}
         other["batched_1200x800_64_shots"] = batched_rate(mfdm, small, local, args.warmup)
         other["uneven_32_models"] = uneven_rate(mfdm, local)
+        other["adjoint_800x400"] = adjoint_rate(mfdm, local)
 
     clocks = clk.summary()
     solver.close()

@@ -133,3 +133,40 @@ def test_adjoint_rejects_misuse(lib, cases):
     with lib.Batch.from_model(cases.flat_small(), [(60, 40, 25.0, 5.0)]) as b:
         with pytest.raises(lib.MfdmError):
             b.adjoint_forward(10)
+
+
+def test_shot_gradients_sum_over_shots(lib):
+    shots_mod = importlib.import_module("marineseis-fdm-2d_b200.shots")
+    model = tiny_model()
+    model.src_x, model.src_z = [20, 30], [17, 15]
+    rng = np.random.default_rng(5)
+    with lib.Solver.from_model(model) as s:
+        ns = -(-NSTEPS // s.info()["gap"])
+    obs = {k: {q: rng.standard_normal((ns, model.nx)).astype(np.float32) * 1e-9
+               for q in ("svx", "svz", "fp")} for k in range(2)}
+    j, g = shots_mod.shot_gradients_on_gpu(model, [0, 1], obs, ckpt_every=40)
+    parts = [shots_mod.shot_gradients_on_gpu(model, [k], obs, ckpt_every=40) for k in range(2)]
+    assert j == pytest.approx(parts[0][0] + parts[1][0], rel=1e-12)
+    for k in g:
+        assert np.allclose(g[k], parts[0][1][k] + parts[1][1][k], rtol=1e-6, atol=0.0), k
+
+
+def test_autograd_function_returns_the_adjoint_gradient(lib):
+    torch = pytest.importorskip("torch")
+    model = tiny_model()
+    p = grads.params_of(model)
+    t = {k: torch.tensor(v, dtype=torch.float64, requires_grad=True) for k, v in p.items()}
+    with lib.Solver.from_model(model) as s:
+        s.set_shot(0, reset=True)
+        rec = grads.SeismicRecords.apply(t["vp"], t["vs"], t["rho"], t["vp_f"], t["rho_f"], s,
+                                         model, NSTEPS, 40)
+        w = torch.linspace(-1.0, 1.0, rec.numel(), dtype=torch.float64).reshape(rec.shape)
+        (rec * w).sum().backward()
+        # the same through the C ABI directly
+        s.load_model(grads.with_params(model, p))
+        s.set_shot(0, reset=True)
+        s.adjoint_forward(NSTEPS, 40)
+        wn = w.numpy().astype(np.float32)
+        g = grads.chain_rule(s.adjoint_backward({"svx": wn[:, 0], "svz": wn[:, 1], "fp": wn[:, 2]}), p)
+    for k in p:
+        assert np.array_equal(t[k].grad.numpy(), g[k]), k

@@ -57,3 +57,37 @@ def test_two_ranks_gather_all_records(tmp_path):
     assert a[:, 0].tolist() == [0, 1, 2, 3, 4]
     # shot s was solved by rank s % 2 (round robin)
     assert a[:, 1].tolist() == [s + 100.0 * (s % 2) for s in range(5)]
+
+
+SHAPES = {"K": (2, 3), "rcp_rho_f": (2, 3), "C11": (4, 3), "C13": (4, 3), "C33": (4, 3),
+          "C55": (4, 3), "rcp_rho_s": (4, 3)}
+
+
+def _fake_grad(model, shot_list):
+    if not shot_list:
+        return 0.0, None
+    g = {k: sum(np.full(v, float(s + 1)) for s in shot_list) for k, v in SHAPES.items()}
+    return float(sum(10 * (s + 1) for s in shot_list)), g
+
+
+def _grad_worker(rank, world, port, out, nshots):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        j, g = shots.gradient_shots(_Model(nshots), {}, SHAPES, grad=_fake_grad, dist=dist)
+        np.save(os.path.join(out, f"grad{rank}.npy"), np.concatenate([[j], g["C55"].ravel(), g["K"].ravel()]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("nshots", [5, 1])
+def test_two_ranks_sum_gradients(tmp_path, nshots):
+    port = _free_port()
+    mp.spawn(_grad_worker, args=(2, port, str(tmp_path), nshots), nprocs=2, join=True)
+    a = np.load(tmp_path / "grad0.npy")
+    b = np.load(tmp_path / "grad1.npy")
+    assert np.array_equal(a, b)  # every rank holds the totals
+    total = sum(range(1, nshots + 1))
+    assert a[0] == 10 * total
+    assert np.all(a[1:] == total)  # each shot once (one rank may have no shot)
