@@ -315,9 +315,24 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="only the warm-up and timed steps (a short launch list for ncu)")
+    ap.add_argument("--adjoint-profile", action="store_true",
+                    help="only a short adjoint run on the 800x400 model (16 steps, checkpoint "
+                         "every 8, seeded residuals): a launch list of the adjoint kernels for ncu")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
+    if args.adjoint_profile:
+        mfdm = importlib.import_module("marineseis-fdm-2d_b200")
+        mfdm.load_library()
+        m = modelgen.curvilinear(800, 400, nt=16)
+        with mfdm.Solver.from_model(m) as s:
+            s.set_shot(0, reset=True)
+            rec = s.adjoint_forward(16, 8)
+            rng = np.random.default_rng(1)
+            g = s.adjoint_backward({k: rng.standard_normal(v.shape).astype(np.float32)
+                                    for k, v in rec.items()})
+        print(json.dumps({"adjoint_profile_run": True, "max_abs_dC11": float(np.abs(g["C11"]).max())}))
+        return
     world, rank, local, dist = dist_setup(args)
     model = WORKLOADS[args.workload]()
     if args.impl == "reference":
