@@ -36,7 +36,7 @@ EXPORTS = ("mfdm_last_error", "mfdm_open_json", "mfdm_open_desc", "mfdm_load_des
            "mfdm_run_cli", "mfdm_step_noalloc", "mfdm_open_batch", "mfdm_batch_reset",
            "mfdm_batch_get_records", "mfdm_batch_get_field", "mfdm_set_tile", "mfdm_autotune",
            "mfdm_group_open", "mfdm_group_step", "mfdm_group_time_steps", "mfdm_group_close",
-           "mfdm_adjoint_forward", "mfdm_adjoint_backward")
+           "mfdm_adjoint_forward", "mfdm_adjoint_backward", "mfdm_adjoint_set_memory")
 
 # Coefficient arrays the adjoint differentiates (mfdm_coef_grad order).
 GRAD_COEFS = ("K", "rcp_rho_f", "C11", "C13", "C33", "C55", "rcp_rho_s")
@@ -141,6 +141,7 @@ def load_library(path: str = LIB_PATH):
         "mfdm_group_time_steps": (ctypes.c_int, [vp, ctypes.c_int, _fp]),
         "mfdm_group_close": (ctypes.c_int, [vp]),
         "mfdm_adjoint_forward": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+        "mfdm_adjoint_set_memory": (ctypes.c_int, [vp, ctypes.c_longlong]),
         "mfdm_adjoint_backward": (ctypes.c_int, [vp, _fp, _fp, _fp, ctypes.POINTER(CoefGrad)]),
     }
     for name, (res, args) in sig.items():
@@ -265,6 +266,11 @@ class Solver:
         _check(self._lib.mfdm_synchronize(self._h))
 
     # -- adjoint ----------------------------------------------------------------
+    def adjoint_memory(self, nbytes: int):
+        """Device memory the adjoint may use to keep whole checkpoint segments'
+        stage inputs from the forward pass (mfdm_adjoint_set_memory; 0: recompute all)."""
+        _check(self._lib.mfdm_adjoint_set_memory(self._h, int(nbytes)))
+
     def adjoint_forward(self, nsteps: int, ckpt_every: int = 50) -> Dict[str, np.ndarray]:
         """Runs the current shot from rest with checkpoints (mfdm_adjoint_forward)
         and returns its records {'svx', 'svz', 'fp'}: [samples][nx]."""

@@ -134,6 +134,7 @@ struct mfdm_model {
   float* fcoef = nullptr;  // [6][nz_f][P]: xi_x, xi_z, ze_x, ze_z, rho, K
   float* scoef = nullptr;  // [9][nz_s][P]: xi_x, xi_z, ze_x, ze_z, rho, C11, C13, C33, C55
   AdjointState* adj = nullptr;  // adjoint operators and buffers (mfdm_adjoint_*)
+  long long adj_keep_budget = 0;  // mfdm_adjoint_set_memory
 };
 
 // Device buffers of the adjoint (one plain handle): the transposed stage
@@ -150,6 +151,9 @@ struct AdjointState {
   size_t ckpt_sets = 0;
   float* seg = nullptr;    // 4 stage-input sets per step of one segment
   size_t seg_steps = 0;
+  float* keep = nullptr;   // stage inputs of the last `nkeep` segments, kept by the forward pass
+  size_t keep_floats = 0;
+  int nkeep = 0;
   float* res = nullptr;    // residual samples [ns][3][nx]
   size_t res_floats = 0;
   void* scan_tmp = nullptr;
@@ -166,7 +170,7 @@ struct AdjointState {
     cudaFree(H[0].qx);
     cudaFree(H[0].qz);
     cudaFree(mask); cudaFree(lam); cudaFree(mu); cudaFree(kb[0]); cudaFree(kb[1]);
-    cudaFree(tmp); cudaFree(grad); cudaFree(ckpt); cudaFree(seg); cudaFree(res);
+    cudaFree(tmp); cudaFree(grad); cudaFree(ckpt); cudaFree(seg); cudaFree(res); cudaFree(keep);
     cudaFree(scan_tmp);
   }
 };
@@ -1486,6 +1490,8 @@ int adjoint_build(mfdm_model* m) {
   return MFDM_OK;
 }
 
+int ncp_of(int nsteps, int every) { return (nsteps + every - 1) / every; }
+
 int adjoint_prepare(mfdm_model* m) {
   if (m->batch || m->nshots != 1)
     return fail(MFDM_ERR_ARG, "the adjoint runs on plain (single-shot) handles");
@@ -1548,6 +1554,24 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
 
 extern "C" {
 
+int mfdm_adjoint_set_memory(mfdm_model* m, long long bytes) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  if (bytes < 0) return fail(MFDM_ERR_ARG, "negative memory budget");
+  DeviceGuard g(m->device);
+  m->adj_keep_budget = bytes;
+  if (m->adj) {
+    if (bytes == 0) {
+      MFDM_CU(cudaStreamSynchronize(m->stream));
+      cudaFree(m->adj->keep);
+      m->adj->keep = nullptr;
+      m->adj->keep_floats = 0;
+      m->adj->nkeep = 0;
+    }
+    m->adj->nsteps = -1;  // takes effect with the next mfdm_adjoint_forward
+  }
+  return MFDM_OK;
+}
+
 int mfdm_adjoint_forward(mfdm_model* m, int nsteps, int ckpt_every) {
   if (!m) return fail(MFDM_ERR_ARG, "null handle");
   if (nsteps < 1 || ckpt_every < 1) return fail(MFDM_ERR_ARG, "need nsteps >= 1 and ckpt_every >= 1");
@@ -1564,6 +1588,19 @@ int mfdm_adjoint_forward(mfdm_model* m, int nsteps, int ckpt_every) {
     if ((rc = dalloc(&a->ckpt, ncp * len)) != MFDM_OK) return rc;
     a->ckpt_sets = ncp;
   }
+  // whole segments whose stage inputs fit the caller's memory budget are kept
+  // now (the last ones, which the backward pass reaches first) and not recomputed
+  const size_t seg_floats = size_t(ckpt_every) * 4 * len;
+  const size_t nkeep = std::min(ncp, size_t(std::max<long long>(m->adj_keep_budget, 0)) /
+                                         (seg_floats * sizeof(float)));
+  if (nkeep * seg_floats > a->keep_floats) {
+    cudaFree(a->keep);
+    a->keep = nullptr;
+    a->keep_floats = 0;
+    if ((rc = dalloc(&a->keep, nkeep * seg_floats)) != MFDM_OK) return rc;
+    a->keep_floats = nkeep * seg_floats;
+  }
+  a->nkeep = int(nkeep);
   a->nsteps = -1;
   if ((rc = clear_state(m)) != MFDM_OK) return rc;
   if ((rc = rewind(m)) != MFDM_OK) return rc;
@@ -1572,7 +1609,17 @@ int mfdm_adjoint_forward(mfdm_model* m, int nsteps, int ckpt_every) {
     MFDM_CU(cudaMemcpyAsync(a->ckpt + k * len, m->S[0].fvx, len * sizeof(float),
                             cudaMemcpyDeviceToDevice, m->stream));
     const int todo = std::min(ckpt_every, nsteps - int(k) * ckpt_every);
-    if ((rc = enqueue_steps(m, todo)) != MFDM_OK) return rc;
+    if (k + nkeep >= ncp) {
+      float* base = a->keep + (k + nkeep - ncp) * seg_floats;
+      for (int j = 0; j < todo; ++j) {
+        float* slot = base + size_t(j) * 4 * len;
+        float* save[4] = {slot, slot + len, slot + 2 * len, slot + 3 * len};
+        if ((rc = enqueue_step(m, m->host_step, m->stream, nullptr, save)) != MFDM_OK) return rc;
+        ++m->host_step;
+      }
+    } else if ((rc = enqueue_steps(m, todo)) != MFDM_OK) {
+      return rc;
+    }
   }
   MFDM_CU(cudaStreamSynchronize(m->stream));
   if ((rc = check_status(m)) != MFDM_OK) return rc;
@@ -1609,7 +1656,8 @@ int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_
         if (src[q]) std::memcpy(&h[(size_t(j) * 3 + q) * nx], src[q] + size_t(j) * nx, nx * sizeof(float));
     MFDM_CU(cudaMemcpy(a->res, h.data(), rf * sizeof(float), cudaMemcpyHostToDevice));
   }
-  if (size_t(every) > a->seg_steps) {
+  const int ncp = ncp_of(nsteps, every);
+  if (a->nkeep < ncp && size_t(every) > a->seg_steps) {
     cudaFree(a->seg);
     a->seg = nullptr;
     a->seg_steps = 0;
@@ -1621,20 +1669,25 @@ int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_
   MFDM_CU(cudaMemsetAsync(a->grad, 0, gbytes, st));
   MFDM_CU(cudaMemsetAsync(a->lam, 0, len * sizeof(float), st));
   a->nsteps = -1;
-  const int ncp = (nsteps + every - 1) / every;
   for (int k = ncp - 1; k >= 0; --k) {
     const int t0 = k * every, t1 = std::min(nsteps, t0 + every);
-    // recompute the segment from its checkpoint, keeping every stage input
-    MFDM_CU(cudaMemcpyAsync(m->S[0].fvx, a->ckpt + size_t(k) * len, len * sizeof(float),
-                            cudaMemcpyDeviceToDevice, st));
-    MFDM_CU(mfdm::launch_set_step(m->C, t0, st));
-    for (int n = t0; n < t1; ++n) {
-      float* slot = a->seg + size_t(n - t0) * 4 * len;
-      float* save[4] = {slot, slot + len, slot + 2 * len, slot + 3 * len};
-      if ((rc = enqueue_step(m, n, st, nullptr, save)) != MFDM_OK) return rc;
+    float* base = a->seg;
+    if (k + a->nkeep >= ncp) {
+      // kept by the forward pass
+      base = a->keep + size_t(k + a->nkeep - ncp) * size_t(every) * 4 * len;
+    } else {
+      // recompute the segment from its checkpoint, keeping every stage input
+      MFDM_CU(cudaMemcpyAsync(m->S[0].fvx, a->ckpt + size_t(k) * len, len * sizeof(float),
+                              cudaMemcpyDeviceToDevice, st));
+      MFDM_CU(mfdm::launch_set_step(m->C, t0, st));
+      for (int n = t0; n < t1; ++n) {
+        float* slot = a->seg + size_t(n - t0) * 4 * len;
+        float* save[4] = {slot, slot + len, slot + 2 * len, slot + 3 * len};
+        if ((rc = enqueue_step(m, n, st, nullptr, save)) != MFDM_OK) return rc;
+      }
     }
     for (int n = t1 - 1; n >= t0; --n)
-      if ((rc = reverse_step(m, n, a->seg + size_t(n - t0) * 4 * len)) != MFDM_OK) return rc;
+      if ((rc = reverse_step(m, n, base + size_t(n - t0) * 4 * len)) != MFDM_OK) return rc;
   }
   MFDM_CU(cudaStreamSynchronize(st));
   if (out) {

@@ -86,6 +86,32 @@ def test_checkpoint_interval_does_not_change_the_gradient(lib):
             assert np.array_equal(g[k], out[0][k]), k
 
 
+def test_kept_segments_give_the_same_gradient(lib):
+    """Stage inputs kept from the forward pass (mfdm_adjoint_set_memory) instead of
+    recomputed from checkpoints: the same kernels on the same inputs, bit for bit."""
+    model = tiny_model()
+    rng = np.random.default_rng(11)
+    out = []
+    with lib.Solver.from_model(model) as s:
+        s.set_shot(0, reset=True)
+        ns = -(-NSTEPS // s.info()["gap"])
+        res = {k: rng.standard_normal((ns, model.nx)).astype(np.float32) for k in ("svx", "svz", "fp")}
+        info = s.info()
+        # bytes of one segment's stage inputs, at least (4 states per step, 25 steps,
+        # the 8 main fields; the ADE strips make a set a little larger)
+        seg_bytes = 25 * 4 * 4 * 8 * (info["nz_f"] + info["nz_s"]) * info["pitch"]
+        for nb in (0, 2 * seg_bytes, 1 << 40, 0):  # none, one or two, all five, none
+            s.adjoint_memory(nb)
+            s.adjoint_forward(NSTEPS, ckpt_every=25)
+            out.append(s.adjoint_backward(res))
+    for g in out[1:]:
+        for k in g:
+            assert np.array_equal(g[k], out[0][k]), k
+    with lib.Solver.from_model(model) as s:
+        with pytest.raises(lib.MfdmError):
+            s.adjoint_memory(-1)
+
+
 def test_gradient_matches_finite_differences(lib):
     model = tiny_model()
     p = grads.params_of(model)
