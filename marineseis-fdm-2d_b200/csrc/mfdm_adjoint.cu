@@ -506,15 +506,14 @@ __device__ __forceinline__ float t_stencil(const SetLayout& L, const float* __re
 // One thread per row of L^T: the sparse rest plus, on main-field cells, the
 // transposed interior stencil; then the RK bookkeeping of the reverse stage.
 template <int DIR, int MODE>  // MODE 0: y only; 1: lam += y; 2: lam += M y, kbn; 3: lam += M y
-__global__ void k_reverse_h(const long long* __restrict__ rowptr, const int* __restrict__ col,
-                            const float* __restrict__ val, const float* __restrict__ kb,
-                            const float* __restrict__ qx, const float* __restrict__ qz, SetLayout L,
-                            float* y_or_lam, const uint8_t* __restrict__ mask, float* kbn,
+// `t` holds the CSR part of every row (k_rows_csr; rows without entries keep 0).
+__global__ void k_reverse_h(const float* __restrict__ t, const float* __restrict__ qx,
+                            const float* __restrict__ qz, SetLayout L, float* y_or_lam,
+                            const uint8_t* __restrict__ mask, float* kbn,
                             const float* __restrict__ mu, float w, float cw) {
   const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (j >= L.len) return;
-  float y = 0.0f;
-  for (long long k = rowptr[j]; k < rowptr[j + 1]; ++k) y = fmaf(val[k], __ldg(kb + col[k]), y);
+  float y = t[j];
   {
     // the fluid block (3 arrays of nz_f rows) and the solid block (5 of nz_s)
     // are contiguous at pitch P
@@ -541,6 +540,31 @@ __global__ void k_reverse_h(const long long* __restrict__ rowptr, const int* __r
   const float m = mask[j] ? 1.0f : 0.0f;
   y_or_lam[j] += MODE == 1 ? y : m * y;
   if (MODE == 2) kbn[j] = m * fmaf(cw, y, w * mu[j]);
+}
+
+// The CSR part of L^T x on the rows that have entries, kLanes threads per row:
+// t[nzrow[r]] = sum over row r.
+__global__ void k_rows_csr(const int* __restrict__ nzrow, const long long* __restrict__ rowptr,
+                           const int* __restrict__ col, const float* __restrict__ val,
+                           const float* __restrict__ x, long long nrows, float* t) {
+  const long long r = (blockIdx.x * (long long)blockDim.x + threadIdx.x) / kLanes;
+  const int lane = threadIdx.x % kLanes;
+  if (r >= nrows) return;  // whole groups leave together
+  const int j = nzrow[r];
+  const float s = row_dot(rowptr, col, val, x, j, lane);
+  if (lane == 0) t[j] = s;
+}
+
+__global__ void k_flag_rows(const long long* __restrict__ rowptr, long long len,
+                            unsigned long long* flag) {
+  const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (j < len) flag[j] = rowptr[j + 1] > rowptr[j] ? 1ull : 0ull;
+}
+
+__global__ void k_list_rows(const long long* __restrict__ rowptr, const long long* __restrict__ pos,
+                            long long len, int* nzrow) {
+  const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (j < len && rowptr[j + 1] > rowptr[j]) nzrow[pos[j]] = int(j);
 }
 
 __global__ void k_random(float* x, long long n, unsigned seed) {
@@ -624,6 +648,31 @@ cudaError_t drop_interior(const CsrT& full, const SetLayout& L, CsrT* rest,
   return cudaGetLastError();
 }
 
+cudaError_t list_rows(HybridT* H, const SetLayout& L, unsigned long long* flag, void** tmp,
+                      size_t* tmp_bytes, cudaStream_t st) {
+  const unsigned g = unsigned((L.len + kBlock - 1) / kBlock);
+  k_flag_rows<<<g, kBlock, 0, st>>>(H->rest.rowptr, L.len, flag);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(flag + L.len, 0, sizeof(unsigned long long), st)) != cudaSuccess) return e;
+  long long* pos = nullptr;
+  if ((e = cudaMalloc(&pos, size_t(L.len + 1) * sizeof(long long))) != cudaSuccess) return e;
+  e = scan(flag, pos, L.len, tmp, tmp_bytes, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&H->nrows, pos + L.len, sizeof(long long), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaMalloc(&H->nzrow, size_t(std::max<long long>(H->nrows, 1)) * sizeof(int));
+  if (e == cudaSuccess) {
+    k_list_rows<<<g, kBlock, 0, st>>>(H->rest.rowptr, pos, L.len, H->nzrow);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&H->t, size_t(L.len) * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemsetAsync(H->t, 0, size_t(L.len) * sizeof(float), st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(pos);
+  return e;
+}
+
 cudaError_t random_fill(float* x, long long n, unsigned seed, cudaStream_t st) {
   k_random<<<grid_for(n, kBlock), kBlock, 0, st>>>(x, n, seed);
   return cudaGetLastError();
@@ -640,8 +689,14 @@ static cudaError_t hybrid_t(const HybridT& H, const Coef& C, const SetLayout& L,
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
+  if (H.nrows > 0) {
+    k_rows_csr<<<unsigned((H.nrows * kLanes + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+        H.nzrow, H.rest.rowptr, H.rest.col, H.rest.val, kb, H.nrows, H.t);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
   k_reverse_h<DIR, MODE><<<unsigned((L.len + kBlock - 1) / kBlock), kBlock, 0, st>>>(
-      H.rest.rowptr, H.rest.col, H.rest.val, kb, H.qx, H.qz, L, out, mask, kbn, mu, w, c);
+      H.t, H.qx, H.qz, L, out, mask, kbn, mu, w, c);
   return cudaGetLastError();
 }
 

@@ -65,6 +65,9 @@ struct CsrT {
 // interior outputs dropped).
 struct HybridT {
   CsrT rest;              // CSR of L^T restricted to non-interior outputs
+  int* nzrow = nullptr;   // rows of `rest` that have entries
+  long long nrows = 0;
+  float* t = nullptr;     // set-sized: the CSR part of each row (0 on rows without entries)
   float* qx = nullptr;    // set-sized: xi-direction products, by input field
   float* qz = nullptr;    // set-sized: zeta-direction products
 };
@@ -101,6 +104,10 @@ cudaError_t reverse_stage(const HybridT& H, const Coef& C, const SetLayout& L, i
                           const float* kb, float* lam, const uint8_t* mask, bool mask_lam,
                           float* kbn, const float* mu, float w, float c, bool q_ready,
                           cudaStream_t st);
+// Lists the rows of H->rest that have entries and allocates H->t (zeroed);
+// flag (len + 1) and tmp are scratch.
+cudaError_t list_rows(HybridT* H, const SetLayout& L, unsigned long long* flag, void** tmp,
+                      size_t* tmp_bytes, cudaStream_t st);
 // x = uniform pseudo-random values in [-1, 1) (self-checks).
 cudaError_t random_fill(float* x, long long n, unsigned seed, cudaStream_t st);
 // y = L^T x through the hybrid (H) or through a plain CSR (H.qx == nullptr).

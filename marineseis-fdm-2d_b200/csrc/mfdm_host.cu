@@ -166,6 +166,8 @@ struct AdjointState {
       cudaFree(h.rest.rowptr);
       cudaFree(h.rest.col);
       cudaFree(h.rest.val);
+      cudaFree(h.nzrow);
+      cudaFree(h.t);
     }
     cudaFree(H[0].qx);
     cudaFree(H[0].qz);
@@ -1455,6 +1457,7 @@ int adjoint_build(mfdm_model* m) {
     H.qx = a->H[0].qx;
     H.qz = a->H[0].qz;
     cudaError_t e = mfdm::adj::drop_interior(A, L, &H.rest, count, &a->scan_tmp, &a->scan_bytes, st);
+    if (e == cudaSuccess) e = mfdm::adj::list_rows(&H, L, count, &a->scan_tmp, &a->scan_bytes, st);
     float *x = a->mu, *y0 = a->kb[0], *y1 = a->kb[1];
     if (e == cudaSuccess) e = mfdm::adj::random_fill(x, n, 12345u + unsigned(d), st);
     if (e == cudaSuccess) e = mfdm::adj::apply_t(full, C, L, d, x, y0, st);
