@@ -258,6 +258,21 @@ int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_
  * in the reference layout. Returns MFDM_OK or an error code (the CLI exits 1). */
 int mfdm_run_cli(const char* json_path, const char* out_root, int device);
 
+/* Snapshots of the command line are drained asynchronously: at a snapshot
+ * step the fields are copied on the device into a staging slot and the
+ * stepping goes on while a copy stream and a writer thread produce the files.
+ * With the environment variable MFDM_SNAPSHOT_PRESSURE=1 the fluid pressure is
+ * also written, <shot>/snapshot/fluid/p/p_%06d.bin (listed in the reference's
+ * docs/io.md:18, not written by its main.cu). */
+
+/* Every source of the JSON as one batch (mfdm_open_batch with the JSON's
+ * fpeak and beta0 for every shot): each shot starts from rest - unlike
+ * mfdm_run_cli and the reference, which carry the wavefield from one shot to
+ * the next (src/main.cu:94-136) - and all shots step in one launch per RK
+ * stage. Writes the same <out_root>/<shot>/ tree per shot. The CLI binary
+ * takes this path when MFDM_BATCH=1. */
+int mfdm_run_cli_batch(const char* json_path, const char* out_root, int device);
+
 /* ---- stepping without allocating ------------------------------------------
  * No counterpart in the reference. For callers that cannot allocate device
  * memory (a fixed device-memory budget set at start-up, a framework pool that

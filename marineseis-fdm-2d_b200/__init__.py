@@ -33,7 +33,7 @@ FIELDS = {"fluid_vx": 0, "fluid_vz": 1, "fluid_p": 2, "solid_vx": 3, "solid_vz":
 EXPORTS = ("mfdm_last_error", "mfdm_open_json", "mfdm_open_desc", "mfdm_load_desc", "mfdm_close",
            "mfdm_get_info", "mfdm_set_shot", "mfdm_update_rk4", "mfdm_step", "mfdm_time_steps",
            "mfdm_synchronize", "mfdm_get_records", "mfdm_get_field", "mfdm_set_field",
-           "mfdm_run_cli", "mfdm_step_noalloc", "mfdm_open_batch", "mfdm_batch_reset",
+           "mfdm_run_cli", "mfdm_run_cli_batch", "mfdm_step_noalloc", "mfdm_open_batch", "mfdm_batch_reset",
            "mfdm_batch_get_records", "mfdm_batch_get_field", "mfdm_set_tile", "mfdm_autotune",
            "mfdm_group_open", "mfdm_group_step", "mfdm_group_time_steps", "mfdm_group_close",
            "mfdm_adjoint_forward", "mfdm_adjoint_backward", "mfdm_adjoint_set_memory")
@@ -126,6 +126,7 @@ def load_library(path: str = LIB_PATH):
         "mfdm_get_field": (ctypes.c_int, [vp, ctypes.c_int, _fp]),
         "mfdm_set_field": (ctypes.c_int, [vp, ctypes.c_int, _fp]),
         "mfdm_run_cli": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]),
+        "mfdm_run_cli_batch": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]),
         "mfdm_step_noalloc": (ctypes.c_int, [ctypes.POINTER(DeviceModel), ctypes.c_int,
                                              ctypes.c_int, vp]),
         "mfdm_open_batch": (ctypes.c_int, [ctypes.POINTER(Desc), ctypes.c_int,
@@ -432,6 +433,11 @@ def step_noalloc(dm: DeviceModel, it: int, nsteps: int, stream: Optional[int] = 
 def run_cli(json_path: str, out_root: str, device: int = 0):
     """In-process equivalent of ``main_debug <model.json> <out_root>``."""
     _check(load_library().mfdm_run_cli(os.fsencode(json_path), os.fsencode(out_root), device))
+
+
+def run_cli_batch(json_path: str, out_root: str, device: int = 0):
+    """Every source of the JSON as one batch, each shot from rest (mfdm_run_cli_batch)."""
+    _check(load_library().mfdm_run_cli_batch(os.fsencode(json_path), os.fsencode(out_root), device))
 
 
 def build(verbose: bool = False, force: bool = False) -> str:

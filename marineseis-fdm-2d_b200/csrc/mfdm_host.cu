@@ -18,6 +18,7 @@
 #include <cstring>
 #include <filesystem>
 #include <fstream>
+#include <future>
 #include <iomanip>
 #include <iostream>
 #include <map>
@@ -1730,25 +1731,195 @@ int make_dirs(const fs::path& p) {
   return MFDM_OK;
 }
 
-// Snapshot files <field>_%06d.bin of solid and fluid vx, vz (src/main.cu:227-243, 327-339).
-int write_snapshot(mfdm_model* m, const fs::path& shot_dir, int it) {
-  const int nx = m->cfg.nx;
-  std::vector<float> buf(size_t(nx) * std::max(m->cfg.nzf, m->cfg.nzs));
-  struct S { int field; const char* medium; const char* comp; } order[] = {
-      {MFDM_SOLID_VZ, "solid", "vz"}, {MFDM_SOLID_VX, "solid", "vx"},
-      {MFDM_FLUID_VZ, "fluid", "vz"}, {MFDM_FLUID_VX, "fluid", "vx"}};
-  for (const S& s : order) {
-    int rc = mfdm_get_field(m, s.field, buf.data());
-    if (rc != MFDM_OK) return rc;
-    const fs::path dir = shot_dir / "snapshot" / s.medium / s.comp;
-    if ((rc = make_dirs(dir)) != MFDM_OK) return rc;
-    std::ostringstream name;
-    name << s.comp << "_" << std::setw(6) << std::setfill('0') << it << ".bin";
-    const int rows = s.field < 3 ? m->cfg.nzf : m->cfg.nzs;
-    if ((rc = write_floats(dir / name.str(), buf.data(), size_t(rows) * nx, false)) != MFDM_OK)
-      return rc;
+// Asynchronous snapshot drain (src/main.cu:227-243, 327-339 write the files
+// synchronously between steps). At a snapshot step the fields of every shot
+// are copied device to device into a staging slot on the compute stream, so
+// the stepping goes on at once; a copy stream moves the slot to pinned host
+// memory and a worker thread writes the files <field>_%06d.bin. Two slots: the
+// third snapshot waits for the first one's files. Fields: solid and fluid vx,
+// vz as the reference, plus fluid p when `pressure` (documented in docs/io.md
+// but not written by the reference).
+class SnapshotDrain {
+ public:
+  ~SnapshotDrain() {
+    for (auto& j : job_)
+      if (j.valid()) j.wait();
+    if (m_) {
+      DeviceGuard g(m_->device);
+      for (int s = 0; s < 2; ++s) {
+        if (dev_[s]) cudaFree(dev_[s]);
+        if (host_[s]) cudaFreeHost(host_[s]);
+        if (staged_[s]) cudaEventDestroy(staged_[s]);
+        if (copied_[s]) cudaEventDestroy(copied_[s]);
+      }
+      if (copy_) cudaStreamDestroy(copy_);
+    }
   }
+
+  int init(mfdm_model* m, bool pressure) {
+    m_ = m;
+    items_ = {{MFDM_SOLID_VZ, "solid", "vz"}, {MFDM_SOLID_VX, "solid", "vx"},
+              {MFDM_FLUID_VZ, "fluid", "vz"}, {MFDM_FLUID_VX, "fluid", "vx"}};
+    if (pressure) items_.push_back({MFDM_FLUID_P, "fluid", "p"});
+    per_shot_ = 0;
+    for (const Item& it : items_) per_shot_ += size_t(rows_of(it.field)) * m->cfg.nx;
+    const size_t n = per_shot_ * size_t(m->nshots);
+    DeviceGuard g(m->device);
+    MFDM_CU(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking));
+    for (int s = 0; s < 2; ++s) {
+      MFDM_CU(cudaMalloc(&dev_[s], n * sizeof(float)));
+      MFDM_CU(cudaMallocHost(&host_[s], n * sizeof(float)));
+      MFDM_CU(cudaEventCreateWithFlags(&staged_[s], cudaEventDisableTiming));
+      MFDM_CU(cudaEventCreateWithFlags(&copied_[s], cudaEventDisableTiming));
+    }
+    return MFDM_OK;
+  }
+
+  // Snapshot of step `it` of every shot of the handle; shot b's files go under dirs[b].
+  int push(const std::vector<fs::path>& dirs, int it) {
+    const int s = next_;
+    next_ ^= 1;
+    int rc = wait(s);
+    if (rc != MFDM_OK) return rc;
+    DeviceGuard g(m_->device);
+    const int nx = m_->cfg.nx;
+    size_t off = 0;
+    for (int b = 0; b < m_->nshots; ++b)
+      for (const Item& item : items_) {
+        float* p = nullptr;
+        int rows = 0;
+        if ((rc = field_ptr(m_, item.field, &p, &rows, b)) != MFDM_OK) return rc;
+        MFDM_CU(cudaMemcpy2DAsync(dev_[s] + off, size_t(nx) * sizeof(float), p,
+                                  size_t(m_->P) * sizeof(float), size_t(nx) * sizeof(float),
+                                  size_t(rows), cudaMemcpyDeviceToDevice, m_->stream));
+        off += size_t(rows) * nx;
+      }
+    MFDM_CU(cudaEventRecord(staged_[s], m_->stream));
+    MFDM_CU(cudaStreamWaitEvent(copy_, staged_[s], 0));
+    MFDM_CU(cudaMemcpyAsync(host_[s], dev_[s], off * sizeof(float), cudaMemcpyDeviceToHost, copy_));
+    MFDM_CU(cudaEventRecord(copied_[s], copy_));
+    const float* host = host_[s];
+    cudaEvent_t done = copied_[s];
+    const std::vector<Item> items = items_;
+    const int nshots = m_->nshots, device = m_->device;
+    std::vector<int> rows(items.size());
+    for (size_t q = 0; q < items.size(); ++q) rows[q] = rows_of(items[q].field);
+    job_[s] = std::async(std::launch::async, [=]() -> Result {
+      cudaSetDevice(device);
+      const cudaError_t e = cudaEventSynchronize(done);
+      if (e != cudaSuccess)
+        return {MFDM_ERR_CUDA, std::string("snapshot copy: ") + cudaGetErrorString(e)};
+      size_t o = 0;
+      for (int b = 0; b < nshots; ++b)
+        for (size_t q = 0; q < items.size(); ++q) {
+          const fs::path dir = dirs[size_t(b)] / "snapshot" / items[q].medium / items[q].comp;
+          std::error_code ec;
+          fs::create_directories(dir, ec);
+          if (ec) return {MFDM_ERR_IO, "cannot create " + dir.string() + ": " + ec.message()};
+          std::ostringstream name;
+          name << items[q].comp << "_" << std::setw(6) << std::setfill('0') << it << ".bin";
+          const size_t n = size_t(rows[q]) * nx;
+          std::ofstream f(dir / name.str(), std::ios::binary | std::ios::trunc);
+          if (!f) return {MFDM_ERR_IO, "cannot write " + (dir / name.str()).string()};
+          f.write(reinterpret_cast<const char*>(host + o), std::streamsize(n * sizeof(float)));
+          if (!f) return {MFDM_ERR_IO, "failed to write " + (dir / name.str()).string()};
+          o += n;
+        }
+      return {MFDM_OK, ""};
+    });
+    return MFDM_OK;
+  }
+
+  // Waits for every pending write; the first failure.
+  int finish() {
+    int rc = MFDM_OK;
+    for (int s = 0; s < 2; ++s) {
+      const int r = wait(s);
+      if (rc == MFDM_OK) rc = r;
+    }
+    return rc;
+  }
+
+ private:
+  struct Item { int field; const char* medium; const char* comp; };
+  struct Result { int code; std::string msg; };
+  int rows_of(int field) const { return field < 3 ? m_->cfg.nzf : m_->cfg.nzs; }
+  int wait(int s) {
+    if (!job_[s].valid()) return MFDM_OK;
+    const Result r = job_[s].get();
+    return r.code == MFDM_OK ? MFDM_OK : fail(r.code, r.msg);
+  }
+  mfdm_model* m_ = nullptr;
+  cudaStream_t copy_ = nullptr;
+  std::vector<Item> items_;
+  size_t per_shot_ = 0;
+  float* dev_[2] = {nullptr, nullptr};
+  float* host_[2] = {nullptr, nullptr};
+  cudaEvent_t staged_[2] = {nullptr, nullptr}, copied_[2] = {nullptr, nullptr};
+  std::future<Result> job_[2];
+  int next_ = 0;
+};
+
+bool env_on(const char* name) {
+  const char* v = std::getenv(name);
+  return v && *v && std::strcmp(v, "0") != 0;
+}
+
+// Steps the handle's current shot(s) through nt steps, draining a snapshot of
+// every shot at each it % snapshot == 0, then writes each shot's records.
+int run_shots_cli(mfdm_model* m, const std::vector<fs::path>& dirs) {
+  const HostModel& h = m->cfg;
+  const int nx = h.nx;
+  int rc;
+  for (const fs::path& d : dirs) {
+    if ((rc = make_dirs(d / "snapshot")) != MFDM_OK) return rc;
+    if ((rc = make_dirs(d / "record")) != MFDM_OK) return rc;
+  }
+  SnapshotDrain drain;
+  if ((rc = drain.init(m, env_on("MFDM_SNAPSHOT_PRESSURE"))) != MFDM_OK) return rc;
+  int it = 0;
+  while (it < h.nt) {
+    // run through the next snapshot step (it % snapshot == 0), inclusive
+    const int next_snap = ((it + h.snapshot - 1) / h.snapshot) * h.snapshot;
+    const int last = std::min(h.nt - 1, next_snap);
+    if ((rc = mfdm_step(m, last - it + 1)) != MFDM_OK) return rc;
+    it = last + 1;
+    if (last % h.snapshot == 0) {
+      std::printf("finished %0.2f%%\r", 100.0 * last / h.nt);
+      std::fflush(stdout);
+      if ((rc = drain.push(dirs, last)) != MFDM_OK) return rc;
+    }
+  }
+  const int ns = (h.nt + m->gap - 1) / m->gap;
+  std::vector<float> a(size_t(ns) * nx), b(size_t(ns) * nx), c(size_t(ns) * nx);
+  for (size_t k = 0; k < dirs.size(); ++k) {
+    if (ns > 0 && (rc = get_records(m, int(k), 0, ns, a.data(), b.data(), c.data())) != MFDM_OK)
+      return rc;
+    const fs::path rd = dirs[k] / "record";
+    if ((rc = write_floats(rd / "solid_vx.bin", a.data(), a.size(), false)) != MFDM_OK) return rc;
+    if ((rc = write_floats(rd / "solid_vz.bin", b.data(), b.size(), false)) != MFDM_OK) return rc;
+    if ((rc = write_floats(rd / "fluid_p.bin", c.data(), c.size(), false)) != MFDM_OK) return rc;
+  }
+  return drain.finish();
+}
+
+int clear_out_root(const fs::path& out_root) {
+  const std::string s = out_root.string();
+  if (s.empty() || s == "/" || s == "." || s == "..")
+    return fail(MFDM_ERR_ARG, "Invalid output dir: " + s);
+  std::error_code ec;
+  fs::remove_all(out_root, ec);
+  if (ec) return fail(MFDM_ERR_IO, "cannot clear " + s + ": " + ec.message());
+  int rc;
+  if ((rc = make_dirs(out_root)) != MFDM_OK) return rc;
+  std::printf("[output] cleared %s\n", s.c_str());
   return MFDM_OK;
+}
+
+void print_pml(const HostModel& h) {
+  std::printf("[PML] beta0 = %.3f, p_beta = %.2f, p_alpha = %.2f, alpha0 = %.1f 1/s, d0 = %.1f 1/s\n",
+              h.beta0, 2.0, 1.0, 2.0 * M_PI * h.fpeak,
+              -(h.npow + 1) * double(h.vp_max) * std::log(double(h.rc)) / (2.0 * h.thickness));
 }
 
 int run_cli(const char* json_path, const char* out_root_c, int device) {
@@ -1760,45 +1931,40 @@ int run_cli(const char* json_path, const char* out_root_c, int device) {
   int rc = mfdm_open_json(json_path, device, &m);
   if (rc != MFDM_OK) return rc;
   struct Closer { mfdm_model* m; ~Closer() { mfdm_close(m); } } closer{m};
-  const HostModel& h = m->cfg;
-  std::printf("[PML] beta0 = %.3f, p_beta = %.2f, p_alpha = %.2f, alpha0 = %.1f 1/s, d0 = %.1f 1/s\n",
-              h.beta0, 2.0, 1.0, 2.0 * M_PI * h.fpeak,
-              -(h.npow + 1) * double(h.vp_max) * std::log(double(h.rc)) / (2.0 * h.thickness));
-  std::error_code ec;
-  fs::remove_all(out_root, ec);
-  if (ec) return fail(MFDM_ERR_IO, "cannot clear " + s + ": " + ec.message());
-  if ((rc = make_dirs(out_root)) != MFDM_OK) return rc;
-  std::printf("[output] cleared %s\n", s.c_str());
-  const int nx = h.nx;
-  const int nsrc = int(h.srcx.size());
+  print_pml(m->cfg);
+  if ((rc = clear_out_root(out_root)) != MFDM_OK) return rc;
+  const int nsrc = int(m->cfg.srcx.size());
   for (int isrc = 0; isrc < nsrc; ++isrc) {
-    const fs::path shot_dir = out_root / std::to_string(isrc);
-    if ((rc = make_dirs(shot_dir / "snapshot")) != MFDM_OK) return rc;
-    if ((rc = make_dirs(shot_dir / "record")) != MFDM_OK) return rc;
     // The reference keeps the wavefield across shots (src/main.cu:94-136).
     if ((rc = mfdm_set_shot(m, isrc, 0)) != MFDM_OK) return rc;
-    int it = 0;
-    while (it < h.nt) {
-      // run through the next snapshot step (it % snapshot == 0), inclusive
-      const int next_snap = ((it + h.snapshot - 1) / h.snapshot) * h.snapshot;
-      const int last = std::min(h.nt - 1, next_snap);
-      if ((rc = mfdm_step(m, last - it + 1)) != MFDM_OK) return rc;
-      it = last + 1;
-      if (last % h.snapshot == 0) {
-        std::printf("finished %0.2f%%\r", 100.0 * last / h.nt);
-        std::fflush(stdout);
-        if ((rc = write_snapshot(m, shot_dir, last)) != MFDM_OK) return rc;
-      }
-    }
-    const int ns = (h.nt + m->gap - 1) / m->gap;
-    std::vector<float> a(size_t(ns) * nx), b(size_t(ns) * nx), c(size_t(ns) * nx);
-    if (ns > 0 && (rc = mfdm_get_records(m, 0, ns, a.data(), b.data(), c.data())) != MFDM_OK) return rc;
-    const fs::path rd = shot_dir / "record";
-    if ((rc = write_floats(rd / "solid_vx.bin", a.data(), a.size(), false)) != MFDM_OK) return rc;
-    if ((rc = write_floats(rd / "solid_vz.bin", b.data(), b.size(), false)) != MFDM_OK) return rc;
-    if ((rc = write_floats(rd / "fluid_p.bin", c.data(), c.size(), false)) != MFDM_OK) return rc;
+    if ((rc = run_shots_cli(m, {out_root / std::to_string(isrc)})) != MFDM_OK) return rc;
   }
   return MFDM_OK;
+}
+
+// Every source of the JSON as one batch: each shot from rest, all shots in
+// one launch per RK stage, a <shot>/ tree per shot.
+int run_cli_batch(const char* json_path, const char* out_root_c, int device) {
+  const fs::path out_root = out_root_c;
+  HostModel h;
+  int rc = load_json(json_path, h);
+  if (rc != MFDM_OK) return rc;
+  if (h.srcx.empty()) return fail(MFDM_ERR_CONFIG, "the JSON lists no source");
+  std::vector<ShotCfg> shots(h.srcx.size());
+  for (size_t b = 0; b < shots.size(); ++b) {
+    shots[b].x = h.srcx[b];
+    shots[b].z = h.srcz[b];
+    shots[b].fpeak = h.fpeak;
+    shots[b].beta0 = h.beta0;
+  }
+  print_pml(h);
+  mfdm_model* m = nullptr;
+  if ((rc = open_common(std::move(h), device, &m, &shots)) != MFDM_OK) return rc;
+  struct Closer { mfdm_model* m; ~Closer() { mfdm_close(m); } } closer{m};
+  if ((rc = clear_out_root(out_root)) != MFDM_OK) return rc;
+  std::vector<fs::path> dirs;
+  for (size_t b = 0; b < shots.size(); ++b) dirs.push_back(out_root / std::to_string(b));
+  return run_shots_cli(m, dirs);
 }
 
 }  // namespace
@@ -1807,6 +1973,15 @@ extern "C" int mfdm_run_cli(const char* json_path, const char* out_root, int dev
   if (!json_path || !out_root) return fail(MFDM_ERR_ARG, "null argument");
   try {
     return run_cli(json_path, out_root, device);
+  } catch (const std::exception& e) {
+    return fail(MFDM_ERR_IO, e.what());
+  }
+}
+
+extern "C" int mfdm_run_cli_batch(const char* json_path, const char* out_root, int device) {
+  if (!json_path || !out_root) return fail(MFDM_ERR_ARG, "null argument");
+  try {
+    return run_cli_batch(json_path, out_root, device);
   } catch (const std::exception& e) {
     return fail(MFDM_ERR_IO, e.what());
   }
