@@ -92,6 +92,54 @@ class Model:
         }
 
 
+@dataclass
+class SolidModel:
+    """A solid with a free surface on top (calc_type 0, boundary_type 2, the
+    reference's PmlFs::SolidOnly): all arrays are [nz][nx], the free surface is
+    global row 3, CFS-PML left, right and bottom."""
+
+    nx: int
+    nz: int
+    h: float
+    fpeak: float
+    dt: float
+    nt: int
+    snapshot: int
+    src_x: List[int]
+    src_z: List[int]
+    npd: int
+    npow: int
+    thickness: float
+    vp_max: float
+    rc: float
+    beta0: float
+    solid: Dict[str, np.ndarray] = field(default_factory=dict)   # [nz][nx]
+    metric: Dict[str, np.ndarray] = field(default_factory=dict)  # [nz][nx]
+    boundary_type: int = 2
+
+    @property
+    def cells(self) -> int:
+        return self.nx * self.nz
+
+    def config(self, paths: Dict[str, str]) -> dict:
+        """JSON document in the reference schema with calc_type 0 (no fluid section)."""
+        return {
+            "base": {"fpeak": self.fpeak, "dt": self.dt, "nt": int(self.nt),
+                     "snapshot": int(self.snapshot)},
+            "grid": {
+                "calc_type": 0,
+                "boundary_type": int(self.boundary_type),
+                "src_pos": {"posx": [int(v) for v in self.src_x],
+                            "posz": [int(v) for v in self.src_z]},
+                "solid": {"nx": self.nx, "nz": self.nz,
+                          **{k: paths["solid/" + k] for k in SOLID_FIELDS}},
+                "jacob": {k: paths["jacob/" + k] for k in METRIC_FIELDS},
+            },
+            "PML": {"npd": self.npd, "thickness": self.thickness, "NPOW": self.npow,
+                    "Vp_max": self.vp_max, "Rc": self.rc, "beta0": self.beta0},
+        }
+
+
 def write_model(model: Model, directory: str, name: str = "model",
                 relative_to: Optional[str] = None) -> str:
     """Writes ``<directory>/<name>.json`` and the float32 binaries; returns the JSON path.
@@ -102,8 +150,9 @@ def write_model(model: Model, directory: str, name: str = "model",
     """
     os.makedirs(directory, exist_ok=True)
     paths = {}
-    groups = (("solid", model.solid, SOLID_FIELDS), ("fluid", model.fluid, FLUID_FIELDS),
-              ("jacob", model.metric, METRIC_FIELDS))
+    groups = [("solid", model.solid, SOLID_FIELDS), ("jacob", model.metric, METRIC_FIELDS)]
+    if not isinstance(model, SolidModel):
+        groups.append(("fluid", model.fluid, FLUID_FIELDS))
     for sub, arrays, names in groups:
         os.makedirs(os.path.join(directory, sub), exist_ok=True)
         for k in names:
@@ -210,6 +259,58 @@ def make_model(nx: int, nz_f: int, nz_s: int, *, h: float = 5.0, npd: int = 20,
                  src_x=list(src_x), src_z=list(src_z), npd=npd, npow=npow,
                  thickness=(npd - 1) * h, vp_max=vpmax, rc=rc, beta0=beta0,
                  fluid=fluid, solid=solid, metric=metric)
+
+
+def _solid_metric(nx: int, nz: int, npd: int, h: float, amp: float,
+                  wavelength: float) -> Dict[str, np.ndarray]:
+    """FP64 metric of z(xi, zeta) = h (zeta - 3) + amp sin(2 pi x / wavelength) w(zeta):
+    a free surface with topography on row 3, w = cos^2 falling 1 -> 0 between
+    row 3 and b = nz - 4 - npd (flat below, so the bottom band is flat)."""
+    zeta = np.arange(nz, dtype=np.float64)
+    b = float(nz - 4 - npd)
+    t = np.clip((zeta - 3.0) / (b - 3.0), 0.0, 1.0)
+    w = np.cos(0.5 * math.pi * t) ** 2
+    dw = np.where((t > 0.0) & (t < 1.0), -0.5 * math.pi / (b - 3.0) * np.sin(math.pi * t), 0.0)
+    x = h * np.arange(nx, dtype=np.float64)
+    s = np.sin(2.0 * math.pi * x / wavelength) if amp else np.zeros(nx)
+    c = np.cos(2.0 * math.pi * x / wavelength) if amp else np.zeros(nx)
+    z_xi = amp * (2.0 * math.pi * h / wavelength) * c[None, :] * w[:, None]
+    z_ze = h + amp * s[None, :] * dw[:, None]
+    if np.any(z_ze <= 0.0):
+        raise ValueError("grid folds: z_zeta <= 0")
+    J = h * z_ze
+    return {"J": J, "xi_x": np.full((nz, nx), 1.0 / h), "xi_z": np.zeros((nz, nx)),
+            "ze_x": -z_xi / J, "ze_z": h / J}
+
+
+def make_solid_model(nx: int, nz: int, *, h: float = 5.0, npd: int = 20, fpeak: float = 15.0,
+                     dt: float = 5e-4, nt: int = 2000, snapshot: Optional[int] = None,
+                     src_x: Optional[List[int]] = None, src_z: Optional[List[int]] = None,
+                     vp: float = 3000.0, vs: float = 1732.0, rho: float = 2000.0,
+                     amp: float = 0.0, wavelength: float = 600.0, perturb: float = 0.0,
+                     corr_len: float = 50.0, seed: int = 0, ppw: float = 8.0, npow: int = 2,
+                     rc: float = 1e-3) -> SolidModel:
+    """A solid half-space with a free surface (flat, or with topography when amp > 0)."""
+    metric = _solid_metric(nx, nz, npd, h, amp, wavelength)
+    shape = (nz, nx)
+    vp_s, vs_s, rho_s = np.full(shape, vp), np.full(shape, vs), np.full(shape, rho)
+    if perturb:
+        rng = np.random.default_rng(seed)
+        corr = corr_len / h
+        vp_s *= 1.0 + perturb * _correlated_field(rng, shape, corr)
+        vs_s *= 1.0 + perturb * _correlated_field(rng, shape, corr)
+        rho_s *= 1.0 + perturb * _correlated_field(rng, shape, corr)
+    mu = rho_s * vs_s ** 2
+    lam = rho_s * (vp_s ** 2 - 2.0 * vs_s ** 2)
+    solid = {"C11": lam + 2.0 * mu, "C13": lam, "C33": lam + 2.0 * mu, "C55": mu, "rho": rho_s}
+    beta0 = round(float(np.min(vs_s)) / (0.5 * ppw * h * fpeak), 4)
+    return SolidModel(nx=nx, nz=nz, h=h, fpeak=fpeak, dt=dt, nt=nt,
+                      snapshot=snapshot if snapshot is not None else nt + 1,
+                      src_x=list(src_x if src_x is not None else [nx // 2]),
+                      src_z=list(src_z if src_z is not None else [10]),
+                      npd=npd, npow=npow, thickness=(npd - 1) * h,
+                      vp_max=float(np.max(vp_s)), rc=rc, beta0=max(1.0, beta0),
+                      solid=solid, metric=metric)
 
 
 def beta0_rule(model: Model, fpeak: float, ppw: float = 8.0) -> float:

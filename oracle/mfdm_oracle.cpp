@@ -140,6 +140,45 @@ struct orc_model {
 
 namespace {
 
+// CFS-PML 1-D profile over n cells with a band of npd cells at the low and/or
+// high end (src/elements.cu:824-860): d = d0 r^NPOW, beta = 1 + (beta0 - 1) r^2,
+// alpha = alpha0 (1 - r), r = k / npd. The FP32 oracle evaluates it with float
+// std::log / std::pow like the reference; the FP64 oracle in double from the
+// float-valued inputs.
+template <class R>
+void pml_profile(const orc_model& m, float fpeak_f, int npd, R* al, R* be, R* dp, int n, bool lo,
+                 bool hi) {
+  const float vpmax = float(m.vp_max), rc = float(m.rc), thick = float(m.thickness);
+  const float beta0 = float(m.beta0);
+  const int npow = m.npow;
+  const float alpha0_f = 2 * float(M_PI) * fpeak_f;
+  const float damp0_f = -(npow + 1) * vpmax * std::log(rc) / (2.0f * thick);
+  const double alpha0_d = 2.0 * M_PI * double(fpeak_f);
+  const double damp0_d = -(npow + 1) * double(vpmax) * std::log(double(rc)) / (2.0 * double(thick));
+  for (int i = 0; i < n; ++i) {
+    int k = -1;
+    if (lo && i >= 3 && i <= 2 + npd) k = 3 + npd - i;
+    if (hi && i >= n - 3 - npd && i <= n - 4) k = i - (n - 4 - npd);
+    if constexpr (std::is_same<R, float>::value) {
+      if (k <= 0) { dp[i] = 0.0f; be[i] = 1.0f; al[i] = alpha0_f; }
+      else {
+        float r = float(k) / float(npd);
+        dp[i] = damp0_f * std::pow(r, float(npow));
+        be[i] = 1.0f + (beta0 - 1.0f) * std::pow(r, 2.0f);
+        al[i] = alpha0_f * (1.0f - std::pow(r, 1.0f));
+      }
+    } else {
+      if (k <= 0) { dp[i] = 0.0; be[i] = 1.0; al[i] = R(alpha0_d); }
+      else {
+        double r = double(k) / double(npd);
+        dp[i] = R(damp0_d * std::pow(r, double(npow)));
+        be[i] = R(1.0 + (double(beta0) - 1.0) * r * r);
+        al[i] = R(alpha0_d * (1.0 - r));
+      }
+    }
+  }
+}
+
 template <class R>
 struct Oracle {
   int nx, nzf, nzs, npd;
@@ -193,41 +232,10 @@ struct Oracle {
     alx.assign(nx, 0); bex.assign(nx, 0); dpx.assign(nx, 0);
     alz.assign(nzs, 0); bez.assign(nzs, 0); dpz.assign(nzs, 0);
     alzf.assign(nzf, 0); bezf.assign(nzf, 0); dpzf.assign(nzf, 0);
-    const float vpmax = float(m.vp_max), rc = float(m.rc), thick = float(m.thickness);
-    const float beta0 = float(m.beta0);
-    const int npow = m.npow;
-    const float alpha0_f = 2 * float(M_PI) * fpeak_f;
-    const float damp0_f = -(npow + 1) * vpmax * std::log(rc) / (2.0f * thick);
-    const double alpha0_d = 2.0 * M_PI * double(fpeak_f);
-    const double damp0_d = -(npow + 1) * double(vpmax) * std::log(double(rc)) / (2.0 * double(thick));
-    auto profile = [&](R* al, R* be, R* dp, int n, bool lo, bool hi) {
-      for (int i = 0; i < n; ++i) {
-        int k = -1;
-        if (lo && i >= 3 && i <= 2 + npd) k = 3 + npd - i;
-        if (hi && i >= n - 3 - npd && i <= n - 4) k = i - (n - 4 - npd);
-        if constexpr (std::is_same<R, float>::value) {
-          if (k <= 0) { dp[i] = 0.0f; be[i] = 1.0f; al[i] = alpha0_f; }
-          else {
-            float r = float(k) / float(npd);
-            dp[i] = damp0_f * std::pow(r, float(npow));
-            be[i] = 1.0f + (beta0 - 1.0f) * std::pow(r, 2.0f);
-            al[i] = alpha0_f * (1.0f - std::pow(r, 1.0f));
-          }
-        } else {
-          if (k <= 0) { dp[i] = 0.0; be[i] = 1.0; al[i] = R(alpha0_d); }
-          else {
-            double r = double(k) / double(npd);
-            dp[i] = R(damp0_d * std::pow(r, double(npow)));
-            be[i] = R(1.0 + (double(beta0) - 1.0) * r * r);
-            al[i] = R(alpha0_d * (1.0 - r));
-          }
-        }
-      }
-    };
-    profile(alx.data(), bex.data(), dpx.data(), nx, true, true);
-    profile(alz.data(), bez.data(), dpz.data(), nzs, false, true);
+    pml_profile(m, fpeak_f, npd, alx.data(), bex.data(), dpx.data(), nx, true, true);
+    pml_profile(m, fpeak_f, npd, alz.data(), bez.data(), dpz.data(), nzs, false, true);
     // fluid zeta axis: a top band for CPML only (src/elements.cu:866-869)
-    profile(alzf.data(), bezf.data(), dpzf.data(), nzf, cpml, false);
+    pml_profile(m, fpeak_f, npd, alzf.data(), bezf.data(), dpzf.data(), nzf, cpml, false);
   }
 
   // Unit normal of the interface from the zeta gradient (src/elements.cu:892-905).
@@ -706,6 +714,345 @@ struct Oracle {
   }
 };
 
+// ---- solid only with a free surface on top (PmlFs::SolidOnly) ----------------
+// include/pml_fs_kernels.cuh:8-307, src/pml_fs_kernels.cu:5-381,
+// src/elements.cu:824-873 (PML tables), 907-977 (ALM free-surface coefficients),
+// src/main.cu:252-300 (the record: solid vz on row 3).
+// The model's solid arrays and the metric are all [nz][nx] (nz = nz_s, nz_f
+// unused): the solid fills the grid, the free surface is row 3, CFS-PML on the
+// left, right and bottom.
+enum SField { TVX, TVZ, TSX, TSZ, TSXZ, XVX, XVZ, XEX, XEZ, ZVX, ZVZ, ZEX, ZEZ, NSFIELD };
+
+template <class R>
+struct SolidOracle {
+  int nx, nz, npd;
+  float fpeak_f, dt_f;
+  int srcx, srcz;
+  std::vector<R> C11, C13, C33, C55, rho, J, xx, xz, zx, zz;
+  std::vector<R> alx, bex, dpx, alz, bez, dpz;
+  std::vector<R> alm;  // [nx][6]: al1_xx, al1_zz, al1_xz, al2_xx, al2_zz, al2_xz
+  using Set = std::vector<std::vector<R>>;
+  Set U, Ub, Ut, Kk;
+
+  static std::vector<R> conv(const double* p, size_t n) {
+    std::vector<R> v(n);
+    for (size_t i = 0; i < n; ++i) v[i] = R(p[i]);
+    return v;
+  }
+  void alloc(Set& S) { S.assign(NSFIELD, std::vector<R>(size_t(nz) * nx, R(0))); }
+
+  explicit SolidOracle(const orc_model& m) {
+    nx = m.nx; nz = m.nz_s; npd = m.npd;
+    fpeak_f = float(m.fpeak); dt_f = float(m.dt);
+    srcx = m.src_x; srcz = m.src_z;
+    const size_t n = size_t(nz) * nx;
+    C11 = conv(m.C11, n); C13 = conv(m.C13, n); C33 = conv(m.C33, n); C55 = conv(m.C55, n);
+    rho = conv(m.rho_s, n);
+    J = conv(m.J, n); xx = conv(m.xi_x, n); xz = conv(m.xi_z, n);
+    zx = conv(m.ze_x, n); zz = conv(m.ze_z, n);
+    alx.assign(nx, 0); bex.assign(nx, 0); dpx.assign(nx, 0);
+    alz.assign(nz, 0); bez.assign(nz, 0); dpz.assign(nz, 0);
+    pml_profile(m, fpeak_f, npd, alx.data(), bex.data(), dpx.data(), nx, true, true);
+    pml_profile(m, fpeak_f, npd, alz.data(), bez.data(), dpz.data(), nz, false, true);
+    free_surface(m);
+    alloc(U); alloc(Ub); alloc(Ut); alloc(Kk);
+  }
+
+  // ALM coefficients of the free-surface row (src/elements.cu:907-977): from
+  // the traction-free condition the zeta derivatives of the velocity on row 3
+  // are eliminated in favour of the xi derivatives; evaluated in double from
+  // the model's float values (the FP64 oracle from its own values) and stored
+  // at the oracle's precision.
+  void free_surface(const orc_model& m) {
+    alm.assign(size_t(nx) * 6, R(0));
+    for (int ix = 0; ix < nx; ++ix) {
+      const size_t i = size_t(3) * nx + ix;
+      auto val = [&](const double* a) {
+        return std::is_same<R, float>::value ? double(float(a[i])) : a[i];
+      };
+      const double xi_x = val(m.xi_x), xi_z = val(m.xi_z), ze_x = val(m.ze_x), ze_z = val(m.ze_z);
+      const double c11 = val(m.C11), c13 = val(m.C13), c33 = val(m.C33), c55 = val(m.C55);
+      const double Dz11 = c11 * ze_x * ze_x + c55 * ze_z * ze_z;
+      const double Dz12 = (c13 + c55) * ze_x * ze_z;
+      const double Dz22 = c55 * ze_x * ze_x + c33 * ze_z * ze_z;
+      const double Dx11 = c11 * ze_x * xi_x + c55 * ze_z * xi_z;
+      const double Dx12 = c13 * ze_x * xi_z + c55 * ze_z * xi_x;
+      const double Dx21 = c13 * ze_z * xi_x + c55 * ze_x * xi_z;
+      const double Dx22 = c55 * ze_x * xi_x + c33 * ze_z * xi_z;
+      const double det = Dz11 * Dz22 - Dz12 * Dz12;
+      double m11 = 0, m12 = 0, m21 = 0, m22 = 0;
+      if (std::abs(det) >= 1e-14) {
+        const double i11 = Dz22 / det, i12 = -Dz12 / det, i22 = Dz11 / det;
+        m11 = i11 * Dx11 + i12 * Dx21;
+        m12 = i11 * Dx12 + i12 * Dx22;
+        m21 = i12 * Dx11 + i22 * Dx21;
+        m22 = i12 * Dx12 + i22 * Dx22;
+      }
+      R* a = &alm[size_t(ix) * 6];
+      a[0] = R(xi_x - ze_x * m11);
+      a[1] = R(-ze_z * m21);
+      a[2] = R(xi_z - ze_z * m11 - ze_x * m21);
+      a[3] = R(-ze_x * m12);
+      a[4] = R(xi_z - ze_z * m22);
+      a[5] = R(xi_x - ze_z * m12 - ze_x * m22);
+    }
+  }
+
+  R ricker(R time) const {
+    if constexpr (std::is_same<R, float>::value) {
+      const float T = float(1.2 / double(fpeak_f));
+      float t = float(time) - T;
+      if (t > T) return 0.0f;
+      float temp = float(M_PI * double(fpeak_f) * double(t));
+      temp *= temp;
+      return (1 - 2 * temp) * std::exp(-temp);
+    }
+    const double T = 1.2 / double(fpeak_f);
+    double t = double(time) - T;
+    if (t > T) return 0.0;
+    double temp = M_PI * double(fpeak_f) * t;
+    temp *= temp;
+    return R((1 - 2 * temp) * std::exp(-temp));
+  }
+
+  // Solid flux rows (src/tools_func.cu:19-65 with no fluid above: no row offset).
+  P2<R> flux_ze(const Set& S, int r, int ix) const {
+    const size_t i = size_t(r) * nx + ix;
+    return {J[i] * (zx[i] * S[TSX][i] + zz[i] * S[TSXZ][i]),
+            J[i] * (zx[i] * S[TSXZ][i] + zz[i] * S[TSZ][i])};
+  }
+  P2<R> flux_xi(const Set& S, size_t i) const {
+    return {J[i] * (xx[i] * S[TSX][i] + xz[i] * S[TSXZ][i]),
+            J[i] * (xx[i] * S[TSXZ][i] + xz[i] * S[TSZ][i])};
+  }
+
+  void stress(int dir, const Set& S) {
+#pragma omp parallel for schedule(static)
+    for (int iz = 3; iz <= nz - 4; ++iz)
+      for (int ix = 3; ix <= nx - 4; ++ix) {
+        const size_t i = size_t(iz) * nx + ix;
+        const int dist = iz - 3, distx = std::min(ix - 3, nx - 4 - ix);
+        const R dvx_dxi = dmac(dir, &S[TVX][i], 1), dvz_dxi = dmac(dir, &S[TVZ][i], 1);
+        const bool side = distx < npd, bottom = iz >= nz - 3 - npd;
+        const R c11 = C11[i], c13 = C13[i], c33 = C33[i], c55 = C55[i];
+        if (dist == 0) {
+          const R* a = &alm[size_t(ix) * 6];
+          Kk[TSX][i] = (c11 * a[0] + c13 * a[1]) * dvx_dxi + (c11 * a[3] + c13 * a[4]) * dvz_dxi;
+          Kk[TSZ][i] = (c13 * a[0] + c33 * a[1]) * dvx_dxi + (c13 * a[3] + c33 * a[4]) * dvz_dxi;
+          Kk[TSXZ][i] = c55 * (a[2] * dvx_dxi + a[5] * dvz_dxi);
+          if (side) {
+            const R dpb = dpx[ix] / bex[ix], apdpb = alx[ix] + dpb, invb = R(1) / bex[ix];
+            const R E0 = S[XEX][i], E1 = S[XEZ][i];
+            Kk[XEX][i] = -apdpb * E0 + dpb * dvx_dxi;
+            Kk[XEZ][i] = -apdpb * E1 + dpb * dvz_dxi;
+            const R cxx_x = c11 * a[0] + c13 * a[1], cxx_z = c11 * a[3] + c13 * a[4];
+            Kk[TSX][i] += (invb - R(1)) * (cxx_x * dvx_dxi + cxx_z * dvz_dxi) -
+                          invb * (cxx_x * E0 + cxx_z * E1);
+            const R czz_x = c13 * a[0] + c33 * a[1], czz_z = c13 * a[3] + c33 * a[4];
+            Kk[TSZ][i] += (invb - R(1)) * (czz_x * dvx_dxi + czz_z * dvz_dxi) -
+                          invb * (czz_x * E0 + czz_z * E1);
+            Kk[TSXZ][i] += c55 * ((invb - R(1)) * (a[2] * dvx_dxi + a[5] * dvz_dxi) -
+                                  invb * (a[2] * E0 + a[5] * E1));
+          }
+          continue;
+        }
+        const R dvx_dze = dz_near(dir, &S[TVX][i], nx, dist, true);
+        const R dvz_dze = dz_near(dir, &S[TVZ][i], nx, dist, true);
+        const R xix = xx[i], xiz = xz[i], zex = zx[i], zez = zz[i];
+        Kk[TSX][i] = c11 * (xix * dvx_dxi + zex * dvx_dze) + c13 * (xiz * dvz_dxi + zez * dvz_dze);
+        Kk[TSZ][i] = c13 * (xix * dvx_dxi + zex * dvx_dze) + c33 * (xiz * dvz_dxi + zez * dvz_dze);
+        Kk[TSXZ][i] = c55 * (xiz * dvx_dxi + zez * dvx_dze + xix * dvz_dxi + zex * dvz_dze);
+        if (!side && !bottom) continue;
+        const R gxixi = xix * xix + xiz * xiz, gxize = xix * zex + xiz * zez,
+                gzeze = zex * zex + zez * zez;
+        if (side) {
+          const R Dvx = dvx_dxi + (gxize / gxixi) * dvx_dze, Dvz = dvz_dxi + (gxize / gxixi) * dvz_dze;
+          const R dpb = dpx[ix] / bex[ix], apdpb = alx[ix] + dpb, invb = R(1) / bex[ix];
+          const R E0 = S[XEX][i], E1 = S[XEZ][i];
+          Kk[XEX][i] = -apdpb * E0 + dpb * Dvx;
+          Kk[XEZ][i] = -apdpb * E1 + dpb * Dvz;
+          Kk[TSX][i] += c11 * (invb - R(1)) * xix * Dvx + c13 * (invb - R(1)) * xiz * Dvz -
+                        invb * c11 * xix * E0 - invb * c13 * xiz * E1;
+          Kk[TSZ][i] += c13 * (invb - R(1)) * xix * Dvx + c33 * (invb - R(1)) * xiz * Dvz -
+                        invb * c13 * xix * E0 - invb * c33 * xiz * E1;
+          Kk[TSXZ][i] += c55 * (invb - R(1)) * (xiz * Dvx + xix * Dvz) - invb * c55 * xiz * E0 -
+                         invb * c55 * xix * E1;
+        }
+        if (bottom) {
+          const R Dvx = dvx_dze + (gxize / gzeze) * dvx_dxi, Dvz = dvz_dze + (gxize / gzeze) * dvz_dxi;
+          const R dpb = dpz[iz] / bez[iz], apdpb = alz[iz] + dpb, invb = R(1) / bez[iz];
+          const R E0 = S[ZEX][i], E1 = S[ZEZ][i];
+          Kk[ZEX][i] = -apdpb * E0 + dpb * Dvx;
+          Kk[ZEZ][i] = -apdpb * E1 + dpb * Dvz;
+          Kk[TSX][i] += c11 * (invb - R(1)) * zex * Dvx + c13 * (invb - R(1)) * zez * Dvz -
+                        invb * c11 * zex * E0 - invb * c13 * zez * E1;
+          Kk[TSZ][i] += c13 * (invb - R(1)) * zex * Dvx + c33 * (invb - R(1)) * zez * Dvz -
+                        invb * c13 * zex * E0 - invb * c33 * zez * E1;
+          Kk[TSXZ][i] += c55 * (invb - R(1)) * (zez * Dvx + zex * Dvz) - invb * c55 * zez * E0 -
+                         invb * c55 * zex * E1;
+        }
+      }
+  }
+
+  void velocity(int dir, const Set& S) {
+#pragma omp parallel for schedule(static)
+    for (int iz = 3; iz <= nz - 4; ++iz)
+      for (int ix = 3; ix <= nx - 4; ++ix) {
+        const size_t i = size_t(iz) * nx + ix;
+        const int dist = iz - 3;
+        const R xix = xx[i], xiz = xz[i], zex = zx[i], zez = zz[i];
+        const R gxixi = xix * xix + xiz * xiz, gzeze = zex * zex + zez * zez;
+        R rvx, rvz, dxx, dxz, dzx, dzz;
+        if (dist < 3) {
+          // conservative rows below the free surface; above it the image G = -F
+          // of the rows below (src/pml_fs_kernels.cu:7-19)
+          auto Fxi = [&](int j) { return flux_xi(S, i + j); };
+          auto Fze = [&](int j) -> P2<R> {
+            const int r = iz + j;
+            if (r >= 3) return flux_ze(S, r, ix);
+            const P2<R> b = flux_ze(S, 6 - r, ix);
+            return {-b.x, -b.y};
+          };
+          const P2<R> a = dflux<R>(dir, Fxi), b = dflux<R>(dir, Fze);
+          rvx = (a.x + b.x) / J[i];
+          rvz = (a.y + b.y) / J[i];
+          const R gxize = xix * zex + xiz * zez;
+          const R dxsx = dmac(dir, &S[TSX][i], 1), dxsz = dmac(dir, &S[TSZ][i], 1),
+                  dxsxz = dmac(dir, &S[TSXZ][i], 1);
+          const R dzsx = dz_near(dir, &S[TSX][i], nx, dist, true),
+                  dzsz = dz_near(dir, &S[TSZ][i], nx, dist, true),
+                  dzsxz = dz_near(dir, &S[TSXZ][i], nx, dist, true);
+          dxx = xix * (dxsx + gxize / gxixi * dzsx) + xiz * (dxsxz + gxize / gxixi * dzsxz);
+          dxz = xix * (dxsxz + gxize / gxixi * dzsxz) + xiz * (dxsz + gxize / gxixi * dzsz);
+          dzx = 0;
+          dzz = 0;
+        } else {
+          const R sxdx = dmac(dir, &S[TSX][i], 1), sxdz = dmac(dir, &S[TSX][i], nx);
+          const R szdx = dmac(dir, &S[TSZ][i], 1), szdz = dmac(dir, &S[TSZ][i], nx);
+          const R tdx = dmac(dir, &S[TSXZ][i], 1), tdz = dmac(dir, &S[TSXZ][i], nx);
+          rvx = xix * sxdx + zex * sxdz + xiz * tdx + zez * tdz;
+          rvz = xix * tdx + zex * tdz + xiz * szdx + zez * szdz;
+          const R gxize = xix * zex + xiz * zez;
+          dxx = xix * (sxdx + gxize / gxixi * sxdz) + xiz * (tdx + gxize / gxixi * tdz);
+          dxz = xix * (tdx + gxize / gxixi * tdz) + xiz * (szdx + gxize / gxixi * szdz);
+          dzx = zex * (sxdz + gxize / gzeze * sxdx) + zez * (gxize / gzeze * tdx + tdz);
+          dzz = zex * (gxize / gzeze * tdx + tdz) + zez * (gxize / gzeze * szdx + szdz);
+        }
+        const int distx = std::min(ix - 3, nx - 4 - ix);
+        const bool side = distx < npd, bottom = iz >= nz - 3 - npd;
+        const R r0 = rho[i];
+        R kvx = rvx / r0, kvz = rvz / r0;
+        if (side) {
+          const R dpb = dpx[ix] / bex[ix], apdpb = alx[ix] + dpb, invb = R(1) / bex[ix];
+          const R V0 = S[XVX][i], V1 = S[XVZ][i];
+          Kk[XVX][i] = -apdpb * V0 + dpb * dxx;
+          Kk[XVZ][i] = -apdpb * V1 + dpb * dxz;
+          kvx += ((invb - R(1)) * dxx - invb * V0) / r0;
+          kvz += ((invb - R(1)) * dxz - invb * V1) / r0;
+        }
+        if (bottom) {
+          const R dpb = dpz[iz] / bez[iz], apdpb = alz[iz] + dpb, invb = R(1) / bez[iz];
+          const R V0 = S[ZVX][i], V1 = S[ZVZ][i];
+          Kk[ZVX][i] = -apdpb * V0 + dpb * dzx;
+          Kk[ZVZ][i] = -apdpb * V1 + dpb * dzz;
+          kvx += ((invb - R(1)) * dzx - invb * V0) / r0;
+          kvz += ((invb - R(1)) * dzz - invb * V1) / r0;
+        }
+        Kk[TVX][i] = kvx;
+        Kk[TVZ][i] = kvz;
+      }
+  }
+
+  // Explosive source: the 5x5 Gaussian added to both normal stresses
+  // (src/pml_fs_kernels.cu:22-26, include/tools_func.cuh:21-37).
+  void add_source(R amp) {
+    for (int j = -2; j <= 2; ++j)
+      for (int q = -2; q <= 2; ++q) {
+        const int ix = srcx + q, iz = srcz + j;
+        if (ix <= 2 || ix >= nx - 3 || iz <= 2 || iz >= nz - 3) continue;
+        const R w = amp * R(kSrcW[j + 2][q + 2]);
+        const size_t i = size_t(iz) * nx + ix;
+        Kk[TSX][i] += w;
+        Kk[TSZ][i] += w;
+      }
+  }
+
+  void stage(int dir, R t, const Set& S) {
+    velocity(dir, S);
+    stress(dir, S);
+    add_source(ricker(t));
+  }
+
+  // Live cells: every cell of the five state fields, the strip cells of the ADE fields.
+  bool live(int f, int iz, int ix) const {
+    if (f < XVX) return true;
+    if (f < ZVX) {
+      const int d = std::min(ix - 3, nx - 4 - ix);
+      return ix >= 3 && ix <= nx - 4 && d < npd;
+    }
+    return iz >= nz - 3 - npd && iz <= nz - 4;
+  }
+  template <class Fn> void for_cells(Fn fn) {
+#pragma omp parallel for schedule(static)
+    for (int iz = 0; iz < nz; ++iz)
+      for (int f = 0; f < NSFIELD; ++f)
+        for (int ix = 0; ix < nx; ++ix)
+          if (live(f, iz, ix)) fn(f, size_t(iz) * nx + ix);
+  }
+
+  // One RK4 step (src/pml_fs_kernels.cu:95-380), the same stage weights and
+  // direction order as the fluid-solid step.
+  void step(int it) {
+    const int d0 = (it & 1) ? kB : kF, d1 = 1 - d0;
+    R time, half, dt;
+    if constexpr (std::is_same<R, float>::value) {
+      time = R(float(it) * dt_f);
+      half = R(float(double(dt_f) * 0.5));
+      dt = R(dt_f);
+    } else {
+      time = R(double(it) * double(dt_f));
+      half = R(0.5 * double(dt_f));
+      dt = R(dt_f);
+    }
+    const R c_half = dt / 2, c_full = dt, w6 = dt / 6, w3 = dt / 3, w_last = dt / R(6.0f);
+    stage(d0, time, U);
+    for_cells([&](int f, size_t k) {
+      Ut[f][k] = R(1) * U[f][k] + c_half * Kk[f][k];
+      Ub[f][k] = U[f][k] + w6 * Kk[f][k];
+    });
+    stage(d1, time + half, Ut);
+    for_cells([&](int f, size_t k) {
+      Ut[f][k] = R(1) * U[f][k] + c_half * Kk[f][k];
+      Ub[f][k] += w3 * Kk[f][k];
+    });
+    stage(d0, time + half, Ut);
+    for_cells([&](int f, size_t k) {
+      Ut[f][k] = R(1) * U[f][k] + c_full * Kk[f][k];
+      Ub[f][k] += w3 * Kk[f][k];
+    });
+    stage(d1, time + dt, Ut);
+    for_cells([&](int f, size_t k) { U[f][k] = R(1) * Ub[f][k] + w_last * Kk[f][k]; });
+  }
+};
+
+template <class R>
+int run_solid(const orc_model* m, int nsteps, int gap, double* rvz, double* out) {
+  SolidOracle<R> o(*m);
+  const int nx = m->nx;
+  for (int it = 0; it < nsteps; ++it) {
+    o.step(it);
+    if (gap > 0 && it % gap == 0 && rvz)
+      for (int ix = 0; ix < nx; ++ix)
+        rvz[size_t(it / gap) * nx + ix] = double(o.U[TVZ][size_t(3) * nx + ix]);
+  }
+  if (out) {
+    const size_t n = size_t(m->nz_s) * nx;
+    for (int q = 0; q < 5; ++q)
+      for (size_t k = 0; k < n; ++k) out[q * n + k] = double(o.U[q][k]);
+  }
+  return 0;
+}
+
 template <class R>
 int run(const orc_model* m, int nsteps, int gap, double* rvx, double* rvz, double* rp,
         double* out_fluid, double* out_solid) {
@@ -768,6 +1115,30 @@ int orc_forward(const orc_model* m, int precision, int nsteps, int gap, double* 
   const int rc = precision == 64
                      ? run<double>(m, nsteps, gap, rec_svx, rec_svz, rec_fp, out_fluid, out_solid)
                      : run<float>(m, nsteps, gap, rec_svx, rec_svz, rec_fp, out_fluid, out_solid);
+#pragma omp parallel
+  { _mm_setcsr(saved); }
+  _mm_setcsr(saved);
+  return rc;
+}
+
+// Solid only with a free surface (PmlFs::SolidOnly): nz_s is the grid's row
+// count, the solid and metric arrays are [nz_s][nx], nz_f and the fluid arrays
+// are unused. Records: solid vz on row 3 every `gap` steps ([ceil(nsteps/gap)][nx]);
+// out_solid: the final [5][nz_s][nx] (vx, vz, sx, sz, sxz).
+int orc_forward_solid(const orc_model* m, int precision, int nsteps, int gap, double* rec_vz,
+                      double* out_solid, int nthreads) {
+  if (!m || m->nx < 8 || m->nz_s < 8 || nsteps < 0) return -1;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+  unsigned saved = _mm_getcsr();
+#pragma omp parallel
+  { _mm_setcsr(_mm_getcsr() | 0x8040u); }
+  _mm_setcsr(saved | 0x8040u);
+  const int rc = precision == 64 ? run_solid<double>(m, nsteps, gap, rec_vz, out_solid)
+                                 : run_solid<float>(m, nsteps, gap, rec_vz, out_solid);
 #pragma omp parallel
   { _mm_setcsr(saved); }
   _mm_setcsr(saved);

@@ -47,6 +47,9 @@ def lib():
         _lib.orc_forward.restype = ctypes.c_int
         _lib.orc_forward.argtypes = [ctypes.POINTER(_Model), ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int, _dp, _dp, _dp, _dp, _dp, ctypes.c_int]
+        _lib.orc_forward_solid.restype = ctypes.c_int
+        _lib.orc_forward_solid.argtypes = [ctypes.POINTER(_Model), ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, _dp, _dp, ctypes.c_int]
         _lib.orc_max_threads.restype = ctypes.c_int
         _lib.orc_create.restype = ctypes.c_void_p
         _lib.orc_create.argtypes = [ctypes.POINTER(_Model), ctypes.c_int]
@@ -112,6 +115,48 @@ def _model_struct(model, shot=0, round_inputs=True):
     m.ze_x, m.ze_z = arr(model.metric["ze_x"]), arr(model.metric["ze_z"])
     m.cpml = 1 if getattr(model, "boundary_type", 2) == 1 else 0
     return m, keep
+
+
+def forward_solid(model, nsteps: int, gap: int, precision: int = 32, shot: int = 0,
+                  final_fields: bool = False, nthreads: int = 0,
+                  round_inputs: bool = True) -> Dict[str, np.ndarray]:
+    """Solid-only oracle (PmlFs::SolidOnly) for a modelgen.SolidModel, from rest.
+
+    Returns the record ``svz`` (solid vz on row 3) [ceil(nsteps/gap)][nx] and,
+    when asked, the final ``solid`` [5][nz][nx] (vx, vz, sx, sz, sxz)."""
+    keep = []
+
+    def arr(a):
+        a = np.asarray(a, dtype=np.float64)
+        if round_inputs:
+            a = a.astype(np.float32).astype(np.float64)
+        a = np.ascontiguousarray(a)
+        keep.append(a)
+        return _ptr(a)
+
+    m = _Model()
+    m.nx, m.nz_f, m.nz_s = model.nx, 0, model.nz
+    m.npd, m.npow = model.npd, model.npow
+    m.fpeak, m.dt, m.thickness = model.fpeak, model.dt, model.thickness
+    m.vp_max, m.rc, m.beta0 = model.vp_max, model.rc, model.beta0
+    m.src_x, m.src_z = model.src_x[shot], model.src_z[shot]
+    m.C11, m.C13 = arr(model.solid["C11"]), arr(model.solid["C13"])
+    m.C33, m.C55 = arr(model.solid["C33"]), arr(model.solid["C55"])
+    m.rho_s = arr(model.solid["rho"])
+    m.J, m.xi_x, m.xi_z = arr(model.metric["J"]), arr(model.metric["xi_x"]), arr(model.metric["xi_z"])
+    m.ze_x, m.ze_z = arr(model.metric["ze_x"]), arr(model.metric["ze_z"])
+    m.cpml = 0
+    ns = -(-nsteps // gap) if gap > 0 else 0
+    rec = np.zeros((ns, model.nx))
+    so = np.zeros((5, model.nz, model.nx)) if final_fields else None
+    rc = lib().orc_forward_solid(ctypes.byref(m), int(precision), int(nsteps), int(gap), _ptr(rec),
+                                 _ptr(so), int(nthreads))
+    if rc != 0:
+        raise RuntimeError(f"oracle failed ({rc})")
+    out = {"svz": rec}
+    if final_fields:
+        out["solid"] = so
+    return out
 
 
 class Stepper:

@@ -64,6 +64,22 @@ def cpml_curv_small():
     return m
 
 
+def solid_flat_small():
+    """Solid only with a flat free surface (calc_type 0, PmlFs::SolidOnly): 120 x 100,
+    10-cell PML, 25 Hz explosive source 20 rows below the surface, 400 steps."""
+    return modelgen.make_solid_model(120, 100, npd=10, fpeak=25.0, dt=5e-4, nt=400,
+                                     src_x=[60], src_z=[20])
+
+
+def solid_curv_small():
+    """Solid only with surface topography (15 m sinusoid) and 5% perturbations, 400 steps."""
+    return modelgen.make_solid_model(120, 100, npd=10, fpeak=25.0, dt=5e-4, nt=400,
+                                     src_x=[55], src_z=[22], amp=15.0, wavelength=300.0,
+                                     perturb=0.05, seed=3)
+
+
+SOLID_CASES = ("solid_flat_small", "solid_curv_small")
+
 # name -> (builder, receiver stride kept in the fixture, keep final snapshot)
 CASES = {
     "flat_small": (flat_small, 1, True),
@@ -73,6 +89,8 @@ CASES = {
     "curvilinear_1200x800": (curvilinear_1200x800, 40, False),
     "cpml_flat_small": (cpml_flat_small, 1, True),
     "cpml_curv_small": (cpml_curv_small, 1, True),
+    "solid_flat_small": (solid_flat_small, 1, True),
+    "solid_curv_small": (solid_curv_small, 1, True),
 }
 
 

@@ -34,9 +34,11 @@ def run_reference(jpath: str, out: str) -> float:
     return time.time() - t0
 
 
-def load_records(out: str, nx: int):
+def load_records(out: str, nx: int, solid_only: bool = False):
     rec = {}
-    for key, fname in (("svx", "solid_vx.bin"), ("svz", "solid_vz.bin"), ("fp", "fluid_p.bin")):
+    files = (("svz", "solid_vz.bin"),) if solid_only else (
+        ("svx", "solid_vx.bin"), ("svz", "solid_vz.bin"), ("fp", "fluid_p.bin"))
+    for key, fname in files:
         a = np.fromfile(os.path.join(out, "0", "record", fname), dtype="<f4")
         rec[key] = a.reshape(-1, nx)
     return rec
@@ -44,7 +46,9 @@ def load_records(out: str, nx: int):
 
 def load_snapshot(out: str, it: int, model):
     snap = {}
-    for medium, rows in (("solid", model.nz_s), ("fluid", model.nz_f)):
+    media = ((("solid", model.nz),) if isinstance(model, cases.modelgen.SolidModel)
+             else (("solid", model.nz_s), ("fluid", model.nz_f)))
+    for medium, rows in media:
         for comp in ("vx", "vz"):
             p = os.path.join(out, "0", "snapshot", medium, comp, f"{comp}_{it:06d}.bin")
             snap[f"{medium}_{comp}"] = np.fromfile(p, dtype="<f4").reshape(rows, model.nx)
@@ -101,7 +105,9 @@ def main():
         jpath = cases.modelgen.write_model(model, os.path.join(work, "model"))
         outs = [os.path.join(work, "out_a"), os.path.join(work, "out_b")]
         secs = [run_reference(jpath, o) for o in outs]
-        ra, rb = load_records(outs[0], model.nx), load_records(outs[1], model.nx)
+        solid_only = isinstance(model, cases.modelgen.SolidModel)
+        ra = load_records(outs[0], model.nx, solid_only)
+        rb = load_records(outs[1], model.nx, solid_only)
         spread = max(rel(ra[k], rb[k]) for k in ra)
         data = {k: ra[k][:, ::stride].astype(np.float32) for k in ra}
         data["receiver_stride"] = np.int32(stride)
@@ -116,11 +122,14 @@ def main():
         os.makedirs(args.outdir, exist_ok=True)
         np.savez_compressed(os.path.join(args.outdir, name + ".npz"), **data)
         summary[name] = {"seconds": secs, "run_to_run_rel_l2": spread,
-                         "samples": int(ra["svx"].shape[0])}
+                         "samples": int(ra["svz"].shape[0])}
         print(name, json.dumps(summary[name]), flush=True)
         shutil.rmtree(work, ignore_errors=True)
-    with open(os.path.join(args.outdir, "golden_summary.json"), "w") as f:
-        json.dump(summary, f, indent=1)
+    sp = os.path.join(args.outdir, "golden_summary.json")
+    merged = json.load(open(sp)) if os.path.exists(sp) else {}
+    merged.update(summary)
+    with open(sp, "w") as f:
+        json.dump(merged, f, indent=1)
 
 
 if __name__ == "__main__":

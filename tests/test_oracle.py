@@ -76,3 +76,17 @@ def test_record_gap_rounding(oracle):
     assert oracle.record_gap(5e-4) == 2
     assert oracle.record_gap(4e-4) == 3
     assert oracle.record_gap(1e-4) == 10
+
+
+@pytest.mark.parametrize("name", ["solid_flat_small", "solid_curv_small"])
+def test_solid_only_oracle_matches_reference(oracle, cases, name):
+    """PmlFs::SolidOnly (calc_type 0): the FP32 restatement against the reference
+    build's solid vz record on row 3 and its final solid snapshot."""
+    model = cases.CASES[name][0]()
+    d = np.load(cases.fixture_path(name))
+    r = oracle.forward_solid(model, int(d["nt"]), oracle.record_gap(model.dt), 32,
+                             final_fields=True)
+    assert np.linalg.norm(r["svz"] - d["svz"]) <= 2e-6 * np.linalg.norm(d["svz"])
+    for q, comp in ((0, "vx"), (1, "vz")):
+        ref = d["snap_solid_" + comp]
+        assert np.linalg.norm(r["solid"][q] - ref) <= 5e-6 * np.linalg.norm(ref), comp
