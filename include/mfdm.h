@@ -251,6 +251,45 @@ int mfdm_adjoint_forward(mfdm_model* m, int nsteps, int ckpt_every);
 int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_svz,
                           const float* res_fp, mfdm_coef_grad* grad);
 
+/* ---- solid only with a free surface --------------------------------------
+ * calc_type 0 with boundary_type 2: the reference's PmlFs::SolidOnly
+ * (include/pml_fs_kernels.cuh:8-307, src/pml_fs_kernels.cu:5-381): an elastic
+ * solid filling the grid, a traction-free surface on row 3 (ALM coefficients,
+ * src/elements.cu:907-977), CFS-PML left, right and bottom, an explosive source
+ * on sx and sz. The receiver row is solid vz on row 3 (src/main.cu:284-300).
+ * The drop-in command line takes this path when the JSON has calc_type 0. */
+typedef struct mfdm_solid mfdm_solid;
+
+/* A solid-only model from caller memory: every array [nz][nx] row-major. */
+typedef struct mfdm_solid_desc {
+  int nx, nz;
+  float fpeak, dt;
+  int nt, snapshot;
+  int npd, npow;
+  float thickness, vp_max, rc, beta0;
+  int nsrc;
+  const int* src_x;
+  const int* src_z;
+  const float *C11, *C13, *C33, *C55, *rho;
+  const float *J, *xi_x, *xi_z, *ze_x, *ze_z;
+} mfdm_solid_desc;
+
+int mfdm_solid_open_json(const char* json_path, int device, mfdm_solid** out);
+int mfdm_solid_open_desc(const mfdm_solid_desc* d, int device, mfdm_solid** out);
+/* Selects source `isrc`, rewinds to step 0 and clears the records; the
+ * wavefield is kept unless reset_state (as mfdm_set_shot). */
+int mfdm_solid_set_shot(mfdm_solid* m, int isrc, int reset_state);
+/* Advances nsteps steps (graph-captured time loop, as mfdm_step). */
+int mfdm_solid_step(mfdm_solid* m, int nsteps);
+/* As mfdm_solid_step, reporting the device time (ms) of the whole run. */
+int mfdm_solid_time_steps(mfdm_solid* m, int nsteps, float* total_ms);
+/* Receiver samples [first, first + count) of solid vz on row 3: [count][nx]. */
+int mfdm_solid_get_records(mfdm_solid* m, int first, int count, float* solid_vz);
+/* One field (MFDM_SOLID_VX .. MFDM_SOLID_SXZ) to a host [nz][nx] array. */
+int mfdm_solid_get_field(mfdm_solid* m, int field, float* host);
+int mfdm_solid_get_info(const mfdm_solid* m, int* nx, int* nz, int* gap, int* step);
+int mfdm_solid_close(mfdm_solid* m);
+
 /* The drop-in command line: `main_debug <model.json> <out_root>`
  * (src/main.cu:58-216). Clears out_root, runs every shot and writes
  * <out_root>/<shot>/record/{solid_vx,solid_vz,fluid_p}.bin and

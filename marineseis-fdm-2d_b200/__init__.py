@@ -36,7 +36,10 @@ EXPORTS = ("mfdm_last_error", "mfdm_open_json", "mfdm_open_desc", "mfdm_load_des
            "mfdm_run_cli", "mfdm_run_cli_batch", "mfdm_step_noalloc", "mfdm_open_batch", "mfdm_batch_reset",
            "mfdm_batch_get_records", "mfdm_batch_get_field", "mfdm_set_tile", "mfdm_autotune",
            "mfdm_group_open", "mfdm_group_step", "mfdm_group_time_steps", "mfdm_group_close",
-           "mfdm_adjoint_forward", "mfdm_adjoint_backward", "mfdm_adjoint_set_memory")
+           "mfdm_adjoint_forward", "mfdm_adjoint_backward", "mfdm_adjoint_set_memory",
+           "mfdm_solid_open_json", "mfdm_solid_open_desc", "mfdm_solid_set_shot", "mfdm_solid_step",
+           "mfdm_solid_time_steps", "mfdm_solid_get_records", "mfdm_solid_get_field",
+           "mfdm_solid_get_info", "mfdm_solid_close")
 
 # Coefficient arrays the adjoint differentiates (mfdm_coef_grad order).
 GRAD_COEFS = ("K", "rcp_rho_f", "C11", "C13", "C33", "C55", "rcp_rho_s")
@@ -72,6 +75,19 @@ class Info(ctypes.Structure):
                 ("step", ctypes.c_int), ("nsamples", ctypes.c_int),
                 ("cells", ctypes.c_longlong), ("device_bytes", ctypes.c_longlong),
                 ("nshots", ctypes.c_int), ("seg_rows", ctypes.c_int)]
+
+
+class SolidDesc(ctypes.Structure):
+    """mfdm_solid_desc: a solid-only model (calc_type 0) in caller memory."""
+    _fields_ = [("nx", ctypes.c_int), ("nz", ctypes.c_int),
+                ("fpeak", ctypes.c_float), ("dt", ctypes.c_float),
+                ("nt", ctypes.c_int), ("snapshot", ctypes.c_int),
+                ("npd", ctypes.c_int), ("npow", ctypes.c_int),
+                ("thickness", ctypes.c_float), ("vp_max", ctypes.c_float),
+                ("rc", ctypes.c_float), ("beta0", ctypes.c_float),
+                ("nsrc", ctypes.c_int), ("src_x", _ip), ("src_z", _ip),
+                ("C11", _fp), ("C13", _fp), ("C33", _fp), ("C55", _fp), ("rho", _fp),
+                ("J", _fp), ("xi_x", _fp), ("xi_z", _fp), ("ze_x", _fp), ("ze_z", _fp)]
 
 
 class CoefGrad(ctypes.Structure):
@@ -143,6 +159,19 @@ def load_library(path: str = LIB_PATH):
         "mfdm_group_close": (ctypes.c_int, [vp]),
         "mfdm_adjoint_forward": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
         "mfdm_adjoint_set_memory": (ctypes.c_int, [vp, ctypes.c_longlong]),
+        "mfdm_solid_open_json": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(vp)]),
+        "mfdm_solid_open_desc": (ctypes.c_int, [ctypes.POINTER(SolidDesc), ctypes.c_int,
+                                                ctypes.POINTER(vp)]),
+        "mfdm_solid_set_shot": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
+        "mfdm_solid_step": (ctypes.c_int, [vp, ctypes.c_int]),
+        "mfdm_solid_time_steps": (ctypes.c_int, [vp, ctypes.c_int, _fp]),
+        "mfdm_solid_get_records": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, _fp]),
+        "mfdm_solid_get_field": (ctypes.c_int, [vp, ctypes.c_int, _fp]),
+        "mfdm_solid_get_info": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int),
+                                               ctypes.POINTER(ctypes.c_int),
+                                               ctypes.POINTER(ctypes.c_int),
+                                               ctypes.POINTER(ctypes.c_int)]),
+        "mfdm_solid_close": (ctypes.c_int, [vp]),
         "mfdm_adjoint_backward": (ctypes.c_int, [vp, _fp, _fp, _fp, ctypes.POINTER(CoefGrad)]),
     }
     for name, (res, args) in sig.items():
@@ -383,6 +412,95 @@ class Batch(Solver):
         out = np.zeros((rows, info["nx"]), dtype=np.float32)
         _check(self._lib.mfdm_batch_get_field(self._h, int(shot), fid, out.ctypes.data_as(_fp)))
         return out
+
+
+class SolidSolver:
+    """A solid-only model with a free surface (mfdm_solid_*; the reference's
+    PmlFs::SolidOnly, calc_type 0)."""
+
+    def __init__(self, handle: ctypes.c_void_p):
+        self._lib = load_library()
+        self._h = handle
+
+    @classmethod
+    def from_json(cls, path: str, device: int = 0) -> "SolidSolver":
+        h = ctypes.c_void_p()
+        _check(load_library().mfdm_solid_open_json(os.fsencode(path), device, ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_model(cls, model, device: int = 0) -> "SolidSolver":
+        """From a modelgen.SolidModel (arrays read in place, float32)."""
+        keep = []
+
+        def ptr(a):
+            a = _f32(a)
+            keep.append(a)
+            return a.ctypes.data_as(_fp)
+
+        d = SolidDesc()
+        d.nx, d.nz = model.nx, model.nz
+        d.fpeak, d.dt, d.nt, d.snapshot = model.fpeak, model.dt, model.nt, model.snapshot
+        d.npd, d.npow, d.thickness = model.npd, model.npow, model.thickness
+        d.vp_max, d.rc, d.beta0 = model.vp_max, model.rc, model.beta0
+        sx = np.ascontiguousarray(model.src_x, dtype=np.int32)
+        sz = np.ascontiguousarray(model.src_z, dtype=np.int32)
+        keep += [sx, sz]
+        d.nsrc, d.src_x, d.src_z = len(sx), sx.ctypes.data_as(_ip), sz.ctypes.data_as(_ip)
+        d.C11, d.C13 = ptr(model.solid["C11"]), ptr(model.solid["C13"])
+        d.C33, d.C55, d.rho = ptr(model.solid["C33"]), ptr(model.solid["C55"]), ptr(model.solid["rho"])
+        d.J, d.xi_x, d.xi_z = ptr(model.metric["J"]), ptr(model.metric["xi_x"]), ptr(model.metric["xi_z"])
+        d.ze_x, d.ze_z = ptr(model.metric["ze_x"]), ptr(model.metric["ze_z"])
+        h = ctypes.c_void_p()
+        _check(load_library().mfdm_solid_open_desc(ctypes.byref(d), device, ctypes.byref(h)))
+        return cls(h)
+
+    def info(self) -> Dict[str, int]:
+        v = [ctypes.c_int() for _ in range(4)]
+        _check(self._lib.mfdm_solid_get_info(self._h, *[ctypes.byref(x) for x in v]))
+        return dict(zip(("nx", "nz", "gap", "step"), [x.value for x in v]))
+
+    def set_shot(self, isrc: int = 0, reset: bool = True):
+        _check(self._lib.mfdm_solid_set_shot(self._h, int(isrc), 1 if reset else 0))
+
+    def step(self, nsteps: int):
+        _check(self._lib.mfdm_solid_step(self._h, int(nsteps)))
+
+    def time_steps(self, nsteps: int) -> float:
+        total = ctypes.c_float()
+        _check(self._lib.mfdm_solid_time_steps(self._h, int(nsteps), ctypes.byref(total)))
+        return total.value
+
+    def records(self) -> Dict[str, np.ndarray]:
+        """{'svz': solid vz on row 3, [samples][nx]}."""
+        i = self.info()
+        ns = -(-i["step"] // i["gap"])
+        out = np.zeros((ns, i["nx"]), dtype=np.float32)
+        _check(self._lib.mfdm_solid_get_records(self._h, 0, ns, out.ctypes.data_as(_fp)))
+        return {"svz": out}
+
+    def field(self, name: str) -> np.ndarray:
+        i = self.info()
+        out = np.zeros((i["nz"], i["nx"]), dtype=np.float32)
+        _check(self._lib.mfdm_solid_get_field(self._h, FIELDS[name], out.ctypes.data_as(_fp)))
+        return out
+
+    def close(self):
+        if self._h:
+            self._lib.mfdm_solid_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Group:

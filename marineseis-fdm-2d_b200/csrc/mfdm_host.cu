@@ -31,6 +31,7 @@
 #include "json_config.h"
 #include "mfdm_adjoint.h"
 #include "mfdm_kernels.h"
+#include "mfdm_solid.h"
 
 namespace fs = std::filesystem;
 using mfdm::Coef;
@@ -1712,6 +1713,478 @@ int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_
 
 }  // extern "C"
 
+// ---- solid only with a free surface (PmlFs::SolidOnly) -------------------------
+
+struct mfdm_solid {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int nx = 0, nz = 0, npd = 0, P = 0, Ps = 0;
+  float dt = 0.f, fpeak = 0.f;
+  int nt = 0, snapshot = 1, gap = 1;
+  std::vector<int> srcx, srcz;
+  int isrc = 0, host_step = 0;
+  char* dmem = nullptr;
+  size_t dbytes = 0;
+  mfdm::solid::SFields S[4];  // U, stage A, stage B, accumulator
+  mfdm::solid::SCoef C{};
+  float* d_src = nullptr;
+  int src_steps = 0;
+  float* d_rec = nullptr;
+  int rec_cap = 0;
+  HostModel pml;  // PML scalars and the time step for the table builders
+  cudaGraphExec_t graph = nullptr;
+};
+
+namespace {
+
+// The arrays of one solid-only model, [nz][nx], in the caller's memory or in `own`.
+struct SolidHost {
+  int nx = 0, nz = 0;
+  HostModel p;  // scalars: npd, npow, thickness, vp_max, rc, beta0, fpeak, dt, nt, snapshot, sources
+  std::vector<float> own[10];
+  const float* a[10] = {};  // C11, C13, C33, C55, rho, J, xi_x, xi_z, ze_x, ze_z
+};
+
+// Reads a calc_type 0 JSON (src/elements.cu:64-176 with the solid-only branches).
+int load_json_solid(const char* path, SolidHost& h) {
+  try {
+    const mfdm::JsonConfig J = mfdm::JsonConfig::from_file(path);
+    HostModel& p = h.p;
+    p.fpeak = J.get_float("base.fpeak");
+    p.dt = J.get_float("base.dt");
+    p.nt = J.get_int("base.nt");
+    p.snapshot = J.get_int("base.snapshot");
+    if (J.get_int("grid.calc_type") != 0 || J.get_int("grid.boundary_type") != 2)
+      return fail(MFDM_ERR_ARG,
+                  "unsupported configuration: solid-only runs need calc_type 0 with "
+                  "boundary_type 2 (free surface on top, CFS-PML sides and bottom)");
+    const size_t nsrc = J.size("grid.src_pos.posx");
+    for (size_t i = 0; i < nsrc; ++i) {
+      p.srcx.push_back(J.get_int("grid.src_pos.posx", i));
+      p.srcz.push_back(J.get_int("grid.src_pos.posz", i));
+    }
+    h.nx = J.get_int("grid.solid.nx");
+    h.nz = J.get_int("grid.solid.nz");
+    p.npd = J.get_int("PML.npd");
+    p.thickness = J.get_float("PML.thickness");
+    p.npow = J.get_int("PML.NPOW");
+    p.vp_max = J.get_float("PML.Vp_max");
+    p.rc = J.get_float("PML.Rc");
+    p.beta0 = J.get_float("PML.beta0");
+    if (h.nx <= 0 || h.nz <= 0) return fail(MFDM_ERR_CONFIG, "bad grid size");
+    const size_t n = size_t(h.nx) * h.nz;
+    const char* keys[10] = {"grid.solid.C11", "grid.solid.C13", "grid.solid.C33",
+                            "grid.solid.C55", "grid.solid.rho", "grid.jacob.J",
+                            "grid.jacob.xi_x", "grid.jacob.xi_z", "grid.jacob.ze_x",
+                            "grid.jacob.ze_z"};
+    for (int k = 0; k < 10; ++k) {
+      const int rc = read_bin(J.get_string(keys[k]), n, h.own[k]);
+      if (rc != MFDM_OK) return rc;
+      h.a[k] = h.own[k].data();
+    }
+  } catch (const std::exception& e) {
+    return fail(MFDM_ERR_CONFIG, e.what());
+  }
+  return MFDM_OK;
+}
+
+int json_calc_type(const char* path, int* calc_type) {
+  try {
+    *calc_type = mfdm::JsonConfig::from_file(path).get_int("grid.calc_type");
+  } catch (const std::exception& e) {
+    return fail(MFDM_ERR_CONFIG, e.what());
+  }
+  return MFDM_OK;
+}
+
+void solid_release_graph(mfdm_solid* m) {
+  if (m->graph) {
+    cudaGraphExecDestroy(m->graph);
+    m->graph = nullptr;
+  }
+}
+
+void solid_destroy(mfdm_solid* m) {
+  if (!m) return;
+  DeviceGuard g(m->device);
+  solid_release_graph(m);
+  if (m->stream) cudaStreamSynchronize(m->stream);
+  if (m->d_src) cudaFree(m->d_src);
+  if (m->d_rec) cudaFree(m->d_rec);
+  if (m->dmem) cudaFree(m->dmem);
+  if (m->stream) cudaStreamDestroy(m->stream);
+  delete m;
+}
+
+int solid_capacity(mfdm_solid* m, int steps) {
+  if (steps > m->src_steps) {
+    const int cap = std::max(steps, m->src_steps * 2);
+    std::vector<float> amp(size_t(cap) * 4);
+    fill_src_table(m->pml, m->fpeak, cap, amp.data());
+    float* d = nullptr;
+    MFDM_CU(cudaMalloc(&d, amp.size() * sizeof(float)));
+    MFDM_CU(cudaMemcpy(d, amp.data(), amp.size() * sizeof(float), cudaMemcpyHostToDevice));
+    if (m->d_src) cudaFree(m->d_src);
+    m->d_src = d;
+    m->src_steps = cap;
+    solid_release_graph(m);
+  }
+  const int need = (steps + m->gap - 1) / m->gap;
+  if (need > m->rec_cap) {
+    const int cap = std::max(need, m->rec_cap * 2);
+    float* d = nullptr;
+    MFDM_CU(cudaMalloc(&d, size_t(cap) * m->nx * sizeof(float)));
+    MFDM_CU(cudaMemset(d, 0, size_t(cap) * m->nx * sizeof(float)));
+    if (m->d_rec) {
+      MFDM_CU(cudaMemcpy(d, m->d_rec, size_t(m->rec_cap) * m->nx * sizeof(float),
+                         cudaMemcpyDeviceToDevice));
+      cudaFree(m->d_rec);
+    }
+    m->d_rec = d;
+    m->rec_cap = cap;
+    solid_release_graph(m);
+  }
+  m->C.src_amp = m->d_src;
+  m->C.src_steps = m->src_steps;
+  m->C.rec = m->d_rec;
+  m->C.rec_cap = m->rec_cap;
+  return MFDM_OK;
+}
+
+int solid_enqueue_step(mfdm_solid* m, int it, cudaStream_t st) {
+  const int d0 = (it & 1) ? mfdm::kDirB : mfdm::kDirF, d1 = 1 - d0;
+  const mfdm::solid::SFields &U = m->S[0], &A = m->S[1], &B = m->S[2], &Acc = m->S[3];
+  const mfdm::solid::SFields* in[4] = {&U, &A, &B, &A};
+  const mfdm::solid::SFields* out[4] = {&A, &B, &A, &U};
+  const int dir[4] = {d0, d1, d0, d1};
+  for (int s = 0; s < 4; ++s)
+    MFDM_CU(mfdm::solid::launch_stage(m->C, *in[s], *out[s], U, Acc, s, dir[s], st));
+  MFDM_CU(mfdm::solid::launch_finish(m->C, U, st));
+  return MFDM_OK;
+}
+
+int solid_enqueue_steps(mfdm_solid* m, int nsteps) {
+  int rc;
+  while (nsteps > 0) {
+    if ((m->host_step & 1) == 0 && nsteps >= kGraphSteps) {
+      if (!m->graph) {
+        cudaGraph_t g = nullptr;
+        MFDM_CU(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+        rc = MFDM_OK;
+        for (int k = 0; k < kGraphSteps && rc == MFDM_OK; ++k) rc = solid_enqueue_step(m, k, m->stream);
+        const cudaError_t e = cudaStreamEndCapture(m->stream, &g);
+        if (rc != MFDM_OK) {
+          if (g) cudaGraphDestroy(g);
+          return rc;
+        }
+        if (e != cudaSuccess) return fail(MFDM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        const cudaError_t e2 = cudaGraphInstantiate(&m->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e2 != cudaSuccess)
+          return fail(MFDM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e2));
+      }
+      MFDM_CU(cudaGraphLaunch(m->graph, m->stream));
+      m->host_step += kGraphSteps;
+      nsteps -= kGraphSteps;
+    } else {
+      if ((rc = solid_enqueue_step(m, m->host_step, m->stream)) != MFDM_OK) return rc;
+      ++m->host_step;
+      --nsteps;
+    }
+  }
+  return MFDM_OK;
+}
+
+int solid_rewind(mfdm_solid* m, bool clear) {
+  const size_t set_bytes = size_t(reinterpret_cast<char*>(m->S[1].vx) - reinterpret_cast<char*>(m->S[0].vx));
+  if (clear) MFDM_CU(cudaMemsetAsync(m->S[0].vx, 0, 4 * set_bytes, m->stream));
+  if (m->d_rec)
+    MFDM_CU(cudaMemsetAsync(m->d_rec, 0, size_t(m->rec_cap) * m->nx * sizeof(float), m->stream));
+  MFDM_CU(cudaMemsetAsync(m->C.status, 0, sizeof(int), m->stream));
+  m->host_step = 0;
+  MFDM_CU(mfdm::solid::launch_set_step(m->C, 0, m->stream));
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  return MFDM_OK;
+}
+
+int solid_build(mfdm_solid* m, const SolidHost& h, int device) {
+  const HostModel& p = h.p;
+  if (h.nx < 8 || h.nz < 8) return fail(MFDM_ERR_ARG, "grid too small: need nx, nz >= 8");
+  if (p.npd < 0 || 2 * p.npd > h.nx - 6 || p.npd + 7 > h.nz)
+    return fail(MFDM_ERR_ARG, "PML width npd does not fit the grid");
+  if (!(p.dt > 0.f) || !(p.fpeak > 0.f)) return fail(MFDM_ERR_ARG, "dt and fpeak must be > 0");
+  if (p.snapshot < 1 || p.nt < 0) return fail(MFDM_ERR_ARG, "need snapshot >= 1 and nt >= 0");
+  for (size_t i = 0; i < p.srcx.size(); ++i)
+    if (p.srcx[i] < 0 || p.srcx[i] >= h.nx || p.srcz[i] < 0 || p.srcz[i] >= h.nz)
+      return fail(MFDM_ERR_ARG, "source outside the grid");
+  m->device = device;
+  int ndev = 0;
+  MFDM_CU(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(MFDM_ERR_ARG, "no such CUDA device");
+  MFDM_CU(cudaSetDevice(device));
+  MFDM_CU(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+  const int nx = h.nx, nz = h.nz, npd = p.npd;
+  m->nx = nx; m->nz = nz; m->npd = npd;
+  m->dt = p.dt; m->fpeak = p.fpeak; m->nt = p.nt; m->snapshot = p.snapshot;
+  m->gap = std::max(1, int(1e-3 / double(p.dt) + 0.5));  // src/main.cu:92
+  m->srcx = p.srcx; m->srcz = p.srcz;
+  m->pml = p;
+  const int P = round_up(nx, 32), Ps = round_up(std::max(2 * npd, 1), 4), npdr = std::max(npd, 1);
+  m->P = P; m->Ps = Ps;
+  size_t off = 0;
+  auto take = [&](size_t nfloats) {
+    const size_t o = off;
+    off += (nfloats * sizeof(float) + 255) / 256 * 256;
+    return o;
+  };
+  const size_t n = size_t(nz) * P;
+  size_t o_arr[10];
+  for (int k = 0; k < 10; ++k) o_arr[k] = take(n);
+  const size_t o_alm = take(size_t(6) * P), o_px = take(size_t(nx) * 4), o_pz = take(size_t(nz) * 4),
+               o_misc = take(64);
+  size_t o_set[4];
+  for (int s = 0; s < 4; ++s) {
+    o_set[s] = take(5 * n);
+    for (int q = 0; q < 4; ++q) take(size_t(nz) * Ps);
+    for (int q = 0; q < 4; ++q) take(size_t(npdr) * P);
+  }
+  const size_t set_floats = (o_set[1] - o_set[0]) / sizeof(float);
+  m->dbytes = off;
+  MFDM_CU(cudaMalloc(&m->dmem, off));
+  MFDM_CU(cudaMemsetAsync(m->dmem, 0, off, m->stream));
+  char* base = m->dmem;
+  auto F = [&](size_t o) { return reinterpret_cast<float*>(base + o); };
+  for (int s = 0; s < 4; ++s) {
+    mfdm::solid::SFields& S = m->S[s];
+    float* b = F(o_set[s]);
+    S.vx = b; S.vz = b + n; S.sx = b + 2 * n; S.sz = b + 3 * n; S.sxz = b + 4 * n;
+    size_t o = (5 * n * sizeof(float) + 255) / 256 * 256;
+    for (int q = 0; q < 4; ++q) {
+      S.x[q] = reinterpret_cast<float*>(reinterpret_cast<char*>(b) + o);
+      o += (size_t(nz) * Ps * sizeof(float) + 255) / 256 * 256;
+    }
+    for (int q = 0; q < 4; ++q) {
+      S.z[q] = reinterpret_cast<float*>(reinterpret_cast<char*>(b) + o);
+      o += (size_t(npdr) * P * sizeof(float) + 255) / 256 * 256;
+    }
+    if (o / sizeof(float) > set_floats) return fail(MFDM_ERR_ARG, "internal layout error");
+  }
+  mfdm::solid::SCoef& C = m->C;
+  C.nx = nx; C.nz = nz; C.P = P; C.Ps = Ps; C.npd = npd;
+  const float* arr[10];
+  for (int k = 0; k < 10; ++k) {
+    arr[k] = F(o_arr[k]);
+    MFDM_CU(cudaMemcpy2DAsync(F(o_arr[k]), size_t(P) * sizeof(float), h.a[k], size_t(nx) * sizeof(float),
+                              size_t(nx) * sizeof(float), size_t(nz), cudaMemcpyHostToDevice, m->stream));
+  }
+  C.C11 = arr[0]; C.C13 = arr[1]; C.C33 = arr[2]; C.C55 = arr[3]; C.rho = arr[4];
+  C.J = arr[5]; C.xix = arr[6]; C.xiz = arr[7]; C.zex = arr[8]; C.zez = arr[9];
+  // ALM coefficients of the free-surface row, in double from the model's floats
+  // (src/elements.cu:907-977)
+  std::vector<float> alm(size_t(6) * P, 0.f);
+  for (int ix = 0; ix < nx; ++ix) {
+    const size_t i = size_t(3) * nx + ix;
+    const double xi_x = h.a[6][i], xi_z = h.a[7][i], ze_x = h.a[8][i], ze_z = h.a[9][i];
+    const double c11 = h.a[0][i], c13 = h.a[1][i], c33 = h.a[2][i], c55 = h.a[3][i];
+    const double Dz11 = c11 * ze_x * ze_x + c55 * ze_z * ze_z;
+    const double Dz12 = (c13 + c55) * ze_x * ze_z;
+    const double Dz22 = c55 * ze_x * ze_x + c33 * ze_z * ze_z;
+    const double Dx11 = c11 * ze_x * xi_x + c55 * ze_z * xi_z;
+    const double Dx12 = c13 * ze_x * xi_z + c55 * ze_z * xi_x;
+    const double Dx21 = c13 * ze_z * xi_x + c55 * ze_x * xi_z;
+    const double Dx22 = c55 * ze_x * xi_x + c33 * ze_z * xi_z;
+    const double det = Dz11 * Dz22 - Dz12 * Dz12;
+    double m11 = 0, m12 = 0, m21 = 0, m22 = 0;
+    if (std::abs(det) >= 1e-14) {
+      const double i11 = Dz22 / det, i12 = -Dz12 / det, i22 = Dz11 / det;
+      m11 = i11 * Dx11 + i12 * Dx21;
+      m12 = i11 * Dx12 + i12 * Dx22;
+      m21 = i12 * Dx11 + i22 * Dx21;
+      m22 = i12 * Dx12 + i22 * Dx22;
+    }
+    alm[0 * size_t(P) + ix] = float(xi_x - ze_x * m11);
+    alm[1 * size_t(P) + ix] = float(-ze_z * m21);
+    alm[2 * size_t(P) + ix] = float(xi_z - ze_z * m11 - ze_x * m21);
+    alm[3 * size_t(P) + ix] = float(-ze_x * m12);
+    alm[4 * size_t(P) + ix] = float(xi_z - ze_z * m22);
+    alm[5 * size_t(P) + ix] = float(xi_x - ze_z * m12 - ze_x * m22);
+  }
+  MFDM_CU(cudaMemcpyAsync(F(o_alm), alm.data(), alm.size() * sizeof(float), cudaMemcpyHostToDevice, m->stream));
+  C.alm = F(o_alm);
+  std::vector<float4> px, pz;
+  pml_profile(p, nx, true, true, p.fpeak, p.beta0, px);
+  pml_profile(p, nz, false, true, p.fpeak, p.beta0, pz);  // free surface on top
+  MFDM_CU(cudaMemcpyAsync(F(o_px), px.data(), px.size() * sizeof(float4), cudaMemcpyHostToDevice, m->stream));
+  MFDM_CU(cudaMemcpyAsync(F(o_pz), pz.data(), pz.size() * sizeof(float4), cudaMemcpyHostToDevice, m->stream));
+  C.pmlx = reinterpret_cast<const float4*>(F(o_px));
+  C.pmlz = reinterpret_cast<const float4*>(F(o_pz));
+  int* misc = reinterpret_cast<int*>(F(o_misc));
+  C.step = misc;
+  C.done = reinterpret_cast<unsigned*>(misc + 1);
+  C.status = misc + 2;
+  // RK4 weights formed in float like the reference (src/pml_fs_kernels.cu:95-380)
+  const float dt = p.dt;
+  C.rk_c[0] = dt / 2; C.rk_c[1] = dt / 2; C.rk_c[2] = dt; C.rk_c[3] = dt / 6;
+  C.rk_w[0] = dt / 6; C.rk_w[1] = dt / 3; C.rk_w[2] = dt / 3;
+  C.gap = m->gap;
+  C.srcx = m->srcx.empty() ? -1 : m->srcx[0];
+  C.srcz = m->srcx.empty() ? 0 : m->srcz[0];
+  int rc;
+  if ((rc = solid_capacity(m, std::max(p.nt, 1))) != MFDM_OK) return rc;
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  return solid_rewind(m, false);
+}
+
+int solid_open(SolidHost&& h, int device, mfdm_solid** out) {
+  if (!out) return fail(MFDM_ERR_ARG, "null output handle");
+  *out = nullptr;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  mfdm_solid* m = new mfdm_solid();
+  const int rc = solid_build(m, h, device);
+  if (prev >= 0) cudaSetDevice(prev);
+  if (rc != MFDM_OK) {
+    const std::string msg = g_err;
+    solid_destroy(m);
+    g_err = msg;
+    return rc;
+  }
+  *out = m;
+  return MFDM_OK;
+}
+
+int solid_field_ptr(mfdm_solid* m, int field, float** p) {
+  const mfdm::solid::SFields& U = m->S[0];
+  switch (field) {
+    case MFDM_SOLID_VX: *p = U.vx; break;
+    case MFDM_SOLID_VZ: *p = U.vz; break;
+    case MFDM_SOLID_SX: *p = U.sx; break;
+    case MFDM_SOLID_SZ: *p = U.sz; break;
+    case MFDM_SOLID_SXZ: *p = U.sxz; break;
+    default: return fail(MFDM_ERR_ARG, "a solid-only model has only the solid fields");
+  }
+  return MFDM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mfdm_solid_open_json(const char* json_path, int device, mfdm_solid** out) {
+  if (!json_path) return fail(MFDM_ERR_ARG, "null JSON path");
+  SolidHost h;
+  const int rc = load_json_solid(json_path, h);
+  if (rc != MFDM_OK) return rc;
+  return solid_open(std::move(h), device, out);
+}
+
+int mfdm_solid_open_desc(const mfdm_solid_desc* d, int device, mfdm_solid** out) {
+  if (!d) return fail(MFDM_ERR_ARG, "null descriptor");
+  SolidHost h;
+  h.nx = d->nx; h.nz = d->nz;
+  HostModel& p = h.p;
+  p.fpeak = d->fpeak; p.dt = d->dt; p.nt = d->nt; p.snapshot = d->snapshot;
+  p.npd = d->npd; p.npow = d->npow; p.thickness = d->thickness; p.vp_max = d->vp_max;
+  p.rc = d->rc; p.beta0 = d->beta0;
+  for (int i = 0; i < d->nsrc; ++i) {
+    if (!d->src_x || !d->src_z) return fail(MFDM_ERR_ARG, "null source arrays");
+    p.srcx.push_back(d->src_x[i]);
+    p.srcz.push_back(d->src_z[i]);
+  }
+  const float* a[10] = {d->C11, d->C13, d->C33, d->C55, d->rho, d->J, d->xi_x, d->xi_z, d->ze_x, d->ze_z};
+  for (int k = 0; k < 10; ++k) {
+    if (!a[k]) return fail(MFDM_ERR_ARG, "null model array");
+    h.a[k] = a[k];
+  }
+  return solid_open(std::move(h), device, out);
+}
+
+int mfdm_solid_set_shot(mfdm_solid* m, int isrc, int reset_state) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  if (isrc < 0 || (isrc >= int(m->srcx.size()) && !m->srcx.empty()))
+    return fail(MFDM_ERR_ARG, "shot index out of range");
+  DeviceGuard g(m->device);
+  m->isrc = isrc;
+  m->C.srcx = m->srcx.empty() ? -1 : m->srcx[size_t(isrc)];
+  m->C.srcz = m->srcx.empty() ? 0 : m->srcz[size_t(isrc)];
+  solid_release_graph(m);  // the source cell is baked into the kernel arguments
+  return solid_rewind(m, reset_state != 0);
+}
+
+int mfdm_solid_step(mfdm_solid* m, int nsteps) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  if (nsteps < 0) return fail(MFDM_ERR_ARG, "negative step count");
+  DeviceGuard g(m->device);
+  int rc;
+  if ((rc = solid_capacity(m, m->host_step + nsteps)) != MFDM_OK) return rc;
+  if ((rc = solid_enqueue_steps(m, nsteps)) != MFDM_OK) return rc;
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  int st = 0;
+  MFDM_CU(cudaMemcpy(&st, m->C.status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st) return fail(MFDM_ERR_NONFINITE, "non-finite values reached the receiver row");
+  return MFDM_OK;
+}
+
+int mfdm_solid_time_steps(mfdm_solid* m, int nsteps, float* total_ms) {
+  if (!m || !total_ms) return fail(MFDM_ERR_ARG, "null argument");
+  if (nsteps < 0) return fail(MFDM_ERR_ARG, "negative step count");
+  DeviceGuard g(m->device);
+  int rc;
+  if ((rc = solid_capacity(m, m->host_step + nsteps)) != MFDM_OK) return rc;
+  cudaEvent_t e[2] = {};
+  MFDM_CU(cudaEventCreate(&e[0]));
+  struct Free { cudaEvent_t* e; ~Free() { for (int i = 0; i < 2; ++i) if (e[i]) cudaEventDestroy(e[i]); } } fr{e};
+  MFDM_CU(cudaEventCreate(&e[1]));
+  MFDM_CU(cudaEventRecord(e[0], m->stream));
+  if ((rc = solid_enqueue_steps(m, nsteps)) != MFDM_OK) return rc;
+  MFDM_CU(cudaEventRecord(e[1], m->stream));
+  MFDM_CU(cudaEventSynchronize(e[1]));
+  MFDM_CU(cudaEventElapsedTime(total_ms, e[0], e[1]));
+  return MFDM_OK;
+}
+
+int mfdm_solid_get_records(mfdm_solid* m, int first, int count, float* vz) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  const int avail = (m->host_step + m->gap - 1) / m->gap;
+  if (first < 0 || count < 0 || first + count > avail || first + count > m->rec_cap)
+    return fail(MFDM_ERR_ARG, "record range out of bounds");
+  if (count == 0 || !vz) return MFDM_OK;
+  DeviceGuard g(m->device);
+  MFDM_CU(cudaMemcpyAsync(vz, m->d_rec + size_t(first) * m->nx, size_t(count) * m->nx * sizeof(float),
+                          cudaMemcpyDeviceToHost, m->stream));
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  return MFDM_OK;
+}
+
+int mfdm_solid_get_field(mfdm_solid* m, int field, float* host) {
+  if (!m || !host) return fail(MFDM_ERR_ARG, "null argument");
+  float* p = nullptr;
+  int rc = solid_field_ptr(m, field, &p);
+  if (rc != MFDM_OK) return rc;
+  DeviceGuard g(m->device);
+  MFDM_CU(cudaMemcpy2DAsync(host, size_t(m->nx) * sizeof(float), p, size_t(m->P) * sizeof(float),
+                            size_t(m->nx) * sizeof(float), size_t(m->nz), cudaMemcpyDeviceToHost,
+                            m->stream));
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  return MFDM_OK;
+}
+
+int mfdm_solid_get_info(const mfdm_solid* m, int* nx, int* nz, int* gap, int* step) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  if (nx) *nx = m->nx;
+  if (nz) *nz = m->nz;
+  if (gap) *gap = m->gap;
+  if (step) *step = m->host_step;
+  return MFDM_OK;
+}
+
+int mfdm_solid_close(mfdm_solid* m) {
+  solid_destroy(m);
+  return MFDM_OK;
+}
+
+}  // extern "C"
+
 // ---- drop-in command line (src/main.cu:58-339) -------------------------------
 
 namespace {
@@ -1922,11 +2395,62 @@ void print_pml(const HostModel& h) {
               -(h.npow + 1) * double(h.vp_max) * std::log(double(h.rc)) / (2.0 * h.thickness));
 }
 
+// Solid-only runs (calc_type 0): records hold solid vz on row 3 only and the
+// snapshots solid vx, vz (src/main.cu:252-339); shots carry the wavefield over
+// like the fluid-solid path.
+int run_cli_solid(const char* json_path, const fs::path& out_root, int device) {
+  mfdm_solid* m = nullptr;
+  int rc = mfdm_solid_open_json(json_path, device, &m);
+  if (rc != MFDM_OK) return rc;
+  struct Closer { mfdm_solid* m; ~Closer() { mfdm_solid_close(m); } } closer{m};
+  print_pml(m->pml);
+  if ((rc = clear_out_root(out_root)) != MFDM_OK) return rc;
+  const int nx = m->nx, nz = m->nz, nt = m->nt, snap = m->snapshot;
+  std::vector<float> buf(size_t(nx) * nz);
+  for (int isrc = 0; isrc < std::max(1, int(m->srcx.size())); ++isrc) {
+    if (m->srcx.empty()) break;
+    if ((rc = mfdm_solid_set_shot(m, isrc, 0)) != MFDM_OK) return rc;
+    const fs::path dir = out_root / std::to_string(isrc);
+    if ((rc = make_dirs(dir / "snapshot")) != MFDM_OK) return rc;
+    if ((rc = make_dirs(dir / "record")) != MFDM_OK) return rc;
+    int it = 0;
+    while (it < nt) {
+      const int next_snap = ((it + snap - 1) / snap) * snap;
+      const int last = std::min(nt - 1, next_snap);
+      if ((rc = mfdm_solid_step(m, last - it + 1)) != MFDM_OK) return rc;
+      it = last + 1;
+      if (last % snap == 0) {
+        std::printf("finished %0.2f%%\r", 100.0 * last / nt);
+        std::fflush(stdout);
+        const struct { int field; const char* comp; } items[] = {{MFDM_SOLID_VZ, "vz"}, {MFDM_SOLID_VX, "vx"}};
+        for (const auto& item : items) {
+          if ((rc = mfdm_solid_get_field(m, item.field, buf.data())) != MFDM_OK) return rc;
+          const fs::path d = dir / "snapshot" / "solid" / item.comp;
+          if ((rc = make_dirs(d)) != MFDM_OK) return rc;
+          std::ostringstream name;
+          name << item.comp << "_" << std::setw(6) << std::setfill('0') << last << ".bin";
+          if ((rc = write_floats(d / name.str(), buf.data(), buf.size(), false)) != MFDM_OK) return rc;
+        }
+      }
+    }
+    const int ns = (nt + m->gap - 1) / m->gap;
+    std::vector<float> rec(size_t(ns) * nx);
+    if (ns > 0 && (rc = mfdm_solid_get_records(m, 0, ns, rec.data())) != MFDM_OK) return rc;
+    if ((rc = write_floats(dir / "record" / "solid_vz.bin", rec.data(), rec.size(), false)) != MFDM_OK)
+      return rc;
+  }
+  return MFDM_OK;
+}
+
 int run_cli(const char* json_path, const char* out_root_c, int device) {
   const fs::path out_root = out_root_c;
   const std::string s = out_root.string();
   if (s.empty() || s == "/" || s == "." || s == "..")
     return fail(MFDM_ERR_ARG, "Invalid output dir: " + s);
+  int calc_type = 1;
+  int rc0 = json_calc_type(json_path, &calc_type);
+  if (rc0 != MFDM_OK) return rc0;
+  if (calc_type == 0) return run_cli_solid(json_path, out_root, device);
   mfdm_model* m = nullptr;
   int rc = mfdm_open_json(json_path, device, &m);
   if (rc != MFDM_OK) return rc;
