@@ -317,6 +317,25 @@ def adjoint_rate(mfdm, device: int, nsteps: int = 4000, every: int = 50):
                               "adjoint_over_forward": round((kfwd + kbwd) / fwd, 3)}}
 
 
+def solid_only_rate(mfdm, device: int, n: int = 2048, steps: int = 256):
+    """Solid only with a free surface (calc_type 0) on an n x n grid with surface
+    topography: device time of `steps` graph-captured steps, and the whole
+    step's share of the HBM roofline at the solid's algorithmic 464 B per
+    cell-step (16 state + 4 x 9 coefficient floats x 4 B)."""
+    m = modelgen.make_solid_model(n, n, npd=20, fpeak=15.0, dt=5e-4, nt=10, src_x=[n // 2],
+                                  src_z=[20], amp=20.0, wavelength=600.0)
+    with mfdm.SolidSolver.from_model(m, device=device) as s:
+        s.set_shot(0, reset=True)
+        s.step(32)
+        ms = s.time_steps(steps)
+    gcells = m.cells * steps / (ms / 1e3) / 1e9
+    gbs = m.cells * 464 * steps / (ms / 1e3) / 1e9
+    peak, _ = peaks()
+    return {"grid": f"{n}x{n}", "steps": steps, "value": round(gcells, 3), "unit": "Gcell/s",
+            "ms_per_step": round(ms / steps, 4), "achieved_gbs": round(gbs, 1),
+            "frac_of_measured_hbm": round(gbs / peak, 4)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -438,6 +457,7 @@ def main():
         other["batched_1200x800_64_shots"] = batched_rate(mfdm, small, local, args.warmup)
         other["uneven_32_models"] = uneven_rate(mfdm, local)
         other["adjoint_800x400"] = adjoint_rate(mfdm, local)
+        other["solid_only_2048x2048"] = solid_only_rate(mfdm, local)
 
     clocks = clk.summary()
     solver.close()
