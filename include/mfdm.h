@@ -71,6 +71,7 @@ typedef struct mfdm_info {
   long long device_bytes;         /* device memory held by the handle */
   int nshots;                     /* shots stepped together (1 unless opened with mfdm_open_batch) */
   int seg_rows;                   /* rows per segment block of the stage launches */
+  int blocks_per_sm;              /* stage kernel build in use: 2 or 3 resident blocks per SM */
 } mfdm_info;
 
 /* Field ids for mfdm_get_field / mfdm_set_field. */
@@ -184,7 +185,14 @@ int mfdm_batch_get_field(mfdm_model* m, int shot, int field, float* host);
  * (24). Results do not depend on it beyond FP32 rounding of the last bit. */
 int mfdm_set_tile(mfdm_model* m, int seg_rows);
 
-/* Times every candidate segment height on this handle's model and shots
+/* Selects the stage kernel build: 2 resident blocks per SM (deeper TMA rings,
+ * 96 registers) or 3 (shallower rings, 72 registers, more bytes in flight per
+ * SM: faster on large grids, slower on small ones); 0 (default) picks by grid
+ * size (3 from 6 M cells per launch). Results agree to FP32 rounding. */
+int mfdm_set_blocks_per_sm(mfdm_model* m, int blocks);
+
+/* Times every candidate segment height and both stage builds (2 and 3 blocks
+ * per SM) on this handle's model and shots
  * (a few steps each, CUDA events on the handle's stream), keeps the fastest and
  * writes it to *seg_rows (may be NULL). The choice is cached per device, grid
  * shape, PML width, boundary type and shot count, so a second handle of the

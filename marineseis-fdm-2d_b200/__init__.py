@@ -39,7 +39,7 @@ EXPORTS = ("mfdm_last_error", "mfdm_open_json", "mfdm_open_desc", "mfdm_load_des
            "mfdm_adjoint_forward", "mfdm_adjoint_backward", "mfdm_adjoint_set_memory",
            "mfdm_solid_open_json", "mfdm_solid_open_desc", "mfdm_solid_set_shot", "mfdm_solid_step",
            "mfdm_solid_time_steps", "mfdm_solid_get_records", "mfdm_solid_get_field",
-           "mfdm_solid_get_info", "mfdm_solid_close")
+           "mfdm_solid_get_info", "mfdm_solid_close", "mfdm_set_blocks_per_sm")
 
 # Coefficient arrays the adjoint differentiates (mfdm_coef_grad order).
 GRAD_COEFS = ("K", "rcp_rho_f", "C11", "C13", "C33", "C55", "rcp_rho_s")
@@ -74,7 +74,8 @@ class Info(ctypes.Structure):
                 ("gap", ctypes.c_int), ("nsrc", ctypes.c_int), ("shot", ctypes.c_int),
                 ("step", ctypes.c_int), ("nsamples", ctypes.c_int),
                 ("cells", ctypes.c_longlong), ("device_bytes", ctypes.c_longlong),
-                ("nshots", ctypes.c_int), ("seg_rows", ctypes.c_int)]
+                ("nshots", ctypes.c_int), ("seg_rows", ctypes.c_int),
+                ("blocks_per_sm", ctypes.c_int)]
 
 
 class SolidDesc(ctypes.Structure):
@@ -152,6 +153,7 @@ def load_library(path: str = LIB_PATH):
                                                   _fp, _fp, _fp]),
         "mfdm_batch_get_field": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, _fp]),
         "mfdm_set_tile": (ctypes.c_int, [vp, ctypes.c_int]),
+        "mfdm_set_blocks_per_sm": (ctypes.c_int, [vp, ctypes.c_int]),
         "mfdm_autotune": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int)]),
         "mfdm_group_open": (ctypes.c_int, [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]),
         "mfdm_group_step": (ctypes.c_int, [vp, ctypes.c_int]),
@@ -336,6 +338,10 @@ class Solver:
     def set_tile(self, seg_rows: int):
         """Rows per segment block of the stage launches (multiple of 4 in [4, 128]; 0: 24)."""
         _check(self._lib.mfdm_set_tile(self._h, int(seg_rows)))
+
+    def set_blocks_per_sm(self, blocks: int):
+        """Stage kernel build: 2 or 3 resident blocks per SM, 0 by grid size (mfdm_set_blocks_per_sm)."""
+        _check(self._lib.mfdm_set_blocks_per_sm(self._h, int(blocks)))
 
     def autotune(self) -> int:
         """Times the candidate segment heights, keeps the fastest and returns it.

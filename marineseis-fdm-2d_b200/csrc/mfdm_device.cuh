@@ -86,6 +86,7 @@ struct Coef {
   float* ipre;                      // interface rows before the filter [8][P]
   int* status;                      // sticky error word (non-finite detector)
   int seg;                          // rows per segment block of the stage launches (0: 24)
+  int variant;                      // stage kernel build: 2 or 3 blocks per SM (0: by grid size)
   // Shots stepped together (the stage launch's fastest block index, blockIdx.y
   // of the finish kernel). Every per-shot
   // buffer of shot b sits b strides after shot 0's: the RK sets, ADE strips,

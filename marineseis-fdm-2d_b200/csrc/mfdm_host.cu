@@ -921,6 +921,7 @@ int mfdm_get_info(const mfdm_model* m, mfdm_info* info) {
                        (long long)m->nshots * m->rec_cap * 12 * m->cfg.nx;
   info->nshots = m->nshots;
   info->seg_rows = mfdm::stage_seg_rows(m->C);
+  info->blocks_per_sm = mfdm::stage_blocks_per_sm(m->C);
   return MFDM_OK;
 }
 
@@ -1072,12 +1073,15 @@ namespace {
 const int kSegCandidates[] = {8, 12, 16, 24, 32, 48};
 
 std::mutex g_tune_mu;
-std::map<std::vector<int>, int> g_tune;  // (device, nx, nz_f, nz_s, npd, bdy, nshots) -> rows
+// (device, nx, nz_f, nz_s, npd, bdy, nshots) -> (rows, blocks per SM)
+std::map<std::vector<int>, std::pair<int, int>> g_tune;
 
 // Device time of one captured kGraphSteps-step replay with `seg` rows per segment
-// (after one untimed replay that also captures the graph).
-int time_segment_rows(mfdm_model* m, int seg, float* ms) {
+// and the stage build of `variant` blocks per SM (after one untimed replay that
+// also captures the graph).
+int time_segment_rows(mfdm_model* m, int seg, int variant, float* ms) {
   m->C.seg = seg;
+  m->C.variant = variant;
   release_graph(m);
   int rc;
   if ((rc = enqueue_steps(m, kGraphSteps)) != MFDM_OK) return rc;
@@ -1102,36 +1106,49 @@ int mfdm_autotune(mfdm_model* m, int* seg_rows) {
   DeviceGuard g(m->device);
   const HostModel& h = m->cfg;
   const std::vector<int> key = {m->device, h.nx, h.nzf, h.nzs, h.npd, h.bdy, m->nshots};
-  int best = 0;
+  std::pair<int, int> best(0, 0);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune.find(key);
     if (it != g_tune.end()) best = it->second;
   }
   int rc;
-  if (best == 0) {
+  if (best.first == 0) {
     // from rest at step 0, so no state of the caller's is stepped
     if ((rc = clear_state(m)) != MFDM_OK) return rc;
     if ((rc = rewind(m)) != MFDM_OK) return rc;
     const int n = int(sizeof(kSegCandidates) / sizeof(int));
-    if ((rc = ensure_capacity(m, 2 * kGraphSteps * n)) != MFDM_OK) return rc;
+    if ((rc = ensure_capacity(m, 2 * kGraphSteps * n * 2)) != MFDM_OK) return rc;
     float best_ms = 0.f;
-    for (int i = 0; i < n; ++i) {
-      float ms = 0.f;
-      if ((rc = time_segment_rows(m, kSegCandidates[i], &ms)) != MFDM_OK) return rc;
-      if (best == 0 || ms < best_ms) {
-        best = kSegCandidates[i];
-        best_ms = ms;
+    for (int variant = 2; variant <= 3; ++variant)
+      for (int i = 0; i < n; ++i) {
+        float ms = 0.f;
+        if ((rc = time_segment_rows(m, kSegCandidates[i], variant, &ms)) != MFDM_OK) return rc;
+        if (best.first == 0 || ms < best_ms) {
+          best = {kSegCandidates[i], variant};
+          best_ms = ms;
+        }
       }
-    }
     std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[key] = best;
   }
-  m->C.seg = best;
+  m->C.seg = best.first;
+  m->C.variant = best.second;
   release_graph(m);
   if ((rc = clear_state(m)) != MFDM_OK) return rc;
   if ((rc = rewind(m)) != MFDM_OK) return rc;
-  if (seg_rows) *seg_rows = best;
+  if (seg_rows) *seg_rows = best.first;
+  return MFDM_OK;
+}
+
+int mfdm_set_blocks_per_sm(mfdm_model* m, int blocks) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  if (blocks != 0 && blocks != 2 && blocks != 3)
+    return fail(MFDM_ERR_ARG, "blocks per SM must be 2, 3 or 0 (by grid size)");
+  DeviceGuard g(m->device);
+  MFDM_CU(cudaStreamSynchronize(m->stream));
+  m->C.variant = blocks;
+  release_graph(m);
   return MFDM_OK;
 }
 

@@ -36,7 +36,16 @@
 #include "mfdm_device.cuh"
 #include "mfdm_kernels.h"
 
+// This file is compiled twice: as it is (the stage kernels in namespace v2,
+// two blocks per SM, 5 stencil and 3 point-wise ring slots, 96 registers) and
+// by mfdm_kernels_b3.cu (namespace v3, three blocks per SM, 4 + 2 slots, 72
+// registers). The shared kernels and the dispatching launchers are built once.
+#ifndef MFDM_VNS
+#define MFDM_VNS v2
+#endif
+
 namespace mfdm {
+namespace MFDM_VNS {
 
 constexpr int kTX = kStageTX;            // computed columns per strip
 constexpr int kSW = kStageSW;            // staged row width (4-column halo each side)
@@ -47,6 +56,9 @@ constexpr int kR = kStageR;              // rows per chunk
 #ifndef MFDM_PW_SLOTS
 #define MFDM_PW_SLOTS 3
 #endif
+#ifndef MFDM_MIN_BLOCKS
+#define MFDM_MIN_BLOCKS 2  // stage blocks resident per SM (registers: 96 at 2)
+#endif
 constexpr int kNS = MFDM_STENCIL_SLOTS;   // stencil chunk slots
 constexpr int kNP = MFDM_PW_SLOTS;        // point-wise chunk slots
 constexpr int kRing = kR * kNS;          // ring rows
@@ -54,7 +66,6 @@ constexpr int kConsumers = 256;          // warps 0-7
 constexpr int kThreads = kConsumers + 32;  // + producer warp
 constexpr int kSeg = 24;                 // default rows per segment block
 constexpr int kBarBytes = 256;           // full/empty barriers of both rings
-constexpr int kFinishThreads = 256;      // filter / receiver kernel
 
 
 static_assert(kTX * kR == kConsumers, "one cell per consumer thread per chunk");
@@ -525,7 +536,7 @@ __device__ __forceinline__ void interface_strip(const Coef& C, const Fields& in,
 // One RK stage: `s` indexes the Ricker table; cc and w are the stage's RK
 // weights (out = base + cc k, accumulator += w k).
 template <int DIR, int KIND, bool CPML>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, MFDM_MIN_BLOCKS)
     stage_kernel(Coef C0, Fields in0, Fields out0, Fields un0, Fields acc0,
                  const __grid_constant__ StageMaps maps, int s, float cc, float w, int ntx,
                  int nbi, int nbf, int nbs, int seg, int nshots) {
@@ -547,6 +558,105 @@ __global__ void __launch_bounds__(kThreads, 2)
                                    smem);
   }
 }
+
+// ---- host-side launchers of this build's stage kernels ------------------------
+
+template <int KIND>
+static size_t smem_for_kind() {
+  const size_t f = segment_smem<3, PW<3, 6, KIND>::n>(), so = segment_smem<5, PW<5, 9, KIND>::n>();
+  return f > so ? f : so;
+}
+
+size_t smem_bytes() { return smem_for_kind<kStageMid>(); }
+
+static int seg_rows_of(const Coef& C) { return C.seg > 0 ? C.seg : kSeg; }
+
+static void grid_of(int nx, int nzf, int nzs, int seg, int* ntx, int* nbf, int* nbs, int* nbi) {
+  *ntx = (nx + kTX - 1) / kTX;
+  const int frows = nzf - 1 - 3;  // fluid rows 3..nz_f-2
+  const int srows = nzs - 4;      // solid rows 1..nz_s-4
+  *nbf = frows > 0 ? *ntx * ((frows + seg - 1) / seg) : 0;
+  *nbs = srows > 0 ? *ntx * ((srows + seg - 1) / seg) : 0;
+  *nbi = (nx + kConsumers - 1) / kConsumers;
+}
+
+template <int DIR, int KIND, bool CPML>
+static cudaError_t launch_one(const Coef& C, const Fields& in, const Fields& out, const Fields& un,
+                              const Fields& acc, const StageMaps& maps, int s, cudaStream_t st) {
+  int ntx, nbf, nbs, nbi;
+  const int seg = seg_rows_of(C), nshots = C.nshots > 0 ? C.nshots : 1;
+  grid_of(C.nx, C.nzf, C.nzs, seg, &ntx, &nbf, &nbs, &nbi);
+  const float cc = C.rk_c[s], w = (KIND == kStageLast) ? 0.f : C.rk_w[s];
+  const unsigned grid = unsigned(nbi + nbf + nbs) * unsigned(nshots);
+  stage_kernel<DIR, KIND, CPML><<<grid, kThreads, smem_for_kind<KIND>(), st>>>(
+      C, in, out, un, acc, maps, s, cc, w, ntx, nbi, nbf, nbs, seg, nshots);
+  return cudaGetLastError();
+}
+
+template <int DIR, int KIND>
+static cudaError_t configure_one() {
+  cudaError_t e = cudaFuncSetAttribute(stage_kernel<DIR, KIND, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem_for_kind<KIND>());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(stage_kernel<DIR, KIND, true>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_for_kind<KIND>());
+}
+
+cudaError_t configure() {
+  cudaError_t e;
+  if ((e = configure_one<kDirF, kStageFirst>()) != cudaSuccess) return e;
+  if ((e = configure_one<kDirF, kStageMid>()) != cudaSuccess) return e;
+  if ((e = configure_one<kDirF, kStageLast>()) != cudaSuccess) return e;
+  if ((e = configure_one<kDirB, kStageFirst>()) != cudaSuccess) return e;
+  if ((e = configure_one<kDirB, kStageMid>()) != cudaSuccess) return e;
+  return configure_one<kDirB, kStageLast>();
+}
+
+template <bool CPML>
+static cudaError_t launch_stage_bc(const Coef& C, const Fields& in, const Fields& out,
+                                  const Fields& un, const Fields& acc, const StageMaps& maps,
+                                  int stage, int dir, cudaStream_t st) {
+  const int kind = stage == 0 ? kStageFirst : (stage == 3 ? kStageLast : kStageMid);
+  if (dir == kDirF) {
+    if (kind == kStageFirst) return launch_one<kDirF, kStageFirst, CPML>(C, in, out, un, acc, maps, stage, st);
+    if (kind == kStageMid) return launch_one<kDirF, kStageMid, CPML>(C, in, out, un, acc, maps, stage, st);
+    return launch_one<kDirF, kStageLast, CPML>(C, in, out, un, acc, maps, stage, st);
+  }
+  if (kind == kStageFirst) return launch_one<kDirB, kStageFirst, CPML>(C, in, out, un, acc, maps, stage, st);
+  if (kind == kStageMid) return launch_one<kDirB, kStageMid, CPML>(C, in, out, un, acc, maps, stage, st);
+  return launch_one<kDirB, kStageLast, CPML>(C, in, out, un, acc, maps, stage, st);
+}
+
+cudaError_t launch_stage_v(const Coef& C, const Fields& in, const Fields& out, const Fields& un,
+                           const Fields& acc, const StageMaps& maps, int stage, int dir,
+                           cudaStream_t st) {
+  // the four-side CPML variant runs its own kernel instantiations
+  return C.cpml ? launch_stage_bc<true>(C, in, out, un, acc, maps, stage, dir, st)
+                : launch_stage_bc<false>(C, in, out, un, acc, maps, stage, dir, st);
+}
+
+// The stage kernels' constant weights live in this build's own constant bank.
+cudaError_t upload_constants_v(const float* srcw25, const float* w7) {
+  cudaError_t e = cudaMemcpyToSymbol(c_srcw, srcw25, 25 * sizeof(float));
+  if (e != cudaSuccess) return e;
+  return cudaMemcpyToSymbol(c_w7, w7, 7 * sizeof(float));
+}
+
+}  // namespace MFDM_VNS
+
+#ifndef MFDM_VARIANT_TU
+// ---- built once: the finish kernel, small kernels and the dispatching launchers ----
+
+namespace v3 {
+cudaError_t configure();
+cudaError_t launch_stage_v(const Coef& C, const Fields& in, const Fields& out, const Fields& un,
+                           const Fields& acc, const StageMaps& maps, int stage, int dir,
+                           cudaStream_t st);
+cudaError_t upload_constants_v(const float* srcw25, const float* w7);
+}  // namespace v3
+
+constexpr int kFinishThreads = 256;  // filter / receiver kernel
 
 // Post-step interface filter (7-point Gaussian along x, renormalised at the
 // clamped ends) and continuity average (src/pml_fs_kernels.cu:428-525),
@@ -631,82 +741,34 @@ __global__ void set_step_kernel(int* step, unsigned* done, int it) {
   *done = 0u;
 }
 
-// ---- host-side launchers ----------------------------------------------------
+// ---- host-side launchers ------------------------------------------------------
 
+size_t stage_smem_bytes() { return v2::smem_bytes(); }
 
-template <int KIND>
-static size_t smem_for_kind() {
-  const size_t f = segment_smem<3, PW<3, 6, KIND>::n>(), so = segment_smem<5, PW<5, 9, KIND>::n>();
-  return f > so ? f : so;
-}
-
-size_t stage_smem_bytes() { return smem_for_kind<kStageMid>(); }
-
-int stage_seg_rows(const Coef& C) { return C.seg > 0 ? C.seg : kSeg; }
+int stage_seg_rows(const Coef& C) { return C.seg > 0 ? C.seg : v2::kSeg; }
 
 void stage_grid(int nx, int nzf, int nzs, int seg, int* ntx, int* nbf, int* nbs, int* nbi) {
-  *ntx = (nx + kTX - 1) / kTX;
-  const int frows = nzf - 1 - 3;  // fluid rows 3..nz_f-2
-  const int srows = nzs - 4;      // solid rows 1..nz_s-4
-  *nbf = frows > 0 ? *ntx * ((frows + seg - 1) / seg) : 0;
-  *nbs = srows > 0 ? *ntx * ((srows + seg - 1) / seg) : 0;
-  *nbi = (nx + kConsumers - 1) / kConsumers;
+  v2::grid_of(nx, nzf, nzs, seg, ntx, nbf, nbs, nbi);
 }
 
-template <int DIR, int KIND, bool CPML>
-static cudaError_t launch_one(const Coef& C, const Fields& in, const Fields& out, const Fields& un,
-                              const Fields& acc, const StageMaps& maps, int s, cudaStream_t st) {
-  int ntx, nbf, nbs, nbi;
-  const int seg = stage_seg_rows(C), nshots = C.nshots > 0 ? C.nshots : 1;
-  stage_grid(C.nx, C.nzf, C.nzs, seg, &ntx, &nbf, &nbs, &nbi);
-  const float cc = C.rk_c[s], w = (KIND == kStageLast) ? 0.f : C.rk_w[s];
-  const unsigned grid = unsigned(nbi + nbf + nbs) * unsigned(nshots);
-  stage_kernel<DIR, KIND, CPML><<<grid, kThreads, smem_for_kind<KIND>(), st>>>(
-      C, in, out, un, acc, maps, s, cc, w, ntx, nbi, nbf, nbs, seg, nshots);
-  return cudaGetLastError();
-}
-
-template <int DIR, int KIND>
-static cudaError_t configure_one() {
-  cudaError_t e = cudaFuncSetAttribute(stage_kernel<DIR, KIND, false>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem_for_kind<KIND>());
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(stage_kernel<DIR, KIND, true>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_for_kind<KIND>());
+int stage_blocks_per_sm(const Coef& C) {
+  if (C.variant == 2 || C.variant == 3) return C.variant;
+  // large grids stream best with three blocks per SM, small ones fill the GPU
+  // better with two (measured at 4096x2048, 2048x1024 and 1200x800)
+  const long long cells = (long long)C.nx * (C.nzf + C.nzs) * (C.nshots > 0 ? C.nshots : 1);
+  return cells >= 6000000LL ? 3 : 2;
 }
 
 cudaError_t configure_device() {
-  cudaError_t e;
-  if ((e = configure_one<kDirF, kStageFirst>()) != cudaSuccess) return e;
-  if ((e = configure_one<kDirF, kStageMid>()) != cudaSuccess) return e;
-  if ((e = configure_one<kDirF, kStageLast>()) != cudaSuccess) return e;
-  if ((e = configure_one<kDirB, kStageFirst>()) != cudaSuccess) return e;
-  if ((e = configure_one<kDirB, kStageMid>()) != cudaSuccess) return e;
-  return configure_one<kDirB, kStageLast>();
-}
-
-template <bool CPML>
-static cudaError_t launch_stage_bc(const Coef& C, const Fields& in, const Fields& out,
-                                  const Fields& un, const Fields& acc, const StageMaps& maps,
-                                  int stage, int dir, cudaStream_t st) {
-  const int kind = stage == 0 ? kStageFirst : (stage == 3 ? kStageLast : kStageMid);
-  if (dir == kDirF) {
-    if (kind == kStageFirst) return launch_one<kDirF, kStageFirst, CPML>(C, in, out, un, acc, maps, stage, st);
-    if (kind == kStageMid) return launch_one<kDirF, kStageMid, CPML>(C, in, out, un, acc, maps, stage, st);
-    return launch_one<kDirF, kStageLast, CPML>(C, in, out, un, acc, maps, stage, st);
-  }
-  if (kind == kStageFirst) return launch_one<kDirB, kStageFirst, CPML>(C, in, out, un, acc, maps, stage, st);
-  if (kind == kStageMid) return launch_one<kDirB, kStageMid, CPML>(C, in, out, un, acc, maps, stage, st);
-  return launch_one<kDirB, kStageLast, CPML>(C, in, out, un, acc, maps, stage, st);
+  const cudaError_t e = v2::configure();
+  return e != cudaSuccess ? e : v3::configure();
 }
 
 cudaError_t launch_stage(const Coef& C, const Fields& in, const Fields& out, const Fields& un,
                          const Fields& acc, const StageMaps& maps, int stage, int dir,
                          cudaStream_t st) {
-  // the four-side CPML variant runs its own kernel instantiations
-  return C.cpml ? launch_stage_bc<true>(C, in, out, un, acc, maps, stage, dir, st)
-                : launch_stage_bc<false>(C, in, out, un, acc, maps, stage, dir, st);
+  return stage_blocks_per_sm(C) == 3 ? v3::launch_stage_v(C, in, out, un, acc, maps, stage, dir, st)
+                                     : v2::launch_stage_v(C, in, out, un, acc, maps, stage, dir, st);
 }
 
 cudaError_t launch_finish(const Coef& C, const Fields& U, cudaStream_t st) {
@@ -728,8 +790,11 @@ cudaError_t launch_set_step(const Coef& C, int it, cudaStream_t st) {
 
 cudaError_t upload_constants(const float* srcw25, const float* w7) {
   cudaError_t e = cudaMemcpyToSymbol(c_srcw, srcw25, 25 * sizeof(float));
-  if (e != cudaSuccess) return e;
-  return cudaMemcpyToSymbol(c_w7, w7, 7 * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_w7, w7, 7 * sizeof(float));
+  if (e == cudaSuccess) e = v2::upload_constants_v(srcw25, w7);
+  return e != cudaSuccess ? e : v3::upload_constants_v(srcw25, w7);
 }
+
+#endif  // MFDM_VARIANT_TU
 
 }  // namespace mfdm

@@ -23,6 +23,9 @@ cudaError_t launch_reciprocal(float* a, int rows, int nx, int P, cudaStream_t st
 cudaError_t launch_set_step(const Coef& C, int it, cudaStream_t st);
 // Dynamic shared memory of one stage block.
 size_t stage_smem_bytes();
+// Resident stage blocks per SM of the build a launch uses: C.variant (2 or 3),
+// or by grid size when 0 (three from 6 M cells per launch).
+int stage_blocks_per_sm(const Coef& C);
 // Rows per segment block of a stage launch (C.seg, or the default 24 when unset).
 int stage_seg_rows(const Coef& C);
 // Block counts of one stage launch (per shot) with `seg` rows per segment:
