@@ -346,6 +346,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="only the warm-up and timed steps (a short launch list for ncu)")
+    ap.add_argument("--blocks-per-sm", type=int, default=0, choices=[0, 2, 3],
+                    help="stage kernel build (0: picked by grid size, as for any model)")
     ap.add_argument("--adjoint-profile", action="store_true",
                     help="only a short adjoint run on the 800x400 model (16 steps, checkpoint "
                          "every 8, seeded residuals): a launch list of the adjoint kernels for ncu")
@@ -375,6 +377,7 @@ def main():
     mfdm = importlib.import_module("marineseis-fdm-2d_b200")
     mfdm.load_library()
     solver = mfdm.Solver.from_model(model, device=local)
+    solver.set_blocks_per_sm(args.blocks_per_sm)
     solver.set_shot(0, reset=True)
     solver.step(args.warmup)
 
