@@ -155,6 +155,12 @@ struct AdjointState {
   size_t seg_steps = 0;
   float* keep = nullptr;   // stage inputs of the last `nkeep` segments, kept by the forward pass
   size_t keep_floats = 0;
+  // TMA maps of every kept step's four stage-input sets (stencil boxes) and of
+  // its first set as U^n (point-wise boxes): the kept steps run their stages
+  // in place in the keep buffer
+  struct SlotMaps { CUtensorMap fst[4], sst[4], fun, sun; };
+  std::vector<SlotMaps> keep_maps;
+  const float* keep_maps_for = nullptr;
   int nkeep = 0;
   float* res = nullptr;    // residual samples [ns][3][nx]
   size_t res_floats = 0;
@@ -1542,6 +1548,63 @@ double* grad_array(mfdm_model* m, int k) {
   return m->adj->grad + (k < 2 ? size_t(k) * nf : 2 * nf + size_t(k - 2) * ns);
 }
 
+// Encodes the TMA maps of every step slot of the keep buffer (once per buffer).
+int keep_maps(mfdm_model* m, size_t nslots) {
+  AdjointState* a = m->adj;
+  if (a->keep_maps_for == a->keep && a->keep_maps.size() >= nslots) return MFDM_OK;
+  const mfdm::SetLayout& L = a->L;
+  const size_t len = size_t(L.len);
+  const int P = m->P, nzf = m->cfg.nzf, nzs = m->cfg.nzs;
+  a->keep_maps.assign(nslots, AdjointState::SlotMaps{});
+  int rc;
+  for (size_t j = 0; j < nslots; ++j) {
+    AdjointState::SlotMaps& M = a->keep_maps[j];
+    for (int s = 0; s < 4; ++s) {
+      const float* base = a->keep + (j * 4 + size_t(s)) * len;
+      if ((rc = encode_block(&M.fst[s], base + L.off[0], P, nzf, 3, mfdm::kStageSW, true, m->nshots, m->region)) ||
+          (rc = encode_block(&M.sst[s], base + L.off[3], P, nzs, 5, mfdm::kStageSW, true, m->nshots, m->region)))
+        return rc;
+    }
+    const float* y1 = a->keep + j * 4 * len;
+    if ((rc = encode_block(&M.fun, y1 + L.off[0], P, nzf, 3, mfdm::kStageTX, false, m->nshots, m->region)) ||
+        (rc = encode_block(&M.sun, y1 + L.off[3], P, nzs, 5, mfdm::kStageTX, false, m->nshots, m->region)))
+      return rc;
+  }
+  a->keep_maps_for = a->keep;
+  return MFDM_OK;
+}
+
+// One step of a kept segment, run in place in its slot j: stage 0 reads U^n
+// from the slot's first set, stages 0-2 write the next three sets (the stage
+// inputs the backward pass reads), the last stage writes U^{n+1} into the next
+// slot's first set, or into the handle's state U after the run's last step.
+int enqueue_kept_step(mfdm_model* m, int it, size_t j, bool last_of_run, cudaStream_t st) {
+  AdjointState* a = m->adj;
+  const mfdm::SetLayout& L = a->L;
+  const size_t len = size_t(L.len);
+  const int d0 = (it & 1) ? mfdm::kDirB : mfdm::kDirF, d1 = 1 - d0;
+  const int dir[4] = {d0, d1, d0, d1};
+  Fields Y[4];
+  for (int s = 0; s < 4; ++s) Y[s] = fields_at(L, a->keep + (j * 4 + size_t(s)) * len);
+  const Fields next = last_of_run ? m->S[0] : fields_at(L, a->keep + (j + 1) * 4 * len);
+  const AdjointState::SlotMaps& M = a->keep_maps[j];
+  const Fields& Acc = m->S[3];
+  for (int s = 0; s < 4; ++s) {
+    mfdm::StageMaps maps;
+    maps.fin = M.fst[s];
+    maps.sin = M.sst[s];
+    maps.fun = M.fun;
+    maps.sun = M.sun;
+    maps.facc = m->fpw[3];
+    maps.sacc = m->spw[3];
+    maps.fcoef = m->fco;
+    maps.scoef = m->sco;
+    MFDM_CU(mfdm::launch_stage(m->C, Y[s], s < 3 ? Y[s + 1] : next, Y[0], Acc, maps, s, dir[s], st));
+  }
+  MFDM_CU(mfdm::launch_finish(m->C, next, st));
+  return MFDM_OK;
+}
+
 // Transposed step n: lam holds lambda^{n+1} on entry and lambda^n on return;
 // `slot` holds the step's four stage inputs.
 int reverse_step(mfdm_model* m, int n, float* slot) {
@@ -1621,26 +1684,34 @@ int mfdm_adjoint_forward(mfdm_model* m, int nsteps, int ckpt_every) {
     a->keep_floats = 0;
     if ((rc = dalloc(&a->keep, nkeep * seg_floats)) != MFDM_OK) return rc;
     a->keep_floats = nkeep * seg_floats;
+    // cells a stage never writes (frozen rows and columns, ADE cells off the
+    // strips) must read 0, as in the handle's own sets
+    MFDM_CU(cudaMemset(a->keep, 0, nkeep * seg_floats * sizeof(float)));
   }
+  if (nkeep > 0 && (rc = keep_maps(m, nkeep * size_t(ckpt_every))) != MFDM_OK) return rc;
   a->nkeep = int(nkeep);
   a->nsteps = -1;
   if ((rc = clear_state(m)) != MFDM_OK) return rc;
   if ((rc = rewind(m)) != MFDM_OK) return rc;
   if ((rc = ensure_capacity(m, nsteps)) != MFDM_OK) return rc;
   for (size_t k = 0; k < ncp; ++k) {
-    MFDM_CU(cudaMemcpyAsync(a->ckpt + k * len, m->S[0].fvx, len * sizeof(float),
-                            cudaMemcpyDeviceToDevice, m->stream));
     const int todo = std::min(ckpt_every, nsteps - int(k) * ckpt_every);
     if (k + nkeep >= ncp) {
-      float* base = a->keep + (k + nkeep - ncp) * seg_floats;
+      // kept: no checkpoint needed; the stages run in place in the keep buffer
+      const size_t j0 = (k + nkeep - ncp) * size_t(ckpt_every);
+      if (k + nkeep == ncp)  // the first kept step starts from the handle's state
+        MFDM_CU(cudaMemcpyAsync(a->keep + j0 * 4 * len, m->S[0].fvx, len * sizeof(float),
+                                cudaMemcpyDeviceToDevice, m->stream));
       for (int j = 0; j < todo; ++j) {
-        float* slot = base + size_t(j) * 4 * len;
-        float* save[4] = {slot, slot + len, slot + 2 * len, slot + 3 * len};
-        if ((rc = enqueue_step(m, m->host_step, m->stream, nullptr, save)) != MFDM_OK) return rc;
+        const bool last = k + 1 == ncp && j + 1 == todo;
+        if ((rc = enqueue_kept_step(m, m->host_step, j0 + size_t(j), last, m->stream)) != MFDM_OK)
+          return rc;
         ++m->host_step;
       }
-    } else if ((rc = enqueue_steps(m, todo)) != MFDM_OK) {
-      return rc;
+    } else {
+      MFDM_CU(cudaMemcpyAsync(a->ckpt + k * len, m->S[0].fvx, len * sizeof(float),
+                              cudaMemcpyDeviceToDevice, m->stream));
+      if ((rc = enqueue_steps(m, todo)) != MFDM_OK) return rc;
     }
   }
   MFDM_CU(cudaStreamSynchronize(m->stream));

@@ -100,13 +100,18 @@ def test_kept_segments_give_the_same_gradient(lib):
         # bytes of one segment's stage inputs, at least (4 states per step, 25 steps,
         # the 8 main fields; the ADE strips make a set a little larger)
         seg_bytes = 25 * 4 * 4 * 8 * (info["nz_f"] + info["nz_s"]) * info["pitch"]
+        recs = []
         for nb in (0, 2 * seg_bytes, 1 << 40, 0):  # none, one or two, all five, none
             s.adjoint_memory(nb)
-            s.adjoint_forward(NSTEPS, ckpt_every=25)
+            recs.append(s.adjoint_forward(NSTEPS, ckpt_every=25))
             out.append(s.adjoint_backward(res))
     for g in out[1:]:
         for k in g:
             assert np.array_equal(g[k], out[0][k]), k
+    # kept steps run their stages in place in the keep buffer: the same records
+    for r in recs[1:]:
+        for k in r:
+            assert np.array_equal(r[k], recs[0][k]), k
     with lib.Solver.from_model(model) as s:
         with pytest.raises(lib.MfdmError):
             s.adjoint_memory(-1)
