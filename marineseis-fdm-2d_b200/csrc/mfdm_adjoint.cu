@@ -217,7 +217,11 @@ __global__ void k_filter_t_a(const float* lam, SetLayout L, const float2* __rest
 }
 
 // Transposed smoothing: lam at interface cell (f, j) = sum_k w_k tmp[f][j - k].
-__global__ void k_filter_t_b(float* lam, SetLayout L, const float* __restrict__ tmp, W7 w7) {
+// With mu / kb (the step's mu = F^T lam and kb = c M mu, formed elsewhere by the
+// previous step's last transposed stage) the filtered interface cells are
+// written to those too.
+__global__ void k_filter_t_b(float* lam, SetLayout L, const float* __restrict__ tmp, W7 w7,
+                             float* mu, float* kb, const uint8_t* __restrict__ mask, float c) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int nx = L.nx;
   if (j < 3 || j > nx - 4) return;
@@ -229,19 +233,15 @@ __global__ void k_filter_t_b(float* lam, SetLayout L, const float* __restrict__ 
       const int i = j - k;
       if (i >= 3 && i <= nx - 4) s = fmaf(w7.w[k + 3], tmp[f * nx + i], s);
     }
-    lam[iface_index(L, f, j)] = s;
+    const long long q = iface_index(L, f, j);
+    lam[q] = s;
+    if (mu) {
+      mu[q] = s;
+      kb[q] = mask[q] ? c * s : 0.0f;
+    }
   }
 }
 
-__global__ void k_start(const float* __restrict__ lam, float* mu, float* kb,
-                        const uint8_t* __restrict__ mask, long long n, float c) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const float l = lam[i];
-    mu[i] = l;
-    kb[i] = mask[i] ? c * l : 0.0f;
-  }
-}
 
 __global__ void k_drop_count(const long long* __restrict__ rowptr, const int* __restrict__ col,
                              SetLayout L, unsigned long long* count) {
@@ -505,12 +505,14 @@ __device__ __forceinline__ float t_stencil(const SetLayout& L, const float* __re
 
 // One thread per row of L^T: the sparse rest plus, on main-field cells, the
 // transposed interior stencil; then the RK bookkeeping of the reverse stage.
-template <int DIR, int MODE>  // MODE 0: y only; 1: lam += y; 2: lam += M y, kbn; 3: lam += M y
+// MODE 0: y only; 1: lam += y and, with kbn, the start of the next transposed
+// step: mu = lam, kbn = w M lam; 2: lam += M y, kbn = M (w mu + c y); 3: lam += M y
 // `t` holds the CSR part of every row (k_rows_csr; rows without entries keep 0).
+template <int DIR, int MODE>
 __global__ void k_reverse_h(const float* __restrict__ t, const float* __restrict__ qx,
                             const float* __restrict__ qz, SetLayout L, float* y_or_lam,
-                            const uint8_t* __restrict__ mask, float* kbn,
-                            const float* __restrict__ mu, float w, float cw) {
+                            const uint8_t* __restrict__ mask, float* kbn, float* mu, float w,
+                            float cw) {
   const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (j >= L.len) return;
   float y = t[j];
@@ -538,7 +540,16 @@ __global__ void k_reverse_h(const float* __restrict__ t, const float* __restrict
     return;
   }
   const float m = mask[j] ? 1.0f : 0.0f;
-  y_or_lam[j] += MODE == 1 ? y : m * y;
+  if (MODE == 1) {
+    const float l = y_or_lam[j] + y;
+    y_or_lam[j] = l;
+    if (kbn) {
+      mu[j] = l;
+      kbn[j] = mask[j] ? w * l : 0.0f;
+    }
+    return;
+  }
+  y_or_lam[j] += m * y;
   if (MODE == 2) kbn[j] = m * fmaf(cw, y, w * mu[j]);
 }
 
@@ -680,7 +691,7 @@ cudaError_t random_fill(float* x, long long n, unsigned seed, cudaStream_t st) {
 
 template <int DIR, int MODE>
 static cudaError_t hybrid_t(const HybridT& H, const Coef& C, const SetLayout& L, const float* kb,
-                            float* out, const uint8_t* mask, float* kbn, const float* mu, float w,
+                            float* out, const uint8_t* mask, float* kbn, float* mu, float w,
                             float c, bool q_ready, cudaStream_t st) {
   if (!q_ready) {
     const dim3 gq(unsigned((L.nx + 127) / 128), unsigned(L.nzf + L.nzs));
@@ -703,14 +714,14 @@ static cudaError_t hybrid_t(const HybridT& H, const Coef& C, const SetLayout& L,
 template <int MODE>
 static cudaError_t hybrid_dir(const HybridT& H, const Coef& C, const SetLayout& L, int dir,
                               const float* kb, float* out, const uint8_t* mask, float* kbn,
-                              const float* mu, float w, float c, bool q_ready, cudaStream_t st) {
+                              float* mu, float w, float c, bool q_ready, cudaStream_t st) {
   return dir == kDirF ? hybrid_t<kDirF, MODE>(H, C, L, kb, out, mask, kbn, mu, w, c, q_ready, st)
                       : hybrid_t<kDirB, MODE>(H, C, L, kb, out, mask, kbn, mu, w, c, q_ready, st);
 }
 
 cudaError_t reverse_stage(const HybridT& H, const Coef& C, const SetLayout& L, int dir,
                           const float* kb, float* lam, const uint8_t* mask, bool mask_lam,
-                          float* kbn, const float* mu, float w, float c, bool q_ready,
+                          float* kbn, float* mu, float w, float c, bool q_ready,
                           cudaStream_t st) {
   if (!mask_lam) return hybrid_dir<1>(H, C, L, dir, kb, lam, mask, kbn, mu, w, c, q_ready, st);
   if (kbn) return hybrid_dir<2>(H, C, L, dir, kb, lam, mask, kbn, mu, w, c, q_ready, st);
@@ -730,22 +741,18 @@ cudaError_t inject(float* lam, const SetLayout& L, const float* res, cudaStream_
   return cudaGetLastError();
 }
 
-cudaError_t filter_t(float* lam, const SetLayout& L, const Coef& C, float* tmp, cudaStream_t st) {
+cudaError_t filter_t(float* lam, const SetLayout& L, const Coef& C, float* tmp, cudaStream_t st,
+                     float* mu, float* kb, const uint8_t* mask, float c) {
   // the filter taps (src/elements.cu:30-33), as the forward finish kernel uses them
   const W7 w7{{1.1e-13f, 1.678e-06f, 0.03419f, 0.93163f, 0.03419f, 1.678e-06f, 1.1e-13f}};
   const unsigned g = unsigned((L.nx + kBlock - 1) / kBlock);
   k_filter_t_a<<<g, kBlock, 0, st>>>(lam, L, C.nrm, tmp, w7);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_filter_t_b<<<g, kBlock, 0, st>>>(lam, L, tmp, w7);
+  k_filter_t_b<<<g, kBlock, 0, st>>>(lam, L, tmp, w7, mu, kb, mask, c);
   return cudaGetLastError();
 }
 
-cudaError_t start(const float* lam, float* mu, float* kb, const uint8_t* mask, long long n, float c,
-                  cudaStream_t st) {
-  k_start<<<grid_for(n, kBlock), kBlock, 0, st>>>(lam, mu, kb, mask, n, c);
-  return cudaGetLastError();
-}
 
 template <int DIR, bool CPML>
 static cudaError_t gradient_t(const Coef& C, const SetLayout& L, const Fields& Y, const Fields& KB,

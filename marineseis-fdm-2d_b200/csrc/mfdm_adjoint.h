@@ -98,11 +98,12 @@ cudaError_t drop_interior(const CsrT& full, const SetLayout& L, CsrT* rest,
                           unsigned long long* count, void** tmp, size_t* tmp_bytes, cudaStream_t st);
 
 // One reverse stage: y = L^T kb, lam += (mask_lam ? M : 1) y and, when kbn is
-// given, kbn = M (w mu + c y).
+// given, kbn = M (w mu + c y); without mask_lam (the step's last stage) and
+// with kbn, it also starts the next transposed step: mu = lam, kbn = w M lam.
 // q_ready: the Q fields of kb are already in H (written by gradient()).
 cudaError_t reverse_stage(const HybridT& H, const Coef& C, const SetLayout& L, int dir,
                           const float* kb, float* lam, const uint8_t* mask, bool mask_lam,
-                          float* kbn, const float* mu, float w, float c, bool q_ready,
+                          float* kbn, float* mu, float w, float c, bool q_ready,
                           cudaStream_t st);
 // Lists the rows of H->rest that have entries and allocates H->t (zeroed);
 // flag (len + 1) and tmp are scratch.
@@ -117,11 +118,12 @@ cudaError_t apply_t(const HybridT& H, const Coef& C, const SetLayout& L, int dir
 // Adds one receiver sample's residuals (svx, svz, fp rows of nx) to lam.
 cudaError_t inject(float* lam, const SetLayout& L, const float* res, cudaStream_t st);
 // lam <- F^T lam on the interface rows (the transposed post-step filter);
-// tmp holds 8 * nx floats.
-cudaError_t filter_t(float* lam, const SetLayout& L, const Coef& C, float* tmp, cudaStream_t st);
-// mu = lam, kb = c M lam.
-cudaError_t start(const float* lam, float* mu, float* kb, const uint8_t* mask, long long n, float c,
-                  cudaStream_t st);
+// tmp holds 8 * nx floats. With mu and kb the filtered cells also get
+// mu = lam and kb = c M lam (the rest of both was formed by the previous
+// transposed step).
+cudaError_t filter_t(float* lam, const SetLayout& L, const Coef& C, float* tmp, cudaStream_t st,
+                     float* mu = nullptr, float* kb = nullptr, const uint8_t* mask = nullptr,
+                     float c = 0.f);
 
 // Material gradients of one stage: g[m][cell] += kb . dL_dir/dm (Y) over the
 // cell's main fields (and the coupled interface column); Y is a set, kb a

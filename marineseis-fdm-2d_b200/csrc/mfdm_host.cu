@@ -1621,8 +1621,9 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
   const float *c = C.rk_c, *w = C.rk_w;
   if (n % m->gap == 0)
     MFDM_CU(mfdm::adj::inject(a->lam, L, a->res + size_t(n / m->gap) * 3 * m->cfg.nx, st));
-  MFDM_CU(mfdm::adj::filter_t(a->lam, L, C, a->tmp, st));
-  MFDM_CU(mfdm::adj::start(a->lam, a->mu, a->kb[0], a->mask, len, c[3], st));
+  // mu = F^T lam and kb = c3 M mu: off the interface rows both were formed by
+  // the previous transposed step's last stage (zero before the first)
+  MFDM_CU(mfdm::adj::filter_t(a->lam, L, C, a->tmp, st, a->mu, a->kb[0], a->mask, c[3]));
   // each stage: gradient (which also forms the Q fields of kb), then L^T kb
   MFDM_CU(mfdm::adj::gradient(C, L, Y[3], a->kb[0], g, d1, &a->H[d1], st));
   MFDM_CU(mfdm::adj::reverse_stage(a->H[d1], C, L, d1, a->kb[0], a->lam, a->mask, true, a->kb[1], a->mu, w[2], c[2], true, st));
@@ -1631,7 +1632,7 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
   MFDM_CU(mfdm::adj::gradient(C, L, Y[1], a->kb[0], g, d1, &a->H[d1], st));
   MFDM_CU(mfdm::adj::reverse_stage(a->H[d1], C, L, d1, a->kb[0], a->lam, a->mask, true, a->kb[1], a->mu, w[0], c[0], true, st));
   MFDM_CU(mfdm::adj::gradient(C, L, Y[0], a->kb[1], g, d0, &a->H[d0], st));
-  MFDM_CU(mfdm::adj::reverse_stage(a->H[d0], C, L, d0, a->kb[1], a->lam, a->mask, false, nullptr, a->mu, 0.f, 0.f, true, st));
+  MFDM_CU(mfdm::adj::reverse_stage(a->H[d0], C, L, d0, a->kb[1], a->lam, a->mask, false, a->kb[0], a->mu, c[3], 0.f, true, st));
   return MFDM_OK;
 }
 
@@ -1761,6 +1762,8 @@ int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_
   const size_t gbytes = (size_t(2) * m->cfg.nzf * m->P + size_t(5) * m->cfg.nzs * m->P) * sizeof(double);
   MFDM_CU(cudaMemsetAsync(a->grad, 0, gbytes, st));
   MFDM_CU(cudaMemsetAsync(a->lam, 0, len * sizeof(float), st));
+  MFDM_CU(cudaMemsetAsync(a->mu, 0, len * sizeof(float), st));
+  MFDM_CU(cudaMemsetAsync(a->kb[0], 0, len * sizeof(float), st));
   a->nsteps = -1;
   for (int k = ncp - 1; k >= 0; --k) {
     const int t0 = k * every, t1 = std::min(nsteps, t0 + every);
