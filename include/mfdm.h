@@ -244,6 +244,16 @@ typedef struct mfdm_coef_grad {
  * in about 85 GB. Takes effect with the next mfdm_adjoint_forward. */
 int mfdm_adjoint_set_memory(mfdm_model* m, long long bytes);
 
+/* A second checkpoint level for runs whose segments do not fit: with
+ * inner_every > 0 (and below ckpt_every) the backward pass re-runs each
+ * recomputed segment once keeping a state every inner_every steps, then
+ * recomputes and reverses one inner stretch at a time, so it holds
+ * ceil(ckpt_every / inner_every) + 4 * inner_every states instead of
+ * 4 * ckpt_every, for one more forward pass. 0 (the default): one level.
+ * For example 8000 steps of an 8192x4096 model (about 1.1 GB per state) fit
+ * in roughly 110 GB with ckpt_every 200 and inner_every 5. */
+int mfdm_adjoint_set_inner(mfdm_model* m, int inner_every);
+
 /* Runs `nsteps` steps of the current shot from rest, storing the state every
  * `ckpt_every` steps (ceil(nsteps / ckpt_every) state copies on the device).
  * The records are read with mfdm_get_records as after mfdm_step. The first

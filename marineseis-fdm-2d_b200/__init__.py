@@ -39,7 +39,8 @@ EXPORTS = ("mfdm_last_error", "mfdm_open_json", "mfdm_open_desc", "mfdm_load_des
            "mfdm_adjoint_forward", "mfdm_adjoint_backward", "mfdm_adjoint_set_memory",
            "mfdm_solid_open_json", "mfdm_solid_open_desc", "mfdm_solid_set_shot", "mfdm_solid_step",
            "mfdm_solid_time_steps", "mfdm_solid_get_records", "mfdm_solid_get_field",
-           "mfdm_solid_get_info", "mfdm_solid_close", "mfdm_set_blocks_per_sm")
+           "mfdm_solid_get_info", "mfdm_solid_close", "mfdm_set_blocks_per_sm",
+           "mfdm_adjoint_set_inner")
 
 # Coefficient arrays the adjoint differentiates (mfdm_coef_grad order).
 GRAD_COEFS = ("K", "rcp_rho_f", "C11", "C13", "C33", "C55", "rcp_rho_s")
@@ -161,6 +162,7 @@ def load_library(path: str = LIB_PATH):
         "mfdm_group_close": (ctypes.c_int, [vp]),
         "mfdm_adjoint_forward": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int]),
         "mfdm_adjoint_set_memory": (ctypes.c_int, [vp, ctypes.c_longlong]),
+        "mfdm_adjoint_set_inner": (ctypes.c_int, [vp, ctypes.c_int]),
         "mfdm_solid_open_json": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(vp)]),
         "mfdm_solid_open_desc": (ctypes.c_int, [ctypes.POINTER(SolidDesc), ctypes.c_int,
                                                 ctypes.POINTER(vp)]),
@@ -302,6 +304,10 @@ class Solver:
         """Device memory the adjoint may use to keep whole checkpoint segments'
         stage inputs from the forward pass (mfdm_adjoint_set_memory; 0: recompute all)."""
         _check(self._lib.mfdm_adjoint_set_memory(self._h, int(nbytes)))
+
+    def adjoint_inner(self, inner_every: int):
+        """Second checkpoint level of the backward pass (mfdm_adjoint_set_inner; 0: one level)."""
+        _check(self._lib.mfdm_adjoint_set_inner(self._h, int(inner_every)))
 
     def adjoint_forward(self, nsteps: int, ckpt_every: int = 50) -> Dict[str, np.ndarray]:
         """Runs the current shot from rest with checkpoints (mfdm_adjoint_forward)

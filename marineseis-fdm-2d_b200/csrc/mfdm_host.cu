@@ -137,6 +137,7 @@ struct mfdm_model {
   float* scoef = nullptr;  // [9][nz_s][P]: xi_x, xi_z, ze_x, ze_z, rho, C11, C13, C33, C55
   AdjointState* adj = nullptr;  // adjoint operators and buffers (mfdm_adjoint_*)
   long long adj_keep_budget = 0;  // mfdm_adjoint_set_memory
+  int adj_inner = 0;              // mfdm_adjoint_set_inner: second checkpoint level (0: none)
 };
 
 // Device buffers of the adjoint (one plain handle): the transposed stage
@@ -163,6 +164,8 @@ struct AdjointState {
   const float* keep_maps_for = nullptr;
   int nkeep = 0;
   float* res = nullptr;    // residual samples [ns][3][nx]
+  float* inner = nullptr;  // second-level checkpoints of one segment
+  size_t inner_sets = 0;
   size_t res_floats = 0;
   void* scan_tmp = nullptr;
   size_t scan_bytes = 0;
@@ -181,6 +184,7 @@ struct AdjointState {
     cudaFree(H[0].qz);
     cudaFree(mask); cudaFree(lam); cudaFree(mu); cudaFree(kb[0]); cudaFree(kb[1]);
     cudaFree(tmp); cudaFree(grad); cudaFree(ckpt); cudaFree(seg); cudaFree(res); cudaFree(keep);
+    cudaFree(inner);
     cudaFree(scan_tmp);
   }
 };
@@ -1658,6 +1662,13 @@ int mfdm_adjoint_set_memory(mfdm_model* m, long long bytes) {
   return MFDM_OK;
 }
 
+int mfdm_adjoint_set_inner(mfdm_model* m, int inner_every) {
+  if (!m) return fail(MFDM_ERR_ARG, "null handle");
+  if (inner_every < 0) return fail(MFDM_ERR_ARG, "negative inner checkpoint interval");
+  m->adj_inner = inner_every;
+  return MFDM_OK;
+}
+
 int mfdm_adjoint_forward(mfdm_model* m, int nsteps, int ckpt_every) {
   if (!m) return fail(MFDM_ERR_ARG, "null handle");
   if (nsteps < 1 || ckpt_every < 1) return fail(MFDM_ERR_ARG, "need nsteps >= 1 and ckpt_every >= 1");
@@ -1751,12 +1762,23 @@ int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_
     MFDM_CU(cudaMemcpy(a->res, h.data(), rf * sizeof(float), cudaMemcpyHostToDevice));
   }
   const int ncp = ncp_of(nsteps, every);
-  if (a->nkeep < ncp && size_t(every) > a->seg_steps) {
+  // second level: a recomputed segment first re-runs keeping a state every
+  // `inner` steps, then recomputes and reverses one inner stretch at a time
+  const int inner = (m->adj_inner > 0 && m->adj_inner < every) ? m->adj_inner : every;
+  const size_t ninner = size_t((every + inner - 1) / inner);
+  if (a->nkeep < ncp && size_t(inner) > a->seg_steps) {
     cudaFree(a->seg);
     a->seg = nullptr;
     a->seg_steps = 0;
-    if ((rc = dalloc(&a->seg, size_t(every) * 4 * len)) != MFDM_OK) return rc;
-    a->seg_steps = size_t(every);
+    if ((rc = dalloc(&a->seg, size_t(inner) * 4 * len)) != MFDM_OK) return rc;
+    a->seg_steps = size_t(inner);
+  }
+  if (a->nkeep < ncp && inner < every && ninner > a->inner_sets) {
+    cudaFree(a->inner);
+    a->inner = nullptr;
+    a->inner_sets = 0;
+    if ((rc = dalloc(&a->inner, ninner * len)) != MFDM_OK) return rc;
+    a->inner_sets = ninner;
   }
   cudaStream_t st = m->stream;
   const size_t gbytes = (size_t(2) * m->cfg.nzf * m->P + size_t(5) * m->cfg.nzs * m->P) * sizeof(double);
@@ -1767,23 +1789,41 @@ int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_
   a->nsteps = -1;
   for (int k = ncp - 1; k >= 0; --k) {
     const int t0 = k * every, t1 = std::min(nsteps, t0 + every);
-    float* base = a->seg;
     if (k + a->nkeep >= ncp) {
       // kept by the forward pass
-      base = a->keep + size_t(k + a->nkeep - ncp) * size_t(every) * 4 * len;
-    } else {
-      // recompute the segment from its checkpoint, keeping every stage input
-      MFDM_CU(cudaMemcpyAsync(m->S[0].fvx, a->ckpt + size_t(k) * len, len * sizeof(float),
-                              cudaMemcpyDeviceToDevice, st));
+      float* base = a->keep + size_t(k + a->nkeep - ncp) * size_t(every) * 4 * len;
+      for (int n = t1 - 1; n >= t0; --n)
+        if ((rc = reverse_step(m, n, base + size_t(n - t0) * 4 * len)) != MFDM_OK) return rc;
+      continue;
+    }
+    MFDM_CU(cudaMemcpyAsync(m->S[0].fvx, a->ckpt + size_t(k) * len, len * sizeof(float),
+                            cudaMemcpyDeviceToDevice, st));
+    if (inner < every) {
+      // re-run the segment keeping a state every `inner` steps
       MFDM_CU(mfdm::launch_set_step(m->C, t0, st));
-      for (int n = t0; n < t1; ++n) {
-        float* slot = a->seg + size_t(n - t0) * 4 * len;
+      m->host_step = t0;
+      for (int i = 0; t0 + i * inner < t1; ++i) {
+        MFDM_CU(cudaMemcpyAsync(a->inner + size_t(i) * len, m->S[0].fvx, len * sizeof(float),
+                                cudaMemcpyDeviceToDevice, st));
+        const int todo = std::min(inner, t1 - (t0 + i * inner));
+        if (t0 + (i + 1) * inner < t1 && (rc = enqueue_steps(m, todo)) != MFDM_OK) return rc;
+      }
+    }
+    for (int i = (t1 - t0 - 1) / inner; i >= 0; --i) {
+      const int u0 = t0 + i * inner, u1 = std::min(t1, u0 + inner);
+      if (inner < every)
+        MFDM_CU(cudaMemcpyAsync(m->S[0].fvx, a->inner + size_t(i) * len, len * sizeof(float),
+                                cudaMemcpyDeviceToDevice, st));
+      // recompute the stretch, keeping every stage input
+      MFDM_CU(mfdm::launch_set_step(m->C, u0, st));
+      for (int n = u0; n < u1; ++n) {
+        float* slot = a->seg + size_t(n - u0) * 4 * len;
         float* save[4] = {slot, slot + len, slot + 2 * len, slot + 3 * len};
         if ((rc = enqueue_step(m, n, st, nullptr, save)) != MFDM_OK) return rc;
       }
+      for (int n = u1 - 1; n >= u0; --n)
+        if ((rc = reverse_step(m, n, a->seg + size_t(n - u0) * 4 * len)) != MFDM_OK) return rc;
     }
-    for (int n = t1 - 1; n >= t0; --n)
-      if ((rc = reverse_step(m, n, base + size_t(n - t0) * 4 * len)) != MFDM_OK) return rc;
   }
   MFDM_CU(cudaStreamSynchronize(st));
   if (out) {

@@ -117,6 +117,27 @@ def test_kept_segments_give_the_same_gradient(lib):
             s.adjoint_memory(-1)
 
 
+def test_two_checkpoint_levels_give_the_same_gradient(lib):
+    """Inner checkpoints re-run each segment once more; the stage inputs are the
+    same values, so the gradient is the same bit for bit."""
+    model = tiny_model()
+    rng = np.random.default_rng(12)
+    out = []
+    with lib.Solver.from_model(model) as s:
+        s.set_shot(0, reset=True)
+        ns = -(-NSTEPS // s.info()["gap"])
+        res = {k: rng.standard_normal((ns, model.nx)).astype(np.float32) for k in ("svx", "svz", "fp")}
+        for inner in (0, 7, 1, 0):
+            s.adjoint_inner(inner)
+            s.adjoint_forward(NSTEPS, ckpt_every=40)
+            out.append(s.adjoint_backward(res))
+        with pytest.raises(lib.MfdmError):
+            s.adjoint_inner(-1)
+    for g in out[1:]:
+        for k in g:
+            assert np.array_equal(g[k], out[0][k]), k
+
+
 def test_gradient_matches_finite_differences(lib):
     model = tiny_model()
     p = grads.params_of(model)
