@@ -355,8 +355,24 @@ def main():
     ap.add_argument("--adjoint-profile", action="store_true",
                     help="only a short adjoint run on the 800x400 model (16 steps, checkpoint "
                          "every 8, seeded residuals): a launch list of the adjoint kernels for ncu")
+    ap.add_argument("--solid-profile", type=int, default=0, metavar="N",
+                    help="only a short solid-only run on an N x N model (3 + 8 steps): a launch "
+                         "list of the solid-only kernels for ncu")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+
+    if args.solid_profile:
+        mfdm = importlib.import_module("marineseis-fdm-2d_b200")
+        mfdm.load_library()
+        n = args.solid_profile
+        m = modelgen.make_solid_model(n, n, npd=20, fpeak=15.0, dt=5e-4, nt=10, src_x=[n // 2],
+                                      src_z=[20], amp=20.0, wavelength=600.0)
+        with mfdm.SolidSolver.from_model(m) as s:
+            s.set_shot(0, reset=True)
+            s.step(3)
+            ms = s.time_steps(8)
+        print(json.dumps({"solid_profile_run": True, "grid": f"{n}x{n}", "ms_per_step": ms / 8}))
+        return
 
     if args.adjoint_profile:
         mfdm = importlib.import_module("marineseis-fdm-2d_b200")

@@ -2102,13 +2102,18 @@ int solid_build(mfdm_solid* m, const SolidHost& h, int device) {
   }
   mfdm::solid::SCoef& C = m->C;
   C.nx = nx; C.nz = nz; C.P = P; C.Ps = Ps; C.npd = npd;
+  // the density slot holds 1/rho (FP64 reciprocal rounded once): the momentum
+  // right-hand side multiplies instead of dividing
+  std::vector<float> rcp_rho(size_t(nx) * nz);
+  for (size_t k = 0; k < rcp_rho.size(); ++k) rcp_rho[k] = float(1.0 / double(h.a[4][k]));
   const float* arr[10];
   for (int k = 0; k < 10; ++k) {
     arr[k] = F(o_arr[k]);
-    MFDM_CU(cudaMemcpy2DAsync(F(o_arr[k]), size_t(P) * sizeof(float), h.a[k], size_t(nx) * sizeof(float),
-                              size_t(nx) * sizeof(float), size_t(nz), cudaMemcpyHostToDevice, m->stream));
+    MFDM_CU(cudaMemcpy2DAsync(F(o_arr[k]), size_t(P) * sizeof(float), k == 4 ? rcp_rho.data() : h.a[k],
+                              size_t(nx) * sizeof(float), size_t(nx) * sizeof(float), size_t(nz),
+                              cudaMemcpyHostToDevice, m->stream));
   }
-  C.C11 = arr[0]; C.C13 = arr[1]; C.C33 = arr[2]; C.C55 = arr[3]; C.rho = arr[4];
+  C.C11 = arr[0]; C.C13 = arr[1]; C.C33 = arr[2]; C.C55 = arr[3]; C.rcp_rho = arr[4];
   C.J = arr[5]; C.xix = arr[6]; C.xiz = arr[7]; C.zex = arr[8]; C.zez = arr[9];
   // ALM coefficients of the free-surface row, in double from the model's floats
   // (src/elements.cu:907-977)

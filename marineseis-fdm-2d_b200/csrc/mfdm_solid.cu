@@ -7,8 +7,11 @@
 // build_ghost_flux launch), the explosive source and the fused RK4 update
 // (the reference's vector_add / vector_self_add launches over full grids).
 // A fifth launch per step samples the receiver row and advances the device
-// step counter. Reads go through the read-only cache: at the sizes of
-// solid-only runs a cell's 5x5 neighbourhood is served from L1/L2.
+// step counter. Each block stages the five stage-input fields of its 32x24
+// cells and their 3-cell halo in shared memory with independent float4 loads
+// (all in flight at once), then every thread computes three rows from shared
+// memory; coefficients, ADE memory and the RK operands are point-wise global
+// reads.
 #include "mfdm_device.cuh"
 #include "mfdm_solid.h"
 
@@ -17,6 +20,14 @@ namespace solid {
 namespace {
 
 constexpr int kBX = 32, kBY = 8;
+#ifndef MFDM_SOLID_ROWS
+#define MFDM_SOLID_ROWS 24
+#endif
+constexpr int kTZ = MFDM_SOLID_ROWS;  // rows per block (kTZ / kBY per thread)
+static_assert(kTZ % kBY == 0 && 5 * (kTZ + 6) * (kBX + 8) * 4 <= 48 * 1024, "tile rows");
+constexpr int kHW = kBX + 8;     // tile row: columns c0 .. c0 + 39, c0 = first cell - 3
+constexpr int kHH = kTZ + 6;     // tile rows: r0 .. r0 + kTZ + 5, r0 = first row - 3
+enum { kVX = 0, kVZ, kSX, kSZ, kSXZ };
 
 struct SrcW { float w[25]; };
 
@@ -26,46 +37,49 @@ struct Out {
 };
 
 // Right-hand side of cell (iz, ix), 3 <= iz <= nz-4 (include/pml_fs_kernels.cuh:10-307).
-template <int DIR>
-__device__ __forceinline__ Out rhs(const SCoef& C, const SFields& S, int iz, int ix) {
+// `A(q, dz, dx)` returns stage-input field q (kVX..kSXZ) dz rows and dx columns
+// away, |dz|, |dx| <= 3; the ADE memory of S is read from global memory.
+// IN: the caller guarantees a cell at least three rows below the free surface
+// and outside every absorbing strip (the branch-free body of interior blocks).
+template <int DIR, bool IN, class Acc>
+__device__ __forceinline__ Out rhs(const SCoef& C, const SFields& S, const Acc& A, int iz, int ix) {
   Out o;
   const int P = C.P, nx = C.nx, nz = C.nz, npd = C.npd;
   const size_t i = (size_t)iz * P + ix;
-  const int dist = iz - 3, distx = min(ix - 3, nx - 4 - ix);
-  const bool side = distx < npd, bottom = iz >= nz - 3 - npd;
+  const int dist = IN ? 3 : iz - 3, distx = min(ix - 3, nx - 4 - ix);
+  const bool side = !IN && distx < npd, bottom = !IN && iz >= nz - 3 - npd;
   const int scol = side ? xstrip_col(ix, nx, npd) : 0;
   const size_t si = (size_t)iz * C.Ps + scol, zi = (size_t)(iz - (nz - 3 - npd)) * P + ix;
   const float xix = __ldg(C.xix + i), xiz = __ldg(C.xiz + i), zex = __ldg(C.zex + i),
               zez = __ldg(C.zez + i);
   const float gxixi = xix * xix + xiz * xiz, gzeze = zex * zex + zez * zez;
   const float gxize = xix * zex + xiz * zez;
-  auto at = [&](const float* f, int dz, int dx) { return __ldg(f + i + (ptrdiff_t)dz * P + dx); };
-  auto dx5 = [&](const float* f) {
-    return d5<DIR>(at(f, 0, -3), at(f, 0, -2), at(f, 0, -1), at(f, 0, 0), at(f, 0, 1), at(f, 0, 2),
-                   at(f, 0, 3));
+  auto dx5 = [&](int q) {
+    return d5<DIR>(A(q, 0, -3), A(q, 0, -2), A(q, 0, -1), A(q, 0, 0), A(q, 0, 1), A(q, 0, 2),
+                   A(q, 0, 3));
   };
-  auto dzn = [&](const float* f, int d) {
-    auto col = [&](int j) { return at(f, j, 0); };
+  auto dzn = [&](int q, int d) {
+    auto col = [&](int j) { return A(q, j, 0); };
     return dz_near<DIR>(col, d, true);
   };
   o.XV0 = o.XV1 = o.XE0 = o.XE1 = o.ZV0 = o.ZV1 = o.ZE0 = o.ZE1 = 0.f;
 
   // ---- momentum: rho dv/dt = div sigma ----
   {
-    float rvx, rvz, dxx, dxz, dzx = 0.f, dzz = 0.f;
-    if (dist < 3) {
+    float rvx, rvz, dxx = 0.f, dxz = 0.f, dzx = 0.f, dzz = 0.f;
+    if (!IN && dist < 3) {
       // conservative rows under the free surface; above it the image G = -F of
       // the rows below (src/pml_fs_kernels.cu:7-19)
       auto Fs = [&](int r) -> float2 {
         const size_t k = (size_t)r * P + ix;
         const float Jk = __ldg(C.J + k), ax = __ldg(C.zex + k), az = __ldg(C.zez + k);
-        const float sx = __ldg(S.sx + k), sz = __ldg(S.sz + k), sxz = __ldg(S.sxz + k);
+        const float sx = A(kSX, r - iz, 0), sz = A(kSZ, r - iz, 0), sxz = A(kSXZ, r - iz, 0);
         return make_float2(Jk * (ax * sx + az * sxz), Jk * (ax * sxz + az * sz));
       };
       auto Fxi = [&](int j) -> float2 {
         const size_t k = i + j;
         const float Jk = __ldg(C.J + k), ax = __ldg(C.xix + k), az = __ldg(C.xiz + k);
-        const float sx = __ldg(S.sx + k), sz = __ldg(S.sz + k), sxz = __ldg(S.sxz + k);
+        const float sx = A(kSX, 0, j), sz = A(kSZ, 0, j), sxz = A(kSXZ, 0, j);
         return make_float2(Jk * (ax * sx + az * sxz), Jk * (ax * sxz + az * sz));
       };
       auto Fze = [&](int j) -> float2 {
@@ -78,46 +92,48 @@ __device__ __forceinline__ Out rhs(const SCoef& C, const SFields& S, int iz, int
       const float Jc = __ldg(C.J + i);
       rvx = (a.x + b.x) / Jc;
       rvz = (a.y + b.y) / Jc;
-      const float dxsx = dx5(S.sx), dxsz = dx5(S.sz), dxsxz = dx5(S.sxz);
-      const float dzsx = dzn(S.sx, dist), dzsz = dzn(S.sz, dist), dzsxz = dzn(S.sxz, dist);
+      const float dxsx = dx5(kSX), dxsz = dx5(kSZ), dxsxz = dx5(kSXZ);
+      const float dzsx = dzn(kSX, dist), dzsz = dzn(kSZ, dist), dzsxz = dzn(kSXZ, dist);
       dxx = xix * (dxsx + gxize / gxixi * dzsx) + xiz * (dxsxz + gxize / gxixi * dzsxz);
       dxz = xix * (dxsxz + gxize / gxixi * dzsxz) + xiz * (dxsz + gxize / gxixi * dzsz);
     } else {
-      const float sxdx = dx5(S.sx), sxdz = dzn(S.sx, 3), szdx = dx5(S.sz), szdz = dzn(S.sz, 3);
-      const float tdx = dx5(S.sxz), tdz = dzn(S.sxz, 3);
+      const float sxdx = dx5(kSX), sxdz = dzn(kSX, 3), szdx = dx5(kSZ), szdz = dzn(kSZ, 3);
+      const float tdx = dx5(kSXZ), tdz = dzn(kSXZ, 3);
       rvx = xix * sxdx + zex * sxdz + xiz * tdx + zez * tdz;
       rvz = xix * tdx + zex * tdz + xiz * szdx + zez * szdz;
-      dxx = xix * (sxdx + gxize / gxixi * sxdz) + xiz * (tdx + gxize / gxixi * tdz);
-      dxz = xix * (tdx + gxize / gxixi * tdz) + xiz * (szdx + gxize / gxixi * szdz);
-      dzx = zex * (sxdz + gxize / gzeze * sxdx) + zez * (gxize / gzeze * tdx + tdz);
-      dzz = zex * (gxize / gzeze * tdx + tdz) + zez * (gxize / gzeze * szdx + szdz);
+      if (side || bottom) {
+        dxx = xix * (sxdx + gxize / gxixi * sxdz) + xiz * (tdx + gxize / gxixi * tdz);
+        dxz = xix * (tdx + gxize / gxixi * tdz) + xiz * (szdx + gxize / gxixi * szdz);
+        dzx = zex * (sxdz + gxize / gzeze * sxdx) + zez * (gxize / gzeze * tdx + tdz);
+        dzz = zex * (gxize / gzeze * tdx + tdz) + zez * (gxize / gzeze * szdx + szdz);
+      }
     }
-    const float r0 = __ldg(C.rho + i);
-    o.vx = rvx / r0;
-    o.vz = rvz / r0;
+    const float ir = __ldg(C.rcp_rho + i);
+    o.vx = rvx * ir;
+    o.vz = rvz * ir;
     if (side) {
       const float4 p = __ldg(C.pmlx + ix);
       const float V0 = __ldg(S.x[0] + si), V1 = __ldg(S.x[1] + si);
       o.XV0 = -p.y * V0 + p.x * dxx;
       o.XV1 = -p.y * V1 + p.x * dxz;
-      o.vx += ((p.z - 1.0f) * dxx - p.z * V0) / r0;
-      o.vz += ((p.z - 1.0f) * dxz - p.z * V1) / r0;
+      o.vx += ((p.z - 1.0f) * dxx - p.z * V0) * ir;
+      o.vz += ((p.z - 1.0f) * dxz - p.z * V1) * ir;
     }
     if (bottom) {
       const float4 p = __ldg(C.pmlz + iz);
       const float V0 = __ldg(S.z[0] + zi), V1 = __ldg(S.z[1] + zi);
       o.ZV0 = -p.y * V0 + p.x * dzx;
       o.ZV1 = -p.y * V1 + p.x * dzz;
-      o.vx += ((p.z - 1.0f) * dzx - p.z * V0) / r0;
-      o.vz += ((p.z - 1.0f) * dzz - p.z * V1) / r0;
+      o.vx += ((p.z - 1.0f) * dzx - p.z * V0) * ir;
+      o.vz += ((p.z - 1.0f) * dzz - p.z * V1) * ir;
     }
   }
   // ---- stress ----
   {
     const float c11 = __ldg(C.C11 + i), c13 = __ldg(C.C13 + i), c33 = __ldg(C.C33 + i),
                 c55 = __ldg(C.C55 + i);
-    const float dvx_dxi = dx5(S.vx), dvz_dxi = dx5(S.vz);
-    if (dist == 0) {
+    const float dvx_dxi = dx5(kVX), dvz_dxi = dx5(kVZ);
+    if (!IN && dist == 0) {
       // traction-free row: the zeta derivatives eliminated through the ALM
       // coefficients (src/elements.cu:907-977)
       const float a0 = __ldg(C.alm + ix), a1 = __ldg(C.alm + P + ix), a2 = __ldg(C.alm + 2 * P + ix),
@@ -139,7 +155,7 @@ __device__ __forceinline__ Out rhs(const SCoef& C, const SFields& S, int iz, int
       }
       return o;
     }
-    const float dvx_dze = dzn(S.vx, dist), dvz_dze = dzn(S.vz, dist);
+    const float dvx_dze = dzn(kVX, dist), dvz_dze = dzn(kVZ, dist);
     o.sx = c11 * (xix * dvx_dxi + zex * dvx_dze) + c13 * (xiz * dvz_dxi + zez * dvz_dze);
     o.sz = c13 * (xix * dvx_dxi + zex * dvx_dze) + c33 * (xiz * dvz_dxi + zez * dvz_dze);
     o.sxz = c55 * (xiz * dvx_dxi + zez * dvx_dze + xix * dvz_dxi + zex * dvz_dze);
@@ -179,41 +195,123 @@ __device__ __forceinline__ void upd(float k, const float* in, const float* un, f
   rk_update<KIND>(k, KIND == kStageFirst ? __ldg(in + i) : 0.f, un, out, acc, i, c, w);
 }
 
-template <int DIR, int KIND>
-__global__ void __launch_bounds__(kBX * kBY) k_stage(SCoef C, SFields in, SFields out, SFields un,
-                                                      SFields acc, int s, float c, float w, SrcW W) {
-  const int ix = 3 + blockIdx.x * kBX + threadIdx.x, iz = 3 + blockIdx.y * kBY + threadIdx.y;
+// The RK operands of the five fields of one cell, loaded before any store of
+// the row so that their DRAM round trips overlap (the output and accumulator
+// pointers may alias the inputs as far as the compiler knows, which would
+// otherwise order each field's loads after the previous field's stores).
+// `u`: U^n (the stage input itself at stage 0), `a`: the accumulator.
+struct Rk5 { float u[5], a[5]; };
+
+template <int KIND>
+__device__ __forceinline__ void store5(const Out& o, const Rk5& r, const SFields& out,
+                                       const SFields& acc, size_t i, float c, float w) {
+  float* const po[5] = {out.vx, out.vz, out.sx, out.sz, out.sxz};
+  float* const pa[5] = {acc.vx, acc.vz, acc.sx, acc.sz, acc.sxz};
+  const float k[5] = {o.vx, o.vz, o.sx, o.sz, o.sxz};
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    if (KIND == kStageFirst) {
+      po[q][i] = fmaf(c, k[q], r.u[q]);
+      pa[q][i] = fmaf(w, k[q], r.u[q]);
+    } else if (KIND == kStageMid) {
+      po[q][i] = fmaf(c, k[q], r.u[q]);
+      pa[q][i] = fmaf(w, k[q], r.a[q]);
+    } else {
+      po[q][i] = fmaf(c, k[q], r.a[q]);
+    }
+  }
+}
+
+// The kTZ / kBY rows of column ix owned by this thread, from the staged tile.
+template <int DIR, int KIND, bool IN>
+__device__ __forceinline__ void rows(const SCoef& C, const SFields& in, const SFields& out,
+                                     const SFields& un, const SFields& acc,
+                                     const float (&tile)[5][kHH][kHW], int r0, int ix, int s,
+                                     float c, float w, const SrcW& W) {
   const int nx = C.nx, nz = C.nz, npd = C.npd, P = C.P;
-  if (ix > nx - 4 || iz > nz - 4) return;
-  Out o = rhs<DIR>(C, in, iz, ix);
-  // explosive source on both normal stresses (src/pml_fs_kernels.cu:22-26)
-  const int it = __ldg(C.step);
-  const int sx = ix - C.srcx, sz = iz - C.srcz;
-  if (C.srcx >= 0 && sx >= -2 && sx <= 2 && sz >= -2 && sz <= 2 && it >= 0 && it < C.src_steps) {
-    const float q = __ldg(C.src_amp + (size_t)it * 4 + s) * W.w[(sz + 2) * 5 + (sx + 2)];
-    o.sx += q;
-    o.sz += q;
+  const int it = IN ? 0 : __ldg(C.step);
+#pragma unroll 1
+  for (int k = 0; k < kTZ / kBY; ++k) {
+    const int lz = 3 + threadIdx.y + k * kBY, iz = r0 + lz;
+    if (iz > nz - 4) return;
+    auto A = [&](int q, int dz, int dx) { return tile[q][lz + dz][3 + threadIdx.x + dx]; };
+    const size_t i = (size_t)iz * P + ix;
+    Rk5 r;
+    {
+      const float* const pu[5] = {un.vx, un.vz, un.sx, un.sz, un.sxz};
+      const float* const pa[5] = {acc.vx, acc.vz, acc.sx, acc.sz, acc.sxz};
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        r.u[q] = KIND == kStageFirst ? A(q, 0, 0) : KIND == kStageMid ? __ldg(pu[q] + i) : 0.f;
+        r.a[q] = KIND == kStageFirst ? 0.f : pa[q][i];
+      }
+    }
+    Out o = rhs<DIR, IN>(C, in, A, iz, ix);
+    if (!IN) {
+      // explosive source on both normal stresses (src/pml_fs_kernels.cu:22-26)
+      const int sx = ix - C.srcx, sz = iz - C.srcz;
+      if (C.srcx >= 0 && sx >= -2 && sx <= 2 && sz >= -2 && sz <= 2 && it >= 0 && it < C.src_steps) {
+        const float q = __ldg(C.src_amp + (size_t)it * 4 + s) * W.w[(sz + 2) * 5 + (sx + 2)];
+        o.sx += q;
+        o.sz += q;
+      }
+    }
+    store5<KIND>(o, r, out, acc, i, c, w);
+    if (!IN && min(ix - 3, nx - 4 - ix) < npd) {
+      const size_t si = (size_t)iz * C.Ps + xstrip_col(ix, nx, npd);
+      upd<KIND>(o.XV0, in.x[0], un.x[0], out.x[0], acc.x[0], si, c, w);
+      upd<KIND>(o.XV1, in.x[1], un.x[1], out.x[1], acc.x[1], si, c, w);
+      upd<KIND>(o.XE0, in.x[2], un.x[2], out.x[2], acc.x[2], si, c, w);
+      upd<KIND>(o.XE1, in.x[3], un.x[3], out.x[3], acc.x[3], si, c, w);
+    }
+    if (!IN && iz >= nz - 3 - npd) {
+      const size_t zi = (size_t)(iz - (nz - 3 - npd)) * P + ix;
+      upd<KIND>(o.ZV0, in.z[0], un.z[0], out.z[0], acc.z[0], zi, c, w);
+      upd<KIND>(o.ZV1, in.z[1], un.z[1], out.z[1], acc.z[1], zi, c, w);
+      upd<KIND>(o.ZE0, in.z[2], un.z[2], out.z[2], acc.z[2], zi, c, w);
+      upd<KIND>(o.ZE1, in.z[3], un.z[3], out.z[3], acc.z[3], zi, c, w);
+    }
   }
-  const size_t i = (size_t)iz * P + ix;
-  upd<KIND>(o.vx, in.vx, un.vx, out.vx, acc.vx, i, c, w);
-  upd<KIND>(o.vz, in.vz, un.vz, out.vz, acc.vz, i, c, w);
-  upd<KIND>(o.sx, in.sx, un.sx, out.sx, acc.sx, i, c, w);
-  upd<KIND>(o.sz, in.sz, un.sz, out.sz, acc.sz, i, c, w);
-  upd<KIND>(o.sxz, in.sxz, un.sxz, out.sxz, acc.sxz, i, c, w);
-  if (min(ix - 3, nx - 4 - ix) < npd) {
-    const size_t si = (size_t)iz * C.Ps + xstrip_col(ix, nx, npd);
-    upd<KIND>(o.XV0, in.x[0], un.x[0], out.x[0], acc.x[0], si, c, w);
-    upd<KIND>(o.XV1, in.x[1], un.x[1], out.x[1], acc.x[1], si, c, w);
-    upd<KIND>(o.XE0, in.x[2], un.x[2], out.x[2], acc.x[2], si, c, w);
-    upd<KIND>(o.XE1, in.x[3], un.x[3], out.x[3], acc.x[3], si, c, w);
+}
+
+template <int DIR, int KIND>
+__global__ void __launch_bounds__(kBX * kBY, 4) k_stage(SCoef C, SFields in, SFields out, SFields un,
+                                                      SFields acc, int s, float c, float w, SrcW W) {
+  __shared__ __align__(16) float tile[5][kHH][kHW];
+  const int nx = C.nx, nz = C.nz, npd = C.npd, P = C.P;
+  const int c0 = blockIdx.x * kBX, r0 = blockIdx.y * kTZ;
+  // Stage the tile: rows r0.. (below nz), float4 columns c0.. (below P; the
+  // pitch is a multiple of 32 floats, so every float4 lies in one row and no
+  // column at or beyond nx is ever read back). 250 of the 256 threads each own
+  // one float4 column of every 25th tile row.
+  {
+    constexpr int kV = kHW / 4, kRowsPerPass = (kBX * kBY) / kV;
+    const int tid = threadIdx.y * kBX + threadIdx.x, vr = tid / kV, vc = (tid - vr * kV) * 4;
+    if (vr < kRowsPerPass && c0 + vc < P) {
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        const float* f = q == kVX ? in.vx : q == kVZ ? in.vz : q == kSX ? in.sx : q == kSZ ? in.sz : in.sxz;
+#pragma unroll
+        for (int rr = vr; rr < kHH; rr += kRowsPerPass)
+          if (r0 + rr < nz)
+            *reinterpret_cast<float4*>(&tile[q][rr][vc]) =
+                __ldg(reinterpret_cast<const float4*>(f + (size_t)(r0 + rr) * P + c0 + vc));
+      }
+    }
   }
-  if (iz >= nz - 3 - npd) {
-    const size_t zi = (size_t)(iz - (nz - 3 - npd)) * P + ix;
-    upd<KIND>(o.ZV0, in.z[0], un.z[0], out.z[0], acc.z[0], zi, c, w);
-    upd<KIND>(o.ZV1, in.z[1], un.z[1], out.z[1], acc.z[1], zi, c, w);
-    upd<KIND>(o.ZE0, in.z[2], un.z[2], out.z[2], acc.z[2], zi, c, w);
-    upd<KIND>(o.ZE1, in.z[3], un.z[3], out.z[3], acc.z[3], zi, c, w);
-  }
+  __syncthreads();
+  const int ix = 3 + c0 + threadIdx.x;
+  if (ix > nx - 4) return;
+  // Blocks whose cells are all at least three rows below the free surface, in
+  // no absorbing strip and away from the source take the branch-free body.
+  const bool interior = r0 >= 3 && r0 + kTZ + 2 < nz - 3 - npd && c0 >= npd &&
+                        c0 + kBX + 2 <= nx - 4 - npd &&
+                        (C.srcx < 0 || C.srcx + 2 < c0 + 3 || C.srcx - 2 > c0 + kBX + 2 ||
+                         C.srcz + 2 < r0 + 3 || C.srcz - 2 > r0 + kTZ + 2);
+  if (interior)
+    rows<DIR, KIND, true>(C, in, out, un, acc, tile, r0, ix, s, c, w, W);
+  else
+    rows<DIR, KIND, false>(C, in, out, un, acc, tile, r0, ix, s, c, w, W);
 }
 
 __global__ void k_finish(SCoef C, SFields U) {
@@ -251,7 +349,7 @@ cudaError_t launch_t(const SCoef& C, const SFields& in, const SFields& out, cons
   const SrcW W{{0.0030f, 0.0133f, 0.0219f, 0.0133f, 0.0030f, 0.0133f, 0.0596f, 0.0983f, 0.0596f,
                 0.0133f, 0.0219f, 0.0983f, 0.1621f, 0.0983f, 0.0219f, 0.0133f, 0.0596f, 0.0983f,
                 0.0596f, 0.0133f, 0.0030f, 0.0133f, 0.0219f, 0.0133f, 0.0030f}};
-  const dim3 grid(unsigned((C.nx - 6 + kBX - 1) / kBX), unsigned((C.nz - 6 + kBY - 1) / kBY));
+  const dim3 grid(unsigned((C.nx - 6 + kBX - 1) / kBX), unsigned((C.nz - 6 + kTZ - 1) / kTZ));
   const float c = C.rk_c[s], w = KIND == kStageLast ? 0.f : C.rk_w[s];
   k_stage<DIR, KIND><<<grid, dim3(kBX, kBY), 0, st>>>(C, in, out, un, acc, s, c, w, W);
   return cudaGetLastError();

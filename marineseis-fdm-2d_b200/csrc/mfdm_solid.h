@@ -15,7 +15,7 @@ struct SCoef {
   const float* __restrict__ C13;
   const float* __restrict__ C33;
   const float* __restrict__ C55;
-  const float* __restrict__ rho;
+  const float* __restrict__ rcp_rho;  // 1/rho: FP64 reciprocal rounded once
   const float* __restrict__ J;
   const float* __restrict__ xix;
   const float* __restrict__ xiz;
