@@ -7,11 +7,12 @@
 // build_ghost_flux launch), the explosive source and the fused RK4 update
 // (the reference's vector_add / vector_self_add launches over full grids).
 // A fifth launch per step samples the receiver row and advances the device
-// step counter. Each block stages the five stage-input fields of its 32x24
+// step counter. Each block stages the five stage-input fields of its 32x16
 // cells and their 3-cell halo in shared memory with independent float4 loads
-// (all in flight at once), then every thread computes three rows from shared
-// memory; coefficients, ADE memory and the RK operands are point-wise global
-// reads.
+// (all in flight at once, together with the point-wise operands of every
+// thread's first row), then every thread computes two rows from shared memory;
+// coefficients, ADE memory and the RK operands are point-wise global reads,
+// all of a row's issued before its arithmetic and its stores.
 #include "mfdm_device.cuh"
 #include "mfdm_solid.h"
 
@@ -21,7 +22,7 @@ namespace {
 
 constexpr int kBX = 32, kBY = 8;
 #ifndef MFDM_SOLID_ROWS
-#define MFDM_SOLID_ROWS 24
+#define MFDM_SOLID_ROWS 16
 #endif
 constexpr int kTZ = MFDM_SOLID_ROWS;  // rows per block (kTZ / kBY per thread)
 static_assert(kTZ % kBY == 0 && 5 * (kTZ + 6) * (kBX + 8) * 4 <= 48 * 1024, "tile rows");
@@ -29,7 +30,13 @@ constexpr int kHW = kBX + 8;     // tile row: columns c0 .. c0 + 39, c0 = first 
 constexpr int kHH = kTZ + 6;     // tile rows: r0 .. r0 + kTZ + 5, r0 = first row - 3
 enum { kVX = 0, kVZ, kSX, kSZ, kSXZ };
 
-struct SrcW { float w[25]; };
+// The 5x5 weights of the explosive source (src/elements.cu:34-40).
+__constant__ float kSrcW[25] = {0.0030f, 0.0133f, 0.0219f, 0.0133f, 0.0030f, 0.0133f, 0.0596f,
+                                0.0983f, 0.0596f, 0.0133f, 0.0219f, 0.0983f, 0.1621f, 0.0983f,
+                                0.0219f, 0.0133f, 0.0596f, 0.0983f, 0.0596f, 0.0133f, 0.0030f,
+                                0.0133f, 0.0219f, 0.0133f, 0.0030f};
+// Point-wise coefficients of a cell, in this order.
+enum { kCXIX = 0, kCXIZ, kCZEX, kCZEZ, kCRR, kC11, kC13, kC33, kC55, kNCoef };
 
 struct Out {
   float vx, vz, sx, sz, sxz;
@@ -41,8 +48,10 @@ struct Out {
 // away, |dz|, |dx| <= 3; the ADE memory of S is read from global memory.
 // IN: the caller guarantees a cell at least three rows below the free surface
 // and outside every absorbing strip (the branch-free body of interior blocks).
-template <int DIR, bool IN, class Acc>
-__device__ __forceinline__ Out rhs(const SCoef& C, const SFields& S, const Acc& A, int iz, int ix) {
+// `K(c)` returns point-wise coefficient c (kCXIX..kC55) of the cell.
+template <int DIR, bool IN, class Acc, class Kc>
+__device__ __forceinline__ Out rhs(const SCoef& C, const SFields& S, const Acc& A, const Kc& K,
+                                   int iz, int ix) {
   Out o;
   const int P = C.P, nx = C.nx, nz = C.nz, npd = C.npd;
   const size_t i = (size_t)iz * P + ix;
@@ -50,8 +59,7 @@ __device__ __forceinline__ Out rhs(const SCoef& C, const SFields& S, const Acc& 
   const bool side = !IN && distx < npd, bottom = !IN && iz >= nz - 3 - npd;
   const int scol = side ? xstrip_col(ix, nx, npd) : 0;
   const size_t si = (size_t)iz * C.Ps + scol, zi = (size_t)(iz - (nz - 3 - npd)) * P + ix;
-  const float xix = __ldg(C.xix + i), xiz = __ldg(C.xiz + i), zex = __ldg(C.zex + i),
-              zez = __ldg(C.zez + i);
+  const float xix = K(kCXIX), xiz = K(kCXIZ), zex = K(kCZEX), zez = K(kCZEZ);
   const float gxixi = xix * xix + xiz * xiz, gzeze = zex * zex + zez * zez;
   const float gxize = xix * zex + xiz * zez;
   auto dx5 = [&](int q) {
@@ -108,7 +116,7 @@ __device__ __forceinline__ Out rhs(const SCoef& C, const SFields& S, const Acc& 
         dzz = zex * (gxize / gzeze * tdx + tdz) + zez * (gxize / gzeze * szdx + szdz);
       }
     }
-    const float ir = __ldg(C.rcp_rho + i);
+    const float ir = K(kCRR);
     o.vx = rvx * ir;
     o.vz = rvz * ir;
     if (side) {
@@ -130,8 +138,7 @@ __device__ __forceinline__ Out rhs(const SCoef& C, const SFields& S, const Acc& 
   }
   // ---- stress ----
   {
-    const float c11 = __ldg(C.C11 + i), c13 = __ldg(C.C13 + i), c33 = __ldg(C.C33 + i),
-                c55 = __ldg(C.C55 + i);
+    const float c11 = K(kC11), c13 = K(kC13), c33 = K(kC33), c55 = K(kC55);
     const float dvx_dxi = dx5(kVX), dvz_dxi = dx5(kVZ);
     if (!IN && dist == 0) {
       // traction-free row: the zeta derivatives eliminated through the ALM
@@ -195,15 +202,39 @@ __device__ __forceinline__ void upd(float k, const float* in, const float* un, f
   rk_update<KIND>(k, KIND == kStageFirst ? __ldg(in + i) : 0.f, un, out, acc, i, c, w);
 }
 
-// The RK operands of the five fields of one cell, loaded before any store of
-// the row so that their DRAM round trips overlap (the output and accumulator
-// pointers may alias the inputs as far as the compiler knows, which would
-// otherwise order each field's loads after the previous field's stores).
-// `u`: U^n (the stage input itself at stage 0), `a`: the accumulator.
-struct Rk5 { float u[5], a[5]; };
+// The point-wise operands of one cell: U^n (`u`, the stage input itself at
+// stage 0, taken from the tile), the accumulator (`a`) and the coefficients
+// (`k`). They are loaded into registers before any store of the row -- the
+// first row's before the tile barrier, so that their DRAM round trips overlap
+// the tile load (the output and accumulator pointers may alias the inputs as
+// far as the compiler knows, which would otherwise order each field's loads
+// after the previous field's stores). Loading the next row's under the
+// current row's arithmetic needs 80 registers and was slower.
+struct Pt { float u[5], a[5], k[kNCoef]; };
 
 template <int KIND>
-__device__ __forceinline__ void store5(const Out& o, const Rk5& r, const SFields& out,
+__device__ __forceinline__ void load_pt(Pt& p, const SCoef& C, const SFields& un,
+                                        const SFields& acc, size_t i) {
+  const float* const pu[5] = {un.vx, un.vz, un.sx, un.sz, un.sxz};
+  const float* const pa[5] = {acc.vx, acc.vz, acc.sx, acc.sz, acc.sxz};
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    if (KIND == kStageMid) p.u[q] = __ldg(pu[q] + i);
+    if (KIND != kStageFirst) p.a[q] = pa[q][i];
+  }
+  p.k[kCXIX] = __ldg(C.xix + i);
+  p.k[kCXIZ] = __ldg(C.xiz + i);
+  p.k[kCZEX] = __ldg(C.zex + i);
+  p.k[kCZEZ] = __ldg(C.zez + i);
+  p.k[kCRR] = __ldg(C.rcp_rho + i);
+  p.k[kC11] = __ldg(C.C11 + i);
+  p.k[kC13] = __ldg(C.C13 + i);
+  p.k[kC33] = __ldg(C.C33 + i);
+  p.k[kC55] = __ldg(C.C55 + i);
+}
+
+template <int KIND>
+__device__ __forceinline__ void store5(const Out& o, const Pt& r, const SFields& out,
                                        const SFields& acc, size_t i, float c, float w) {
   float* const po[5] = {out.vx, out.vz, out.sx, out.sz, out.sxz};
   float* const pa[5] = {acc.vx, acc.vz, acc.sx, acc.sz, acc.sxz};
@@ -222,12 +253,13 @@ __device__ __forceinline__ void store5(const Out& o, const Rk5& r, const SFields
   }
 }
 
-// The kTZ / kBY rows of column ix owned by this thread, from the staged tile.
+// The kTZ / kBY rows of column ix owned by this thread, from the staged tile;
+// `p` holds the first row's point-wise operands on entry.
 template <int DIR, int KIND, bool IN>
 __device__ __forceinline__ void rows(const SCoef& C, const SFields& in, const SFields& out,
                                      const SFields& un, const SFields& acc,
                                      const float (&tile)[5][kHH][kHW], int r0, int ix, int s,
-                                     float c, float w, const SrcW& W) {
+                                     float c, float w, Pt& p) {
   const int nx = C.nx, nz = C.nz, npd = C.npd, P = C.P;
   const int it = IN ? 0 : __ldg(C.step);
 #pragma unroll 1
@@ -236,27 +268,23 @@ __device__ __forceinline__ void rows(const SCoef& C, const SFields& in, const SF
     if (iz > nz - 4) return;
     auto A = [&](int q, int dz, int dx) { return tile[q][lz + dz][3 + threadIdx.x + dx]; };
     const size_t i = (size_t)iz * P + ix;
-    Rk5 r;
-    {
-      const float* const pu[5] = {un.vx, un.vz, un.sx, un.sz, un.sxz};
-      const float* const pa[5] = {acc.vx, acc.vz, acc.sx, acc.sz, acc.sxz};
+    if (k > 0) load_pt<KIND>(p, C, un, acc, i);
+    if (KIND == kStageFirst) {
 #pragma unroll
-      for (int q = 0; q < 5; ++q) {
-        r.u[q] = KIND == kStageFirst ? A(q, 0, 0) : KIND == kStageMid ? __ldg(pu[q] + i) : 0.f;
-        r.a[q] = KIND == kStageFirst ? 0.f : pa[q][i];
-      }
+      for (int q = 0; q < 5; ++q) p.u[q] = A(q, 0, 0);
     }
-    Out o = rhs<DIR, IN>(C, in, A, iz, ix);
+    auto K = [&](int cf) { return p.k[cf]; };
+    Out o = rhs<DIR, IN>(C, in, A, K, iz, ix);
     if (!IN) {
       // explosive source on both normal stresses (src/pml_fs_kernels.cu:22-26)
       const int sx = ix - C.srcx, sz = iz - C.srcz;
       if (C.srcx >= 0 && sx >= -2 && sx <= 2 && sz >= -2 && sz <= 2 && it >= 0 && it < C.src_steps) {
-        const float q = __ldg(C.src_amp + (size_t)it * 4 + s) * W.w[(sz + 2) * 5 + (sx + 2)];
+        const float q = __ldg(C.src_amp + (size_t)it * 4 + s) * kSrcW[(sz + 2) * 5 + (sx + 2)];
         o.sx += q;
         o.sz += q;
       }
     }
-    store5<KIND>(o, r, out, acc, i, c, w);
+    store5<KIND>(o, p, out, acc, i, c, w);
     if (!IN && min(ix - 3, nx - 4 - ix) < npd) {
       const size_t si = (size_t)iz * C.Ps + xstrip_col(ix, nx, npd);
       upd<KIND>(o.XV0, in.x[0], un.x[0], out.x[0], acc.x[0], si, c, w);
@@ -275,11 +303,16 @@ __device__ __forceinline__ void rows(const SCoef& C, const SFields& in, const SF
 }
 
 template <int DIR, int KIND>
-__global__ void __launch_bounds__(kBX * kBY, 4) k_stage(SCoef C, SFields in, SFields out, SFields un,
-                                                      SFields acc, int s, float c, float w, SrcW W) {
+__global__ void __launch_bounds__(kBX * kBY, 4) k_stage(SCoef C, SFields in, SFields out,
+                                                                      SFields un, SFields acc, int s,
+                                                                      float c, float w) {
   __shared__ __align__(16) float tile[5][kHH][kHW];
   const int nx = C.nx, nz = C.nz, npd = C.npd, P = C.P;
   const int c0 = blockIdx.x * kBX, r0 = blockIdx.y * kTZ;
+  const int ix = 3 + c0 + threadIdx.x, iz0 = r0 + 3 + threadIdx.y;
+  // the first row's point-wise operands, in flight together with the tile
+  Pt p;
+  if (ix <= nx - 4 && iz0 <= nz - 4) load_pt<KIND>(p, C, un, acc, (size_t)iz0 * P + ix);
   // Stage the tile: rows r0.. (below nz), float4 columns c0.. (below P; the
   // pitch is a multiple of 32 floats, so every float4 lies in one row and no
   // column at or beyond nx is ever read back). 250 of the 256 threads each own
@@ -300,7 +333,6 @@ __global__ void __launch_bounds__(kBX * kBY, 4) k_stage(SCoef C, SFields in, SFi
     }
   }
   __syncthreads();
-  const int ix = 3 + c0 + threadIdx.x;
   if (ix > nx - 4) return;
   // Blocks whose cells are all at least three rows below the free surface, in
   // no absorbing strip and away from the source take the branch-free body.
@@ -309,9 +341,9 @@ __global__ void __launch_bounds__(kBX * kBY, 4) k_stage(SCoef C, SFields in, SFi
                         (C.srcx < 0 || C.srcx + 2 < c0 + 3 || C.srcx - 2 > c0 + kBX + 2 ||
                          C.srcz + 2 < r0 + 3 || C.srcz - 2 > r0 + kTZ + 2);
   if (interior)
-    rows<DIR, KIND, true>(C, in, out, un, acc, tile, r0, ix, s, c, w, W);
+    rows<DIR, KIND, true>(C, in, out, un, acc, tile, r0, ix, s, c, w, p);
   else
-    rows<DIR, KIND, false>(C, in, out, un, acc, tile, r0, ix, s, c, w, W);
+    rows<DIR, KIND, false>(C, in, out, un, acc, tile, r0, ix, s, c, w, p);
 }
 
 __global__ void k_finish(SCoef C, SFields U) {
@@ -345,13 +377,9 @@ __global__ void k_set_step(int* step, unsigned* done, int it) {
 template <int DIR, int KIND>
 cudaError_t launch_t(const SCoef& C, const SFields& in, const SFields& out, const SFields& un,
                      const SFields& acc, int s, cudaStream_t st) {
-  // the 5x5 source weights (src/elements.cu:34-40)
-  const SrcW W{{0.0030f, 0.0133f, 0.0219f, 0.0133f, 0.0030f, 0.0133f, 0.0596f, 0.0983f, 0.0596f,
-                0.0133f, 0.0219f, 0.0983f, 0.1621f, 0.0983f, 0.0219f, 0.0133f, 0.0596f, 0.0983f,
-                0.0596f, 0.0133f, 0.0030f, 0.0133f, 0.0219f, 0.0133f, 0.0030f}};
   const dim3 grid(unsigned((C.nx - 6 + kBX - 1) / kBX), unsigned((C.nz - 6 + kTZ - 1) / kTZ));
   const float c = C.rk_c[s], w = KIND == kStageLast ? 0.f : C.rk_w[s];
-  k_stage<DIR, KIND><<<grid, dim3(kBX, kBY), 0, st>>>(C, in, out, un, acc, s, c, w, W);
+  k_stage<DIR, KIND><<<grid, dim3(kBX, kBY), 0, st>>>(C, in, out, un, acc, s, c, w);
   return cudaGetLastError();
 }
 
