@@ -71,7 +71,7 @@ typedef struct mfdm_info {
   long long device_bytes;         /* device memory held by the handle */
   int nshots;                     /* shots stepped together (1 unless opened with mfdm_open_batch) */
   int seg_rows;                   /* rows per segment block of the stage launches */
-  int blocks_per_sm;              /* stage kernel build in use: 2 or 3 resident blocks per SM */
+  int blocks_per_sm;              /* stage kernel build in use: 2 or 3 (TMA rings), 4 (tiles) */
 } mfdm_info;
 
 /* Field ids for mfdm_get_field / mfdm_set_field. */
@@ -182,17 +182,22 @@ int mfdm_batch_get_field(mfdm_model* m, int shot, int field, float* host);
  * fixed 16x16 blocks (src/pml_fs_kernels.cu:533-622) and has no tuner. */
 
 /* Sets the segment height: a multiple of 4 in [4, 128], or 0 for the default
- * (24). Results do not depend on it beyond FP32 rounding of the last bit. */
+ * (24; the tile build, mfdm_set_blocks_per_sm 4, rounds it up to a multiple of
+ * 8 and caps it at 48, 16 by default). Results do not depend on it beyond FP32
+ * rounding of the last bit. */
 int mfdm_set_tile(mfdm_model* m, int seg_rows);
 
 /* Selects the stage kernel build: 2 resident blocks per SM (deeper TMA rings,
  * 96 registers) or 3 (shallower rings, 72 registers, more bytes in flight per
- * SM: faster on large grids, slower on small ones); 0 (default) picks by grid
- * size (3 from 6 M cells per launch). Results agree to FP32 rounding. */
+ * SM: faster on large grids, slower on small ones); 4: the tile build (no
+ * rings: 256-thread blocks stage 32 x 16 cells and their halo in shared
+ * memory with plain loads while the point-wise operands of each thread's
+ * first row are already in flight); 0 (default) picks by grid size (3 from
+ * 6 M cells per launch). Results agree to FP32 rounding. */
 int mfdm_set_blocks_per_sm(mfdm_model* m, int blocks);
 
-/* Times every candidate segment height and both stage builds (2 and 3 blocks
- * per SM) on this handle's model and shots
+/* Times every candidate segment height with both ring builds (2 and 3 blocks
+ * per SM), and the tile build, on this handle's model and shots
  * (a few steps each, CUDA events on the handle's stream), keeps the fastest and
  * writes it to *seg_rows (may be NULL). The choice is cached per device, grid
  * shape, PML width, boundary type and shot count, so a second handle of the

@@ -1130,8 +1130,9 @@ int mfdm_autotune(mfdm_model* m, int* seg_rows) {
     const int n = int(sizeof(kSegCandidates) / sizeof(int));
     if ((rc = ensure_capacity(m, 2 * kGraphSteps * n * 2)) != MFDM_OK) return rc;
     float best_ms = 0.f;
-    for (int variant = 2; variant <= 3; ++variant)
+    for (int variant = 2; variant <= 4; ++variant)
       for (int i = 0; i < n; ++i) {
+        if (variant == 4 && kSegCandidates[i] % 8 != 0) continue;  // tile heights: multiples of 8
         float ms = 0.f;
         if ((rc = time_segment_rows(m, kSegCandidates[i], variant, &ms)) != MFDM_OK) return rc;
         if (best.first == 0 || ms < best_ms) {
@@ -1153,8 +1154,8 @@ int mfdm_autotune(mfdm_model* m, int* seg_rows) {
 
 int mfdm_set_blocks_per_sm(mfdm_model* m, int blocks) {
   if (!m) return fail(MFDM_ERR_ARG, "null handle");
-  if (blocks != 0 && blocks != 2 && blocks != 3)
-    return fail(MFDM_ERR_ARG, "blocks per SM must be 2, 3 or 0 (by grid size)");
+  if (blocks != 0 && blocks != 2 && blocks != 3 && blocks != 4)
+    return fail(MFDM_ERR_ARG, "stage build must be 2, 3 (blocks per SM), 4 (tiles) or 0 (by grid size)");
   DeviceGuard g(m->device);
   MFDM_CU(cudaStreamSynchronize(m->stream));
   m->C.variant = blocks;

@@ -643,6 +643,351 @@ cudaError_t upload_constants_v(const float* srcw25, const float* w7) {
   return cudaMemcpyToSymbol(c_w7, w7, 7 * sizeof(float));
 }
 
+#ifndef MFDM_VARIANT_TU
+// ---- the tile build: shared-memory stencil tiles and plain loads ------------------
+//
+// Blocks of 256 threads own 32 columns x `tr` rows of the fluid or the solid
+// (tr: the segment height rounded up to a multiple of 8, at most 48; two rows
+// per thread at the default 16). A block stages the stage-input fields of its cells with their 3-row,
+// 4-column halo in shared memory with independent float4 loads (zero outside
+// the arrays, as the tensor maps of the ring builds fill), while every thread
+// already has the point-wise operands of its first row in flight: U^n, the
+// accumulator and the coefficient block's values (metric copies, 1/rho and K
+// or the stiffnesses). 32 warps per SM, no producer warp, no ring barriers.
+// The interface strip is the ring builds' (global loads).
+
+constexpr int kTileX = 32;                 // columns per tile block
+constexpr int kTileRowsMax = 48;           // tallest tile block
+constexpr int kTileW = kTileX + 8;         // staged row: columns x0-4 .. x0+35
+constexpr int kTileHMax = kTileRowsMax + 6;  // staged rows: z0-3 .. z0+tr+2
+constexpr int kTileThreads = 256;
+constexpr int kTileRowStep = kTileThreads / kTileX;  // rows between a thread's cells (8)
+#ifndef MFDM_TILE_MIN_BLOCKS
+#define MFDM_TILE_MIN_BLOCKS 4  // tile blocks resident per SM (the register cap)
+#endif
+static_assert(kTileThreads == kConsumers, "the interface strip's blocks");
+
+// Stage input staged as [row][field][column] (like the ring, so the same
+// compile-time offsets reach every neighbour).
+template <int NST>
+struct TileAcc {
+  const float* base;
+  __device__ __forceinline__ void init(const float* tile, int lz, int c) {
+    base = tile + lz * (NST * kTileW) + c;
+  }
+  __device__ __forceinline__ float at(int f, int dz, int dx) const {
+    return base[dz * (NST * kTileW) + f * kTileW + dx];
+  }
+};
+struct FluidTile : TileAcc<3> {
+  __device__ __forceinline__ float fvx(int dz, int dx) const { return at(0, dz, dx); }
+  __device__ __forceinline__ float fvz(int dz, int dx) const { return at(1, dz, dx); }
+  __device__ __forceinline__ float fp(int dz, int dx) const { return at(2, dz, dx); }
+};
+struct SolidTile : TileAcc<5> {
+  __device__ __forceinline__ float svx(int dz, int dx) const { return at(0, dz, dx); }
+  __device__ __forceinline__ float svz(int dz, int dx) const { return at(1, dz, dx); }
+  __device__ __forceinline__ float ssx(int dz, int dx) const { return at(2, dz, dx); }
+  __device__ __forceinline__ float ssz(int dz, int dx) const { return at(3, dz, dx); }
+  __device__ __forceinline__ float ssxz(int dz, int dx) const { return at(4, dz, dx); }
+};
+
+// Point-wise operands of one cell, loaded before any store of its row (the
+// output and accumulator pointers may alias the inputs as far as the compiler
+// knows, which would otherwise order each field's loads after the previous
+// field's stores).
+template <int NST, int NCOEF>
+struct TilePt { float u[NST], a[NST], k[NCOEF]; };
+
+template <int NST, int NCOEF, int KIND>
+__device__ __forceinline__ void tile_load_pt(TilePt<NST, NCOEF>& p, const float* const* un,
+                                             const float* const* acc, const float* coef,
+                                             size_t nblk, size_t i) {
+#pragma unroll
+  for (int f = 0; f < NST; ++f) {
+    if (KIND == kStageMid) p.u[f] = __ldg(un[f] + i);
+    if (KIND != kStageFirst) p.a[f] = acc[f][i];
+  }
+#pragma unroll
+  for (int q = 0; q < NCOEF; ++q) p.k[q] = __ldg(coef + q * nblk + i);
+}
+
+// Stage rows z0-3 .. z0+tr+2 of the NST fields (rows of `rows`, pitch P),
+// columns x0-4 .. x0+35; zero where a ring build's tensor map reads zero.
+template <int NST>
+__device__ __forceinline__ void tile_stage(float* tile, const float* const* f, int x0, int z0,
+                                           int tr, int rows, int P) {
+  constexpr int kV = kTileW / 4, kPer = NST * kV;
+  for (int e = threadIdx.x; e < (tr + 6) * kPer; e += kTileThreads) {
+    const int rr = e / kPer, rem = e - rr * kPer, q = rem / kV, vc = (rem - q * kV) * 4;
+    const int r = z0 - 3 + rr, col = x0 - 4 + vc;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (r >= 0 && r < rows && col >= 0 && col < P)
+      v = __ldg(reinterpret_cast<const float4*>(f[q] + (size_t)r * P + col));
+    *reinterpret_cast<float4*>(tile + (rr * NST + q) * kTileW + vc) = v;
+  }
+}
+
+template <int DIR, int KIND, bool CPML>
+__device__ __forceinline__ void fluid_tile(const Coef& C, const Fields& in, const Fields& out,
+                                           const Fields& un, const Fields& acc, int s, float cc,
+                                           float w, int blk, int ntx, int tr, float* tile) {
+  constexpr int NST = 3, NCOEF = 6;
+  const int P = C.P, nx = C.nx, nzf = C.nzf, npd = C.npd;
+  const size_t nf = (size_t)nzf * P;
+  const int x0 = (blk % ntx) * kTileX, z0 = 3 + (blk / ntx) * tr;
+  const int z1 = min(z0 + tr, nzf - 1);
+  const int tx = threadIdx.x % kTileX, ty = threadIdx.x / kTileX;
+  const int ix = x0 + tx;
+  const bool colok = ix >= 3 && ix <= nx - 4;
+  const float* const uns[3] = {un.fvx, un.fvz, un.fp};
+  const float* const accs_c[3] = {acc.fvx, acc.fvz, acc.fp};
+  const float* coef = C.rhof - 4 * nf;  // the fluid coefficient block [6][nz_f][P]
+  TilePt<NST, NCOEF> p;
+  if (colok && z0 + ty < z1)
+    tile_load_pt<NST, NCOEF, KIND>(p, uns, accs_c, coef, nf, (size_t)(z0 + ty) * P + ix);
+  {
+    const float* const f[3] = {in.fvx, in.fvz, in.fp};
+    tile_stage<NST>(tile, f, x0, z0, tr, nzf, P);
+  }
+  __syncthreads();
+  if (!colok) return;
+  const int it = __ldg(C.step);
+  const bool side = min(ix - 3, nx - 4 - ix) < npd;
+  const int scol = side ? xstrip_col(ix, nx, npd) : 0;
+  const bool general = x0 < 3 + npd || x0 + kTileX > nx - 3 - npd || z0 < 6 || z1 - 1 > nzf - 4 ||
+                       (CPML && z0 <= npd + 2) ||
+                       (C.srcx >= 0 && C.srcx >= x0 - 2 && C.srcx < x0 + kTileX + 2 &&
+                        C.srcz >= z0 - 2 && C.srcz < z1 + 2);
+  auto cell = [&](auto gen_tag, int k) {
+    constexpr bool GEN = decltype(gen_tag)::value;
+    const int iz = z0 + ty + k * kTileRowStep;
+    const size_t i = (size_t)iz * P + ix;
+    if (k > 0) tile_load_pt<NST, NCOEF, KIND>(p, uns, accs_c, coef, nf, i);
+    const bool sd = GEN && side;
+    FluidTile A;
+    A.init(tile, 3 + iz - z0, 4 + tx);
+    const FluidCoefs cf{p.k[0], p.k[1], p.k[2], p.k[3], p.k[4], p.k[5]};
+    float ade[4] = {0.f, 0.f, 0.f, 0.f}, zade[4] = {0.f, 0.f, 0.f, 0.f};
+    const size_t si = (size_t)iz * C.Ps + scol;
+    if (sd) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) ade[q] = __ldg(in.fx[q] + si);
+    }
+    const bool tp = GEN && CPML && iz <= npd + 2;
+    const size_t zi = (size_t)(iz - 3) * P + ix;
+    if (tp) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) zade[q] = __ldg(in.fz[q] + zi);
+    }
+    FluidK kk = (!GEN || (iz >= 6 && iz <= nzf - 4))
+                    ? fluid_rhs<DIR, true, CPML>(C, A, iz, ix, sd, ade, cf, tp, zade)
+                    : fluid_rhs<DIR, false, CPML>(C, A, iz, ix, sd, ade, cf, tp, zade);
+    if (GEN) kk.p += source_term(C, iz, ix, it, s);
+    const float kv[3] = {kk.vx, kk.vz, kk.p};
+    float* const outs[3] = {out.fvx, out.fvz, out.fp};
+    float* const accs[3] = {acc.fvx, acc.fvz, acc.fp};
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      if (KIND == kStageFirst) {
+        const float u0 = A.at(f, 0, 0);
+        outs[f][i] = fmaf(cc, kv[f], u0);
+        accs[f][i] = fmaf(w, kv[f], u0);
+      } else if (KIND == kStageMid) {
+        outs[f][i] = fmaf(cc, kv[f], p.u[f]);
+        accs[f][i] = fmaf(w, kv[f], p.a[f]);
+      } else {
+        outs[f][i] = fmaf(cc, kv[f], p.a[f]);
+      }
+    }
+    if (sd) {
+      rk_update<KIND>(kk.V0, ade[0], un.fx[0], out.fx[0], acc.fx[0], si, cc, w);
+      rk_update<KIND>(kk.V1, ade[1], un.fx[1], out.fx[1], acc.fx[1], si, cc, w);
+      if (kk.has_E) {
+        rk_update<KIND>(kk.E0, ade[2], un.fx[2], out.fx[2], acc.fx[2], si, cc, w);
+        rk_update<KIND>(kk.E1, ade[3], un.fx[3], out.fx[3], acc.fx[3], si, cc, w);
+      }
+    }
+    if (tp) {
+      rk_update<KIND>(kk.ZV0, zade[0], un.fz[0], out.fz[0], acc.fz[0], zi, cc, w);
+      rk_update<KIND>(kk.ZV1, zade[1], un.fz[1], out.fz[1], acc.fz[1], zi, cc, w);
+      rk_update<KIND>(kk.ZE0, zade[2], un.fz[2], out.fz[2], acc.fz[2], zi, cc, w);
+      rk_update<KIND>(kk.ZE1, zade[3], un.fz[3], out.fz[3], acc.fz[3], zi, cc, w);
+    }
+  };
+#pragma unroll 1
+  for (int k = 0; k < tr / kTileRowStep; ++k) {
+    if (z0 + ty + k * kTileRowStep >= z1) return;
+    if (general)
+      cell(std::true_type{}, k);
+    else
+      cell(std::false_type{}, k);
+  }
+}
+
+template <int DIR, int KIND, bool CPML>
+__device__ __forceinline__ void solid_tile(const Coef& C, const Fields& in, const Fields& out,
+                                           const Fields& un, const Fields& acc, float cc, float w,
+                                           int blk, int ntx, int tr, float* tile) {
+  constexpr int NST = 5, NCOEF = 9;
+  const int P = C.P, nx = C.nx, nzs = C.nzs, npd = C.npd;
+  const size_t ns = (size_t)nzs * P;
+  const int x0 = (blk % ntx) * kTileX, z0 = 1 + (blk / ntx) * tr;
+  const int z1 = min(z0 + tr, nzs - 3);
+  const int tx = threadIdx.x % kTileX, ty = threadIdx.x / kTileX;
+  const int ix = x0 + tx;
+  const bool colok = ix >= 3 && ix <= nx - 4;
+  const float* const uns[5] = {un.svx, un.svz, un.ssx, un.ssz, un.ssxz};
+  const float* const accs_c[5] = {acc.svx, acc.svz, acc.ssx, acc.ssz, acc.ssxz};
+  const float* coef = C.rhos - 4 * ns;  // the solid coefficient block [9][nz_s][P]
+  TilePt<NST, NCOEF> p;
+  if (colok && z0 + ty < z1)
+    tile_load_pt<NST, NCOEF, KIND>(p, uns, accs_c, coef, ns, (size_t)(z0 + ty) * P + ix);
+  {
+    const float* const f[5] = {in.svx, in.svz, in.ssx, in.ssz, in.ssxz};
+    tile_stage<NST>(tile, f, x0, z0, tr, nzs, P);
+  }
+  __syncthreads();
+  if (!colok) return;
+  const bool side = min(ix - 3, nx - 4 - ix) < npd;
+  const int scol = side ? xstrip_col(ix, nx, npd) : 0;
+  const int zb0 = nzs - 3 - npd;  // first row of the bottom strip
+  const bool general = x0 < 3 + npd || x0 + kTileX > nx - 3 - npd || z1 > zb0 || z0 < 3;
+  auto cell = [&](auto gen_tag, int k) {
+    constexpr bool GEN = decltype(gen_tag)::value;
+    const int iz = z0 + ty + k * kTileRowStep;
+    const size_t i = (size_t)iz * P + ix;
+    if (k > 0) tile_load_pt<NST, NCOEF, KIND>(p, uns, accs_c, coef, ns, i);
+    const bool sd = GEN && side;
+    const bool bottom = GEN && iz >= zb0;
+    SolidTile A;
+    A.init(tile, 3 + iz - z0, 4 + tx);
+    const SolidCoefs cf{p.k[0], p.k[1], p.k[2], p.k[3], p.k[4], p.k[5], p.k[6], p.k[7], p.k[8]};
+    float xade[4] = {0.f, 0.f, 0.f, 0.f}, zade[4] = {0.f, 0.f, 0.f, 0.f};
+    const size_t sxi = (size_t)iz * C.Ps + scol;
+    const size_t szi = (size_t)(iz - zb0) * P + ix;
+    if (sd) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) xade[q] = __ldg(in.sx[q] + sxi);
+    }
+    if (bottom) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) zade[q] = __ldg(in.sz[q] + szi);
+    }
+    SolidK kk = (!GEN || iz >= 3)
+                    ? solid_rhs<DIR, true, CPML>(C, A, iz, ix, sd, bottom, xade, zade, cf)
+                    : solid_rhs<DIR, false, CPML>(C, A, iz, ix, sd, bottom, xade, zade, cf);
+    const float kv[5] = {kk.vx, kk.vz, kk.sx, kk.sz, kk.sxz};
+    float* const outs[5] = {out.svx, out.svz, out.ssx, out.ssz, out.ssxz};
+    float* const accs[5] = {acc.svx, acc.svz, acc.ssx, acc.ssz, acc.ssxz};
+#pragma unroll
+    for (int f = 0; f < 5; ++f) {
+      if (KIND == kStageFirst) {
+        const float u0 = A.at(f, 0, 0);
+        outs[f][i] = fmaf(cc, kv[f], u0);
+        accs[f][i] = fmaf(w, kv[f], u0);
+      } else if (KIND == kStageMid) {
+        outs[f][i] = fmaf(cc, kv[f], p.u[f]);
+        accs[f][i] = fmaf(w, kv[f], p.a[f]);
+      } else {
+        outs[f][i] = fmaf(cc, kv[f], p.a[f]);
+      }
+    }
+    if (sd) {
+      rk_update<KIND>(kk.XV0, xade[0], un.sx[0], out.sx[0], acc.sx[0], sxi, cc, w);
+      rk_update<KIND>(kk.XV1, xade[1], un.sx[1], out.sx[1], acc.sx[1], sxi, cc, w);
+      rk_update<KIND>(kk.XE0, xade[2], un.sx[2], out.sx[2], acc.sx[2], sxi, cc, w);
+      rk_update<KIND>(kk.XE1, xade[3], un.sx[3], out.sx[3], acc.sx[3], sxi, cc, w);
+    }
+    if (bottom) {
+      rk_update<KIND>(kk.ZV0, zade[0], un.sz[0], out.sz[0], acc.sz[0], szi, cc, w);
+      rk_update<KIND>(kk.ZV1, zade[1], un.sz[1], out.sz[1], acc.sz[1], szi, cc, w);
+      rk_update<KIND>(kk.ZE0, zade[2], un.sz[2], out.sz[2], acc.sz[2], szi, cc, w);
+      rk_update<KIND>(kk.ZE1, zade[3], un.sz[3], out.sz[3], acc.sz[3], szi, cc, w);
+    }
+  };
+#pragma unroll 1
+  for (int k = 0; k < tr / kTileRowStep; ++k) {
+    if (z0 + ty + k * kTileRowStep >= z1) return;
+    if (general)
+      cell(std::true_type{}, k);
+    else
+      cell(std::false_type{}, k);
+  }
+}
+
+template <int DIR, int KIND, bool CPML>
+__global__ void __launch_bounds__(kTileThreads, MFDM_TILE_MIN_BLOCKS)
+    stage_kernel_tile(Coef C0, Fields in0, Fields out0, Fields un0, Fields acc0, int s, float cc,
+                      float w, int ntx, int nbi, int nbf, int tr, int nshots) {
+  __shared__ __align__(16) float tile[kTileHMax * 5 * kTileW];
+  const int shot = int(blockIdx.x % unsigned(nshots));
+  const int b = int(blockIdx.x / unsigned(nshots));
+  const size_t so = size_t(shot) * C0.shot_stride;
+  const Coef C = shot_coef(C0, shot);
+  const Fields in = shot_fields(in0, so), out = shot_fields(out0, so), un = shot_fields(un0, so),
+               acc = shot_fields(acc0, so);
+  if (b < nbi) {
+    interface_strip<DIR, KIND, CPML>(C, in, out, un, acc, cc, w, b);
+  } else if (b < nbi + nbf) {
+    fluid_tile<DIR, KIND, CPML>(C, in, out, un, acc, s, cc, w, b - nbi, ntx, tr, tile);
+  } else {
+    solid_tile<DIR, KIND, CPML>(C, in, out, un, acc, cc, w, b - nbi - nbf, ntx, tr, tile);
+  }
+}
+
+// Tile height of a launch: the segment height rounded up to a multiple of 8,
+// at most 48 (16 by default).
+static int tile_rows_of(const Coef& C) {
+  const int seg = C.seg > 0 ? C.seg : 16;
+  const int tr = (seg + kTileRowStep - 1) / kTileRowStep * kTileRowStep;
+  return tr < kTileRowsMax ? tr : kTileRowsMax;
+}
+
+static void tile_grid_of(int nx, int nzf, int nzs, int tr, int* ntx, int* nbf, int* nbs, int* nbi) {
+  *ntx = (nx + kTileX - 1) / kTileX;
+  const int frows = nzf - 1 - 3;  // fluid rows 3..nz_f-2
+  const int srows = nzs - 4;      // solid rows 1..nz_s-4
+  *nbf = frows > 0 ? *ntx * ((frows + tr - 1) / tr) : 0;
+  *nbs = srows > 0 ? *ntx * ((srows + tr - 1) / tr) : 0;
+  *nbi = (nx + kConsumers - 1) / kConsumers;
+}
+
+template <int DIR, int KIND, bool CPML>
+static cudaError_t launch_tile_one(const Coef& C, const Fields& in, const Fields& out,
+                                   const Fields& un, const Fields& acc, int s, cudaStream_t st) {
+  int ntx, nbf, nbs, nbi;
+  const int nshots = C.nshots > 0 ? C.nshots : 1, tr = tile_rows_of(C);
+  tile_grid_of(C.nx, C.nzf, C.nzs, tr, &ntx, &nbf, &nbs, &nbi);
+  const float cc = C.rk_c[s], w = (KIND == kStageLast) ? 0.f : C.rk_w[s];
+  const unsigned grid = unsigned(nbi + nbf + nbs) * unsigned(nshots);
+  stage_kernel_tile<DIR, KIND, CPML><<<grid, kTileThreads, 0, st>>>(C, in, out, un, acc, s, cc, w,
+                                                                    ntx, nbi, nbf, tr, nshots);
+  return cudaGetLastError();
+}
+
+template <bool CPML>
+static cudaError_t launch_tile_bc(const Coef& C, const Fields& in, const Fields& out,
+                                  const Fields& un, const Fields& acc, int stage, int dir,
+                                  cudaStream_t st) {
+  const int kind = stage == 0 ? kStageFirst : (stage == 3 ? kStageLast : kStageMid);
+  if (dir == kDirF) {
+    if (kind == kStageFirst) return launch_tile_one<kDirF, kStageFirst, CPML>(C, in, out, un, acc, stage, st);
+    if (kind == kStageMid) return launch_tile_one<kDirF, kStageMid, CPML>(C, in, out, un, acc, stage, st);
+    return launch_tile_one<kDirF, kStageLast, CPML>(C, in, out, un, acc, stage, st);
+  }
+  if (kind == kStageFirst) return launch_tile_one<kDirB, kStageFirst, CPML>(C, in, out, un, acc, stage, st);
+  if (kind == kStageMid) return launch_tile_one<kDirB, kStageMid, CPML>(C, in, out, un, acc, stage, st);
+  return launch_tile_one<kDirB, kStageLast, CPML>(C, in, out, un, acc, stage, st);
+}
+
+cudaError_t launch_stage_tile(const Coef& C, const Fields& in, const Fields& out, const Fields& un,
+                              const Fields& acc, int stage, int dir, cudaStream_t st) {
+  return C.cpml ? launch_tile_bc<true>(C, in, out, un, acc, stage, dir, st)
+                : launch_tile_bc<false>(C, in, out, un, acc, stage, dir, st);
+}
+#endif  // MFDM_VARIANT_TU
+
 }  // namespace MFDM_VNS
 
 #ifndef MFDM_VARIANT_TU
@@ -752,7 +1097,7 @@ void stage_grid(int nx, int nzf, int nzs, int seg, int* ntx, int* nbf, int* nbs,
 }
 
 int stage_blocks_per_sm(const Coef& C) {
-  if (C.variant == 2 || C.variant == 3) return C.variant;
+  if (C.variant == 2 || C.variant == 3 || C.variant == 4) return C.variant;
   // large grids stream best with three blocks per SM, small ones fill the GPU
   // better with two (measured at 4096x2048, 2048x1024 and 1200x800)
   const long long cells = (long long)C.nx * (C.nzf + C.nzs) * (C.nshots > 0 ? C.nshots : 1);
@@ -767,8 +1112,10 @@ cudaError_t configure_device() {
 cudaError_t launch_stage(const Coef& C, const Fields& in, const Fields& out, const Fields& un,
                          const Fields& acc, const StageMaps& maps, int stage, int dir,
                          cudaStream_t st) {
-  return stage_blocks_per_sm(C) == 3 ? v3::launch_stage_v(C, in, out, un, acc, maps, stage, dir, st)
-                                     : v2::launch_stage_v(C, in, out, un, acc, maps, stage, dir, st);
+  const int v = stage_blocks_per_sm(C);
+  if (v == 4) return v2::launch_stage_tile(C, in, out, un, acc, stage, dir, st);
+  return v == 3 ? v3::launch_stage_v(C, in, out, un, acc, maps, stage, dir, st)
+                : v2::launch_stage_v(C, in, out, un, acc, maps, stage, dir, st);
 }
 
 cudaError_t launch_finish(const Coef& C, const Fields& U, cudaStream_t st) {

@@ -71,7 +71,7 @@ def test_autotune_picks_a_candidate_and_leaves_rest(lib, cases):
         s.step(10)
         seg = s.autotune()
         assert seg in (8, 12, 16, 24, 32, 48)
-        assert s.info()["blocks_per_sm"] in (2, 3)
+        assert s.info()["blocks_per_sm"] in (2, 3, 4)
         info = s.info()
         assert info["seg_rows"] == seg and info["step"] == 0 and info["nsamples"] == 0
         for n in lib.FIELDS:
@@ -146,11 +146,12 @@ def test_group_with_a_batch_and_timing(lib, cases):
 
 @pytest.mark.parametrize("case", ["curv_small", "cpml_curv_small"])
 def test_stage_builds_agree(lib, cases, case):
-    """The 2- and 3-blocks-per-SM stage builds compute the same stencil; they may
-    contract FMAs differently, so they agree to FP32 rounding."""
+    """The stage builds (TMA rings at 2 and 3 blocks per SM, shared-memory tiles)
+    compute the same stencil on the same staged values; they may contract FMAs
+    differently, so they agree to FP32 rounding."""
     model = getattr(cases, case)()
     out = {}
-    for blocks in (2, 3):
+    for blocks in (2, 3, 4):
         with lib.Solver.from_model(model) as s:
             s.set_blocks_per_sm(blocks)
             s.set_tile(8)
@@ -158,12 +159,13 @@ def test_stage_builds_agree(lib, cases, case):
             s.set_shot(0, reset=True)
             s.step(150)
             out[blocks] = (s.records(), {n: s.field(n) for n in lib.FIELDS})
-    for q in out[2][0]:
-        assert rel_l2(out[3][0][q], out[2][0][q]) <= 1e-6, q
-    for n in lib.FIELDS:
-        assert rel_l2(out[3][1][n], out[2][1][n]) <= 1e-6, n
+    for b in (3, 4):
+        for q in out[2][0]:
+            assert rel_l2(out[b][0][q], out[2][0][q]) <= 1e-6, (b, q)
+        for n in lib.FIELDS:
+            assert rel_l2(out[b][1][n], out[2][1][n]) <= 1e-6, (b, n)
     with lib.Solver.from_model(model) as s:
         with pytest.raises(lib.MfdmError):
-            s.set_blocks_per_sm(4)
+            s.set_blocks_per_sm(5)
         s.set_blocks_per_sm(0)
         assert s.info()["blocks_per_sm"] == 2  # a small grid: two blocks per SM
