@@ -451,9 +451,14 @@ def main():
     t0 = time.perf_counter()
     solver.load_model(host_model)
     solver.set_shot(0, reset=True)
+    t1 = time.perf_counter()
     solver.step(args.steps)
+    t2 = time.perf_counter()
     rec = solver.records()
-    e2e_s = time.perf_counter() - t0
+    t3 = time.perf_counter()
+    e2e_s = t3 - t0
+    e2e_parts = {"upload_s": round(t1 - t0, 4), "steps_s": round(t2 - t1, 4),
+                 "records_s": round(t3 - t2, 4)}
     e2e_s = max_over_ranks(dist, e2e_s, local)
     d2h = sum(a.nbytes for a in rec.values())
     e2e = world * model.cells * args.steps / e2e_s / 1e9
@@ -503,7 +508,7 @@ def main():
             "gpu_launches": 5 * args.steps,
             "e2e": {"value": round(e2e, 3), "unit": "Gcell/s",
                     "h2d_bytes_per_step": int(h2d // args.steps),
-                    "d2h_bytes_per_step": int(d2h // args.steps)},
+                    "d2h_bytes_per_step": int(d2h // args.steps), **e2e_parts},
             "cpu_baseline": cpu,
             "clocks": clocks,
             "other_workloads": other,

@@ -384,6 +384,9 @@ __global__ void __launch_bounds__(128) k_grad_cells(Coef C, SetLayout L, Fields 
   if (row < nfr) {
     const int iz = 3 + row;
     const size_t g = (size_t)iz * P + ix;
+    // the accumulated gradients first: their loads must not wait for a store
+    // (the pointers may alias as far as the compiler knows)
+    const double grf = G.rf[g], gK = G.K[g];
     float ade[4] = {0.f, 0.f, 0.f, 0.f}, zade[4] = {0.f, 0.f, 0.f, 0.f};
     if (side)
       for (int q = 0; q < 4; ++q) ade[q] = __ldg(Y.fx[q] + (size_t)iz * C.Ps + scol);
@@ -395,8 +398,8 @@ __global__ void __launch_bounds__(128) k_grad_cells(Coef C, SetLayout L, Fields 
     FluidGlobal A{Y.fvx, Y.fvz, Y.fp, g, P};
     const FluidK o = fluid_rhs<DIR, false, CPML>(C, A, iz, ix, side, ade, cf, top, zade);
     // velocity terms carry 1/rho, the pressure term K
-    G.rf[g] += double(__ldg(KB.fvx + g)) * o.vx + double(__ldg(KB.fvz + g)) * o.vz;
-    G.K[g] += double(__ldg(KB.fp + g)) * o.p;
+    G.rf[g] = grf + (double(__ldg(KB.fvx + g)) * o.vx + double(__ldg(KB.fvz + g)) * o.vz);
+    G.K[g] = gK + double(__ldg(KB.fp + g)) * o.p;
     if (qx) q_fluid(C, L, kb, qx, qz, iz, ix, false);
     return;
   }
@@ -405,6 +408,7 @@ __global__ void __launch_bounds__(128) k_grad_cells(Coef C, SetLayout L, Fields 
   const size_t m = (size_t)iz * P + ix, g = m + (size_t)(nzf - 1) * P;
   const int zb0 = nzs - 3 - npd;
   const bool bottom = iz >= zb0;
+  const double gc11 = G.c11[m], gc33 = G.c33[m], gc55 = G.c55[m], grs = G.rs[m], gc13 = G.c13[m];
   float xade[4] = {0.f, 0.f, 0.f, 0.f}, zade[4] = {0.f, 0.f, 0.f, 0.f};
   if (side)
     for (int q = 0; q < 4; ++q) xade[q] = __ldg(Y.sx[q] + (size_t)iz * C.Ps + scol);
@@ -420,11 +424,11 @@ __global__ void __launch_bounds__(128) k_grad_cells(Coef C, SetLayout L, Fields 
                                                 SolidCoefs{xix, xiz, zex, zez, 1.f, 1.f, 0.f, 1.f, 1.f});
   const SolidK o2 = solid_rhs<DIR, false, CPML>(C, A, iz, ix, side, bottom, xade, zade,
                                                 SolidCoefs{xix, xiz, zex, zez, 0.f, 0.f, 1.f, 0.f, 0.f});
-  G.c11[m] += ksx * o1.sx;
-  G.c33[m] += ksz * o1.sz;
-  G.c55[m] += ksxz * o1.sxz;
-  G.rs[m] += kvx * o1.vx + kvz * o1.vz;
-  G.c13[m] += ksx * o2.sx + ksz * o2.sz;
+  G.c11[m] = gc11 + ksx * o1.sx;
+  G.c33[m] = gc33 + ksz * o1.sz;
+  G.c55[m] = gc55 + ksxz * o1.sxz;
+  G.rs[m] = grs + (kvx * o1.vx + kvz * o1.vz);
+  G.c13[m] = gc13 + (ksx * o2.sx + ksz * o2.sz);
   if (qx) q_solid<CPML>(C, L, kb, qx, qz, iz, ix, false);
 }
 
@@ -516,6 +520,10 @@ __global__ void k_reverse_h(const float* __restrict__ t, const float* __restrict
   const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (j >= L.len) return;
   float y = t[j];
+  // the RK operands first: their loads must not wait for a store
+  const float lam0 = MODE == 0 ? 0.f : y_or_lam[j];
+  const bool mk = MODE == 0 ? false : mask[j] != 0;
+  const float mu0 = MODE == 2 ? mu[j] : 0.f;
   {
     // the fluid block (3 arrays of nz_f rows) and the solid block (5 of nz_s)
     // are contiguous at pitch P
@@ -539,18 +547,18 @@ __global__ void k_reverse_h(const float* __restrict__ t, const float* __restrict
     y_or_lam[j] = y;
     return;
   }
-  const float m = mask[j] ? 1.0f : 0.0f;
+  const float m = mk ? 1.0f : 0.0f;
   if (MODE == 1) {
-    const float l = y_or_lam[j] + y;
+    const float l = lam0 + y;
     y_or_lam[j] = l;
     if (kbn) {
       mu[j] = l;
-      kbn[j] = mask[j] ? w * l : 0.0f;
+      kbn[j] = mk ? w * l : 0.0f;
     }
     return;
   }
-  y_or_lam[j] += m * y;
-  if (MODE == 2) kbn[j] = m * fmaf(cw, y, w * mu[j]);
+  y_or_lam[j] = lam0 + m * y;
+  if (MODE == 2) kbn[j] = m * fmaf(cw, y, w * mu0);
 }
 
 // The CSR part of L^T x on the rows that have entries, kLanes threads per row:
@@ -700,7 +708,7 @@ static cudaError_t hybrid_t(const HybridT& H, const Coef& C, const SetLayout& L,
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
-  if (H.nrows > 0) {
+  if (H.nrows > 0 && !q_ready) {  // else formed by sparse_rows()
     k_rows_csr<<<unsigned((H.nrows * kLanes + kBlock - 1) / kBlock), kBlock, 0, st>>>(
         H.nzrow, H.rest.rowptr, H.rest.col, H.rest.val, kb, H.nrows, H.t);
     const cudaError_t e = cudaGetLastError();
@@ -717,6 +725,13 @@ static cudaError_t hybrid_dir(const HybridT& H, const Coef& C, const SetLayout& 
                               float* mu, float w, float c, bool q_ready, cudaStream_t st) {
   return dir == kDirF ? hybrid_t<kDirF, MODE>(H, C, L, kb, out, mask, kbn, mu, w, c, q_ready, st)
                       : hybrid_t<kDirB, MODE>(H, C, L, kb, out, mask, kbn, mu, w, c, q_ready, st);
+}
+
+cudaError_t sparse_rows(const HybridT& H, const float* kb, cudaStream_t st) {
+  if (H.nrows <= 0) return cudaSuccess;
+  k_rows_csr<<<unsigned((H.nrows * kLanes + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+      H.nzrow, H.rest.rowptr, H.rest.col, H.rest.val, kb, H.nrows, H.t);
+  return cudaGetLastError();
 }
 
 cudaError_t reverse_stage(const HybridT& H, const Coef& C, const SetLayout& L, int dir,

@@ -100,7 +100,11 @@ cudaError_t drop_interior(const CsrT& full, const SetLayout& L, CsrT* rest,
 // One reverse stage: y = L^T kb, lam += (mask_lam ? M : 1) y and, when kbn is
 // given, kbn = M (w mu + c y); without mask_lam (the step's last stage) and
 // with kbn, it also starts the next transposed step: mu = lam, kbn = w M lam.
-// q_ready: the Q fields of kb are already in H (written by gradient()).
+// q_ready: the Q fields of kb (written by gradient()) and its sparse rows
+// (sparse_rows()) are already in H.
+// The sparse rows of L^T kb into H.t (the rows listed in H.nzrow), so that a
+// stream other than the gradient's can form them concurrently.
+cudaError_t sparse_rows(const HybridT& H, const float* kb, cudaStream_t st);
 cudaError_t reverse_stage(const HybridT& H, const Coef& C, const SetLayout& L, int dir,
                           const float* kb, float* lam, const uint8_t* mask, bool mask_lam,
                           float* kbn, float* mu, float w, float c, bool q_ready,

@@ -170,6 +170,9 @@ struct AdjointState {
   void* scan_tmp = nullptr;
   size_t scan_bytes = 0;
   bool built = false;
+  // a second stream forms each stage's sparse rows while the gradient runs
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_kb = nullptr, ev_rows = nullptr;
   int nsteps = -1, every = 0;  // the forward run a backward pass may follow
   double build_ms = 0.0;       // operator assembly time (host clock)
   ~AdjointState() {
@@ -186,6 +189,9 @@ struct AdjointState {
     cudaFree(tmp); cudaFree(grad); cudaFree(ckpt); cudaFree(seg); cudaFree(res); cudaFree(keep);
     cudaFree(inner);
     cudaFree(scan_tmp);
+    if (ev_kb) cudaEventDestroy(ev_kb);
+    if (ev_rows) cudaEventDestroy(ev_rows);
+    if (side) cudaStreamDestroy(side);
   }
 };
 
@@ -1543,6 +1549,9 @@ int adjoint_prepare(mfdm_model* m) {
     // Q fields off the interior set are never written and must stay 0
     MFDM_CU(cudaMemset(a->H[0].qx, 0, n * sizeof(float)));
     MFDM_CU(cudaMemset(a->H[0].qz, 0, n * sizeof(float)));
+    MFDM_CU(cudaStreamCreateWithFlags(&a->side, cudaStreamNonBlocking));
+    MFDM_CU(cudaEventCreateWithFlags(&a->ev_kb, cudaEventDisableTiming));
+    MFDM_CU(cudaEventCreateWithFlags(&a->ev_rows, cudaEventDisableTiming));
   }
   if (!m->adj->built) return adjoint_build(m);
   return MFDM_OK;
@@ -1629,16 +1638,24 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
   // mu = F^T lam and kb = c3 M mu: off the interface rows both were formed by
   // the previous transposed step's last stage (zero before the first)
   MFDM_CU(mfdm::adj::filter_t(a->lam, L, C, a->tmp, st, a->mu, a->kb[0], a->mask, c[3]));
-  // each stage: gradient (which also forms the Q fields of kb), then L^T kb
-  MFDM_CU(mfdm::adj::gradient(C, L, Y[3], a->kb[0], g, d1, &a->H[d1], st));
-  MFDM_CU(mfdm::adj::reverse_stage(a->H[d1], C, L, d1, a->kb[0], a->lam, a->mask, true, a->kb[1], a->mu, w[2], c[2], true, st));
-  MFDM_CU(mfdm::adj::gradient(C, L, Y[2], a->kb[1], g, d0, &a->H[d0], st));
-  MFDM_CU(mfdm::adj::reverse_stage(a->H[d0], C, L, d0, a->kb[1], a->lam, a->mask, true, a->kb[0], a->mu, w[1], c[1], true, st));
-  MFDM_CU(mfdm::adj::gradient(C, L, Y[1], a->kb[0], g, d1, &a->H[d1], st));
-  MFDM_CU(mfdm::adj::reverse_stage(a->H[d1], C, L, d1, a->kb[0], a->lam, a->mask, true, a->kb[1], a->mu, w[0], c[0], true, st));
-  MFDM_CU(mfdm::adj::gradient(C, L, Y[0], a->kb[1], g, d0, &a->H[d0], st));
-  MFDM_CU(mfdm::adj::reverse_stage(a->H[d0], C, L, d0, a->kb[1], a->lam, a->mask, false, a->kb[0], a->mu, c[3], 0.f, true, st));
-  return MFDM_OK;
+  // each stage: the sparse rows of L^T kb on the side stream, concurrently
+  // with the gradient (which also forms the Q fields of kb); then L^T kb
+  auto stage = [&](int d, int sy, int kin, bool mask_lam, float ws, float cs) -> int {
+    MFDM_CU(cudaEventRecord(a->ev_kb, st));  // kb[kin] is complete
+    MFDM_CU(cudaStreamWaitEvent(a->side, a->ev_kb, 0));
+    MFDM_CU(mfdm::adj::sparse_rows(a->H[d], a->kb[kin], a->side));
+    MFDM_CU(cudaEventRecord(a->ev_rows, a->side));
+    MFDM_CU(mfdm::adj::gradient(C, L, Y[sy], a->kb[kin], g, d, &a->H[d], st));
+    MFDM_CU(cudaStreamWaitEvent(st, a->ev_rows, 0));
+    MFDM_CU(mfdm::adj::reverse_stage(a->H[d], C, L, d, a->kb[kin], a->lam, a->mask, mask_lam,
+                                     a->kb[1 - kin], a->mu, ws, cs, true, st));
+    return MFDM_OK;
+  };
+  int rc;
+  if ((rc = stage(d1, 3, 0, true, w[2], c[2])) != MFDM_OK) return rc;
+  if ((rc = stage(d0, 2, 1, true, w[1], c[1])) != MFDM_OK) return rc;
+  if ((rc = stage(d1, 1, 0, true, w[0], c[0])) != MFDM_OK) return rc;
+  return stage(d0, 0, 1, false, c[3], 0.f);
 }
 
 }  // namespace
