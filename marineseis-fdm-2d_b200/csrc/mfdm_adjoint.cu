@@ -727,6 +727,14 @@ static cudaError_t hybrid_dir(const HybridT& H, const Coef& C, const SetLayout& 
                       : hybrid_t<kDirB, MODE>(H, C, L, kb, out, mask, kbn, mu, w, c, q_ready, st);
 }
 
+cudaError_t q_fields(const HybridT& H, const Coef& C, const SetLayout& L, const float* kb,
+                     cudaStream_t st) {
+  const dim3 gq(unsigned((L.nx + 127) / 128), unsigned(L.nzf + L.nzs));
+  if (L.cpml) k_qfields<true><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz);
+  else k_qfields<false><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz);
+  return cudaGetLastError();
+}
+
 cudaError_t sparse_rows(const HybridT& H, const float* kb, cudaStream_t st) {
   if (H.nrows <= 0) return cudaSuccess;
   k_rows_csr<<<unsigned((H.nrows * kLanes + kBlock - 1) / kBlock), kBlock, 0, st>>>(

@@ -105,6 +105,9 @@ cudaError_t drop_interior(const CsrT& full, const SetLayout& L, CsrT* rest,
 // The sparse rows of L^T kb into H.t (the rows listed in H.nzrow), so that a
 // stream other than the gradient's can form them concurrently.
 cudaError_t sparse_rows(const HybridT& H, const float* kb, cudaStream_t st);
+// The Q fields of kb into H.qx / H.qz (0 off the interior cells).
+cudaError_t q_fields(const HybridT& H, const Coef& C, const SetLayout& L, const float* kb,
+                     cudaStream_t st);
 cudaError_t reverse_stage(const HybridT& H, const Coef& C, const SetLayout& L, int dir,
                           const float* kb, float* lam, const uint8_t* mask, bool mask_lam,
                           float* kbn, float* mu, float w, float c, bool q_ready,

@@ -170,9 +170,10 @@ struct AdjointState {
   void* scan_tmp = nullptr;
   size_t scan_bytes = 0;
   bool built = false;
-  // a second stream forms each stage's sparse rows while the gradient runs
-  cudaStream_t side = nullptr;
-  cudaEvent_t ev_kb = nullptr, ev_rows = nullptr;
+  // side streams: each stage's sparse rows of L^T kb, and its material-gradient
+  // accumulation (which nothing in the transposed chain waits for)
+  cudaStream_t side = nullptr, side_g = nullptr;
+  cudaEvent_t ev_kb = nullptr, ev_rows = nullptr, ev_g[2] = {nullptr, nullptr};
   int nsteps = -1, every = 0;  // the forward run a backward pass may follow
   double build_ms = 0.0;       // operator assembly time (host clock)
   ~AdjointState() {
@@ -191,7 +192,10 @@ struct AdjointState {
     cudaFree(scan_tmp);
     if (ev_kb) cudaEventDestroy(ev_kb);
     if (ev_rows) cudaEventDestroy(ev_rows);
+    for (cudaEvent_t e : ev_g)
+      if (e) cudaEventDestroy(e);
     if (side) cudaStreamDestroy(side);
+    if (side_g) cudaStreamDestroy(side_g);
   }
 };
 
@@ -1550,8 +1554,10 @@ int adjoint_prepare(mfdm_model* m) {
     MFDM_CU(cudaMemset(a->H[0].qx, 0, n * sizeof(float)));
     MFDM_CU(cudaMemset(a->H[0].qz, 0, n * sizeof(float)));
     MFDM_CU(cudaStreamCreateWithFlags(&a->side, cudaStreamNonBlocking));
+    MFDM_CU(cudaStreamCreateWithFlags(&a->side_g, cudaStreamNonBlocking));
     MFDM_CU(cudaEventCreateWithFlags(&a->ev_kb, cudaEventDisableTiming));
     MFDM_CU(cudaEventCreateWithFlags(&a->ev_rows, cudaEventDisableTiming));
+    for (cudaEvent_t& e : a->ev_g) MFDM_CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
   if (!m->adj->built) return adjoint_build(m);
   return MFDM_OK;
@@ -1638,15 +1644,22 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
   // mu = F^T lam and kb = c3 M mu: off the interface rows both were formed by
   // the previous transposed step's last stage (zero before the first)
   MFDM_CU(mfdm::adj::filter_t(a->lam, L, C, a->tmp, st, a->mu, a->kb[0], a->mask, c[3]));
-  // each stage: the sparse rows of L^T kb on the side stream, concurrently
-  // with the gradient (which also forms the Q fields of kb); then L^T kb
+  // Each stage: once kb[kin] is complete, its sparse rows of L^T kb (side
+  // stream) and its material-gradient accumulation (side_g) run beside the Q
+  // fields and the transposed product on the main stream. The product writes
+  // kb[1 - kin], which the previous stage's gradient reads: it waits for that
+  // gradient (ev_g[1 - kin]; a never-recorded event is no wait).
   auto stage = [&](int d, int sy, int kin, bool mask_lam, float ws, float cs) -> int {
-    MFDM_CU(cudaEventRecord(a->ev_kb, st));  // kb[kin] is complete
+    MFDM_CU(cudaEventRecord(a->ev_kb, st));
     MFDM_CU(cudaStreamWaitEvent(a->side, a->ev_kb, 0));
     MFDM_CU(mfdm::adj::sparse_rows(a->H[d], a->kb[kin], a->side));
     MFDM_CU(cudaEventRecord(a->ev_rows, a->side));
-    MFDM_CU(mfdm::adj::gradient(C, L, Y[sy], a->kb[kin], g, d, &a->H[d], st));
+    MFDM_CU(cudaStreamWaitEvent(a->side_g, a->ev_kb, 0));
+    MFDM_CU(mfdm::adj::gradient(C, L, Y[sy], a->kb[kin], g, d, nullptr, a->side_g));
+    MFDM_CU(cudaEventRecord(a->ev_g[kin], a->side_g));
+    MFDM_CU(mfdm::adj::q_fields(a->H[d], C, L, a->kb[kin], st));
     MFDM_CU(cudaStreamWaitEvent(st, a->ev_rows, 0));
+    MFDM_CU(cudaStreamWaitEvent(st, a->ev_g[1 - kin], 0));
     MFDM_CU(mfdm::adj::reverse_stage(a->H[d], C, L, d, a->kb[kin], a->lam, a->mask, mask_lam,
                                      a->kb[1 - kin], a->mu, ws, cs, true, st));
     return MFDM_OK;
@@ -1655,7 +1668,10 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
   if ((rc = stage(d1, 3, 0, true, w[2], c[2])) != MFDM_OK) return rc;
   if ((rc = stage(d0, 2, 1, true, w[1], c[1])) != MFDM_OK) return rc;
   if ((rc = stage(d1, 1, 0, true, w[0], c[0])) != MFDM_OK) return rc;
-  return stage(d0, 0, 1, false, c[3], 0.f);
+  if ((rc = stage(d0, 0, 1, false, c[3], 0.f)) != MFDM_OK) return rc;
+  // the step's stage inputs and kb are not reused before its last gradient ends
+  MFDM_CU(cudaStreamWaitEvent(st, a->ev_g[1], 0));
+  return MFDM_OK;
 }
 
 }  // namespace
