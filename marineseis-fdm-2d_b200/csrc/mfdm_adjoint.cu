@@ -150,12 +150,24 @@ __global__ void k_sort_rows(const long long* __restrict__ rowptr, int* col, floa
 }
 
 // Row sums of L^T x by groups of kLanes threads (coalesced along each row).
+// Each lane loads four of its entries (and their x) before accumulating them,
+// in the same order as one at a time, so four gathers are in flight per lane.
 __device__ __forceinline__ float row_dot(const long long* __restrict__ rowptr,
                                          const int* __restrict__ col, const float* __restrict__ val,
                                          const float* __restrict__ x, long long row, int lane) {
   float s = 0.0f;
   const long long e = rowptr[row + 1];
-  for (long long k = rowptr[row] + lane; k < e; k += kLanes) s = fmaf(val[k], __ldg(x + col[k]), s);
+  long long k = rowptr[row] + lane;
+  for (; k + 3 * kLanes < e; k += 4 * kLanes) {
+    const int c0 = col[k], c1 = col[k + kLanes], c2 = col[k + 2 * kLanes], c3 = col[k + 3 * kLanes];
+    const float v0 = val[k], v1 = val[k + kLanes], v2 = val[k + 2 * kLanes], v3 = val[k + 3 * kLanes];
+    const float x0 = __ldg(x + c0), x1 = __ldg(x + c1), x2 = __ldg(x + c2), x3 = __ldg(x + c3);
+    s = fmaf(v0, x0, s);
+    s = fmaf(v1, x1, s);
+    s = fmaf(v2, x2, s);
+    s = fmaf(v3, x3, s);
+  }
+  for (; k < e; k += kLanes) s = fmaf(val[k], __ldg(x + col[k]), s);
   const unsigned grp = 0xFFu << (threadIdx.x & 24);
 #pragma unroll
   for (int o = kLanes / 2; o > 0; o >>= 1) s += __shfl_xor_sync(grp, s, o);
@@ -344,13 +356,14 @@ __device__ __forceinline__ void q_solid(const Coef& C, const SetLayout& L, const
   }
 }
 
-template <bool CPML>
+// ZERO: also write the zeros off the interior cells (a fresh Q buffer).
+template <bool CPML, bool ZERO = true>
 __global__ void k_qfields(Coef C, SetLayout L, const float* __restrict__ x, float* qx, float* qz) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int row = blockIdx.y;
   if (c >= L.nx) return;
-  if (row < L.nzf) q_fluid(C, L, x, qx, qz, row, c, true);
-  else q_solid<CPML>(C, L, x, qx, qz, row - L.nzf, c, true);
+  if (row < L.nzf) q_fluid(C, L, x, qx, qz, row, c, ZERO);
+  else q_solid<CPML>(C, L, x, qx, qz, row - L.nzf, c, ZERO);
 }
 
 // ---- material gradients ----------------------------------------------------------
@@ -729,9 +742,10 @@ static cudaError_t hybrid_dir(const HybridT& H, const Coef& C, const SetLayout& 
 
 cudaError_t q_fields(const HybridT& H, const Coef& C, const SetLayout& L, const float* kb,
                      cudaStream_t st) {
+  // off the interior cells the Q buffers hold the zeros written when allocated
   const dim3 gq(unsigned((L.nx + 127) / 128), unsigned(L.nzf + L.nzs));
-  if (L.cpml) k_qfields<true><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz);
-  else k_qfields<false><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz);
+  if (L.cpml) k_qfields<true, false><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz);
+  else k_qfields<false, false><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz);
   return cudaGetLastError();
 }
 
