@@ -351,7 +351,7 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="only the warm-up and timed steps (a short launch list for ncu)")
     ap.add_argument("--blocks-per-sm", type=int, default=0, choices=[0, 2, 3, 4],
-                    help="stage kernel build (0: picked by grid size, as for any model)")
+                    help="stage kernel build (0: the default, as for any model)")
     ap.add_argument("--adjoint-profile", action="store_true",
                     help="only a short adjoint run on the 800x400 model (16 steps, checkpoint "
                          "every 8, seeded residuals): a launch list of the adjoint kernels for ncu")

@@ -182,8 +182,9 @@ int mfdm_batch_get_field(mfdm_model* m, int shot, int field, float* host);
  * fixed 16x16 blocks (src/pml_fs_kernels.cu:533-622) and has no tuner. */
 
 /* Sets the segment height: a multiple of 4 in [4, 128], or 0 for the default
- * (24; the tile build, mfdm_set_blocks_per_sm 4, rounds it up to a multiple of
- * 8 and caps it at 48, 16 by default). Results do not depend on it beyond FP32
+ * (24 from 6 M cells per launch, counting every shot of a batch, 8 below; the
+ * tile build, mfdm_set_blocks_per_sm 4, rounds it up to a multiple of 8 and
+ * caps it at 48, 16 by default). Results do not depend on it beyond FP32
  * rounding of the last bit. */
 int mfdm_set_tile(mfdm_model* m, int seg_rows);
 
@@ -192,8 +193,8 @@ int mfdm_set_tile(mfdm_model* m, int seg_rows);
  * SM: faster on large grids, slower on small ones); 4: the tile build (no
  * rings: 256-thread blocks stage 32 x 16 cells and their halo in shared
  * memory with plain loads while the point-wise operands of each thread's
- * first row are already in flight); 0 (default) picks by grid size (3 from
- * 6 M cells per launch). Results agree to FP32 rounding. */
+ * first row are already in flight); 0 (default): the 3-block build. Results
+ * agree to FP32 rounding. */
 int mfdm_set_blocks_per_sm(mfdm_model* m, int blocks);
 
 /* Times every candidate segment height with both ring builds (2 and 3 blocks

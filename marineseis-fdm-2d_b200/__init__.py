@@ -346,8 +346,8 @@ class Solver:
         _check(self._lib.mfdm_set_tile(self._h, int(seg_rows)))
 
     def set_blocks_per_sm(self, blocks: int):
-        """Stage kernel build: 2 or 3 resident blocks per SM (TMA rings), 4 (tiles), 0 by grid
-        size (mfdm_set_blocks_per_sm)."""
+        """Stage kernel build: 2 or 3 resident blocks per SM (TMA rings), 4 (tiles), 0 the
+        default 3 (mfdm_set_blocks_per_sm)."""
         _check(self._lib.mfdm_set_blocks_per_sm(self._h, int(blocks)))
 
     def autotune(self) -> int:

@@ -1165,7 +1165,7 @@ int mfdm_autotune(mfdm_model* m, int* seg_rows) {
 int mfdm_set_blocks_per_sm(mfdm_model* m, int blocks) {
   if (!m) return fail(MFDM_ERR_ARG, "null handle");
   if (blocks != 0 && blocks != 2 && blocks != 3 && blocks != 4)
-    return fail(MFDM_ERR_ARG, "stage build must be 2, 3 (blocks per SM), 4 (tiles) or 0 (by grid size)");
+    return fail(MFDM_ERR_ARG, "stage build must be 2, 3 (blocks per SM), 4 (tiles) or 0 (the default)");
   DeviceGuard g(m->device);
   MFDM_CU(cudaStreamSynchronize(m->stream));
   m->C.variant = blocks;

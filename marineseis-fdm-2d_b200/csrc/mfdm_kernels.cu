@@ -64,7 +64,6 @@ constexpr int kNP = MFDM_PW_SLOTS;        // point-wise chunk slots
 constexpr int kRing = kR * kNS;          // ring rows
 constexpr int kConsumers = 256;          // warps 0-7
 constexpr int kThreads = kConsumers + 32;  // + producer warp
-constexpr int kSeg = 24;                 // default rows per segment block
 constexpr int kBarBytes = 256;           // full/empty barriers of both rings
 
 
@@ -569,7 +568,7 @@ static size_t smem_for_kind() {
 
 size_t smem_bytes() { return smem_for_kind<kStageMid>(); }
 
-static int seg_rows_of(const Coef& C) { return C.seg > 0 ? C.seg : kSeg; }
+static int seg_rows_of(const Coef& C) { return C.seg > 0 ? C.seg : default_seg_rows(C); }
 
 static void grid_of(int nx, int nzf, int nzs, int seg, int* ntx, int* nbf, int* nbs, int* nbi) {
   *ntx = (nx + kTX - 1) / kTX;
@@ -1090,7 +1089,7 @@ __global__ void set_step_kernel(int* step, unsigned* done, int it) {
 
 size_t stage_smem_bytes() { return v2::smem_bytes(); }
 
-int stage_seg_rows(const Coef& C) { return C.seg > 0 ? C.seg : v2::kSeg; }
+int stage_seg_rows(const Coef& C) { return C.seg > 0 ? C.seg : default_seg_rows(C); }
 
 void stage_grid(int nx, int nzf, int nzs, int seg, int* ntx, int* nbf, int* nbs, int* nbi) {
   v2::grid_of(nx, nzf, nzs, seg, ntx, nbf, nbs, nbi);
@@ -1098,10 +1097,9 @@ void stage_grid(int nx, int nzf, int nzs, int seg, int* ntx, int* nbf, int* nbs,
 
 int stage_blocks_per_sm(const Coef& C) {
   if (C.variant == 2 || C.variant == 3 || C.variant == 4) return C.variant;
-  // large grids stream best with three blocks per SM, small ones fill the GPU
-  // better with two (measured at 4096x2048, 2048x1024 and 1200x800)
-  const long long cells = (long long)C.nx * (C.nzf + C.nzs) * (C.nshots > 0 ? C.nshots : 1);
-  return cells >= 6000000LL ? 3 : 2;
+  // with the default segment heights the 3-block build is the fastest at
+  // 4096x2048 (24 rows), 2048x1024 and 1200x800 (8 rows)
+  return 3;
 }
 
 cudaError_t configure_device() {

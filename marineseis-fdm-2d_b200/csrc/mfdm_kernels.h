@@ -23,10 +23,17 @@ cudaError_t launch_reciprocal(float* a, int rows, int nx, int P, cudaStream_t st
 cudaError_t launch_set_step(const Coef& C, int it, cudaStream_t st);
 // Dynamic shared memory of one stage block.
 size_t stage_smem_bytes();
-// Resident stage blocks per SM of the build a launch uses: C.variant (2 or 3),
-// or by grid size when 0 (three from 6 M cells per launch).
+// The stage build a launch uses: C.variant (2 or 3 resident ring blocks per SM,
+// 4 the tile build), or the 3-block ring build when 0.
 int stage_blocks_per_sm(const Coef& C);
-// Rows per segment block of a stage launch (C.seg, or the default 24 when unset).
+// Default rows per segment block when C.seg is unset: 24 from 6 M cells per
+// launch (fewer halo rows re-read), 8 below (more blocks than SMs on smaller
+// grids); the autotuner's picks at 4096x2048, 2048x1024 and 1200x800.
+inline int default_seg_rows(const Coef& C) {
+  const long long cells = (long long)C.nx * (C.nzf + C.nzs) * (C.nshots > 0 ? C.nshots : 1);
+  return cells >= 6000000LL ? 24 : 8;
+}
+// Rows per segment block of a stage launch (C.seg, or the default when unset).
 int stage_seg_rows(const Coef& C);
 // Block counts of one stage launch (per shot) with `seg` rows per segment:
 // column tiles, fluid tiles, solid tiles, interface blocks.

@@ -45,8 +45,8 @@ def rel_l2(a, b):
 def test_segment_heights_agree(lib, cases, case):
     model = getattr(cases, case)()
     rec0, f0, info0 = run(lib, model, 150)
-    assert info0["seg_rows"] == 24
-    for seg in (4, 8, 12, 48, 128):
+    assert info0["seg_rows"] == 8  # the default below 6 M cells per launch
+    for seg in (4, 12, 24, 48, 128):
         rec, f, info = run(lib, model, 150, seg=seg)
         assert info["seg_rows"] == seg
         for q in rec0:
@@ -61,7 +61,7 @@ def test_set_tile_rejects_bad_heights(lib, cases):
             with pytest.raises(lib.MfdmError):
                 s.set_tile(bad)
         s.set_tile(0)
-        assert s.info()["seg_rows"] == 24
+        assert s.info()["seg_rows"] == 8
 
 
 def test_autotune_picks_a_candidate_and_leaves_rest(lib, cases):
@@ -168,4 +168,4 @@ def test_stage_builds_agree(lib, cases, case):
         with pytest.raises(lib.MfdmError):
             s.set_blocks_per_sm(5)
         s.set_blocks_per_sm(0)
-        assert s.info()["blocks_per_sm"] == 2  # a small grid: two blocks per SM
+        assert s.info()["blocks_per_sm"] == 3  # the default build
