@@ -9,7 +9,11 @@ namespace mfdm {
 namespace adj {
 namespace {
 
-constexpr int kLanes = 8;  // threads per CSR row in the transposed products
+#ifndef MFDM_CSR_LANES
+#define MFDM_CSR_LANES 2
+#endif
+constexpr int kLanes = MFDM_CSR_LANES;  // threads per CSR row in the transposed products
+static_assert(kLanes == 1 || kLanes == 2 || kLanes == 4 || kLanes == 8 || kLanes == 16, "lanes per CSR row");
 constexpr int kBlock = 256;
 
 __device__ __forceinline__ int strip_to_col(int s, int nx, int npd) {
@@ -168,7 +172,7 @@ __device__ __forceinline__ float row_dot(const long long* __restrict__ rowptr,
     s = fmaf(v3, x3, s);
   }
   for (; k < e; k += kLanes) s = fmaf(val[k], __ldg(x + col[k]), s);
-  const unsigned grp = 0xFFu << (threadIdx.x & 24);
+  const unsigned grp = ((1u << kLanes) - 1u) << (threadIdx.x & (32 - kLanes));
 #pragma unroll
   for (int o = kLanes / 2; o > 0; o >>= 1) s += __shfl_xor_sync(grp, s, o);
   return s;

@@ -170,10 +170,13 @@ struct AdjointState {
   void* scan_tmp = nullptr;
   size_t scan_bytes = 0;
   bool built = false;
-  // side streams: each stage's sparse rows of L^T kb, and its material-gradient
-  // accumulation (which nothing in the transposed chain waits for)
-  cudaStream_t side = nullptr, side_g = nullptr;
+  // Streams of the backward steps: `hi` runs the transposed chain and `side`
+  // each stage's sparse rows of L^T kb, both at the highest priority; `side_g`
+  // the material-gradient accumulation (which nothing in the chain waits for)
+  // at the lowest, so its blocks take only the SMs the chain leaves idle.
+  cudaStream_t hi = nullptr, side = nullptr, side_g = nullptr;
   cudaEvent_t ev_kb = nullptr, ev_rows = nullptr, ev_g[2] = {nullptr, nullptr};
+  cudaEvent_t ev_enter = nullptr, ev_leave = nullptr;
   int nsteps = -1, every = 0;  // the forward run a backward pass may follow
   double build_ms = 0.0;       // operator assembly time (host clock)
   ~AdjointState() {
@@ -192,6 +195,9 @@ struct AdjointState {
     cudaFree(scan_tmp);
     if (ev_kb) cudaEventDestroy(ev_kb);
     if (ev_rows) cudaEventDestroy(ev_rows);
+    if (ev_enter) cudaEventDestroy(ev_enter);
+    if (ev_leave) cudaEventDestroy(ev_leave);
+    if (hi) cudaStreamDestroy(hi);
     for (cudaEvent_t e : ev_g)
       if (e) cudaEventDestroy(e);
     if (side) cudaStreamDestroy(side);
@@ -1553,8 +1559,13 @@ int adjoint_prepare(mfdm_model* m) {
     // Q fields off the interior set are never written and must stay 0
     MFDM_CU(cudaMemset(a->H[0].qx, 0, n * sizeof(float)));
     MFDM_CU(cudaMemset(a->H[0].qz, 0, n * sizeof(float)));
-    MFDM_CU(cudaStreamCreateWithFlags(&a->side, cudaStreamNonBlocking));
-    MFDM_CU(cudaStreamCreateWithFlags(&a->side_g, cudaStreamNonBlocking));
+    int least = 0, greatest = 0;
+    MFDM_CU(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    MFDM_CU(cudaStreamCreateWithPriority(&a->hi, cudaStreamNonBlocking, greatest));
+    MFDM_CU(cudaStreamCreateWithPriority(&a->side, cudaStreamNonBlocking, greatest));
+    MFDM_CU(cudaStreamCreateWithPriority(&a->side_g, cudaStreamNonBlocking, least));
+    MFDM_CU(cudaEventCreateWithFlags(&a->ev_enter, cudaEventDisableTiming));
+    MFDM_CU(cudaEventCreateWithFlags(&a->ev_leave, cudaEventDisableTiming));
     MFDM_CU(cudaEventCreateWithFlags(&a->ev_kb, cudaEventDisableTiming));
     MFDM_CU(cudaEventCreateWithFlags(&a->ev_rows, cudaEventDisableTiming));
     for (cudaEvent_t& e : a->ev_g) MFDM_CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -1631,7 +1642,10 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
   AdjointState* a = m->adj;
   const mfdm::SetLayout& L = a->L;
   const long long len = L.len;
-  cudaStream_t st = m->stream;
+  // the step runs on the high-priority stream, joined to the handle's stream
+  cudaStream_t st = a->hi;
+  MFDM_CU(cudaEventRecord(a->ev_enter, m->stream));
+  MFDM_CU(cudaStreamWaitEvent(st, a->ev_enter, 0));
   const Coef& C = m->C;
   const int d0 = (n & 1) ? mfdm::kDirB : mfdm::kDirF, d1 = 1 - d0;
   Fields Y[4];
@@ -1654,10 +1668,10 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
     MFDM_CU(cudaStreamWaitEvent(a->side, a->ev_kb, 0));
     MFDM_CU(mfdm::adj::sparse_rows(a->H[d], a->kb[kin], a->side));
     MFDM_CU(cudaEventRecord(a->ev_rows, a->side));
+    MFDM_CU(mfdm::adj::q_fields(a->H[d], C, L, a->kb[kin], st));
     MFDM_CU(cudaStreamWaitEvent(a->side_g, a->ev_kb, 0));
     MFDM_CU(mfdm::adj::gradient(C, L, Y[sy], a->kb[kin], g, d, nullptr, a->side_g));
     MFDM_CU(cudaEventRecord(a->ev_g[kin], a->side_g));
-    MFDM_CU(mfdm::adj::q_fields(a->H[d], C, L, a->kb[kin], st));
     MFDM_CU(cudaStreamWaitEvent(st, a->ev_rows, 0));
     MFDM_CU(cudaStreamWaitEvent(st, a->ev_g[1 - kin], 0));
     MFDM_CU(mfdm::adj::reverse_stage(a->H[d], C, L, d, a->kb[kin], a->lam, a->mask, mask_lam,
@@ -1671,6 +1685,8 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
   if ((rc = stage(d0, 0, 1, false, c[3], 0.f)) != MFDM_OK) return rc;
   // the step's stage inputs and kb are not reused before its last gradient ends
   MFDM_CU(cudaStreamWaitEvent(st, a->ev_g[1], 0));
+  MFDM_CU(cudaEventRecord(a->ev_leave, st));
+  MFDM_CU(cudaStreamWaitEvent(m->stream, a->ev_leave, 0));
   return MFDM_OK;
 }
 
