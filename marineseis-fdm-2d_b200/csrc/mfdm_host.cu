@@ -153,7 +153,8 @@ struct AdjointState {
   float* ckpt = nullptr;   // checkpoint sets
   size_t ckpt_sets = 0;
   float* seg = nullptr;    // 4 stage-input sets per step of one segment
-  size_t seg_steps = 0;
+  float* seg2 = nullptr;   // a second such buffer: the next segment is recomputed into it
+  size_t seg_steps = 0;    // while this one is reversed (when the memory allows)
   float* keep = nullptr;   // stage inputs of the last `nkeep` segments, kept by the forward pass
   size_t keep_floats = 0;
   // TMA maps of every kept step's four stage-input sets (stencil boxes) and of
@@ -177,6 +178,8 @@ struct AdjointState {
   cudaStream_t hi = nullptr, side = nullptr, side_g = nullptr;
   cudaEvent_t ev_kb = nullptr, ev_rows = nullptr, ev_g[2] = {nullptr, nullptr};
   cudaEvent_t ev_enter = nullptr, ev_leave = nullptr;
+  cudaEvent_t ev_seg[2] = {nullptr, nullptr};  // segment recomputed into seg / seg2
+  cudaEvent_t ev_rev[2] = {nullptr, nullptr};  // last reverse reading seg / seg2 done
   int nsteps = -1, every = 0;  // the forward run a backward pass may follow
   double build_ms = 0.0;       // operator assembly time (host clock)
   ~AdjointState() {
@@ -197,6 +200,11 @@ struct AdjointState {
     if (ev_rows) cudaEventDestroy(ev_rows);
     if (ev_enter) cudaEventDestroy(ev_enter);
     if (ev_leave) cudaEventDestroy(ev_leave);
+    for (cudaEvent_t e : ev_seg)
+      if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : ev_rev)
+      if (e) cudaEventDestroy(e);
+    cudaFree(seg2);
     if (hi) cudaStreamDestroy(hi);
     for (cudaEvent_t e : ev_g)
       if (e) cudaEventDestroy(e);
@@ -1566,6 +1574,8 @@ int adjoint_prepare(mfdm_model* m) {
     MFDM_CU(cudaStreamCreateWithPriority(&a->side_g, cudaStreamNonBlocking, least));
     MFDM_CU(cudaEventCreateWithFlags(&a->ev_enter, cudaEventDisableTiming));
     MFDM_CU(cudaEventCreateWithFlags(&a->ev_leave, cudaEventDisableTiming));
+    for (cudaEvent_t& e : a->ev_seg) MFDM_CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (cudaEvent_t& e : a->ev_rev) MFDM_CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     MFDM_CU(cudaEventCreateWithFlags(&a->ev_kb, cudaEventDisableTiming));
     MFDM_CU(cudaEventCreateWithFlags(&a->ev_rows, cudaEventDisableTiming));
     for (cudaEvent_t& e : a->ev_g) MFDM_CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -1642,10 +1652,9 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
   AdjointState* a = m->adj;
   const mfdm::SetLayout& L = a->L;
   const long long len = L.len;
-  // the step runs on the high-priority stream, joined to the handle's stream
+  // the step runs on the high-priority stream (the caller orders it against
+  // the handle's stream)
   cudaStream_t st = a->hi;
-  MFDM_CU(cudaEventRecord(a->ev_enter, m->stream));
-  MFDM_CU(cudaStreamWaitEvent(st, a->ev_enter, 0));
   const Coef& C = m->C;
   const int d0 = (n & 1) ? mfdm::kDirB : mfdm::kDirF, d1 = 1 - d0;
   Fields Y[4];
@@ -1685,8 +1694,6 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
   if ((rc = stage(d0, 0, 1, false, c[3], 0.f)) != MFDM_OK) return rc;
   // the step's stage inputs and kb are not reused before its last gradient ends
   MFDM_CU(cudaStreamWaitEvent(st, a->ev_g[1], 0));
-  MFDM_CU(cudaEventRecord(a->ev_leave, st));
-  MFDM_CU(cudaStreamWaitEvent(m->stream, a->ev_leave, 0));
   return MFDM_OK;
 }
 
@@ -1818,7 +1825,9 @@ int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_
   const size_t ninner = size_t((every + inner - 1) / inner);
   if (a->nkeep < ncp && size_t(inner) > a->seg_steps) {
     cudaFree(a->seg);
+    cudaFree(a->seg2);  // re-made at the new size when the overlap uses it
     a->seg = nullptr;
+    a->seg2 = nullptr;
     a->seg_steps = 0;
     if ((rc = dalloc(&a->seg, size_t(inner) * 4 * len)) != MFDM_OK) return rc;
     a->seg_steps = size_t(inner);
@@ -1837,6 +1846,49 @@ int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_
   MFDM_CU(cudaMemsetAsync(a->mu, 0, len * sizeof(float), st));
   MFDM_CU(cudaMemsetAsync(a->kb[0], 0, len * sizeof(float), st));
   a->nsteps = -1;
+  // The reverse steps run on a->hi (high priority); the handle's stream `st`
+  // restores checkpoints and recomputes segments. With a second stage-input
+  // buffer, segment k-1 is recomputed into it while segment k is reversed.
+  cudaStream_t hi = a->hi;
+  MFDM_CU(cudaEventRecord(a->ev_enter, st));  // the reverse chain starts after the memsets
+  MFDM_CU(cudaStreamWaitEvent(hi, a->ev_enter, 0));
+  bool dbl = inner == every && a->nkeep < ncp - 1;
+  if (dbl && a->seg2 == nullptr) {
+    if (cudaMalloc(&a->seg2, a->seg_steps * 4 * len * sizeof(float)) != cudaSuccess) {
+      (void)cudaGetLastError();  // not enough memory for two: one buffer, no overlap
+      a->seg2 = nullptr;
+      dbl = false;
+    }
+  }
+  auto buf_of = [&](int k) { return (dbl && (k & 1)) ? 1 : 0; };
+  auto buf_ptr = [&](int b) { return b ? a->seg2 : a->seg; };
+  // restore checkpoint k and recompute steps u0..u1-1 keeping every stage
+  // input in buffer b (after the last reverse that read it)
+  auto recompute = [&](int k, int u0, int u1, int b, bool from_ckpt, const float* from) -> int {
+    MFDM_CU(cudaStreamWaitEvent(st, a->ev_rev[b], 0));
+    MFDM_CU(cudaMemcpyAsync(m->S[0].fvx, from_ckpt ? a->ckpt + size_t(k) * len : from,
+                            len * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    MFDM_CU(mfdm::launch_set_step(m->C, u0, st));
+    for (int n = u0; n < u1; ++n) {
+      float* slot = buf_ptr(b) + size_t(n - u0) * 4 * len;
+      float* save[4] = {slot, slot + len, slot + 2 * len, slot + 3 * len};
+      int rc2;
+      if ((rc2 = enqueue_step(m, n, st, nullptr, save)) != MFDM_OK) return rc2;
+    }
+    MFDM_CU(cudaEventRecord(a->ev_seg[b], st));
+    return MFDM_OK;
+  };
+  // reverse steps u1-1..u0 from buffer b, once their recompute is done
+  auto reverse = [&](int u0, int u1, int b) -> int {
+    MFDM_CU(cudaStreamWaitEvent(hi, a->ev_seg[b], 0));
+    for (int n = u1 - 1; n >= u0; --n) {
+      int rc2;
+      if ((rc2 = reverse_step(m, n, buf_ptr(b) + size_t(n - u0) * 4 * len)) != MFDM_OK) return rc2;
+    }
+    MFDM_CU(cudaEventRecord(a->ev_rev[b], hi));
+    return MFDM_OK;
+  };
+  int prepared = -1;  // the segment already recomputed ahead
   for (int k = ncp - 1; k >= 0; --k) {
     const int t0 = k * every, t1 = std::min(nsteps, t0 + every);
     if (k + a->nkeep >= ncp) {
@@ -1846,10 +1898,12 @@ int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_
         if ((rc = reverse_step(m, n, base + size_t(n - t0) * 4 * len)) != MFDM_OK) return rc;
       continue;
     }
-    MFDM_CU(cudaMemcpyAsync(m->S[0].fvx, a->ckpt + size_t(k) * len, len * sizeof(float),
-                            cudaMemcpyDeviceToDevice, st));
     if (inner < every) {
-      // re-run the segment keeping a state every `inner` steps
+      // re-run the segment keeping a state every `inner` steps (after the
+      // last reverse, whose stretch of the segment buffer it overwrites)
+      MFDM_CU(cudaStreamWaitEvent(st, a->ev_rev[0], 0));
+      MFDM_CU(cudaMemcpyAsync(m->S[0].fvx, a->ckpt + size_t(k) * len, len * sizeof(float),
+                              cudaMemcpyDeviceToDevice, st));
       MFDM_CU(mfdm::launch_set_step(m->C, t0, st));
       m->host_step = t0;
       for (int i = 0; t0 + i * inner < t1; ++i) {
@@ -1858,23 +1912,23 @@ int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_
         const int todo = std::min(inner, t1 - (t0 + i * inner));
         if (t0 + (i + 1) * inner < t1 && (rc = enqueue_steps(m, todo)) != MFDM_OK) return rc;
       }
-    }
-    for (int i = (t1 - t0 - 1) / inner; i >= 0; --i) {
-      const int u0 = t0 + i * inner, u1 = std::min(t1, u0 + inner);
-      if (inner < every)
-        MFDM_CU(cudaMemcpyAsync(m->S[0].fvx, a->inner + size_t(i) * len, len * sizeof(float),
-                                cudaMemcpyDeviceToDevice, st));
-      // recompute the stretch, keeping every stage input
-      MFDM_CU(mfdm::launch_set_step(m->C, u0, st));
-      for (int n = u0; n < u1; ++n) {
-        float* slot = a->seg + size_t(n - u0) * 4 * len;
-        float* save[4] = {slot, slot + len, slot + 2 * len, slot + 3 * len};
-        if ((rc = enqueue_step(m, n, st, nullptr, save)) != MFDM_OK) return rc;
+      for (int i = (t1 - t0 - 1) / inner; i >= 0; --i) {
+        const int u0 = t0 + i * inner, u1 = std::min(t1, u0 + inner);
+        if ((rc = recompute(k, u0, u1, 0, false, a->inner + size_t(i) * len)) != MFDM_OK) return rc;
+        if ((rc = reverse(u0, u1, 0)) != MFDM_OK) return rc;
       }
-      for (int n = u1 - 1; n >= u0; --n)
-        if ((rc = reverse_step(m, n, a->seg + size_t(n - u0) * 4 * len)) != MFDM_OK) return rc;
+      continue;
     }
+    if (prepared != k && (rc = recompute(k, t0, t1, buf_of(k), true, nullptr)) != MFDM_OK) return rc;
+    if (dbl && k > 0) {  // the next segment to reverse, recomputed meanwhile
+      const int p0 = (k - 1) * every, p1 = std::min(nsteps, p0 + every);
+      if ((rc = recompute(k - 1, p0, p1, buf_of(k - 1), true, nullptr)) != MFDM_OK) return rc;
+      prepared = k - 1;
+    }
+    if ((rc = reverse(t0, t1, buf_of(k))) != MFDM_OK) return rc;
   }
+  MFDM_CU(cudaEventRecord(a->ev_leave, hi));
+  MFDM_CU(cudaStreamWaitEvent(st, a->ev_leave, 0));
   MFDM_CU(cudaStreamSynchronize(st));
   if (out) {
     double* dst[7] = {out->K, out->rcp_rho_f, out->C11, out->C13, out->C33, out->C55, out->rcp_rho_s};
