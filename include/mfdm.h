@@ -271,7 +271,9 @@ int mfdm_adjoint_forward(mfdm_model* m, int nsteps, int ckpt_every);
  * mfdm_adjoint_forward (no other step in between): res_* are
  * [ceil(nsteps / gap)][nx] (NULL = 0), in the mfdm_get_records layout.
  * Recomputes each checkpoint segment once, keeping its stage inputs
- * (4 * ckpt_every state copies). On return the handle is back at rest at step 0. */
+ * (4 * ckpt_every state copies; a second such buffer, allocated on first use
+ * where memory allows, lets the next segment be recomputed while the current
+ * one is reversed). On return the handle is back at rest at step 0. */
 int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_svz,
                           const float* res_fp, mfdm_coef_grad* grad);
 
