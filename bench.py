@@ -352,6 +352,8 @@ def main():
                     help="only the warm-up and timed steps (a short launch list for ncu)")
     ap.add_argument("--blocks-per-sm", type=int, default=0, choices=[0, 2, 3, 4],
                     help="stage kernel build (0: the default, as for any model)")
+    ap.add_argument("--seg-rows", type=int, default=0,
+                    help="rows per segment block of the stage launches (0: the default for the grid)")
     ap.add_argument("--adjoint-profile", action="store_true",
                     help="only a short adjoint run on the 800x400 model (16 steps, checkpoint "
                          "every 8, seeded residuals): a launch list of the adjoint kernels for ncu")
@@ -398,6 +400,7 @@ def main():
     mfdm.load_library()
     solver = mfdm.Solver.from_model(model, device=local)
     solver.set_blocks_per_sm(args.blocks_per_sm)
+    solver.set_tile(args.seg_rows)
     solver.set_shot(0, reset=True)
     solver.step(args.warmup)
 
