@@ -190,9 +190,10 @@ __global__ void k_apply_t(const long long* __restrict__ rowptr, const int* __res
 
 // Receivers sample the filtered interface rows of columns 3..nx-4
 // (elsewhere the record is 0 whatever the state).
-__global__ void k_inject(float* lam, SetLayout L, const float* __restrict__ res) {
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
-  if (ix < 3 || ix > L.nx - 4) return;
+// Residual injection at column ix (receiver rows: solid vx and vz on the
+// interface row, fluid p on the interface row).
+__device__ __forceinline__ void inject_col(float* lam, const SetLayout& L, const float* __restrict__ res,
+                                           int ix) {
   const int nx = L.nx;
   lam[L.off[3] + ix] += res[ix];
   lam[L.off[4] + ix] += res[nx + ix];
@@ -207,11 +208,10 @@ __device__ __forceinline__ long long iface_index(const SetLayout& L, int f, int 
 
 // Transposed continuity average of column ix, divided by the column's tap sum:
 // tmp[f][ix] = (A^T lam)_f / wsum(ix).
-__global__ void k_filter_t_a(const float* lam, SetLayout L, const float2* __restrict__ nrm,
-                             float* tmp, W7 w7) {
-  const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void filter_t_a_col(const float* lam, const SetLayout& L,
+                                               const float2* __restrict__ nrm, float* tmp,
+                                               const W7& w7, int ix) {
   const int nx = L.nx;
-  if (ix < 3 || ix > nx - 4) return;
   float lv[8];
 #pragma unroll
   for (int f = 0; f < 8; ++f) lv[f] = lam[iface_index(L, f, ix)];
@@ -233,14 +233,13 @@ __global__ void k_filter_t_a(const float* lam, SetLayout L, const float2* __rest
 }
 
 // Transposed smoothing: lam at interface cell (f, j) = sum_k w_k tmp[f][j - k].
-// With mu / kb (the step's mu = F^T lam and kb = c M mu, formed elsewhere by the
-// previous step's last transposed stage) the filtered interface cells are
-// written to those too.
-__global__ void k_filter_t_b(float* lam, SetLayout L, const float* __restrict__ tmp, W7 w7,
-                             float* mu, float* kb, const uint8_t* __restrict__ mask, float c) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+// The filtered interface cells also go to mu and kb (the step's mu = F^T lam
+// and kb = c M mu, formed off the interface rows by the previous step's last
+// transposed stage).
+__device__ __forceinline__ void filter_t_b_col(float* lam, const SetLayout& L, const float* tmp,
+                                               const W7& w7, float* mu, float* kb,
+                                               const uint8_t* __restrict__ mask, float c, int j) {
   const int nx = L.nx;
-  if (j < 3 || j > nx - 4) return;
 #pragma unroll
   for (int f = 0; f < 8; ++f) {
     float s = 0.0f;
@@ -251,13 +250,29 @@ __global__ void k_filter_t_b(float* lam, SetLayout L, const float* __restrict__ 
     }
     const long long q = iface_index(L, f, j);
     lam[q] = s;
-    if (mu) {
-      mu[q] = s;
-      kb[q] = mask[q] ? c * s : 0.0f;
-    }
+    mu[q] = s;
+    kb[q] = mask[q] ? c * s : 0.0f;
   }
 }
 
+// The start of one transposed step in one block (the interface columns only):
+// the residual injection (res != null), the transposed continuity average into
+// tmp, a block barrier, the transposed smoothing -- one launch instead of three
+// dependent ones.
+__global__ void __launch_bounds__(1024) k_step_start(float* lam, SetLayout L,
+                                                     const float2* __restrict__ nrm, float* tmp,
+                                                     W7 w7, const float* __restrict__ res, float* mu,
+                                                     float* kb, const uint8_t* __restrict__ mask,
+                                                     float c) {
+  const int nx = L.nx;
+  for (int ix = 3 + threadIdx.x; ix <= nx - 4; ix += blockDim.x) {
+    if (res) inject_col(lam, L, res, ix);
+    filter_t_a_col(lam, L, nrm, tmp, w7, ix);
+  }
+  __syncthreads();  // tmp of every column written (global memory, one block)
+  for (int j = 3 + threadIdx.x; j <= nx - 4; j += blockDim.x)
+    filter_t_b_col(lam, L, tmp, w7, mu, kb, mask, c, j);
+}
 
 __global__ void k_drop_count(const long long* __restrict__ rowptr, const int* __restrict__ col,
                              SetLayout L, unsigned long long* count) {
@@ -777,20 +792,13 @@ cudaError_t apply_t(const HybridT& H, const Coef& C, const SetLayout& L, int dir
   return cudaGetLastError();
 }
 
-cudaError_t inject(float* lam, const SetLayout& L, const float* res, cudaStream_t st) {
-  k_inject<<<(L.nx + kBlock - 1) / kBlock, kBlock, 0, st>>>(lam, L, res);
-  return cudaGetLastError();
-}
-
-cudaError_t filter_t(float* lam, const SetLayout& L, const Coef& C, float* tmp, cudaStream_t st,
-                     float* mu, float* kb, const uint8_t* mask, float c) {
+cudaError_t step_start(float* lam, const SetLayout& L, const Coef& C, float* tmp,
+                       const float* res, float* mu, float* kb, const uint8_t* mask, float c,
+                       cudaStream_t st) {
   // the filter taps (src/elements.cu:30-33), as the forward finish kernel uses them
   const W7 w7{{1.1e-13f, 1.678e-06f, 0.03419f, 0.93163f, 0.03419f, 1.678e-06f, 1.1e-13f}};
-  const unsigned g = unsigned((L.nx + kBlock - 1) / kBlock);
-  k_filter_t_a<<<g, kBlock, 0, st>>>(lam, L, C.nrm, tmp, w7);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  k_filter_t_b<<<g, kBlock, 0, st>>>(lam, L, tmp, w7, mu, kb, mask, c);
+  const int threads = L.nx < 1024 ? (L.nx + 31) / 32 * 32 : 1024;
+  k_step_start<<<1, threads, 0, st>>>(lam, L, C.nrm, tmp, w7, res, mu, kb, mask, c);
   return cudaGetLastError();
 }
 

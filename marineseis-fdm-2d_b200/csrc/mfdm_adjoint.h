@@ -122,15 +122,14 @@ cudaError_t random_fill(float* x, long long n, unsigned seed, cudaStream_t st);
 cudaError_t apply_t(const HybridT& H, const Coef& C, const SetLayout& L, int dir, const float* x,
                     float* y, cudaStream_t st);
 
-// Adds one receiver sample's residuals (svx, svz, fp rows of nx) to lam.
-cudaError_t inject(float* lam, const SetLayout& L, const float* res, cudaStream_t st);
-// lam <- F^T lam on the interface rows (the transposed post-step filter);
-// tmp holds 8 * nx floats. With mu and kb the filtered cells also get
-// mu = lam and kb = c M lam (the rest of both was formed by the previous
-// transposed step).
-cudaError_t filter_t(float* lam, const SetLayout& L, const Coef& C, float* tmp, cudaStream_t st,
-                     float* mu = nullptr, float* kb = nullptr, const uint8_t* mask = nullptr,
-                     float c = 0.f);
+// The start of one transposed step, in one launch: with res (one receiver
+// sample's residuals, svx, svz, fp rows of nx) it is added to lam; then
+// lam <- F^T lam on the interface rows (the transposed post-step filter; tmp
+// holds 8 * nx floats), and the filtered cells also get mu = lam and
+// kb = c M lam (the rest of both was formed by the previous transposed step).
+cudaError_t step_start(float* lam, const SetLayout& L, const Coef& C, float* tmp,
+                       const float* res, float* mu, float* kb, const uint8_t* mask, float c,
+                       cudaStream_t st);
 
 // Material gradients of one stage: g[m][cell] += kb . dL_dir/dm (Y) over the
 // cell's main fields (and the coupled interface column); Y is a set, kb a

@@ -1662,11 +1662,10 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
   double* g[7];
   for (int k = 0; k < 7; ++k) g[k] = grad_array(m, k);
   const float *c = C.rk_c, *w = C.rk_w;
-  if (n % m->gap == 0)
-    MFDM_CU(mfdm::adj::inject(a->lam, L, a->res + size_t(n / m->gap) * 3 * m->cfg.nx, st));
+  const float* res = n % m->gap == 0 ? a->res + size_t(n / m->gap) * 3 * m->cfg.nx : nullptr;
   // mu = F^T lam and kb = c3 M mu: off the interface rows both were formed by
   // the previous transposed step's last stage (zero before the first)
-  MFDM_CU(mfdm::adj::filter_t(a->lam, L, C, a->tmp, st, a->mu, a->kb[0], a->mask, c[3]));
+  MFDM_CU(mfdm::adj::step_start(a->lam, L, C, a->tmp, res, a->mu, a->kb[0], a->mask, c[3], st));
   // Each stage: once kb[kin] is complete, its sparse rows of L^T kb (side
   // stream) and its material-gradient accumulation (side_g) run beside the Q
   // fields and the transposed product on the main stream. The product writes
