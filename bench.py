@@ -450,6 +450,9 @@ def main():
         getattr(host_model, grp)[k] = t.numpy()
     h2d = sum(t.numel() * 4 for (grp, k), t in pinned.items()
               if k in ("K", "rho", "C11", "C13", "C33", "C55", "J", "xi_x", "xi_z", "ze_x", "ze_z"))
+    # one untimed upload first: on some hosts the first transfer from freshly
+    # pinned pages took 0.33 s instead of 7 ms (the timed pass uploads again)
+    solver.load_model(host_model)
     barrier(dist, local)
     t0 = time.perf_counter()
     solver.load_model(host_model)
