@@ -12,7 +12,8 @@ and coefficients (~0.7 GB) exceed the 126 MB L2, so no flush is needed.
 value  = cells x steps / device time (CUDA events on the solver's stream, max
          over ranks), cells = nx (nz_f + nz_s) as the reference counts them.
 e2e    = the same metric through the public API with host buffers: model
-         upload from pinned host memory, the steps, and the receiver read-back.
+         upload from pinned host memory, the steps, and the receiver read-back
+         (after one untimed upload), with the three parts' times.
 roofline: algorithmic bytes per step (16 S + 4 M floats per cell: 464 B solid,
          288 B fluid, +256 B per PML strip cell and direction) over the summed
          average durations of the four stage launches.
