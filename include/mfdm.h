@@ -383,12 +383,19 @@ typedef struct mfdm_device_model {
  * Allocates nothing: the coefficient blocks, RK stage buffers, accumulator,
  * ADE memory and tables live in one static device array of
  * MFDM_NOALLOC_MAX_BYTES; models that need more are rejected with
- * MFDM_ERR_ARG. The first call on a device resolves that array's address and
- * configures the kernels there, so make it before any stream capture. Calls
- * share the array and it keeps the last call's contents: the ADE memory
- * carries from one call to the next, so start a run with it == 0 (which
- * clears it) and continue one model with consecutive time indices; calls that
- * overlap on the GPU race. No receiver buffer: read the state arrays. */
+ * MFDM_ERR_ARG (the size depends on the grid only: calls of many steps run
+ * them in chunks of 1024 with a fixed Ricker table). A source cell outside the
+ * fluid grid is rejected (src_x < 0: no source). The Ricker and PML tables come
+ * from the same host functions as an open handle's, so the results are
+ * bit-identical to mfdm_step on the same model. The first call on a device
+ * resolves that array's address and configures the kernels there, so make it
+ * before any stream capture; after cudaDeviceReset of that device, do not call
+ * it again in the same process. Calls share the array and it keeps the last
+ * call's contents: the ADE memory carries from one call to the next, so start
+ * a run with it == 0 (which clears it) and continue one model with consecutive
+ * time indices; calls that overlap on the GPU race. A pipeline wait that times
+ * out returns MFDM_ERR_CUDA and leaves the state arrays undefined. No receiver
+ * buffer: read the state arrays. */
 int mfdm_step_noalloc(const mfdm_device_model* dm, int it, int nsteps, void* stream);
 
 #ifdef __cplusplus

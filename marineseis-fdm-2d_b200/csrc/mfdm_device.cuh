@@ -74,7 +74,8 @@ struct Coef {
                                     // CPML kernel instantiations), 0: free surface on top
   const float2* __restrict__ nrm;   // interface unit normal per column
   const float* __restrict__ src_amp;  // Ricker value per (step, stage): [steps][4]
-  int src_steps;
+  int src_steps;                    // steps the table holds
+  int src_it0;                      // time index of the table's first row (0: absolute)
   int srcx, srcz;                   // source column / fluid row (srcx < 0: none)
   float rk_c[4];                    // dt/2, dt/2, dt, dt/6
   float rk_w[3];                    // dt/6, dt/3, dt/3
@@ -614,8 +615,9 @@ __device__ __forceinline__ float source_term(const Coef& C, int iz, int ix, int 
   const int dx = ix - C.srcx, dz = iz - C.srcz;
   if (C.srcx < 0 || dx < -2 || dx > 2 || dz < -2 || dz > 2) return 0.0f;
   if (ix <= 2 || ix >= C.nx - 3 || iz <= 2 || iz >= C.nzf - 3) return 0.0f;
-  if (it < 0 || it >= C.src_steps) return 0.0f;
-  const float amp = ldg(C.src_amp + (size_t)it * 4 + s);
+  const int row = it - C.src_it0;
+  if (row < 0 || row >= C.src_steps) return 0.0f;
+  const float amp = ldg(C.src_amp + (size_t)row * 4 + s);
   return amp * c_srcw[(dz + 2) * 5 + (dx + 2)];
 }
 

@@ -86,6 +86,9 @@ struct HostModel {
 
 int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
+}  // namespace
+
+namespace mfdm {
 // Ricker wavelet in the reference's host arithmetic (src/elements.cu:385-392):
 // float time, T = 1.2 / fpeak, the phase product in double rounded to float.
 float ricker_ref(float fpeak, float time) {
@@ -96,6 +99,34 @@ float ricker_ref(float fpeak, float time) {
   temp *= temp;
   return (1 - 2 * temp) * expf(-temp);
 }
+
+// CFS-PML factors of cell i of an axis of n cells in FP64 (src/elements.cu:121-124,
+// 824-873): d = d0 r^NPOW, beta = 1 + (beta0-1) r^2, alpha = alpha0 (1 - r),
+// r = k/npd, k counted from the inner edge of the band of npd cells inside 3
+// frozen cells (lo: the band at the low end, hi: at the high end). Stored as
+// (d/beta, alpha + d/beta, 1/beta), the factors the reference derives inside
+// every kernel.
+float4 pml_cell(float fpeak, float beta0, int npd, int npow, float vp_max, float rc,
+                float thickness, int i, int n, bool lo, bool hi) {
+  const double alpha0 = 2.0 * M_PI * double(fpeak);
+  const double d0 = -(npow + 1) * double(vp_max) * std::log(double(rc)) / (2.0 * double(thickness));
+  int k = -1;
+  if (lo && i >= 3 && i <= 2 + npd) k = 3 + npd - i;
+  if (hi && i >= n - 3 - npd && i <= n - 4) k = i - (n - 4 - npd);
+  double d = 0.0, be = 1.0, al = alpha0;
+  if (k > 0) {
+    const double r = double(k) / double(npd);
+    d = d0 * std::pow(r, double(npow));
+    be = 1.0 + (double(beta0) - 1.0) * r * r;
+    al = alpha0 * (1.0 - r);
+  }
+  const double dpb = d / be;
+  return make_float4(float(dpb), float(al + dpb), float(1.0 / be), 0.f);
+}
+}  // namespace mfdm
+
+namespace {
+using mfdm::ricker_ref;
 
 // One shot of a handle: source cell and Ricker peak frequency, and the PML
 // beta0 that goes with it (alpha0 = 2 pi fpeak follows the frequency).
@@ -244,31 +275,13 @@ int validate(const HostModel& h) {
   return MFDM_OK;
 }
 
-// CFS-PML profile of one axis in FP64 (src/elements.cu:121-124, 824-873):
-// d = d0 r^NPOW, beta = 1 + (beta0-1) r^2, alpha = alpha0 (1 - r), r = k/npd,
-// k counted from the inner edge of the band of npd cells inside 3 frozen cells.
-// Stored per cell as (d/beta, alpha + d/beta, 1/beta), the factors the
-// reference derives inside every kernel.
+// CFS-PML profile of one axis in FP64: every cell through mfdm::pml_cell.
 void pml_profile(const HostModel& h, int n, bool lo, bool hi, float fpeak, float beta0,
                  std::vector<float4>& out) {
-  const double alpha0 = 2.0 * M_PI * double(fpeak);
-  const double d0 = -(h.npow + 1) * double(h.vp_max) * std::log(double(h.rc)) /
-                    (2.0 * double(h.thickness));
-  out.assign(size_t(n), make_float4(0.f, 1.f, 1.f, 0.f));
-  for (int i = 0; i < n; ++i) {
-    int k = -1;
-    if (lo && i >= 3 && i <= 2 + h.npd) k = 3 + h.npd - i;
-    if (hi && i >= n - 3 - h.npd && i <= n - 4) k = i - (n - 4 - h.npd);
-    double d = 0.0, be = 1.0, al = alpha0;
-    if (k > 0) {
-      const double r = double(k) / double(h.npd);
-      d = d0 * std::pow(r, double(h.npow));
-      be = 1.0 + (double(beta0) - 1.0) * r * r;
-      al = alpha0 * (1.0 - r);
-    }
-    const double dpb = d / be;
-    out[size_t(i)] = make_float4(float(dpb), float(al + dpb), float(1.0 / be), 0.f);
-  }
+  out.resize(size_t(n));
+  for (int i = 0; i < n; ++i)
+    out[size_t(i)] = mfdm::pml_cell(fpeak, beta0, h.npd, h.npow, h.vp_max, h.rc, h.thickness, i, n,
+                                    lo, hi);
 }
 
 int read_bin(const std::string& path, size_t count, std::vector<float>& out) {
@@ -492,11 +505,21 @@ int capture_graph(mfdm_model* m) {
   return MFDM_OK;
 }
 
+// Maps a kernel status word to an error: bit 2 (value 2) is a pipeline wait
+// that timed out, after which the handle's state is undefined (reopen it);
+// bit 1 a non-finite value.
+int status_error(int st, const char* nonfinite_msg) {
+  if (st & 2)
+    return fail(MFDM_ERR_CUDA,
+                "a stage kernel pipeline wait timed out; the handle's state is undefined, reopen it");
+  if (st) return fail(MFDM_ERR_NONFINITE, nonfinite_msg);
+  return MFDM_OK;
+}
+
 int check_status(mfdm_model* m) {
   int st = 0;
   MFDM_CU(cudaMemcpy(&st, m->C.status, sizeof(int), cudaMemcpyDeviceToHost));
-  if (st) return fail(MFDM_ERR_NONFINITE, "non-finite values reached the interface rows");
-  return MFDM_OK;
+  return status_error(st, "non-finite values reached the interface rows");
 }
 
 // Uploads the model arrays, the FP64-derived PML tables and normals, and the
@@ -2360,8 +2383,7 @@ int mfdm_solid_step(mfdm_solid* m, int nsteps) {
   MFDM_CU(cudaStreamSynchronize(m->stream));
   int st = 0;
   MFDM_CU(cudaMemcpy(&st, m->C.status, sizeof(int), cudaMemcpyDeviceToHost));
-  if (st) return fail(MFDM_ERR_NONFINITE, "non-finite values reached the receiver row");
-  return MFDM_OK;
+  return status_error(st, "non-finite values reached the receiver row");
 }
 
 int mfdm_solid_time_steps(mfdm_solid* m, int nsteps, float* total_ms) {

@@ -46,6 +46,13 @@ cudaError_t upload_constants(const float* srcw25, const float* w7);
 // (rows_outer: boxes land as [row][field][col], the stencil-ring layout; with
 // nshots > 0 a fourth dimension, the shot, of stride shot_bytes).
 int set_error(int code, const char* msg);
+// Ricker value at `time` in the reference's host float arithmetic: the one
+// source of every Ricker table the library uploads.
+float ricker_ref(float fpeak, float time);
+// CFS-PML factors (d/beta, alpha + d/beta, 1/beta, 0) of cell i of an axis of n
+// cells, computed in FP64 on the host: the one source of every PML table.
+float4 pml_cell(float fpeak, float beta0, int npd, int npow, float vp_max, float rc,
+                float thickness, int i, int n, bool lo, bool hi);
 int encode_block_map(CUtensorMap* map, const float* base, int P, int rows, int nf, int box_x,
                      bool rows_outer, int nshots = 0, size_t shot_bytes = 0);
 

@@ -15,6 +15,12 @@
 // threads) race and corrupt each other. The ADE memory in the array carries
 // from one call to the next, so a run must start with it == 0 (which clears
 // it) and continue with consecutive time indices on one model at a time.
+// The Ricker and PML values come from the same host functions as the handle
+// path's (mfdm::ricker_ref, mfdm::pml_cell), so both entry points step with
+// bit-identical tables. The first call on a device caches the array's address
+// and configures the kernels there; after cudaDeviceReset of that device the
+// cache is stale, so a process that resets a device must not call this entry
+// point on it again.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -74,59 +80,23 @@ int setup_device(unsigned char** base) {
   return MFDM_OK;
 }
 
-struct Tables {
-  int nx, nzs, nzf, npd, npow, P, it0, nsteps;
-  float fpeak, dt, thickness, vp_max, rc, beta0;
-};
+// Rows of the Ricker table kept in the array: a call of more steps runs them
+// in chunks of this many, refilling the table between chunks.
+constexpr int kAmpSteps = 1024;
+// Host staging of the tables: PML factors in pieces of this many cells.
+constexpr int kPmlChunk = 256;
 
-// CFS-PML factors of one axis cell in FP64 (src/elements.cu:121-124, 824-873).
-__device__ float4 pml_factor(const Tables& t, int i, int n, bool lo, bool hi) {
-  const double alpha0 = 2.0 * M_PI * double(t.fpeak);
-  const double d0 = -(t.npow + 1) * double(t.vp_max) * log(double(t.rc)) / (2.0 * double(t.thickness));
-  int k = -1;
-  if (lo && i >= 3 && i <= 2 + t.npd) k = 3 + t.npd - i;
-  if (hi && i >= n - 3 - t.npd && i <= n - 4) k = i - (n - 4 - t.npd);
-  double d = 0.0, be = 1.0, al = alpha0;
-  if (k > 0) {
-    const double r = double(k) / double(t.npd);
-    d = d0 * pow(r, double(t.npow));
-    be = 1.0 + (double(t.beta0) - 1.0) * r * r;
-    al = alpha0 * (1.0 - r);
-  }
-  const double dpb = d / be;
-  return make_float4(float(dpb), float(al + dpb), float(1.0 / be), 0.f);
-}
-
-// Ricker value in the reference's float arithmetic (src/elements.cu:385-392).
-__device__ float ricker(float fpeak, float time) {
-  const float T = float(1.2 / double(fpeak));
-  const float t = time - T;
-  if (t > T) return 0.0f;
-  float temp = float(M_PI * double(fpeak) * double(t));
-  temp *= temp;
-  return (1 - 2 * temp) * expf(-temp);
-}
-
-// PML factors, interface normals and the Ricker values of steps [it0, it0 + nsteps).
-__global__ void tables_kernel(Tables t, float4* pmlx, float4* pmlz, float2* nrm,
-                              const float* zex, const float* zez, float* amp) {
+// Interface unit normals in FP64 from the metric on the device, with the host
+// path's operations and rounding (no contraction into fused multiply-adds).
+__global__ void normals_kernel(int nx, int nzf, int P, const float* zex, const float* zez,
+                               float2* nrm) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < t.nx) {
-    pmlx[i] = pml_factor(t, i, t.nx, true, true);
-    const size_t g = size_t(t.nzf - 1) * t.P + i;
-    const double a = zex[g], b = zez[g], s = sqrt(a * a + b * b);
-    nrm[i] = s > 0 ? make_float2(float(a / s), float(b / s)) : make_float2(0.f, 1.f);
-  }
-  if (i < t.nzs) pmlz[i] = pml_factor(t, i, t.nzs, false, true);
-  if (i < t.nsteps) {
-    const int it = t.it0 + i;
-    const float time = float(it) * t.dt;
-    const float half = float(double(t.dt) * 0.5);
-    amp[size_t(i) * 4 + 0] = ricker(t.fpeak, time);
-    amp[size_t(i) * 4 + 1] = ricker(t.fpeak, time + half);
-    amp[size_t(i) * 4 + 2] = ricker(t.fpeak, time + half);
-    amp[size_t(i) * 4 + 3] = ricker(t.fpeak, time + t.dt);
-  }
+  if (i >= nx) return;
+  const size_t g = size_t(nzf - 1) * P + i;
+  const double a = zex[g], b = zez[g];
+  const double s = __dsqrt_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)));
+  nrm[i] = s > 0 ? make_float2(float(__ddiv_rn(a, s)), float(__ddiv_rn(b, s)))
+                 : make_float2(0.f, 1.f);
 }
 
 // Density slots hold 1/rho in the kernels' coefficient blocks (see mfdm_device.cuh).
@@ -146,6 +116,8 @@ extern "C" int mfdm_step_noalloc(const mfdm_device_model* dm, int it, int nsteps
   if (npd < 0 || 2 * npd > nx - 6 || npd > nzs) return err(MFDM_ERR_ARG, "PML width npd does not fit the grid");
   if (it < 0 || nsteps < 0) return err(MFDM_ERR_ARG, "negative time index or step count");
   if (!(dm->dt > 0.f) || !(dm->fpeak > 0.f)) return err(MFDM_ERR_ARG, "dt and fpeak must be > 0");
+  if (dm->src_x >= 0 && (dm->src_x >= nx || dm->src_z < 0 || dm->src_z >= nzf))
+    return err(MFDM_ERR_ARG, "source outside the fluid grid (src_x < 0 means no source)");
   const float* ins[12] = {dm->K, dm->rho_f, dm->C11, dm->C13, dm->C33, dm->C55,
                           dm->rho_s, dm->J, dm->xi_x, dm->xi_z, dm->ze_x, dm->ze_z};
   float* state[8] = {dm->vx_f, dm->vz_f, dm->p_f, dm->vx_s, dm->vz_s, dm->sx_s, dm->sz_s, dm->sxz_s};
@@ -170,7 +142,7 @@ extern "C" int mfdm_step_noalloc(const mfdm_device_model* dm, int it, int nsteps
   for (int q = 0; q < 5; ++q) o_met[q] = take(ng);
   const size_t o_pmlx = take(size_t(nx) * 4), o_pmlz = take(size_t(nzs) * 4),
                o_nrm = take(size_t(nx) * 2), o_ipre = take(size_t(8) * P), o_misc = take(64),
-               o_amp = take(size_t(nsteps > 0 ? nsteps : 1) * 4);
+               o_amp = take(size_t(kAmpSteps) * 4);
   size_t o_fb[4], o_sb[4], o_ade[4][12];
   for (int s = 0; s < 4; ++s) {
     o_fb[s] = take(3 * nf);
@@ -185,8 +157,9 @@ extern "C" int mfdm_step_noalloc(const mfdm_device_model* dm, int it, int nsteps
   if (off > kNoAllocBytes) {
     char msg[200];
     snprintf(msg, sizeof msg,
-             "model needs %zu bytes of scratch; the static limit of mfdm_step_noalloc is %zu bytes "
-             "(MFDM_NOALLOC_MAX_BYTES)", off, kNoAllocBytes);
+             "model needs %zu bytes of scratch (%d x (%d + %d) cells); the static limit of "
+             "mfdm_step_noalloc is %zu bytes (MFDM_NOALLOC_MAX_BYTES)",
+             off, nx, nzf, nzs, kNoAllocBytes);
     return err(MFDM_ERR_ARG, msg);
   }
 
@@ -247,14 +220,23 @@ extern "C" int mfdm_step_noalloc(const mfdm_device_model* dm, int it, int nsteps
   for (int f = 0; f < 8; ++f)
     if ((rc = copy_rows(u_dst[f], state[f], 0, f < 3 ? nzf : nzs)) != MFDM_OK) return rc;
 
-  Tables t{nx, nzs, nzf, npd, dm->npow, P, it, nsteps, dm->fpeak, dm->dt, dm->thickness,
-           dm->vp_max, dm->rc, dm->beta0};
-  const int nt_threads = 256;
-  int n_items = nx > nzs ? nx : nzs;
-  if (nsteps > n_items) n_items = nsteps;
-  tables_kernel<<<(n_items + nt_threads - 1) / nt_threads, nt_threads, 0, st>>>(
-      t, reinterpret_cast<float4*>(F(o_pmlx)), reinterpret_cast<float4*>(F(o_pmlz)),
-      reinterpret_cast<float2*>(F(o_nrm)), F(o_met[3]), F(o_met[4]), F(o_amp));
+  // PML factors on the host (the handle path's function), in pieces through a
+  // stack buffer: pageable copies return once the source is staged.
+  {
+    float4 buf[kPmlChunk];
+    float4* const pml[2] = {reinterpret_cast<float4*>(F(o_pmlx)), reinterpret_cast<float4*>(F(o_pmlz))};
+    const int len[2] = {nx, nzs};
+    for (int a = 0; a < 2; ++a)
+      for (int i0 = 0; i0 < len[a]; i0 += kPmlChunk) {
+        const int n = len[a] - i0 < kPmlChunk ? len[a] - i0 : kPmlChunk;
+        for (int i = 0; i < n; ++i)
+          buf[i] = mfdm::pml_cell(dm->fpeak, dm->beta0, npd, dm->npow, dm->vp_max, dm->rc,
+                                  dm->thickness, i0 + i, len[a], a == 0, true);
+        NA_CU(cudaMemcpyAsync(pml[a] + i0, buf, size_t(n) * sizeof(float4), cudaMemcpyHostToDevice, st));
+      }
+  }
+  normals_kernel<<<(nx + 255) / 256, 256, 0, st>>>(nx, nzf, P, F(o_met[3]), F(o_met[4]),
+                                                   reinterpret_cast<float2*>(F(o_nrm)));
   NA_CU(cudaGetLastError());
 
   mfdm::Coef C{};
@@ -266,10 +248,8 @@ extern "C" int mfdm_step_noalloc(const mfdm_device_model* dm, int it, int nsteps
   C.pmlx = reinterpret_cast<const float4*>(F(o_pmlx));
   C.pmlz = reinterpret_cast<const float4*>(F(o_pmlz));
   C.nrm = reinterpret_cast<const float2*>(F(o_nrm));
-  // The kernels index the Ricker table by absolute time index: shift the base by it0 steps.
-  C.src_amp = reinterpret_cast<const float*>(reinterpret_cast<uintptr_t>(F(o_amp)) -
-                                             uintptr_t(it) * 4 * sizeof(float));
-  C.src_steps = it + nsteps;
+  // Ricker table rows: time indices src_it0 .. src_it0 + src_steps - 1 (set per chunk below).
+  C.src_amp = F(o_amp);
   C.srcx = dm->src_x;
   C.srcz = dm->src_z;
   const float dt = dm->dt;
@@ -299,22 +279,42 @@ extern "C" int mfdm_step_noalloc(const mfdm_device_model* dm, int it, int nsteps
 
   NA_CU(mfdm::launch_set_step(C, it, st));
   const int in_set[4] = {0, 1, 2, 1}, out_set[4] = {1, 2, 1, 0};
-  for (int k = 0; k < nsteps; ++k) {
-    const int d0 = ((it + k) & 1) ? mfdm::kDirB : mfdm::kDirF, d1 = 1 - d0;
-    const int dir[4] = {d0, d1, d0, d1};
-    for (int s = 0; s < 4; ++s) {
-      mfdm::StageMaps maps;
-      maps.fin = fst[in_set[s]];
-      maps.sin = sst[in_set[s]];
-      maps.fun = fpw[0];
-      maps.sun = spw[0];
-      maps.facc = fpw[3];
-      maps.sacc = spw[3];
-      maps.fcoef = fcm;
-      maps.scoef = scm;
-      NA_CU(mfdm::launch_stage(C, S[in_set[s]], S[out_set[s]], S[0], S[3], maps, s, dir[s], st));
+  const float half = float(double(dt) * 0.5);
+  for (int k0 = 0; k0 < nsteps; k0 += kAmpSteps) {
+    const int nk = nsteps - k0 < kAmpSteps ? nsteps - k0 : kAmpSteps;
+    // The chunk's Ricker values on the host with the handle path's function
+    // (src/elements.cu:385-392, float time = it * dt), staged from the stack.
+    // The copy is ordered after the previous chunk's kernels on this stream.
+    {
+      float amp[kAmpSteps * 4];
+      for (int k = 0; k < nk; ++k) {
+        const float t = float(it + k0 + k) * dt;
+        amp[k * 4 + 0] = mfdm::ricker_ref(dm->fpeak, t);
+        amp[k * 4 + 1] = mfdm::ricker_ref(dm->fpeak, t + half);
+        amp[k * 4 + 2] = mfdm::ricker_ref(dm->fpeak, t + half);
+        amp[k * 4 + 3] = mfdm::ricker_ref(dm->fpeak, t + dt);
+      }
+      NA_CU(cudaMemcpyAsync(F(o_amp), amp, size_t(nk) * 4 * sizeof(float), cudaMemcpyHostToDevice, st));
     }
-    NA_CU(mfdm::launch_finish(C, S[0], st));
+    C.src_it0 = it + k0;
+    C.src_steps = nk;
+    for (int k = k0; k < k0 + nk; ++k) {
+      const int d0 = ((it + k) & 1) ? mfdm::kDirB : mfdm::kDirF, d1 = 1 - d0;
+      const int dir[4] = {d0, d1, d0, d1};
+      for (int s = 0; s < 4; ++s) {
+        mfdm::StageMaps maps;
+        maps.fin = fst[in_set[s]];
+        maps.sin = sst[in_set[s]];
+        maps.fun = fpw[0];
+        maps.sun = spw[0];
+        maps.facc = fpw[3];
+        maps.sacc = spw[3];
+        maps.fcoef = fcm;
+        maps.scoef = scm;
+        NA_CU(mfdm::launch_stage(C, S[in_set[s]], S[out_set[s]], S[0], S[3], maps, s, dir[s], st));
+      }
+      NA_CU(mfdm::launch_finish(C, S[0], st));
+    }
   }
   // The wavefield out.
   for (int f = 0; f < 8; ++f)
@@ -323,7 +323,8 @@ extern "C" int mfdm_step_noalloc(const mfdm_device_model* dm, int it, int nsteps
   int status = 0;
   NA_CU(cudaMemcpyAsync(&status, C.status, sizeof(int), cudaMemcpyDeviceToHost, st));
   NA_CU(cudaStreamSynchronize(st));
+  if (status & 2)
+    return err(MFDM_ERR_CUDA, "a stage kernel pipeline wait timed out; the state arrays are undefined");
   if (status & 1) return err(MFDM_ERR_NONFINITE, "non-finite values reached the interface rows");
-  if (status & 2) return err(MFDM_ERR_CUDA, "a stage kernel pipeline wait timed out");
   return MFDM_OK;
 }

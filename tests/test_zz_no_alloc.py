@@ -1,10 +1,13 @@
 """mfdm_step_noalloc, the entry point for callers that cannot allocate device
-memory, against the handle-based entry point (mfdm_open_desc + mfdm_step).
+memory, against the handle-based entry point (mfdm_open_desc + mfdm_step) and
+the CPU oracle.
 
 The test owns every device buffer (torch allocates them); the entry point only
 uses its static array. Two calls in a row: the second continues the first
-(time index and ADE memory), as a caller's time loop would. Collected last, so
-a run that stops at the first failure has run everything else before it."""
+(time index and ADE memory), as a caller's time loop would. Both entry points
+build their Ricker and PML tables with the same host functions, so their
+wavefields are bit-identical. Collected last, so a run that stops at the first
+failure has run everything else before it."""
 import numpy as np
 import pytest
 
@@ -64,11 +67,58 @@ def test_noalloc_matches_handle_path_over_two_calls(mfdm, cases):
     for name, field in STATE_TO_FIELD.items():
         got = state[name].cpu().numpy()
         assert rel_l2(got, ref1[field]) <= TOL, (name, "first call")
+        assert np.array_equal(got, ref1[field]), (name, "first call, bitwise")
     mfdm.step_noalloc(dm, n1, n2)
     for name, field in STATE_TO_FIELD.items():
         got = state[name].cpu().numpy()
         assert rel_l2(got, ref2[field]) <= TOL, (name, "second call")
+        assert np.array_equal(got, ref2[field]), (name, "second call, bitwise")
     assert np.abs(state["p_f"].cpu().numpy()).max() > 0
+
+
+def test_noalloc_matches_oracle(mfdm, oracle, cases):
+    """Two calls against the FP32 CPU oracle's wavefield after the same steps."""
+    import torch
+    mfdm.build()
+    model = cases.curv_small()
+    n1, n2 = 37, 45
+    dm, state, keep = _device_model(mfdm, model, torch)
+    mfdm.step_noalloc(dm, 0, n1)
+    mfdm.step_noalloc(dm, n1, n2)
+    ref = oracle.forward(model, n1 + n2, oracle.record_gap(model.dt), 32, final_fields=True)
+    for q, name in enumerate(("vx_f", "vz_f", "p_f")):
+        assert rel_l2(state[name].cpu().numpy(), ref["fluid"][q]) <= TOL, name
+    for q, name in enumerate(("vx_s", "vz_s", "sx_s", "sz_s", "sxz_s")):
+        assert rel_l2(state[name].cpu().numpy(), ref["solid"][q]) <= TOL, name
+
+
+def test_noalloc_long_call_crosses_ricker_table_chunks(mfdm, cases):
+    """A call of more steps than the fixed Ricker table holds (1024) refills the
+    table between chunks; a 5 Hz wavelet is still non-zero across the refill."""
+    import torch
+    mfdm.build()
+    model = cases.curv_small()
+    model.fpeak = 5.0  # Ricker non-zero until 2.4 / 5 Hz = 0.48 s = step 1200
+    n = 1100
+    with mfdm.Solver.from_model(model) as s:
+        s.set_shot(0, reset=True)
+        s.step(n)
+        ref = {f: s.field(f) for f in STATE_TO_FIELD.values()}
+    dm, state, keep = _device_model(mfdm, model, torch)
+    mfdm.step_noalloc(dm, 0, n)
+    for name, field in STATE_TO_FIELD.items():
+        assert np.array_equal(state[name].cpu().numpy(), ref[field]), name
+
+
+def test_noalloc_rejects_a_source_outside_the_grid(mfdm, cases):
+    import torch
+    mfdm.build()
+    model = cases.curv_small()
+    dm, state, keep = _device_model(mfdm, model, torch)
+    dm.src_z = model.nz_f  # one row below the fluid
+    with pytest.raises(mfdm.MfdmError) as ei:
+        mfdm.step_noalloc(dm, 0, 1)
+    assert ei.value.code == -1 and "source outside" in str(ei.value)
 
 
 def test_noalloc_rejects_models_over_the_static_limit(mfdm, modelgen):
