@@ -39,16 +39,6 @@ def _stale(out: str, deps) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build_variant(out: str, defines=(), verbose: bool = False) -> str:
-    """Compiles the library with extra -D definitions to `out` (tuning experiments)."""
-    cmd = [_nvcc()] + NVCC_FLAGS + ["-D" + d for d in defines] + ["-shared", "-o", out] + [
-        s for s in _sources() if not s.endswith("main_debug.cpp")]
-    if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
-    return out
-
-
 def build(verbose: bool = False, force: bool = False) -> str:
     """Compiles libmfdm.so and bin/main_debug; returns the library path."""
     nvcc = _nvcc()

@@ -18,6 +18,7 @@ import os
 import shutil
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -87,7 +88,7 @@ def main():
     ap.add_argument("names", nargs="*")
     ap.add_argument("--fp64", action="store_true",
                     help="add FP64 oracle records to existing fixtures (CPU only)")
-    ap.add_argument("--work", default=os.path.join(cases.ROOT, "gpurun_out", "golden_work"))
+    ap.add_argument("--work", default=os.path.join(tempfile.gettempdir(), "mfdm_golden_work"))
     ap.add_argument("--outdir", default=cases.GOLDEN_DIR)
     args = ap.parse_args()
     names = args.names or list(cases.CASES)

@@ -19,6 +19,7 @@ import shutil
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
@@ -44,7 +45,7 @@ def wall(binary: str, jpath: str, out: str) -> float:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("names", nargs="*")
-    ap.add_argument("--work", default=os.path.join(cases.ROOT, "gpurun_out", "time_reference"))
+    ap.add_argument("--work", default=os.path.join(tempfile.gettempdir(), "mfdm_time_reference"))
     args = ap.parse_args()
     result = {}
     for name in args.names or list(WORKLOADS):
