@@ -2,12 +2,16 @@
 
 Needs a GPU and oracle/_ref/main_debug (built by `make -C oracle ref` from the
 reference sources). For every case in cases.py it writes the model, runs
-`main_debug <model.json> <out>` twice, and stores the records (and, for the
-small cases, the last snapshot) of the first run in tests/golden/<case>.npz,
-plus the largest relative L2 difference between the two runs (the reference's
-own run-to-run spread; its in-place interface filter races across blocks).
+`main_debug <model.json> <out>` twice, and stores the records (and the last
+snapshot, whole or every k-th row and column) of the first run in
+tests/golden/<case>.npz, plus the largest relative L2 difference between the
+two runs (the reference's own run-to-run spread; its in-place interface filter
+races across blocks). For the long cases (cases.NOFMA_CASES) it also runs
+oracle/_ref/main_debug_nofma (`make -C oracle ref-nofma`: the same sources
+with FMA contraction off) and stores each record set's relative L2 distance
+between the two builds, the FP32 noise floor of the scheme at that length.
 
-    python tests/golden/make_golden.py [case ...] [--work DIR]
+    python tests/golden/make_golden.py [case ...] [--work DIR] [--outdir DIR]
     python tests/golden/make_golden.py --fp64 [case ...]   (CPU: FP64 oracle records)
 """
 from __future__ import annotations
@@ -27,11 +31,13 @@ sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 import cases  # noqa: E402
 
 REF_BIN = os.path.join(cases.ROOT, "oracle", "_ref", "main_debug")
+REF_NOFMA_BIN = os.path.join(cases.ROOT, "oracle", "_ref", "main_debug_nofma")
+FP64_STRIDE = 16  # receiver stride of the stored FP64 oracle records (at least the case's)
 
 
-def run_reference(jpath: str, out: str) -> float:
+def run_reference(jpath: str, out: str, binary: str = REF_BIN) -> float:
     t0 = time.time()
-    subprocess.run([REF_BIN, jpath, out], check=True, stdout=subprocess.DEVNULL)
+    subprocess.run([binary, jpath, out], check=True, stdout=subprocess.DEVNULL)
     return time.time() - t0
 
 
@@ -62,7 +68,7 @@ def rel(a, b):
 
 
 def add_fp64_records(name: str, outdir: str):
-    """Adds the FP64 oracle's records (same receiver stride) to an existing fixture.
+    """Adds the FP64 oracle's records (every FP64_STRIDE-th receiver) to an existing fixture.
 
     Runs on the CPU. Over long runs the FP32 rounding noise of this scheme grows
     above 1e-5 (the reference build itself drifts from the FP64 solution), so
@@ -76,9 +82,14 @@ def add_fp64_records(name: str, outdir: str):
     data = dict(np.load(path))
     nt = int(data["nt"])
     r = pyoracle.forward(model, nt, pyoracle.record_gap(model.dt), 64)
+    s64 = max(stride, FP64_STRIDE)
+    sub = s64 // stride
+    data["fp64_stride"] = np.int32(s64)
     for k in ("svx", "svz", "fp"):
-        data["fp64_" + k] = r[k][:, ::stride].astype(np.float64)
-    data["fp64_ref_rel_l2"] = np.float64(max(rel(data[k], data["fp64_" + k]) for k in ("svx", "svz", "fp")))
+        # stored in float32: the rounding (< 1e-7 relative) is far below what is compared
+        data["fp64_" + k] = r[k][:, ::s64].astype(np.float32)
+    data["fp64_ref_rel_l2"] = np.float64(max(rel(data[k][:, ::sub], data["fp64_" + k])
+                                             for k in ("svx", "svz", "fp")))
     np.savez_compressed(path, **data)
     print(name, "reference build vs FP64 oracle:", float(data["fp64_ref_rel_l2"]), flush=True)
 
@@ -90,6 +101,7 @@ def main():
                     help="add FP64 oracle records to existing fixtures (CPU only)")
     ap.add_argument("--work", default=os.path.join(tempfile.gettempdir(), "mfdm_golden_work"))
     ap.add_argument("--outdir", default=cases.GOLDEN_DIR)
+    ap.add_argument("--no-nofma", action="store_true", help="skip the FMA-off reference build")
     args = ap.parse_args()
     names = args.names or list(cases.CASES)
     if args.fp64:
@@ -99,8 +111,9 @@ def main():
     summary = {}
     for name in names:
         build, stride, keep_snap = cases.CASES[name]
+        step = cases.snapshot_step(keep_snap)
         model = build()
-        if keep_snap:
+        if step:
             model.snapshot = model.nt - 1  # snapshots at it = 0 and it = nt - 1
         work = os.path.join(args.work, name)
         jpath = cases.modelgen.write_model(model, os.path.join(work, "model"))
@@ -114,20 +127,32 @@ def main():
         data["receiver_stride"] = np.int32(stride)
         data["nt"] = np.int32(model.nt)
         data["run_to_run_rel_l2"] = np.float64(spread)
-        if keep_snap:
+        entry = {"seconds": secs, "run_to_run_rel_l2": spread, "samples": int(ra["svz"].shape[0])}
+        if name in cases.NOFMA_CASES and not args.no_nofma:
+            out_c = os.path.join(work, "out_nofma")
+            entry["seconds_nofma"] = run_reference(jpath, out_c, REF_NOFMA_BIN)
+            rc = load_records(out_c, model.nx, solid_only)
+            for k in ra:
+                data["nofma_rel_l2_" + k] = np.float64(rel(rc[k], ra[k]))
+                entry["nofma_rel_l2_" + k] = float(data["nofma_rel_l2_" + k])
+        if step:
+            data["snapshot_step"] = np.int32(step)
             sa = load_snapshot(outs[0], model.nt - 1, model)
             sb = load_snapshot(outs[1], model.nt - 1, model)
             for k in sa:
-                data["snap_" + k] = sa[k]
+                data["snap_" + k] = np.ascontiguousarray(sa[k][::step, ::step])
             data["snap_run_to_run_rel_l2"] = np.float64(max(rel(sa[k], sb[k]) for k in sa))
         os.makedirs(args.outdir, exist_ok=True)
         np.savez_compressed(os.path.join(args.outdir, name + ".npz"), **data)
-        summary[name] = {"seconds": secs, "run_to_run_rel_l2": spread,
-                         "samples": int(ra["svz"].shape[0])}
+        summary[name] = entry
         print(name, json.dumps(summary[name]), flush=True)
         shutil.rmtree(work, ignore_errors=True)
     sp = os.path.join(args.outdir, "golden_summary.json")
-    merged = json.load(open(sp)) if os.path.exists(sp) else {}
+    if not os.path.exists(sp) and os.path.exists(os.path.join(cases.GOLDEN_DIR, "golden_summary.json")):
+        sp0 = os.path.join(cases.GOLDEN_DIR, "golden_summary.json")
+        merged = json.load(open(sp0))
+    else:
+        merged = json.load(open(sp)) if os.path.exists(sp) else {}
     merged.update(summary)
     with open(sp, "w") as f:
         json.dump(merged, f, indent=1)

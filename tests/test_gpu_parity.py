@@ -1,7 +1,10 @@
 """Parity of the CUDA path (libmfdm.so through its C ABI) on a B200.
 
 * against records of the reference's own CUDA build (tests/golden, produced by
-  oracle/_ref/main_debug on a B200) for every golden case, full length;
+  oracle/_ref/main_debug on a B200) for every golden case, full length, up to
+  the 1200 x 800 (6000 steps) and 4096 x 2048 (1500 steps) models; past 1500
+  steps also against the FP32 noise floor measured between two builds of the
+  reference that differ only in FMA contraction, and against the FP64 oracle;
 * against the CPU oracle (FP32 and FP64) on whole wavefields;
 * through size-independent properties at the 4096 x 2048 size (linearity,
   oracle agreement over a bounded number of steps);
@@ -23,7 +26,14 @@ from conftest import rel_l2
 pytestmark = pytest.mark.gpu
 TOL = 1e-5
 ALL_CASES = ["flat_small", "curv_small", "shallow_src", "flat_400x400", "curvilinear_1200x800",
-             "cpml_flat_small", "cpml_curv_small"]
+             "curvilinear_4096x2048", "cpml_flat_small", "cpml_curv_small"]
+# Past 1500 steps the distance to the reference build may also be at most this
+# multiple of the distance between the reference build and the same sources
+# built with FMA contraction off (both FP32, same algorithm, same order), when
+# that is the larger bound. Measured (1200 x 800, 6000 steps): this path
+# 3.6-4.0e-6 from the reference build, the two reference builds 6.5-8.6e-7
+# apart, the reference build 3.3-4.6e-6 from the FP64 oracle.
+NOISE_MULT = 8.0
 
 
 @pytest.fixture(scope="module")
@@ -48,39 +58,51 @@ PREFIX_STEPS = 1500
 
 @pytest.mark.parametrize("name", ALL_CASES)
 def test_records_match_reference_build(lib, cases, name):
-    """<= 1e-5 against the reference build over the first 1500 steps (the whole
-    record for every case but the 6000-step one). Beyond that the FP32 rounding
-    noise of the scheme itself grows past 1e-5 - the reference build drifts from
-    the FP64 oracle by 3-5e-5 at 6000 steps - so over the full record the CUDA
-    path must be no less accurate than the reference build, both measured
-    against the FP64 oracle records stored in the fixture."""
-    build, stride, has_snap = cases.CASES[name]
+    """<= 1e-5 against the reference build over the whole record and the final
+    snapshot (whole, or every k-th row and column at the large sizes); the
+    first 1500 steps are also checked on their own. For the long runs the
+    fixture holds the distance between two reference builds that differ only in
+    FMA contraction (the FP32 rounding-noise floor) and the FP64 oracle's
+    records: the CUDA path must stay within max(1e-5, NOISE_MULT x floor) of
+    the reference build and no further from the FP64 records than
+    max(1e-5, 1.5 x the reference build's own distance to them)."""
+    build, stride, keep = cases.CASES[name]
+    step = cases.snapshot_step(keep)
     model = build()
     g = np.load(cases.fixture_path(name))
     nt = int(g["nt"])
-    rec, fields, info = run_solver(lib, model, nt)
+    rec, fields, info = run_solver(lib, model, nt, fields=bool(step))
     assert info["nsamples"] == g["svx"].shape[0]
     gap = info["gap"]
     npre = -(-min(nt, PREFIX_STEPS) // gap)
+    report = {}
     for k in ("svx", "svz", "fp"):
         e = rel_l2(rec[k][:npre, ::stride], g[k][:npre])
+        report[k + "_prefix"] = e
         assert e <= TOL, (name, k, "prefix", e)
-    if has_snap:
+    if step:
         for key, arr in (("snap_solid_vx", fields["solid_vx"]), ("snap_solid_vz", fields["solid_vz"]),
                          ("snap_fluid_vx", fields["fluid_vx"]), ("snap_fluid_vz", fields["fluid_vz"])):
-            e = rel_l2(arr, g[key])
+            e = rel_l2(arr[::step, ::step], g[key])
+            report[key] = e
             assert e <= TOL, (name, key, e)
-    if nt <= PREFIX_STEPS:
-        return
-    for k in ("svx", "svz", "fp"):
-        e_ref = rel_l2(rec[k][:, ::stride], g[k])
-        if "fp64_" + k in g:
-            ours64 = rel_l2(rec[k][:, ::stride], g["fp64_" + k])
-            ref64 = rel_l2(g[k], g["fp64_" + k])
-            assert ours64 <= max(TOL, 1.5 * ref64), (name, k, ours64, ref64)
-            assert e_ref <= max(TOL, 2.0 * ref64), (name, k, e_ref, ref64)
-        else:
-            assert e_ref <= TOL, (name, k, e_ref)
+    if nt > PREFIX_STEPS:
+        for k in ("svx", "svz", "fp"):
+            e_ref = rel_l2(rec[k][:, ::stride], g[k])
+            report[k + "_full"] = e_ref
+            assert e_ref <= TOL, (name, k, "full record", e_ref)
+            if "nofma_rel_l2_" + k in g:
+                floor = float(g["nofma_rel_l2_" + k])
+                report[k + "_noise_floor"] = floor
+                assert e_ref <= max(TOL, NOISE_MULT * floor), (name, k, e_ref, floor)
+            if "fp64_" + k in g:
+                s64 = int(g["fp64_stride"]) if "fp64_stride" in g else stride
+                ours64 = rel_l2(rec[k][:, ::s64], g["fp64_" + k])
+                ref64 = rel_l2(g[k][:, ::s64 // stride], g["fp64_" + k])
+                report[k + "_fp64"] = ours64
+                report[k + "_ref_fp64"] = ref64
+                assert ours64 <= max(TOL, 1.5 * ref64), (name, k, ours64, ref64)
+    print(name, {k: f"{v:.3e}" for k, v in report.items()})
 
 
 @pytest.mark.parametrize("name", ["flat_small", "curv_small", "shallow_src", "cpml_flat_small",

@@ -13,19 +13,20 @@ TOL = 1e-5
 
 
 def _check_case(oracle, cases, name, nsteps=None, precision=32):
-    build, stride, has_snap = cases.CASES[name]
+    build, stride, keep = cases.CASES[name]
+    k = cases.snapshot_step(keep)
     model = build()
     g = np.load(cases.fixture_path(name))
     nt = int(g["nt"]) if nsteps is None else nsteps
     gap = oracle.record_gap(model.dt)
-    out = oracle.forward(model, nt, gap, precision, final_fields=has_snap and nsteps is None)
+    out = oracle.forward(model, nt, gap, precision, final_fields=bool(k) and nsteps is None)
     ns = out["svx"].shape[0]
-    errs = {k: rel_l2(out[k][:, ::stride], g[k][:ns]) for k in ("svx", "svz", "fp")}
-    if has_snap and nsteps is None:
-        errs["snap_solid_vx"] = rel_l2(out["solid"][0], g["snap_solid_vx"])
-        errs["snap_solid_vz"] = rel_l2(out["solid"][1], g["snap_solid_vz"])
-        errs["snap_fluid_vx"] = rel_l2(out["fluid"][0], g["snap_fluid_vx"])
-        errs["snap_fluid_vz"] = rel_l2(out["fluid"][1], g["snap_fluid_vz"])
+    errs = {r: rel_l2(out[r][:, ::stride], g[r][:ns]) for r in ("svx", "svz", "fp")}
+    if k and nsteps is None:
+        errs["snap_solid_vx"] = rel_l2(out["solid"][0][::k, ::k], g["snap_solid_vx"])
+        errs["snap_solid_vz"] = rel_l2(out["solid"][1][::k, ::k], g["snap_solid_vz"])
+        errs["snap_fluid_vx"] = rel_l2(out["fluid"][0][::k, ::k], g["snap_fluid_vx"])
+        errs["snap_fluid_vz"] = rel_l2(out["fluid"][1][::k, ::k], g["snap_fluid_vz"])
     return errs, out, g
 
 
@@ -78,10 +79,13 @@ def test_record_gap_rounding(oracle):
     assert oracle.record_gap(1e-4) == 10
 
 
-@pytest.mark.parametrize("name", ["solid_flat_small", "solid_curv_small"])
+@pytest.mark.parametrize("name", ["solid_flat_small", "solid_curv_small", "cpml_solid_flat_small",
+                                  "cpml_solid_curv_small"])
 def test_solid_only_oracle_matches_reference(oracle, cases, name):
-    """PmlFs::SolidOnly (calc_type 0): the FP32 restatement against the reference
-    build's solid vz record on row 3 and its final solid snapshot."""
+    """Solid only (calc_type 0): PmlFs::SolidOnly (boundary_type 2) and
+    Cpml::SolidOnly (boundary_type 1), the FP32 restatement against the
+    reference build's solid vz record (row 3 / row 30) and its final solid
+    snapshot."""
     model = cases.CASES[name][0]()
     d = np.load(cases.fixture_path(name))
     r = oracle.forward_solid(model, int(d["nt"]), oracle.record_gap(model.dt), 32,
