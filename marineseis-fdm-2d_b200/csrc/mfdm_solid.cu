@@ -1,4 +1,5 @@
-// sm_100a kernels of the solid-only time step with a free surface (see mfdm_solid.h).
+// sm_100a kernels of the solid-only time step with a free surface (see mfdm_solid.h),
+// and of its four-side CFS-PML variant (the CPML instantiations below).
 //
 // One launch per RK stage does the whole stage: velocity and stress
 // right-hand sides of every cell (the reference's update_velocity and
@@ -43,22 +44,34 @@ struct Out {
   float XV0, XV1, XE0, XE1, ZV0, ZV1, ZE0, ZE1;
 };
 
+// Zeta-ADE row of a cell in a zeta-PML band: the bottom band (rows
+// nz-3-npd..nz-4) at 0..npd-1; with CPML the top band (rows 3..npd+2) after it.
+template <bool CPML>
+__device__ __forceinline__ int zeta_row(int iz, int nz, int npd) {
+  if (CPML && iz <= npd + 2) return npd + iz - 3;
+  return iz - (nz - 3 - npd);
+}
+
 // Right-hand side of cell (iz, ix), 3 <= iz <= nz-4 (include/pml_fs_kernels.cuh:10-307).
+// CPML: the four-side variant Cpml::SolidOnly (include/cpml_kernels.cuh:8-217):
+// no free surface, so every row takes the plain biased operators (rows 0..2
+// are zero), and the zeta-PML also covers the top band (rows 3..npd+2).
 // `A(q, dz, dx)` returns stage-input field q (kVX..kSXZ) dz rows and dx columns
 // away, |dz|, |dx| <= 3; the ADE memory of S is read from global memory.
 // IN: the caller guarantees a cell at least three rows below the free surface
 // and outside every absorbing strip (the branch-free body of interior blocks).
 // `K(c)` returns point-wise coefficient c (kCXIX..kC55) of the cell.
-template <int DIR, bool IN, class Acc, class Kc>
+template <int DIR, bool IN, bool CPML, class Acc, class Kc>
 __device__ __forceinline__ Out rhs(const SCoef& C, const SFields& S, const Acc& A, const Kc& K,
                                    int iz, int ix) {
   Out o;
   const int P = C.P, nx = C.nx, nz = C.nz, npd = C.npd;
   const size_t i = (size_t)iz * P + ix;
-  const int dist = IN ? 3 : iz - 3, distx = min(ix - 3, nx - 4 - ix);
-  const bool side = !IN && distx < npd, bottom = !IN && iz >= nz - 3 - npd;
+  const int dist = (IN || CPML) ? 3 : iz - 3, distx = min(ix - 3, nx - 4 - ix);
+  const bool side = !IN && distx < npd;
+  const bool bottom = !IN && (iz >= nz - 3 - npd || (CPML && iz <= npd + 2));
   const int scol = side ? xstrip_col(ix, nx, npd) : 0;
-  const size_t si = (size_t)iz * C.Ps + scol, zi = (size_t)(iz - (nz - 3 - npd)) * P + ix;
+  const size_t si = (size_t)iz * C.Ps + scol, zi = (size_t)zeta_row<CPML>(iz, nz, npd) * P + ix;
   const float xix = K(kCXIX), xiz = K(kCXIZ), zex = K(kCZEX), zez = K(kCZEZ);
   const float gxixi = xix * xix + xiz * xiz, gzeze = zex * zex + zez * zez;
   const float gxize = xix * zex + xiz * zez;
@@ -255,7 +268,7 @@ __device__ __forceinline__ void store5(const Out& o, const Pt& r, const SFields&
 
 // The kTZ / kBY rows of column ix owned by this thread, from the staged tile;
 // `p` holds the first row's point-wise operands on entry.
-template <int DIR, int KIND, bool IN>
+template <int DIR, int KIND, bool IN, bool CPML>
 __device__ __forceinline__ void rows(const SCoef& C, const SFields& in, const SFields& out,
                                      const SFields& un, const SFields& acc,
                                      const float (&tile)[5][kHH][kHW], int r0, int ix, int s,
@@ -274,7 +287,7 @@ __device__ __forceinline__ void rows(const SCoef& C, const SFields& in, const SF
       for (int q = 0; q < 5; ++q) p.u[q] = A(q, 0, 0);
     }
     auto K = [&](int cf) { return p.k[cf]; };
-    Out o = rhs<DIR, IN>(C, in, A, K, iz, ix);
+    Out o = rhs<DIR, IN, CPML>(C, in, A, K, iz, ix);
     if (!IN) {
       // explosive source on both normal stresses (src/pml_fs_kernels.cu:22-26)
       const int sx = ix - C.srcx, sz = iz - C.srcz;
@@ -292,8 +305,8 @@ __device__ __forceinline__ void rows(const SCoef& C, const SFields& in, const SF
       upd<KIND>(o.XE0, in.x[2], un.x[2], out.x[2], acc.x[2], si, c, w);
       upd<KIND>(o.XE1, in.x[3], un.x[3], out.x[3], acc.x[3], si, c, w);
     }
-    if (!IN && iz >= nz - 3 - npd) {
-      const size_t zi = (size_t)(iz - (nz - 3 - npd)) * P + ix;
+    if (!IN && (iz >= nz - 3 - npd || (CPML && iz <= npd + 2))) {
+      const size_t zi = (size_t)zeta_row<CPML>(iz, nz, npd) * P + ix;
       upd<KIND>(o.ZV0, in.z[0], un.z[0], out.z[0], acc.z[0], zi, c, w);
       upd<KIND>(o.ZV1, in.z[1], un.z[1], out.z[1], acc.z[1], zi, c, w);
       upd<KIND>(o.ZE0, in.z[2], un.z[2], out.z[2], acc.z[2], zi, c, w);
@@ -302,7 +315,7 @@ __device__ __forceinline__ void rows(const SCoef& C, const SFields& in, const SF
   }
 }
 
-template <int DIR, int KIND>
+template <int DIR, int KIND, bool CPML>
 __global__ void __launch_bounds__(kBX * kBY, 4) k_stage(SCoef C, SFields in, SFields out,
                                                                       SFields un, SFields acc, int s,
                                                                       float c, float w) {
@@ -334,23 +347,24 @@ __global__ void __launch_bounds__(kBX * kBY, 4) k_stage(SCoef C, SFields in, SFi
   }
   __syncthreads();
   if (ix > nx - 4) return;
-  // Blocks whose cells are all at least three rows below the free surface, in
-  // no absorbing strip and away from the source take the branch-free body.
-  const bool interior = r0 >= 3 && r0 + kTZ + 2 < nz - 3 - npd && c0 >= npd &&
+  // Blocks whose cells are all at least three rows below the free surface (with
+  // CPML: below the top band), in no absorbing strip and away from the source
+  // take the branch-free body.
+  const bool interior = r0 >= (CPML ? npd : 3) && r0 + kTZ + 2 < nz - 3 - npd && c0 >= npd &&
                         c0 + kBX + 2 <= nx - 4 - npd &&
                         (C.srcx < 0 || C.srcx + 2 < c0 + 3 || C.srcx - 2 > c0 + kBX + 2 ||
                          C.srcz + 2 < r0 + 3 || C.srcz - 2 > r0 + kTZ + 2);
   if (interior)
-    rows<DIR, KIND, true>(C, in, out, un, acc, tile, r0, ix, s, c, w, p);
+    rows<DIR, KIND, true, CPML>(C, in, out, un, acc, tile, r0, ix, s, c, w, p);
   else
-    rows<DIR, KIND, false>(C, in, out, un, acc, tile, r0, ix, s, c, w, p);
+    rows<DIR, KIND, false, CPML>(C, in, out, un, acc, tile, r0, ix, s, c, w, p);
 }
 
 __global__ void k_finish(SCoef C, SFields U) {
   const int ix = blockIdx.x * blockDim.x + threadIdx.x;
   const int it = *C.step;
   if (ix < C.nx) {
-    const float v = U.vz[(size_t)3 * C.P + ix];
+    const float v = U.vz[(size_t)C.rec_row * C.P + ix];
     if (!isfinite(v)) atomicOr(C.status, 1);
     if (C.rec != nullptr && C.gap > 0 && it % C.gap == 0) {
       const int j = it / C.gap;
@@ -379,7 +393,10 @@ cudaError_t launch_t(const SCoef& C, const SFields& in, const SFields& out, cons
                      const SFields& acc, int s, cudaStream_t st) {
   const dim3 grid(unsigned((C.nx - 6 + kBX - 1) / kBX), unsigned((C.nz - 6 + kTZ - 1) / kTZ));
   const float c = C.rk_c[s], w = KIND == kStageLast ? 0.f : C.rk_w[s];
-  k_stage<DIR, KIND><<<grid, dim3(kBX, kBY), 0, st>>>(C, in, out, un, acc, s, c, w);
+  if (C.cpml)
+    k_stage<DIR, KIND, true><<<grid, dim3(kBX, kBY), 0, st>>>(C, in, out, un, acc, s, c, w);
+  else
+    k_stage<DIR, KIND, false><<<grid, dim3(kBX, kBY), 0, st>>>(C, in, out, un, acc, s, c, w);
   return cudaGetLastError();
 }
 

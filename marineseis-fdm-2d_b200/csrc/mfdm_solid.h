@@ -1,6 +1,7 @@
 // Solid only with a free surface on top (the reference's PmlFs::SolidOnly,
-// include/pml_fs_kernels.cuh:8-307, src/pml_fs_kernels.cu:5-381): device data
-// and launchers (library-internal).
+// include/pml_fs_kernels.cuh:8-307, src/pml_fs_kernels.cu:5-381) or with
+// CFS-PML on all four sides (Cpml::SolidOnly, include/cpml_kernels.cuh:8-233,
+// src/cpml_kernels.cu:5-361): device data and launchers (library-internal).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -23,14 +24,16 @@ struct SCoef {
   const float* __restrict__ zez;
   const float* __restrict__ alm;    // [6][P]: al1_xx, al1_zz, al1_xz, al2_xx, al2_zz, al2_xz (row 3)
   const float4* __restrict__ pmlx;  // per column: d/beta, alpha + d/beta, 1/beta
-  const float4* __restrict__ pmlz;  // per row (bottom band)
+  const float4* __restrict__ pmlz;  // per row (bottom band; with cpml also the top band)
   const float* __restrict__ src_amp;  // Ricker value per (step, stage): [steps][4]
   int src_steps;
   int srcx, srcz;                   // source cell (srcx < 0: none)
   float rk_c[4];                    // dt/2, dt/2, dt, dt/6
   float rk_w[3];                    // dt/6, dt/3, dt/3
   int gap, rec_cap;
-  float* rec;                       // [rec_cap][nx]: solid vz on row 3
+  float* rec;                       // [rec_cap][nx]: solid vz on row rec_row
+  int rec_row;                      // 3 (free surface) or 30 (cpml), src/main.cu:303-311
+  int cpml;                         // 1: CFS-PML on all four sides, no free surface
   int* step;                        // device step counter
   unsigned* done;                   // block arrival counter of the finish kernel
   int* status;                      // sticky non-finite flag
@@ -38,7 +41,8 @@ struct SCoef {
 
 // One RK set: the five fields [nz][P], the xi-ADE strips [nz][Ps] (Vx, Vz, Ex,
 // Ez; slot s of column 3+s or nx-3-npd+s-npd) and the zeta-ADE band [npd][P]
-// (rows nz-3-npd..nz-4).
+// (rows nz-3-npd..nz-4; with cpml [2 npd][P], the top band's rows 3..npd+2
+// after the bottom band's).
 struct SFields {
   float *vx, *vz, *sx, *sz, *sxz;
   float* x[4];
@@ -49,7 +53,7 @@ struct SFields {
 // (and U^n = `un`, the accumulator `acc`), writes `out` and the accumulator.
 cudaError_t launch_stage(const SCoef& C, const SFields& in, const SFields& out, const SFields& un,
                          const SFields& acc, int stage, int dir, cudaStream_t st);
-// Records solid vz on row 3 when the step index is a multiple of gap, flags
+// Records solid vz on row rec_row when the step index is a multiple of gap, flags
 // non-finite values and advances the device step counter.
 cudaError_t launch_finish(const SCoef& C, const SFields& U, cudaStream_t st);
 // Sets the device step counter.

@@ -721,11 +721,20 @@ struct Oracle {
 // The model's solid arrays and the metric are all [nz][nx] (nz = nz_s, nz_f
 // unused): the solid fills the grid, the free surface is row 3, CFS-PML on the
 // left, right and bottom.
+// With m.cpml = 1 the same structure restates Cpml::SolidOnly
+// (include/cpml_kernels.cuh:8-233, src/cpml_kernels.cu:5-361): CFS-PML on all
+// four sides, no free surface - every row 3..nz-4 takes the plain biased
+// operators (rows 0..2 read as zeros), the zeta-PML tables have a top band
+// (rows 3..npd+2, src/elements.cu:869-871) whose cells share the zeta-ADE
+// memory with the bottom band, and the record is solid vz on row 30
+// (src/main.cu:303-311).
 enum SField { TVX, TVZ, TSX, TSZ, TSXZ, XVX, XVZ, XEX, XEZ, ZVX, ZVZ, ZEX, ZEZ, NSFIELD };
 
 template <class R>
 struct SolidOracle {
   int nx, nz, npd;
+  bool cpml;
+  int rec_row;
   float fpeak_f, dt_f;
   int srcx, srcz;
   std::vector<R> C11, C13, C33, C55, rho, J, xx, xz, zx, zz;
@@ -743,6 +752,8 @@ struct SolidOracle {
 
   explicit SolidOracle(const orc_model& m) {
     nx = m.nx; nz = m.nz_s; npd = m.npd;
+    cpml = m.cpml != 0;
+    rec_row = cpml ? 30 : 3;
     fpeak_f = float(m.fpeak); dt_f = float(m.dt);
     srcx = m.src_x; srcz = m.src_z;
     const size_t n = size_t(nz) * nx;
@@ -753,8 +764,8 @@ struct SolidOracle {
     alx.assign(nx, 0); bex.assign(nx, 0); dpx.assign(nx, 0);
     alz.assign(nz, 0); bez.assign(nz, 0); dpz.assign(nz, 0);
     pml_profile(m, fpeak_f, npd, alx.data(), bex.data(), dpx.data(), nx, true, true);
-    pml_profile(m, fpeak_f, npd, alz.data(), bez.data(), dpz.data(), nz, false, true);
-    free_surface(m);
+    pml_profile(m, fpeak_f, npd, alz.data(), bez.data(), dpz.data(), nz, cpml, true);
+    if (!cpml) free_surface(m);
     alloc(U); alloc(Ub); alloc(Ut); alloc(Kk);
   }
 
@@ -826,14 +837,17 @@ struct SolidOracle {
             J[i] * (xx[i] * S[TSXZ][i] + xz[i] * S[TSZ][i])};
   }
 
+  // A cell of the zeta-PML band(s): the bottom band, and with cpml the top band.
+  bool zeta_band(int iz) const { return iz >= nz - 3 - npd || (cpml && iz <= npd + 2); }
+
   void stress(int dir, const Set& S) {
 #pragma omp parallel for schedule(static)
     for (int iz = 3; iz <= nz - 4; ++iz)
       for (int ix = 3; ix <= nx - 4; ++ix) {
         const size_t i = size_t(iz) * nx + ix;
-        const int dist = iz - 3, distx = std::min(ix - 3, nx - 4 - ix);
+        const int dist = cpml ? 3 : iz - 3, distx = std::min(ix - 3, nx - 4 - ix);
         const R dvx_dxi = dmac(dir, &S[TVX][i], 1), dvz_dxi = dmac(dir, &S[TVZ][i], 1);
-        const bool side = distx < npd, bottom = iz >= nz - 3 - npd;
+        const bool side = distx < npd, bottom = zeta_band(iz);
         const R c11 = C11[i], c13 = C13[i], c33 = C33[i], c55 = C55[i];
         if (dist == 0) {
           const R* a = &alm[size_t(ix) * 6];
@@ -899,7 +913,7 @@ struct SolidOracle {
     for (int iz = 3; iz <= nz - 4; ++iz)
       for (int ix = 3; ix <= nx - 4; ++ix) {
         const size_t i = size_t(iz) * nx + ix;
-        const int dist = iz - 3;
+        const int dist = cpml ? 3 : iz - 3;
         const R xix = xx[i], xiz = xz[i], zex = zx[i], zez = zz[i];
         const R gxixi = xix * xix + xiz * xiz, gzeze = zex * zex + zez * zez;
         R rvx, rvz, dxx, dxz, dzx, dzz;
@@ -939,7 +953,7 @@ struct SolidOracle {
           dzz = zex * (gxize / gzeze * tdx + tdz) + zez * (gxize / gzeze * szdx + szdz);
         }
         const int distx = std::min(ix - 3, nx - 4 - ix);
-        const bool side = distx < npd, bottom = iz >= nz - 3 - npd;
+        const bool side = distx < npd, bottom = zeta_band(iz);
         const R r0 = rho[i];
         R kvx = rvx / r0, kvz = rvz / r0;
         if (side) {
@@ -990,7 +1004,7 @@ struct SolidOracle {
       const int d = std::min(ix - 3, nx - 4 - ix);
       return ix >= 3 && ix <= nx - 4 && d < npd;
     }
-    return iz >= nz - 3 - npd && iz <= nz - 4;
+    return iz >= 3 && iz <= nz - 4 && zeta_band(iz);
   }
   template <class Fn> void for_cells(Fn fn) {
 #pragma omp parallel for schedule(static)
@@ -1043,7 +1057,7 @@ int run_solid(const orc_model* m, int nsteps, int gap, double* rvz, double* out)
     o.step(it);
     if (gap > 0 && it % gap == 0 && rvz)
       for (int ix = 0; ix < nx; ++ix)
-        rvz[size_t(it / gap) * nx + ix] = double(o.U[TVZ][size_t(3) * nx + ix]);
+        rvz[size_t(it / gap) * nx + ix] = double(o.U[TVZ][size_t(o.rec_row) * nx + ix]);
   }
   if (out) {
     const size_t n = size_t(m->nz_s) * nx;
@@ -1121,9 +1135,10 @@ int orc_forward(const orc_model* m, int precision, int nsteps, int gap, double* 
   return rc;
 }
 
-// Solid only with a free surface (PmlFs::SolidOnly): nz_s is the grid's row
-// count, the solid and metric arrays are [nz_s][nx], nz_f and the fluid arrays
-// are unused. Records: solid vz on row 3 every `gap` steps ([ceil(nsteps/gap)][nx]);
+// Solid only with a free surface (PmlFs::SolidOnly), or with CFS-PML on all four
+// sides (Cpml::SolidOnly) when m->cpml: nz_s is the grid's row count, the solid
+// and metric arrays are [nz_s][nx], nz_f and the fluid arrays are unused.
+// Records: solid vz on row 3 (row 30 with cpml) every `gap` steps ([ceil(nsteps/gap)][nx]);
 // out_solid: the final [5][nz_s][nx] (vx, vz, sx, sz, sxz).
 int orc_forward_solid(const orc_model* m, int precision, int nsteps, int gap, double* rec_vz,
                       double* out_solid, int nthreads) {

@@ -120,10 +120,13 @@ def _model_struct(model, shot=0, round_inputs=True):
 def forward_solid(model, nsteps: int, gap: int, precision: int = 32, shot: int = 0,
                   final_fields: bool = False, nthreads: int = 0,
                   round_inputs: bool = True) -> Dict[str, np.ndarray]:
-    """Solid-only oracle (PmlFs::SolidOnly) for a modelgen.SolidModel, from rest.
+    """Solid-only oracle for a modelgen.SolidModel, from rest: PmlFs::SolidOnly
+    (boundary_type 2, free surface on top) or Cpml::SolidOnly (boundary_type 1,
+    CFS-PML on all four sides).
 
-    Returns the record ``svz`` (solid vz on row 3) [ceil(nsteps/gap)][nx] and,
-    when asked, the final ``solid`` [5][nz][nx] (vx, vz, sx, sz, sxz)."""
+    Returns the record ``svz`` (solid vz on row 3; row 30 with boundary_type 1)
+    [ceil(nsteps/gap)][nx] and, when asked, the final ``solid`` [5][nz][nx]
+    (vx, vz, sx, sz, sxz)."""
     keep = []
 
     def arr(a):
@@ -145,7 +148,7 @@ def forward_solid(model, nsteps: int, gap: int, precision: int = 32, shot: int =
     m.rho_s = arr(model.solid["rho"])
     m.J, m.xi_x, m.xi_z = arr(model.metric["J"]), arr(model.metric["xi_x"]), arr(model.metric["xi_z"])
     m.ze_x, m.ze_z = arr(model.metric["ze_x"]), arr(model.metric["ze_z"])
-    m.cpml = 0
+    m.cpml = 1 if getattr(model, "boundary_type", 2) == 1 else 0
     ns = -(-nsteps // gap) if gap > 0 else 0
     rec = np.zeros((ns, model.nx))
     so = np.zeros((5, model.nz, model.nx)) if final_fields else None

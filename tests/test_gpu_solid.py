@@ -1,8 +1,11 @@
-"""Solid only with a free surface (calc_type 0, the reference's PmlFs::SolidOnly) on a B200.
+"""Solid only (calc_type 0) on a B200: with a free surface (boundary_type 2, the
+reference's PmlFs::SolidOnly) and with CFS-PML on all four sides
+(boundary_type 1, Cpml::SolidOnly).
 
-The reference build's records (solid vz on row 3) and final snapshots of two
-seeded models are the golden fixtures (tests/golden/solid_*.npz, pinned to the
-FP32 oracle by tests/test_oracle.py); the CUDA path must match them and the
+The reference build's records (solid vz on row 3; row 30 with four-side PML)
+and final snapshots of two seeded models per boundary type are the golden
+fixtures (tests/golden/solid_*.npz, cpml_solid_*.npz, pinned to the FP32
+oracle by tests/test_oracle.py); the CUDA path must match them and the
 oracle's final fields to a relative L2 of 1e-5.
 """
 import os
@@ -13,7 +16,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-SOLID = ("solid_flat_small", "solid_curv_small")
+SOLID = ("solid_flat_small", "solid_curv_small", "cpml_solid_flat_small", "cpml_solid_curv_small")
 
 
 @pytest.fixture(scope="module")
@@ -89,6 +92,24 @@ def test_cli_writes_the_solid_only_tree(lib, cases, modelgen, tmp_path):
     last = np.fromfile(shot / "snapshot" / "solid" / "vz" / "vz_000100.bin", dtype="<f4")
     _, f101 = run(lib, model, 101)
     assert np.array_equal(last.reshape(model.nz, model.nx), f101["solid_vz"])
+
+
+def test_cli_runs_four_side_cpml_solid(lib, cases, modelgen, tmp_path):
+    """calc_type 0 with boundary_type 1 through the drop-in command line: the
+    record file holds solid vz on row 30 (src/main.cu:303-311)."""
+    model = cases.cpml_solid_curv_small()
+    model.nt, model.snapshot = 150, 100
+    j = modelgen.write_model(model, str(tmp_path / "model"))
+    out = tmp_path / "out"
+    r = subprocess.run([lib.CLI_PATH, j, str(out)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    rec, f = run(lib, model, 150)
+    got = np.fromfile(out / "0" / "record" / "solid_vz.bin", dtype="<f4").reshape(rec["svz"].shape)
+    assert np.array_equal(got, rec["svz"])
+    assert rec["svz"].shape == (75, model.nx) and np.abs(rec["svz"]).max() > 0
+    # the last sample is taken after step it = 148, i.e. row 30 of the state after 149 steps
+    _, f149 = run(lib, model, 149)
+    assert np.array_equal(rec["svz"][-1], f149["solid_vz"][30])
 
 
 def test_solid_only_rejects_bad_input(lib, cases):
