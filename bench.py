@@ -19,6 +19,13 @@ roofline: algorithmic bytes per step (16 S + 4 M floats per cell: 464 B solid,
          average durations of the four stage launches.
 With N > 1 every rank runs its own copy of the workload (independent shots):
 weak scaling, no data-path collective.
+other_workloads.reference_cuda_build: the reference's own CUDA build
+         (oracle/_ref/main_debug, compiled from its sources) and this library's
+         drop-in CLI on the same JSON models, per-step time from the difference
+         of median wall times of a short and a long run (start-up, model
+         loading and file output cancel), snapshots off.
+fp64_error: relative L2 distance of every result to the FP64 oracle over a
+         bounded number of steps (the largest over the state fields).
 """
 from __future__ import annotations
 
@@ -27,9 +34,11 @@ import importlib
 import json
 import math
 import os
+import shutil
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -46,6 +55,94 @@ WORKLOADS = {
 }
 DEFAULT_WORKLOAD = "curvilinear_4096x2048"
 METRIC = "Gcell-updates/s (fluid-solid RK4 step, % HBM roofline)"
+
+
+def bench_config(args, model, world: int) -> dict:
+    """The `config` object both arms print (the same workload)."""
+    return {"workload": args.workload, "nx": model.nx, "nz_f": model.nz_f,
+            "nz_s": model.nz_s, "cells": model.cells, "npd": model.npd,
+            "parallelism": f"independent shots x{world}",
+            "l2": "inputs larger than L2 (state + coefficients > 126 MB)"}
+
+
+def rel_l2(a, b) -> float:
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    n = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / n) if n > 0 else float(np.linalg.norm(a))
+
+
+STATE = ("fluid_vx", "fluid_vz", "fluid_p", "solid_vx", "solid_vz", "solid_sx", "solid_sz",
+         "solid_sxz")
+
+
+def fp64_error(mfdm, model, steps: int, device: int, shot=None) -> dict:
+    """Largest relative L2 distance over the eight state fields between the CUDA
+    path and the FP64 oracle after `steps` steps from rest (a bounded sample of
+    the workload; the oracle runs on the host). `shot` = (x, z, fpeak, beta0)
+    sets the source and frequency of a batched shot."""
+    import copy
+    from oracle import pyoracle
+    pyoracle.build()
+    m = copy.deepcopy(model)
+    if shot is not None:
+        m.src_x, m.src_z, m.fpeak, m.beta0 = [shot[0]], [shot[1]], shot[2], shot[3]
+    with mfdm.Solver.from_model(m, device=device) as s:
+        s.set_shot(0, reset=True)
+        s.step(steps)
+        ours = {n: s.field(n) for n in STATE}
+    ref = pyoracle.forward(m, steps, pyoracle.record_gap(m.dt), 64, final_fields=True)
+    refs = dict(zip(STATE, list(ref["fluid"]) + list(ref["solid"])))
+    errs = {n: rel_l2(ours[n], refs[n]) for n in STATE}
+    worst = max(errs, key=errs.get)
+    return {"rel_l2": float(f"{errs[worst]:.3e}"), "field": worst, "steps": steps}
+
+
+def wall_run(binary: str, jpath: str, out: str) -> float:
+    t0 = time.perf_counter()
+    subprocess.run([binary, jpath, out], check=True, stdout=subprocess.DEVNULL,
+                   stderr=subprocess.DEVNULL)
+    return time.perf_counter() - t0
+
+
+def reference_cuda_build(workloads, repeats: int = 3) -> dict:
+    """The reference's CUDA build (oracle/_ref/main_debug, its own sources compiled
+    for sm_100a) and this library's drop-in CLI on the same JSON models, snapshots
+    off (snapshot > nt). Per-step time = (median wall time of the long run -
+    that of the short run) / step difference, runs interleaved (src/main.cu:136-213
+    is the reference's timed loop; start-up, model reading and record output
+    cancel in the difference)."""
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "main_debug")
+    our_bin = os.path.join(ROOT, "marineseis-fdm-2d_b200", "bin", "main_debug")
+    if not (os.path.exists(ref_bin) and os.path.exists(our_bin)):
+        return {"unavailable": "oracle/_ref/main_debug not built (needs the reference sources)"}
+    out = {}
+    for name, build, n1, n2 in workloads:
+        work = tempfile.mkdtemp(prefix="mfdm_refbuild_")
+        try:
+            model = build(n1)
+            model.snapshot = n2 + 1
+            j1 = modelgen.write_model(model, work, name="short")
+            cfg = json.load(open(j1))
+            cfg["base"]["nt"] = n2
+            j2 = os.path.join(work, "long.json")
+            with open(j2, "w") as f:
+                json.dump(cfg, f)
+            row = {}
+            for label, binary in (("reference", ref_bin), ("library", our_bin)):
+                wall_run(binary, j1, os.path.join(work, "out"))  # page the model files in
+                runs = {n1: [], n2: []}
+                for _ in range(repeats):
+                    for nt, j in ((n1, j1), (n2, j2)):
+                        runs[nt].append(wall_run(binary, j, os.path.join(work, "out")))
+                ms = (statistics.median(runs[n2]) - statistics.median(runs[n1])) / (n2 - n1) * 1e3
+                row[label] = {"ms_per_step": round(ms, 4),
+                              "gcells": round(model.cells / (ms / 1e3) / 1e9, 3)}
+            row["speedup"] = round(row["reference"]["ms_per_step"] / row["library"]["ms_per_step"], 2)
+            row["steps"] = [n1, n2]
+            out[name] = row
+        finally:
+            shutil.rmtree(work, ignore_errors=True)
+    return out
 
 
 def algorithmic_bytes(m) -> int:
@@ -191,8 +288,7 @@ def run_reference(args, model, world, rank):
         "n_gpus": args.gpus, "steps": steps, "warmup": warm + 1,
         "ms_per_step": round(secs / steps * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "nx": model.nx, "nz_f": model.nz_f,
-                   "nz_s": model.nz_s, "cells": model.cells},
+        "config": bench_config(args, model, world),
         "cpu_baseline": {"value": round(value, 4), "unit": "Gcell/s", "cores": threads,
                          "kind": "port", "sample": sample},
         "e2e": {"value": round(value, 4), "unit": "Gcell/s", "h2d_bytes_per_step": 0,
@@ -277,11 +373,18 @@ def uneven_rate(mfdm, device: int, nmodels: int = 32, steps: int = 128):
 
 def adjoint_rate(mfdm, device: int, nsteps: int = 4000, every: int = 50):
     """Cost of the adjoint-state gradient against a plain forward run on the
-    800x400 curvilinear model (4000 RK4 steps, checkpoint every 50): host
-    wall time of the synchronous calls. The adjoint's forward pass (with
-    checkpoints) plus its backward pass is compared with mfdm_step over the
-    same steps; the one-time operator assembly is listed separately."""
-    m = modelgen.curvilinear(800, 400, nt=nsteps)
+    800x400 curvilinear model pair (4000 RK4 steps, checkpoint every 50): host
+    wall time of the synchronous calls. The observed records come from the true
+    model (+10 % vs Gaussian anomaly); the gradient is that of the L2 misfit
+    of the smoothed initial model's records against them. The adjoint's
+    forward pass (with checkpoints) plus its backward pass is compared with
+    mfdm_step over the same steps; the one-time operator assembly is listed
+    separately."""
+    true, m = modelgen.adjoint_pair(800, 400, nt=nsteps)
+    with mfdm.Solver.from_model(true, device=device) as st:
+        st.set_shot(0, reset=True)
+        st.step(nsteps)
+        obs = st.records()
     with mfdm.Solver.from_model(m, device=device) as s:
         s.set_shot(0, reset=True)
         s.step(64)
@@ -295,10 +398,10 @@ def adjoint_rate(mfdm, device: int, nsteps: int = 4000, every: int = 50):
         t0 = time.perf_counter()
         rec = s.adjoint_forward(nsteps, every)
         afwd = time.perf_counter() - t0
-        rng = np.random.default_rng(1)
-        res = {k: rng.standard_normal(v.shape).astype(np.float32) for k, v in rec.items()}
+        res = {k: (rec[k] - obs[k]).astype(np.float32) for k in rec}
+        misfit = 0.5 * sum(float(np.sum(np.float64(r) ** 2)) for r in res.values())
         t0 = time.perf_counter()
-        s.adjoint_backward(res)
+        grad = s.adjoint_backward(res)
         bwd = time.perf_counter() - t0
         # the same with every segment's stage inputs kept in device memory
         # (no recompute; 4 * 4000 states of this model, about 85 GB of HBM)
@@ -313,13 +416,80 @@ def adjoint_rate(mfdm, device: int, nsteps: int = 4000, every: int = 50):
         s.adjoint_backward(res)
         kbwd = time.perf_counter() - t0
         s.adjoint_memory(0)
-    return {"model": "curvilinear 800x400", "steps": nsteps, "ckpt_every": every,
+    # where the vs anomaly sits: the solid C55 gradient should be largest near it
+    g55 = np.abs(grad["C55"])
+    iz, ix = np.unravel_index(int(np.argmax(g55)), g55.shape)
+    return {"model": "curvilinear 800x400, true (+10 % vs anomaly) / smoothed initial",
+            "steps": nsteps, "ckpt_every": every, "misfit": float(f"{misfit:.6e}"),
+            "max_abs_dC55_at": [int(iz), int(ix)],
             "forward_s": round(fwd, 4), "adjoint_forward_s": round(afwd, 4),
             "backward_s": round(bwd, 4), "assembly_s": round(first - afwd, 4),
             "adjoint_over_forward": round((afwd + bwd) / fwd, 3),
             "kept_segments": {"adjoint_forward_s": round(kfwd, 4), "backward_s": round(kbwd, 4),
                               "keep_setup_s": round(kfirst - kfwd, 4),
                               "adjoint_over_forward": round((kfwd + kbwd) / fwd, 3)}}
+
+
+def large_adjoint_rate(mfdm, device: int, nshots: int = 1, nsteps: int = 200, every: int = 100,
+                       inner: int = 5, ckpt_probe_steps: int = 0):
+    """The 8192 x 4096 batched-adjoint workload (von Kármán rough seafloor, Hurst
+    0.7, rms 20 m, correlation 200 m, seed 5; 16 sources, 10 Hz) at a reduced
+    step count: `nshots` of its shots one after another on one handle, two
+    checkpoint levels (a state every `every` steps; the backward pass re-runs
+    each segment keeping a state every `inner` steps), the L2 misfit of the
+    records against zero observations, gradients summed on the device in FP32.
+    Host wall time of the synchronous calls; device memory in use measured with
+    cudaMemGetInfo after each shot (its largest value, minus what was in use
+    before the handle opened). With ckpt_probe_steps > 0 an adjoint forward
+    pass of that many steps also measures the memory of its checkpoints."""
+    import torch
+    m = modelgen.rough_seafloor(8192, 4096, nt=nsteps)
+    torch.cuda.synchronize(device)
+    free0, total = torch.cuda.mem_get_info(device)
+    peak, shots_s = 0, []
+    with mfdm.Solver.from_model(m, device=device) as s:
+        info = s.info()
+        s.set_shot(0, reset=True)
+        s.step(8)
+        s.set_shot(0, reset=True)
+        t0 = time.perf_counter()
+        s.step(nsteps)
+        fwd = time.perf_counter() - t0
+        s.adjoint_inner(inner)
+        acc = torch.zeros((2 * info["nz_f"] + 5 * info["nz_s"]) * info["nx"], dtype=torch.float32,
+                          device=f"cuda:{device}")
+        s.set_shot(0, reset=True)
+        t0 = time.perf_counter()
+        s.adjoint_forward(nsteps, every)  # first call: operator assembly
+        first = time.perf_counter() - t0
+        for shot in range(nshots):
+            s.set_shot(shot, reset=True)
+            t0 = time.perf_counter()
+            rec = s.adjoint_forward(nsteps, every)
+            t1 = time.perf_counter()
+            s.adjoint_backward_only(rec)
+            s.adjoint_accumulate_grad(acc)
+            torch.cuda.synchronize(device)
+            t2 = time.perf_counter()
+            peak = max(peak, free0 - torch.cuda.mem_get_info(device)[0])
+            shots_s.append((t1 - t0, t2 - t1))
+        probe = None
+        if ckpt_probe_steps > 0:
+            s.set_shot(0, reset=True)
+            t0 = time.perf_counter()
+            s.adjoint_forward(ckpt_probe_steps, every)
+            probe = {"steps": ckpt_probe_steps, "adjoint_forward_s": round(time.perf_counter() - t0, 3),
+                     "device_gb_in_use": round((free0 - torch.cuda.mem_get_info(device)[0]) / 1e9, 2)}
+    afwd = statistics.median(a for a, _ in shots_s)
+    bwd = statistics.median(b for _, b in shots_s)
+    return {"model": "rough seafloor 8192x4096 (von Karman H 0.7, rms 20 m, corr 200 m, seed 5), "
+                     "16 sources, 10 Hz", "cells": m.cells, "shots_run": nshots, "steps": nsteps,
+            "ckpt_every": every, "inner_every": inner, "forward_s": round(fwd, 4),
+            "assembly_s": round(first - afwd, 3), "adjoint_forward_s": round(afwd, 4),
+            "backward_s": round(bwd, 4), "adjoint_over_forward": round((afwd + bwd) / fwd, 3),
+            "device_gb_peak": round(peak / 1e9, 2), "device_gb_total": round(total / 1e9, 1),
+            "grad_abs_max": float(f"{float(acc.abs().max()):.4e}"),
+            "checkpoint_probe": probe}
 
 
 def solid_only_rate(mfdm, device: int, n: int = 2048, steps: int = 256):
@@ -333,12 +503,23 @@ def solid_only_rate(mfdm, device: int, n: int = 2048, steps: int = 256):
         s.set_shot(0, reset=True)
         s.step(32)
         ms = s.time_steps(steps)
+        # FP64 error: 40 steps from rest against the FP64 solid-only oracle
+        from oracle import pyoracle
+        pyoracle.build()
+        s.set_shot(0, reset=True)
+        s.step(40)
+        names = ("solid_vx", "solid_vz", "solid_sx", "solid_sz", "solid_sxz")
+        ours = [s.field(k) for k in names]
+    ref = pyoracle.forward_solid(m, 40, pyoracle.record_gap(m.dt), 64, final_fields=True)
+    errs = {k: rel_l2(a, b) for k, a, b in zip(names, ours, ref["solid"])}
+    worst = max(errs, key=errs.get)
     gcells = m.cells * steps / (ms / 1e3) / 1e9
     gbs = m.cells * 464 * steps / (ms / 1e3) / 1e9
     peak, _ = peaks()
     return {"grid": f"{n}x{n}", "steps": steps, "value": round(gcells, 3), "unit": "Gcell/s",
             "ms_per_step": round(ms / steps, 4), "achieved_gbs": round(gbs, 1),
-            "frac_of_measured_hbm": round(gbs / peak, 4)}
+            "frac_of_measured_hbm": round(gbs / peak, 4),
+            "fp64_error": {"rel_l2": float(f"{errs[worst]:.3e}"), "field": worst, "steps": 40}}
 
 
 def main():
@@ -358,11 +539,23 @@ def main():
     ap.add_argument("--adjoint-profile", action="store_true",
                     help="only a short adjoint run on the 800x400 model (16 steps, checkpoint "
                          "every 8, seeded residuals): a launch list of the adjoint kernels for ncu")
+    ap.add_argument("--large-adjoint", type=int, nargs=5, default=None,
+                    metavar=("SHOTS", "STEPS", "EVERY", "INNER", "PROBE"),
+                    help="only the 8192x4096 rough-seafloor adjoint: SHOTS shots of STEPS steps, "
+                         "checkpoints every EVERY / INNER steps, and a PROBE-step checkpoint "
+                         "memory probe (0: none)")
     ap.add_argument("--solid-profile", type=int, default=0, metavar="N",
                     help="only a short solid-only run on an N x N model (3 + 8 steps): a launch "
                          "list of the solid-only kernels for ncu")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+
+    if args.large_adjoint:
+        mfdm = importlib.import_module("marineseis-fdm-2d_b200")
+        mfdm.load_library()
+        sh, st, ev, inn, pr = args.large_adjoint
+        print(json.dumps({"large_adjoint": large_adjoint_rate(mfdm, 0, sh, st, ev, inn, pr)}))
+        return
 
     if args.solid_profile:
         mfdm = importlib.import_module("marineseis-fdm-2d_b200")
@@ -489,23 +682,41 @@ def main():
             other["curvilinear_1200x800"] = {
                 "value": round(small.cells * n2 / (t2 / 1e3) / 1e9, 3), "unit": "Gcell/s",
                 "ms_per_step": round(t2 / n2, 4)}
+        other["curvilinear_1200x800"]["fp64_error"] = fp64_error(mfdm, small, 300, local)
         other["batched_1200x800_64_shots"] = batched_rate(mfdm, small, local, args.warmup)
+        other["batched_1200x800_64_shots"]["fp64_error"] = dict(
+            fp64_error(mfdm, small, 300, local, shot=batched_shots(small, 64)[0]),
+            note="shot 0 with its own frequency; every batched shot is bit-identical to "
+                 "the same shot run alone (tests/test_gpu_batch.py)")
         other["uneven_32_models"] = uneven_rate(mfdm, local)
+        m0 = modelgen.uneven_models(1, seed=3, nt=10)[0]
+        other["uneven_32_models"]["fp64_error"] = dict(
+            fp64_error(mfdm, m0, 200, local),
+            note="model 0; every grouped model is bit-identical to the model stepped alone")
         other["adjoint_800x400"] = adjoint_rate(mfdm, local)
+        _, m_init = modelgen.adjoint_pair(800, 400, nt=10)
+        other["adjoint_800x400"]["fp64_error"] = dict(
+            fp64_error(mfdm, m_init, 400, local),
+            note="forward state of the initial model; the gradient against the FP64 "
+                 "adjoint oracle is checked in tests/test_gpu_adjoint.py (rel-L2 <= 1e-3)")
         other["solid_only_2048x2048"] = solid_only_rate(mfdm, local)
+        other["adjoint_8192x4096_rough_seafloor"] = large_adjoint_rate(mfdm, local)
+        other["reference_cuda_build"] = reference_cuda_build([
+            ("curvilinear_4096x2048", lambda nt: modelgen.curvilinear_4096x2048(nt=nt), 100, 1100),
+            ("curvilinear_1200x800", lambda nt: modelgen.curvilinear_1200x800(nt=nt), 500, 4500)])
 
     clocks = clk.summary()
     solver.close()
+    fp64 = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        fp64 = fp64_error(mfdm, model, 40, local)
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "Gcell/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generator, no dataset)",
-            "config": {"workload": args.workload, "nx": model.nx, "nz_f": model.nz_f,
-                       "nz_s": model.nz_s, "cells": model.cells, "npd": model.npd,
-                       "parallelism": f"independent shots x{world}",
-                       "l2": "inputs larger than L2 (state + coefficients > 126 MB)"},
+            "config": bench_config(args, model, world),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_kind": peak_kind,
@@ -517,6 +728,7 @@ def main():
                     "h2d_bytes_per_step": int(h2d // args.steps),
                     "d2h_bytes_per_step": int(d2h // args.steps), **e2e_parts},
             "cpu_baseline": cpu,
+            "fp64_error": fp64,
             "clocks": clocks,
             "other_workloads": other,
         }

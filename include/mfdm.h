@@ -277,12 +277,24 @@ int mfdm_adjoint_forward(mfdm_model* m, int nsteps, int ckpt_every);
 int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_svz,
                           const float* res_fp, mfdm_coef_grad* grad);
 
-/* ---- solid only with a free surface --------------------------------------
+/* Adds the gradient of the preceding mfdm_adjoint_backward, each value rounded
+ * to FP32, to the caller's device buffer `dst` of (2 nz_f + 5 nz_s) x nx floats
+ * (K, 1/rho_f, C11, C13, C33, C55, 1/rho_s, each [rows][nx], packed), on
+ * `stream` (a cudaStream_t; NULL = legacy default stream) and returns without
+ * waiting. The gradient stays on the device: a rank sums its shots into one
+ * buffer and the ranks all-reduce it there. No counterpart in the reference,
+ * which has no adjoint. */
+int mfdm_adjoint_accumulate_grad_f32(mfdm_model* m, float* dst, void* stream);
+
+/* ---- solid only --------------------------------------------------------------
  * calc_type 0 with boundary_type 2: the reference's PmlFs::SolidOnly
  * (include/pml_fs_kernels.cuh:8-307, src/pml_fs_kernels.cu:5-381): an elastic
  * solid filling the grid, a traction-free surface on row 3 (ALM coefficients,
  * src/elements.cu:907-977), CFS-PML left, right and bottom, an explosive source
  * on sx and sz. The receiver row is solid vz on row 3 (src/main.cu:284-300).
+ * calc_type 0 with boundary_type 1: Cpml::SolidOnly (include/cpml_kernels.cuh:
+ * 8-233, src/cpml_kernels.cu:5-361): CFS-PML on all four sides, no free
+ * surface, receiver row 30 (src/main.cu:303-311).
  * The drop-in command line takes this path when the JSON has calc_type 0. */
 typedef struct mfdm_solid mfdm_solid;
 
@@ -298,6 +310,9 @@ typedef struct mfdm_solid_desc {
   const int* src_z;
   const float *C11, *C13, *C33, *C55, *rho;
   const float *J, *xi_x, *xi_z, *ze_x, *ze_z;
+  int boundary_type;  /* 2 (or 0): free surface on top; 1: CFS-PML on all four
+                         sides, Cpml::SolidOnly (include/cpml_kernels.cuh:8-233),
+                         the record row is then row 30 (src/main.cu:303-311) */
 } mfdm_solid_desc;
 
 int mfdm_solid_open_json(const char* json_path, int device, mfdm_solid** out);
@@ -373,6 +388,25 @@ typedef struct mfdm_device_model {
   float* sz_s;
   float* sxz_s;
 } mfdm_device_model;
+
+/* ---- phase-shift dispersion imaging ----------------------------------------
+ * Replaces the reference's post-processing `dispersion_imaging`
+ * (tools/test.py:50-98) with a GPU pass over a receiver gather: the real FFT
+ * of every trace over time, the phase spectrum conj(S)/|S|, and for every
+ * frequency bin w_k = 2 pi k fs / nt (k = 0 .. nt/2) and test velocity
+ * c_j = c_min + j dc the normalised stack
+ * A[k][j] = |sum_r P[k][r] exp(-i w_k x_r / c_j)| / ntr, all in FP64.
+ * Number of test velocities of (c_min, c_max, dc) (numpy.arange(c_min,
+ * c_max + dc/2, dc)); 0 for an invalid range. */
+int mfdm_dispersion_velocities(double c_min, double c_max, double dc);
+
+/* gather: host [nt][ntr] float32 (the mfdm_get_records layout, traces already
+ * selected); offsets: host [ntr] signed source-receiver offsets (m); fs:
+ * sampling rate (Hz); amplitude: host [nt/2+1][nv] with nv from
+ * mfdm_dispersion_velocities. Allocates its device buffers on `device` and
+ * frees them before it returns. */
+int mfdm_dispersion_image(const float* gather, int nt, int ntr, const double* offsets, double fs,
+                          double c_min, double c_max, double dc, float* amplitude, int device);
 
 /* Size of the library's static device array used by mfdm_step_noalloc; every
  * GPU that loads the library holds it until the process exits. */

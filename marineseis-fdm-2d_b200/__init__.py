@@ -40,7 +40,8 @@ EXPORTS = ("mfdm_last_error", "mfdm_open_json", "mfdm_open_desc", "mfdm_load_des
            "mfdm_solid_open_json", "mfdm_solid_open_desc", "mfdm_solid_set_shot", "mfdm_solid_step",
            "mfdm_solid_time_steps", "mfdm_solid_get_records", "mfdm_solid_get_field",
            "mfdm_solid_get_info", "mfdm_solid_close", "mfdm_set_blocks_per_sm",
-           "mfdm_adjoint_set_inner")
+           "mfdm_adjoint_set_inner", "mfdm_adjoint_accumulate_grad_f32",
+           "mfdm_dispersion_velocities", "mfdm_dispersion_image")
 
 # Coefficient arrays the adjoint differentiates (mfdm_coef_grad order).
 GRAD_COEFS = ("K", "rcp_rho_f", "C11", "C13", "C33", "C55", "rcp_rho_s")
@@ -89,7 +90,8 @@ class SolidDesc(ctypes.Structure):
                 ("rc", ctypes.c_float), ("beta0", ctypes.c_float),
                 ("nsrc", ctypes.c_int), ("src_x", _ip), ("src_z", _ip),
                 ("C11", _fp), ("C13", _fp), ("C33", _fp), ("C55", _fp), ("rho", _fp),
-                ("J", _fp), ("xi_x", _fp), ("xi_z", _fp), ("ze_x", _fp), ("ze_z", _fp)]
+                ("J", _fp), ("xi_x", _fp), ("xi_z", _fp), ("ze_x", _fp), ("ze_z", _fp),
+                ("boundary_type", ctypes.c_int)]
 
 
 class CoefGrad(ctypes.Structure):
@@ -177,6 +179,12 @@ def load_library(path: str = LIB_PATH):
                                                ctypes.POINTER(ctypes.c_int)]),
         "mfdm_solid_close": (ctypes.c_int, [vp]),
         "mfdm_adjoint_backward": (ctypes.c_int, [vp, _fp, _fp, _fp, ctypes.POINTER(CoefGrad)]),
+        "mfdm_adjoint_accumulate_grad_f32": (ctypes.c_int, [vp, vp, vp]),
+        "mfdm_dispersion_velocities": (ctypes.c_int, [ctypes.c_double] * 3),
+        "mfdm_dispersion_image": (ctypes.c_int, [_fp, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.POINTER(ctypes.c_double), ctypes.c_double,
+                                                 ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                 _fp, ctypes.c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -320,7 +328,19 @@ class Solver:
         arrays (mfdm_adjoint_backward): {'K', 'rcp_rho_f'}: [nz_f][nx] and
         {'C11', 'C13', 'C33', 'C55', 'rcp_rho_s'}: [nz_s][nx], float64."""
         info = self.info()
-        nx = info["nx"]
+        out = {k: np.zeros((info["nz_f"] if k in ("K", "rcp_rho_f") else info["nz_s"], info["nx"]))
+               for k in GRAD_COEFS}
+        g = CoefGrad(*[out[k].ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for k in GRAD_COEFS])
+        self._backward(residual, ctypes.byref(g))
+        return out
+
+    def adjoint_backward_only(self, residual: Dict[str, np.ndarray]):
+        """mfdm_adjoint_backward without copying the gradient to the host: it
+        stays on the device for adjoint_accumulate_grad."""
+        self._backward(residual, None)
+
+    def _backward(self, residual, grad):
+        nx = self.info()["nx"]
         keep = []
 
         def res(name):
@@ -333,12 +353,21 @@ class Solver:
             keep.append(a)
             return a.ctypes.data_as(_fp)
 
-        out = {k: np.zeros((info["nz_f"] if k in ("K", "rcp_rho_f") else info["nz_s"], nx))
-               for k in GRAD_COEFS}
-        g = CoefGrad(*[out[k].ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for k in GRAD_COEFS])
-        _check(self._lib.mfdm_adjoint_backward(self._h, res("svx"), res("svz"), res("fp"),
-                                               ctypes.byref(g)))
-        return out
+        _check(self._lib.mfdm_adjoint_backward(self._h, res("svx"), res("svz"), res("fp"), grad))
+
+    def adjoint_accumulate_grad(self, dst, stream: Optional[int] = None):
+        """Adds the last backward pass's gradient, rounded to FP32, to the device
+        buffer `dst` (a CUDA torch tensor of (2 nz_f + 5 nz_s) x nx float32, the
+        seven GRAD_COEFS arrays packed) on `stream` (a CUDA stream handle; None:
+        the legacy default stream), without a host round trip
+        (mfdm_adjoint_accumulate_grad_f32)."""
+        info = self.info()
+        need = (2 * info["nz_f"] + 5 * info["nz_s"]) * info["nx"]
+        if (not getattr(dst, "is_cuda", False) or dst.dtype.itemsize != 4 or dst.numel() != need
+                or not dst.is_contiguous()):
+            raise ValueError(f"dst must be a contiguous CUDA float32 tensor of {need} elements")
+        _check(self._lib.mfdm_adjoint_accumulate_grad_f32(self._h, ctypes.c_void_p(dst.data_ptr()),
+                                                          ctypes.c_void_p(stream or 0)))
 
     # -- tile shape -----------------------------------------------------------
     def set_tile(self, seg_rows: int):
@@ -464,6 +493,7 @@ class SolidSolver:
         d.C33, d.C55, d.rho = ptr(model.solid["C33"]), ptr(model.solid["C55"]), ptr(model.solid["rho"])
         d.J, d.xi_x, d.xi_z = ptr(model.metric["J"]), ptr(model.metric["xi_x"]), ptr(model.metric["xi_z"])
         d.ze_x, d.ze_z = ptr(model.metric["ze_x"]), ptr(model.metric["ze_z"])
+        d.boundary_type = int(getattr(model, "boundary_type", 2))
         h = ctypes.c_void_p()
         _check(load_library().mfdm_solid_open_desc(ctypes.byref(d), device, ctypes.byref(h)))
         return cls(h)
@@ -559,6 +589,31 @@ def step_noalloc(dm: DeviceModel, it: int, nsteps: int, stream: Optional[int] = 
     """mfdm_step_noalloc: steps device-resident arrays without any allocation."""
     _check(load_library().mfdm_step_noalloc(ctypes.byref(dm), int(it), int(nsteps),
                                             ctypes.c_void_p(stream or 0)))
+
+
+def dispersion_image(gather: np.ndarray, offsets, fs: float, c_min: float, c_max: float,
+                     dc: float, device: int = 0):
+    """Phase-shift dispersion image of a gather [nt][ntr] on the GPU
+    (mfdm_dispersion_image; the reference's tools/test.py:50-98). Returns
+    (frequencies [nf], velocities [nv], amplitude [nf][nv])."""
+    lib = load_library()
+    g = np.ascontiguousarray(gather, dtype=np.float32)
+    if g.ndim != 2:
+        raise ValueError("gather must have shape (nt, number_of_receivers)")
+    x = np.ascontiguousarray(offsets, dtype=np.float64)
+    if x.ndim != 1 or x.size != g.shape[1]:
+        raise ValueError("there must be exactly one offset for each trace")
+    nv = lib.mfdm_dispersion_velocities(c_min, c_max, dc)
+    if nv <= 0:
+        raise MfdmError(-1, "velocities must satisfy 0 < c_min <= c_max and dc > 0")
+    nt = g.shape[0]
+    amp = np.zeros((nt // 2 + 1, nv), dtype=np.float32)
+    _check(lib.mfdm_dispersion_image(g.ctypes.data_as(_fp), nt, g.shape[1],
+                                     x.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), fs, c_min,
+                                     c_max, dc, amp.ctypes.data_as(_fp), int(device)))
+    freqs = np.arange(nt // 2 + 1) * (fs / nt)
+    vels = c_min + dc * np.arange(nv)
+    return freqs, vels, amp
 
 
 def run_cli(json_path: str, out_root: str, device: int = 0):

@@ -181,6 +181,7 @@ struct AdjointState {
   uint8_t* mask = nullptr;
   float *lam = nullptr, *mu = nullptr, *kb[2] = {nullptr, nullptr}, *tmp = nullptr;
   double* grad = nullptr;  // K, 1/rho_f [nz_f][P]; C11, C13, C33, C55, 1/rho_s [nz_s][P]
+  bool grad_ready = false;  // grad holds a finished backward pass
   float* ckpt = nullptr;   // checkpoint sets
   size_t ckpt_sets = 0;
   float* seg = nullptr;    // 4 stage-input sets per step of one segment
@@ -1607,6 +1608,27 @@ int adjoint_prepare(mfdm_model* m) {
   return MFDM_OK;
 }
 
+// dst[r][x] += float(grad[r][x]) over the seven gradient arrays stacked as rows
+// (2 nz_f + 5 nz_s rows, device pitch P doubles, packed rows of nx floats).
+__global__ void grad_accumulate_kernel(const double* __restrict__ g, int rows, int nx, int P,
+                                       float* __restrict__ dst) {
+  const size_t n = size_t(rows) * nx;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += size_t(gridDim.x) * blockDim.x) {
+    const size_t r = i / nx, x = i - r * nx;
+    dst[i] += float(g[r * P + x]);
+  }
+}
+
+cudaError_t launch_grad_accumulate(const double* g, int rows, int nx, int P, float* dst,
+                                   cudaStream_t st) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  grad_accumulate_kernel<<<unsigned(sms * 8), 256, 0, st>>>(g, rows, nx, P, dst);
+  return cudaGetLastError();
+}
+
 double* grad_array(mfdm_model* m, int k) {
   const size_t nf = size_t(m->cfg.nzf) * m->P, ns = size_t(m->cfg.nzs) * m->P;
   return m->adj->grad + (k < 2 ? size_t(k) * nf : 2 * nf + size_t(k - 2) * ns);
@@ -1863,6 +1885,7 @@ int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_
   }
   cudaStream_t st = m->stream;
   const size_t gbytes = (size_t(2) * m->cfg.nzf * m->P + size_t(5) * m->cfg.nzs * m->P) * sizeof(double);
+  a->grad_ready = false;
   MFDM_CU(cudaMemsetAsync(a->grad, 0, gbytes, st));
   MFDM_CU(cudaMemsetAsync(a->lam, 0, len * sizeof(float), st));
   MFDM_CU(cudaMemsetAsync(a->mu, 0, len * sizeof(float), st));
@@ -1965,7 +1988,19 @@ int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_
   // the recomputation left a mid-run state: back to rest
   if ((rc = clear_state(m)) != MFDM_OK) return rc;
   if ((rc = rewind(m)) != MFDM_OK) return rc;
+  m->adj->grad_ready = true;
   return check_status(m);
+}
+
+int mfdm_adjoint_accumulate_grad_f32(mfdm_model* m, float* dst, void* stream) {
+  if (!m || !dst) return fail(MFDM_ERR_ARG, "null argument");
+  if (!m->adj || !m->adj->grad || !m->adj->grad_ready)
+    return fail(MFDM_ERR_ARG, "no gradient: call mfdm_adjoint_backward first");
+  DeviceGuard g(m->device);
+  const int rows = 2 * m->cfg.nzf + 5 * m->cfg.nzs;
+  MFDM_CU(launch_grad_accumulate(m->adj->grad, rows, m->cfg.nx, m->P, dst,
+                                 static_cast<cudaStream_t>(stream)));
+  return MFDM_OK;
 }
 
 }  // extern "C"
@@ -2011,10 +2046,13 @@ int load_json_solid(const char* path, SolidHost& h) {
     p.dt = J.get_float("base.dt");
     p.nt = J.get_int("base.nt");
     p.snapshot = J.get_int("base.snapshot");
-    if (J.get_int("grid.calc_type") != 0 || J.get_int("grid.boundary_type") != 2)
+    const int bdy = J.get_int("grid.boundary_type");
+    if (J.get_int("grid.calc_type") != 0 || (bdy != 1 && bdy != 2))
       return fail(MFDM_ERR_ARG,
                   "unsupported configuration: solid-only runs need calc_type 0 with "
-                  "boundary_type 2 (free surface on top, CFS-PML sides and bottom)");
+                  "boundary_type 2 (free surface on top, CFS-PML sides and bottom) or 1 "
+                  "(CFS-PML on all four sides)");
+    p.bdy = bdy;
     const size_t nsrc = J.size("grid.src_pos.posx");
     for (size_t i = 0; i < nsrc; ++i) {
       p.srcx.push_back(J.get_int("grid.src_pos.posx", i));
@@ -2169,6 +2207,11 @@ int solid_build(mfdm_solid* m, const SolidHost& h, int device) {
   if (h.nx < 8 || h.nz < 8) return fail(MFDM_ERR_ARG, "grid too small: need nx, nz >= 8");
   if (p.npd < 0 || 2 * p.npd > h.nx - 6 || p.npd + 7 > h.nz)
     return fail(MFDM_ERR_ARG, "PML width npd does not fit the grid");
+  const bool cpml = p.bdy == 1;
+  if (cpml && 2 * p.npd + 6 > h.nz)
+    return fail(MFDM_ERR_ARG, "the top and bottom PML bands overlap: need nz >= 2 npd + 6");
+  if (cpml && h.nz < 34)
+    return fail(MFDM_ERR_ARG, "CFS-PML on four sides records row 30: need nz >= 34");
   if (!(p.dt > 0.f) || !(p.fpeak > 0.f)) return fail(MFDM_ERR_ARG, "dt and fpeak must be > 0");
   if (p.snapshot < 1 || p.nt < 0) return fail(MFDM_ERR_ARG, "need snapshot >= 1 and nt >= 0");
   for (size_t i = 0; i < p.srcx.size(); ++i)
@@ -2200,10 +2243,11 @@ int solid_build(mfdm_solid* m, const SolidHost& h, int device) {
   const size_t o_alm = take(size_t(6) * P), o_px = take(size_t(nx) * 4), o_pz = take(size_t(nz) * 4),
                o_misc = take(64);
   size_t o_set[4];
+  const int zrows = cpml ? 2 * npdr : npdr;  // zeta-ADE rows: bottom band (+ top band)
   for (int s = 0; s < 4; ++s) {
     o_set[s] = take(5 * n);
     for (int q = 0; q < 4; ++q) take(size_t(nz) * Ps);
-    for (int q = 0; q < 4; ++q) take(size_t(npdr) * P);
+    for (int q = 0; q < 4; ++q) take(size_t(zrows) * P);
   }
   const size_t set_floats = (o_set[1] - o_set[0]) / sizeof(float);
   m->dbytes = off;
@@ -2222,12 +2266,14 @@ int solid_build(mfdm_solid* m, const SolidHost& h, int device) {
     }
     for (int q = 0; q < 4; ++q) {
       S.z[q] = reinterpret_cast<float*>(reinterpret_cast<char*>(b) + o);
-      o += (size_t(npdr) * P * sizeof(float) + 255) / 256 * 256;
+      o += (size_t(zrows) * P * sizeof(float) + 255) / 256 * 256;
     }
     if (o / sizeof(float) > set_floats) return fail(MFDM_ERR_ARG, "internal layout error");
   }
   mfdm::solid::SCoef& C = m->C;
   C.nx = nx; C.nz = nz; C.P = P; C.Ps = Ps; C.npd = npd;
+  C.cpml = cpml ? 1 : 0;
+  C.rec_row = cpml ? 30 : 3;  // src/main.cu:303-311
   // the density slot holds 1/rho (FP64 reciprocal rounded once): the momentum
   // right-hand side multiplies instead of dividing
   std::vector<float> rcp_rho(size_t(nx) * nz);
@@ -2275,7 +2321,7 @@ int solid_build(mfdm_solid* m, const SolidHost& h, int device) {
   C.alm = F(o_alm);
   std::vector<float4> px, pz;
   pml_profile(p, nx, true, true, p.fpeak, p.beta0, px);
-  pml_profile(p, nz, false, true, p.fpeak, p.beta0, pz);  // free surface on top
+  pml_profile(p, nz, cpml, true, p.fpeak, p.beta0, pz);  // top band only without a free surface
   MFDM_CU(cudaMemcpyAsync(F(o_px), px.data(), px.size() * sizeof(float4), cudaMemcpyHostToDevice, m->stream));
   MFDM_CU(cudaMemcpyAsync(F(o_pz), pz.data(), pz.size() * sizeof(float4), cudaMemcpyHostToDevice, m->stream));
   C.pmlx = reinterpret_cast<const float4*>(F(o_px));
@@ -2348,6 +2394,7 @@ int mfdm_solid_open_desc(const mfdm_solid_desc* d, int device, mfdm_solid** out)
   p.fpeak = d->fpeak; p.dt = d->dt; p.nt = d->nt; p.snapshot = d->snapshot;
   p.npd = d->npd; p.npow = d->npow; p.thickness = d->thickness; p.vp_max = d->vp_max;
   p.rc = d->rc; p.beta0 = d->beta0;
+  p.bdy = d->boundary_type == 1 ? 1 : 2;
   for (int i = 0; i < d->nsrc; ++i) {
     if (!d->src_x || !d->src_z) return fail(MFDM_ERR_ARG, "null source arrays");
     p.srcx.push_back(d->src_x[i]);

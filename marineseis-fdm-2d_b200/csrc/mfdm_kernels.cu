@@ -985,6 +985,7 @@ cudaError_t launch_stage_tile(const Coef& C, const Fields& in, const Fields& out
   return C.cpml ? launch_tile_bc<true>(C, in, out, un, acc, stage, dir, st)
                 : launch_tile_bc<false>(C, in, out, un, acc, stage, dir, st);
 }
+
 #endif  // MFDM_VARIANT_TU
 
 }  // namespace MFDM_VNS
