@@ -71,19 +71,27 @@ __device__ __forceinline__ bool locate(const SetLayout& L, long long i, int& a, 
   return r < L.rows[a] && c < L.ncols[a];
 }
 
-// Output cells where the forward stage evaluates the plain interior formula:
-// main fields, outside the xi strips, fluid rows 6..nz_f-4 (four-side CPML:
-// below the top band, npd+3..nz_f-4), solid rows 3 .. nz_s-4-npd (above the
-// zeta strip). Everywhere else (strips, conservative and one-sided rows, the
-// interface) the CSR part of the transposed operator applies.
-__device__ __forceinline__ bool interior_cell(const SetLayout& L, int a, int r, int c) {
-  if (a >= 8) return false;
-  if (c < 3 + L.npd || c > L.nx - 4 - L.npd) return false;
-  if (a < 3) {
-    const int lo = L.cpml ? max(3, L.npd + 3) : 6;
-    return r >= lo && r <= L.nzf - 4;
+// Output cells whose stage right-hand side is (cell coefficients) x (biased
+// derivatives at the cell) plus point-wise ADE terms, all of it transposed by
+// the Q fields and the point-wise ADE transpose: the interior cells and the
+// PML strip cells of the same rows (full-order zeta stencils: fluid rows
+// 6..nz_f-4, below the top band with four-side CPML; solid rows 3..nz_s-4,
+// the bottom band included), main fields and their ADE memory. The interface
+// strip, the conservative and one-sided rows and the four-side CPML's fluid
+// top band stay in the CSR part.
+__device__ __forceinline__ bool structured_cell(const SetLayout& L, int a, int r, int c) {
+  const int flo = L.cpml ? max(6, L.npd + 3) : 6;
+  switch (L.kind[a]) {
+    case 0: return c >= 3 && c <= L.nx - 4 && r >= flo && r <= L.nzf - 4;
+    case 1: return c >= 3 && c <= L.nx - 4 && r >= 3 && r <= L.nzs - 4;
+    case 2: return r >= flo && r <= L.nzf - 4;
+    case 3: return r >= 3 && r <= L.nzs - 4;
+    case 4: {
+      const int rs = L.nzs - 3 - L.npd + r;
+      return rs >= 3 && rs <= L.nzs - 4;
+    }
+    default: return false;
   }
-  return r >= 3 && r < L.nzs - 3 - L.npd;
 }
 
 __global__ void k_set_lattice(float* set, SetLayout L, int a, int cz, int cx, float v) {
@@ -259,12 +267,19 @@ __device__ __forceinline__ void filter_t_b_col(float* lam, const SetLayout& L, c
 // the residual injection (res != null), the transposed continuity average into
 // tmp, a block barrier, the transposed smoothing -- one launch instead of three
 // dependent ones.
+// The transposed step's time index n comes from the device counter `step`
+// (the residuals of step n are injected when n % gap == 0) and the step
+// leaves n - 1 behind, so a captured run of transposed steps replays for any
+// segment once the counter is set.
 __global__ void __launch_bounds__(1024) k_step_start(float* lam, SetLayout L,
                                                      const float2* __restrict__ nrm, float* tmp,
-                                                     W7 w7, const float* __restrict__ res, float* mu,
-                                                     float* kb, const uint8_t* __restrict__ mask,
-                                                     float c) {
+                                                     W7 w7, const float* __restrict__ res_all,
+                                                     int gap, int* step, float* mu, float* kb,
+                                                     const uint8_t* __restrict__ mask, float c) {
   const int nx = L.nx;
+  const int n = *step;
+  const float* res = (res_all && gap > 0 && n % gap == 0) ? res_all + (size_t)(n / gap) * 3 * nx
+                                                           : nullptr;
   for (int ix = 3 + threadIdx.x; ix <= nx - 4; ix += blockDim.x) {
     if (res) inject_col(lam, L, res, ix);
     filter_t_a_col(lam, L, nrm, tmp, w7, ix);
@@ -272,7 +287,11 @@ __global__ void __launch_bounds__(1024) k_step_start(float* lam, SetLayout L,
   __syncthreads();  // tmp of every column written (global memory, one block)
   for (int j = 3 + threadIdx.x; j <= nx - 4; j += blockDim.x)
     filter_t_b_col(lam, L, tmp, w7, mu, kb, mask, c, j);
+  __syncthreads();  // every thread has read the counter
+  if (threadIdx.x == 0) *step = n - 1;
 }
+
+__global__ void k_set_int(int* p, int v) { *p = v; }
 
 __global__ void k_drop_count(const long long* __restrict__ rowptr, const int* __restrict__ col,
                              SetLayout L, unsigned long long* count) {
@@ -281,7 +300,7 @@ __global__ void k_drop_count(const long long* __restrict__ rowptr, const int* __
   unsigned long long n = 0;
   for (long long k = rowptr[j]; k < rowptr[j + 1]; ++k) {
     int a, r, c;
-    if (!(locate(L, col[k], a, r, c) && interior_cell(L, a, r, c))) ++n;
+    if (!(locate(L, col[k], a, r, c) && structured_cell(L, a, r, c))) ++n;
   }
   count[j] = n;
 }
@@ -294,7 +313,7 @@ __global__ void k_drop_fill(const long long* __restrict__ rowptr, const int* __r
   long long o = rp2[j];
   for (long long k = rowptr[j]; k < rowptr[j + 1]; ++k) {
     int a, r, c;
-    if (!(locate(L, col[k], a, r, c) && interior_cell(L, a, r, c))) {
+    if (!(locate(L, col[k], a, r, c) && structured_cell(L, a, r, c))) {
       col2[o] = col[k];
       val2[o] = val[k];
       ++o;
@@ -315,12 +334,128 @@ __global__ void k_drop_fill(const long long* __restrict__ rowptr, const int* __r
 // (r = 1/rho; the primed metric is read at global row iz in the four-side CPML
 // variant, cpml_kernels.cuh:448-455), so the Dx / Dz coefficient of every
 // (output, input) pair times x at i, summed per input field, gives qx / qz.
-// Q fields of fluid cell (r, c); only interior cells are non-zero.
+// Transposes of the stage right-hand side at a PML strip cell of a structured
+// row. There the right-hand side is linear in the cell's biased derivatives
+// and ADE memory (fluid_rhs / solid_rhs, the branches without the conservative
+// form); given the stage adjoint y of the cell's outputs these return the
+// adjoint of every input, i.e. the cell's Q-field entries and the point-wise
+// ADE transpose. R = gxz / gxx and S = gxz / gzz as in the forward.
+//
+// Fluid: y = (vx, vz, p, xi Vx, Vz, Ex, Ez) outputs; d = adjoint of
+// (Dx p, Dz p, Dx vx, Dz vx, Dx vz, Dz vz), e = adjoint of the xi ADE (Vx, Vz, Ex, Ez).
+template <bool CPML>
+__device__ __forceinline__ void fluid_strip_t(const float* y, float xix, float xiz, float zex,
+                                              float zez, float rr, float K, float4 pml, float* d,
+                                              float* e) {
+  const float gxx = xix * xix + xiz * xiz, gxz = xix * zex + xiz * zez, R = gxz / gxx;
+  const float dpb = pml.x, apdpb = pml.y, invb = pml.z;
+  // momentum: vx, vz and the Vx, Vz memory read divx, divz = -(xix, xiz) (Dx p + R Dz p)
+  const float gdx = rr * (invb - 1.0f) * y[0] + dpb * y[3];
+  const float gdz = rr * (invb - 1.0f) * y[1] + dpb * y[4];
+  const float gdiv = -(xix * gdx + xiz * gdz);
+  d[0] = -rr * (xix * y[0] + xiz * y[1]) + gdiv;
+  d[1] = -rr * (zex * y[0] + zez * y[1]) + R * gdiv;
+  e[0] = -rr * invb * y[0] - apdpb * y[3];
+  e[1] = -rr * invb * y[1] - apdpb * y[4];
+  // pressure: p and the Ex, Ez memory read Dvx = Dx vx + R Dz vx, Dvz likewise
+  const float gDvx = -K * (invb - 1.0f) * xix * y[2] + dpb * y[5];
+  const float gDvz = -K * (invb - 1.0f) * xiz * y[2] + dpb * y[6];
+  d[2] = -K * xix * y[2] + gDvx;
+  d[3] = -K * zex * y[2] + R * gDvx;
+  d[4] = -K * xiz * y[2] + gDvz;
+  d[5] = -K * zez * y[2] + R * gDvz;
+  e[2] = K * invb * xix * y[2] - apdpb * y[5];
+  e[3] = K * invb * xiz * y[2] - apdpb * y[6];
+}
+
+// Solid: y = (vx, vz, sx, sz, sxz, xi Vx, Vz, Ex, Ez, zeta Vx, Vz, Ex, Ez);
+// d = adjoint of (Dx sx, Dz sx, Dx sz, Dz sz, Dx sxz, Dz sxz, Dx vx, Dz vx,
+// Dx vz, Dz vz); e = adjoint of the xi then the zeta ADE (Vx, Vz, Ex, Ez).
+// The sxz line's own metric (bxix ..) differs from the cell's only in the
+// four-side CPML variant (cpml_kernels.cuh:448-455); its PML terms use the cell's.
+struct SolidCell {
+  float xix, xiz, zex, zez, bxix, bxiz, bzex, bzez, rr, c11, c13, c33, c55;
+  float4 px, pz;
+  bool side, bottom;
+};
+
+__device__ __forceinline__ void solid_strip_t(const float* y, const SolidCell& k, float* d,
+                                              float* e) {
+  const float xix = k.xix, xiz = k.xiz, zex = k.zex, zez = k.zez;
+  const float gxx = xix * xix + xiz * xiz, gzz = zex * zex + zez * zez, gxz = xix * zex + xiz * zez;
+  const float R = gxz / gxx, S = gxz / gzz;
+  const float gvx = k.rr * y[0], gvz = k.rr * y[1];
+  // momentum: rho v_t = div sigma (+ the projected PML terms dxx, dxz, dzx, dzz)
+  float gxx_ = 0.f, gxz_ = 0.f, gzx_ = 0.f, gzz_ = 0.f;
+  for (int q = 0; q < 8; ++q) e[q] = 0.0f;
+  if (k.side) {
+    const float dp = k.px.x, ap = k.px.y, ib = k.px.z;
+    gxx_ = k.rr * (ib - 1.0f) * y[0] + dp * y[5];
+    gxz_ = k.rr * (ib - 1.0f) * y[1] + dp * y[6];
+    e[0] = -k.rr * ib * y[0] - ap * y[5];
+    e[1] = -k.rr * ib * y[1] - ap * y[6];
+  }
+  if (k.bottom) {
+    const float dq = k.pz.x, aq = k.pz.y, jb = k.pz.z;
+    gzx_ = k.rr * (jb - 1.0f) * y[0] + dq * y[9];
+    gzz_ = k.rr * (jb - 1.0f) * y[1] + dq * y[10];
+    e[4] = -k.rr * jb * y[0] - aq * y[9];
+    e[5] = -k.rr * jb * y[1] - aq * y[10];
+  }
+  // dxx = xix (sxdx + R sxdz) + xiz (tdx + R tdz); dxz = xix (tdx + R tdz) + xiz (szdx + R szdz)
+  // dzx = zex (sxdz + S sxdx) + zez (S tdx + tdz); dzz = zex (S tdx + tdz) + zez (S szdx + szdz)
+  d[0] = gvx * xix + gxx_ * xix + S * gzx_ * zex;
+  d[1] = gvx * zex + R * gxx_ * xix + gzx_ * zex;
+  d[2] = gvz * xiz + gxz_ * xiz + S * gzz_ * zez;
+  d[3] = gvz * zez + R * gxz_ * xiz + gzz_ * zez;
+  d[4] = gvx * xiz + gvz * xix + gxx_ * xiz + gxz_ * xix + S * (gzx_ * zez + gzz_ * zex);
+  d[5] = gvx * zez + gvz * zex + R * (gxx_ * xiz + gxz_ * xix) + gzx_ * zez + gzz_ * zex;
+  // stress: the constitutive law and its projected PML terms
+  const float c11 = k.c11, c13 = k.c13, c33 = k.c33, c55 = k.c55;
+  float vxdx = (c11 * y[2] + c13 * y[3]) * xix + c55 * k.bxiz * y[4];
+  float vxdz = (c11 * y[2] + c13 * y[3]) * zex + c55 * k.bzez * y[4];
+  float vzdx = (c13 * y[2] + c33 * y[3]) * xiz + c55 * k.bxix * y[4];
+  float vzdz = (c13 * y[2] + c33 * y[3]) * zez + c55 * k.bzex * y[4];
+  if (k.side) {
+    const float dp = k.px.x, ap = k.px.y, ib = k.px.z;
+    const float ax = (c11 * y[2] + c13 * y[3]) * xix + c55 * xiz * y[4];
+    const float az = (c13 * y[2] + c33 * y[3]) * xiz + c55 * xix * y[4];
+    const float gDvx = (ib - 1.0f) * ax + dp * y[7], gDvz = (ib - 1.0f) * az + dp * y[8];
+    vxdx += gDvx;
+    vxdz += R * gDvx;
+    vzdx += gDvz;
+    vzdz += R * gDvz;
+    e[2] = -ib * ax - ap * y[7];
+    e[3] = -ib * az - ap * y[8];
+  }
+  if (k.bottom) {
+    const float dq = k.pz.x, aq = k.pz.y, jb = k.pz.z;
+    const float bx = (c11 * y[2] + c13 * y[3]) * zex + c55 * zez * y[4];
+    const float bz = (c13 * y[2] + c33 * y[3]) * zez + c55 * zex * y[4];
+    const float gFvx = (jb - 1.0f) * bx + dq * y[11], gFvz = (jb - 1.0f) * bz + dq * y[12];
+    vxdz += gFvx;
+    vxdx += S * gFvx;
+    vzdz += gFvz;
+    vzdx += S * gFvz;
+    e[6] = -jb * bx - aq * y[11];
+    e[7] = -jb * bz - aq * y[12];
+  }
+  d[6] = vxdx;
+  d[7] = vxdz;
+  d[8] = vzdx;
+  d[9] = vzdz;
+}
+
+// Q fields of fluid cell (r, c); only structured cells are non-zero. A strip
+// cell also writes the point-wise transpose of its ADE inputs into t (those
+// rows have no CSR entries: every output that reads them is at this cell).
+template <bool CPML>
 __device__ __forceinline__ void q_fluid(const Coef& C, const SetLayout& L, const float* __restrict__ x,
-                                        float* qx, float* qz, int r, int c, bool write_zero) {
+                                        float* qx, float* qz, float* t, int r, int c,
+                                        bool write_zero) {
   const size_t g = (size_t)r * C.P + c;
   const long long i0 = L.off[0] + g, i1 = L.off[1] + g, i2 = L.off[2] + g;
-  if (!interior_cell(L, 0, r, c)) {
+  if (!structured_cell(L, 0, r, c)) {
     if (write_zero) {
       qx[i0] = 0.f; qz[i0] = 0.f; qx[i1] = 0.f; qz[i1] = 0.f; qx[i2] = 0.f; qz[i2] = 0.f;
     }
@@ -329,22 +464,48 @@ __device__ __forceinline__ void q_fluid(const Coef& C, const SetLayout& L, const
   const float xix = __ldg(C.xix + g), xiz = __ldg(C.xiz + g), zex = __ldg(C.zex + g),
               zez = __ldg(C.zez + g), rr = __ldg(C.rhof + g), K = __ldg(C.K + g);
   const float kvx = x[i0], kvz = x[i1], kp = x[i2];
-  qx[i2] = -rr * (xix * kvx + xiz * kvz);
-  qz[i2] = -rr * (zex * kvx + zez * kvz);
-  qx[i0] = -K * xix * kp;
-  qz[i0] = -K * zex * kp;
-  qx[i1] = -K * xiz * kp;
-  qz[i1] = -K * zez * kp;
+  const int s = col_to_strip(c, L.nx, L.npd);
+  if (s < 0) {
+    qx[i2] = -rr * (xix * kvx + xiz * kvz);
+    qz[i2] = -rr * (zex * kvx + zez * kvz);
+    qx[i0] = -K * xix * kp;
+    qz[i0] = -K * zex * kp;
+    qx[i1] = -K * xiz * kp;
+    qz[i1] = -K * zez * kp;
+    return;
+  }
+  const float4 pml = __ldg(C.pmlx + c);
+  long long ia[4];
+  float y[7] = {kvx, kvz, kp, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    ia[q] = L.off[8 + q] + (long long)r * L.pitch[8 + q] + s;
+    y[3 + q] = x[ia[q]];
+  }
+  float dq[6], eq[4];
+  fluid_strip_t<CPML>(y, xix, xiz, zex, zez, rr, K, pml, dq, eq);
+  qx[i2] = dq[0];
+  qz[i2] = dq[1];
+  qx[i0] = dq[2];
+  qz[i0] = dq[3];
+  qx[i1] = dq[4];
+  qz[i1] = dq[5];
+  if (t) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) t[ia[q]] = eq[q];
+  }
 }
 
-// Q fields of solid cell (r, c); only interior cells are non-zero.
+// Q fields of solid cell (r, c); only structured cells are non-zero. Strip and
+// bottom-band cells also write the point-wise transpose of their ADE inputs into t.
 template <bool CPML>
 __device__ __forceinline__ void q_solid(const Coef& C, const SetLayout& L, const float* __restrict__ x,
-                                        float* qx, float* qz, int r, int c, bool write_zero) {
+                                        float* qx, float* qz, float* t, int r, int c,
+                                        bool write_zero) {
   const int P = C.P;
   const size_t m = (size_t)r * P + c, g = m + (size_t)(L.nzf - 1) * P;
   float q[10] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // (x, z) for vx, vz, sx, sz, sxz
-  if (interior_cell(L, 3, r, c)) {
+  if (structured_cell(L, 3, r, c)) {
     const float xix = __ldg(C.xix + g), xiz = __ldg(C.xiz + g), zex = __ldg(C.zex + g),
                 zez = __ldg(C.zez + g);
     const size_t b = CPML ? m : g;
@@ -354,17 +515,44 @@ __device__ __forceinline__ void q_solid(const Coef& C, const SetLayout& L, const
                 c33 = __ldg(C.C33 + m), c55 = __ldg(C.C55 + m);
     const float kvx = x[L.off[3] + m], kvz = x[L.off[4] + m], ksx = x[L.off[5] + m],
                 ksz = x[L.off[6] + m], ksxz = x[L.off[7] + m];
-    const float a1 = c11 * ksx + c13 * ksz, a2 = c13 * ksx + c33 * ksz;
-    q[0] = xix * a1 + c55 * bxiz * ksxz;   // vx, x
-    q[1] = zex * a1 + c55 * bzez * ksxz;   // vx, z
-    q[2] = xiz * a2 + c55 * bxix * ksxz;   // vz, x
-    q[3] = zez * a2 + c55 * bzex * ksxz;   // vz, z
-    q[4] = rr * xix * kvx;                 // sx
-    q[5] = rr * zex * kvx;
-    q[6] = rr * xiz * kvz;                 // sz
-    q[7] = rr * zez * kvz;
-    q[8] = rr * (xiz * kvx + xix * kvz);   // sxz
-    q[9] = rr * (zez * kvx + zex * kvz);
+    const int s = col_to_strip(c, L.nx, L.npd), zb0 = L.nzs - 3 - L.npd;
+    if (s < 0 && r < zb0) {
+      const float a1 = c11 * ksx + c13 * ksz, a2 = c13 * ksx + c33 * ksz;
+      q[0] = xix * a1 + c55 * bxiz * ksxz;   // vx, x
+      q[1] = zex * a1 + c55 * bzez * ksxz;   // vx, z
+      q[2] = xiz * a2 + c55 * bxix * ksxz;   // vz, x
+      q[3] = zez * a2 + c55 * bzex * ksxz;   // vz, z
+      q[4] = rr * xix * kvx;                 // sx
+      q[5] = rr * zex * kvx;
+      q[6] = rr * xiz * kvz;                 // sz
+      q[7] = rr * zez * kvz;
+      q[8] = rr * (xiz * kvx + xix * kvz);   // sxz
+      q[9] = rr * (zez * kvx + zex * kvz);
+    } else {
+      SolidCell k{xix, xiz, zex, zez, bxix, bxiz, bzex, bzez, rr, c11, c13, c33, c55,
+                  make_float4(0.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f), s >= 0, r >= zb0};
+      if (k.side) k.px = __ldg(C.pmlx + c);
+      if (k.bottom) k.pz = __ldg(C.pmlz + r);
+      long long ia[8];
+      float y[13] = {kvx, kvz, ksx, ksz, ksxz, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        ia[u] = k.side ? L.off[12 + u] + (long long)r * L.pitch[12 + u] + s : -1;
+        ia[4 + u] = k.bottom ? L.off[16 + u] + (long long)(r - zb0) * L.pitch[16 + u] + c : -1;
+        y[5 + u] = k.side ? x[ia[u]] : 0.f;
+        y[9 + u] = k.bottom ? x[ia[4 + u]] : 0.f;
+      }
+      float dq[10], eq[8];
+      solid_strip_t(y, k, dq, eq);
+      // d order: sx, sz, sxz (x, z) then vx, vz (x, z); q order: vx, vz, sx, sz, sxz (x, z)
+      q[4] = dq[0]; q[5] = dq[1]; q[6] = dq[2]; q[7] = dq[3]; q[8] = dq[4]; q[9] = dq[5];
+      q[0] = dq[6]; q[1] = dq[7]; q[2] = dq[8]; q[3] = dq[9];
+      if (t) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+          if (ia[u] >= 0) t[ia[u]] = eq[u];
+      }
+    }
   } else if (!write_zero) {
     return;
   }
@@ -377,12 +565,13 @@ __device__ __forceinline__ void q_solid(const Coef& C, const SetLayout& L, const
 
 // ZERO: also write the zeros off the interior cells (a fresh Q buffer).
 template <bool CPML, bool ZERO = true>
-__global__ void k_qfields(Coef C, SetLayout L, const float* __restrict__ x, float* qx, float* qz) {
+__global__ void k_qfields(Coef C, SetLayout L, const float* __restrict__ x, float* qx, float* qz,
+                          float* t) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int row = blockIdx.y;
   if (c >= L.nx) return;
-  if (row < L.nzf) q_fluid(C, L, x, qx, qz, row, c, ZERO);
-  else q_solid<CPML>(C, L, x, qx, qz, row - L.nzf, c, ZERO);
+  if (row < L.nzf) q_fluid<CPML>(C, L, x, qx, qz, t, row, c, ZERO);
+  else q_solid<CPML>(C, L, x, qx, qz, t, row - L.nzf, c, ZERO);
 }
 
 // ---- material gradients ----------------------------------------------------------
@@ -432,7 +621,7 @@ __global__ void __launch_bounds__(128) k_grad_cells(Coef C, SetLayout L, Fields 
     // velocity terms carry 1/rho, the pressure term K
     G.rf[g] = grf + (double(__ldg(KB.fvx + g)) * o.vx + double(__ldg(KB.fvz + g)) * o.vz);
     G.K[g] = gK + double(__ldg(KB.fp + g)) * o.p;
-    if (qx) q_fluid(C, L, kb, qx, qz, iz, ix, false);
+    if (qx) q_fluid<CPML>(C, L, kb, qx, qz, nullptr, iz, ix, false);
     return;
   }
   const int iz = 1 + row - nfr;
@@ -461,7 +650,7 @@ __global__ void __launch_bounds__(128) k_grad_cells(Coef C, SetLayout L, Fields 
   G.c55[m] = gc55 + ksxz * o1.sxz;
   G.rs[m] = grs + (kvx * o1.vx + kvz * o1.vz);
   G.c13[m] = gc13 + (ksx * o2.sx + ksz * o2.sz);
-  if (qx) q_solid<CPML>(C, L, kb, qx, qz, iz, ix, false);
+  if (qx) q_solid<CPML>(C, L, kb, qx, qz, nullptr, iz, ix, false);
 }
 
 // Interface column ix: both media's RHS at the interface row, coupled, per coefficient.
@@ -735,8 +924,8 @@ static cudaError_t hybrid_t(const HybridT& H, const Coef& C, const SetLayout& L,
                             float c, bool q_ready, cudaStream_t st) {
   if (!q_ready) {
     const dim3 gq(unsigned((L.nx + 127) / 128), unsigned(L.nzf + L.nzs));
-    if (L.cpml) k_qfields<true><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz);
-    else k_qfields<false><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz);
+    if (L.cpml) k_qfields<true><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz, H.t);
+    else k_qfields<false><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz, H.t);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
@@ -763,8 +952,8 @@ cudaError_t q_fields(const HybridT& H, const Coef& C, const SetLayout& L, const 
                      cudaStream_t st) {
   // off the interior cells the Q buffers hold the zeros written when allocated
   const dim3 gq(unsigned((L.nx + 127) / 128), unsigned(L.nzf + L.nzs));
-  if (L.cpml) k_qfields<true, false><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz);
-  else k_qfields<false, false><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz);
+  if (L.cpml) k_qfields<true, false><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz, H.t);
+  else k_qfields<false, false><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz, H.t);
   return cudaGetLastError();
 }
 
@@ -793,12 +982,17 @@ cudaError_t apply_t(const HybridT& H, const Coef& C, const SetLayout& L, int dir
 }
 
 cudaError_t step_start(float* lam, const SetLayout& L, const Coef& C, float* tmp,
-                       const float* res, float* mu, float* kb, const uint8_t* mask, float c,
-                       cudaStream_t st) {
+                       const float* res_all, int gap, int* step, float* mu, float* kb,
+                       const uint8_t* mask, float c, cudaStream_t st) {
   // the filter taps (src/elements.cu:30-33), as the forward finish kernel uses them
   const W7 w7{{1.1e-13f, 1.678e-06f, 0.03419f, 0.93163f, 0.03419f, 1.678e-06f, 1.1e-13f}};
   const int threads = L.nx < 1024 ? (L.nx + 31) / 32 * 32 : 1024;
-  k_step_start<<<1, threads, 0, st>>>(lam, L, C.nrm, tmp, w7, res, mu, kb, mask, c);
+  k_step_start<<<1, threads, 0, st>>>(lam, L, C.nrm, tmp, w7, res_all, gap, step, mu, kb, mask, c);
+  return cudaGetLastError();
+}
+
+cudaError_t set_step(int* step, int n, cudaStream_t st) {
+  k_set_int<<<1, 1, 0, st>>>(step, n);
   return cudaGetLastError();
 }
 

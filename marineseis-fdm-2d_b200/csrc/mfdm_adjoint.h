@@ -127,9 +127,14 @@ cudaError_t apply_t(const HybridT& H, const Coef& C, const SetLayout& L, int dir
 // lam <- F^T lam on the interface rows (the transposed post-step filter; tmp
 // holds 8 * nx floats), and the filtered cells also get mu = lam and
 // kb = c M lam (the rest of both was formed by the previous transposed step).
+// The time index n is read from the device counter `step` (res_all: the
+// residuals of every sample, [ns][3][nx]; injected when n % gap == 0), which
+// the launch leaves at n - 1.
 cudaError_t step_start(float* lam, const SetLayout& L, const Coef& C, float* tmp,
-                       const float* res, float* mu, float* kb, const uint8_t* mask, float c,
-                       cudaStream_t st);
+                       const float* res_all, int gap, int* step, float* mu, float* kb,
+                       const uint8_t* mask, float c, cudaStream_t st);
+// Sets the device counter of the transposed steps.
+cudaError_t set_step(int* step, int n, cudaStream_t st);
 
 // Material gradients of one stage: g[m][cell] += kb . dL_dir/dm (Y) over the
 // cell's main fields (and the coupled interface column); Y is a set, kb a

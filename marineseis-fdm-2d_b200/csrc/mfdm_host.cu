@@ -214,7 +214,9 @@ struct AdjointState {
   cudaEvent_t ev_rev[2] = {nullptr, nullptr};  // last reverse reading seg / seg2 done
   int nsteps = -1, every = 0;  // the forward run a backward pass may follow
   double build_ms = 0.0;       // operator assembly time (host clock)
+  int* step = nullptr;         // device time index of the transposed steps (step_start)
   ~AdjointState() {
+    cudaFree(step);
     for (auto& h : H) {
       cudaFree(h.rest.rowptr);
       cudaFree(h.rest.col);
@@ -1585,7 +1587,7 @@ int adjoint_prepare(mfdm_model* m) {
     if ((rc = dalloc(&a->mask, n)) || (rc = dalloc(&a->lam, n)) || (rc = dalloc(&a->mu, n)) ||
         (rc = dalloc(&a->H[0].qx, n)) || (rc = dalloc(&a->H[0].qz, n)) ||
         (rc = dalloc(&a->kb[0], n)) || (rc = dalloc(&a->kb[1], n)) ||
-        (rc = dalloc(&a->tmp, size_t(8) * m->cfg.nx)) ||
+        (rc = dalloc(&a->tmp, size_t(8) * m->cfg.nx)) || (rc = dalloc(&a->step, 1)) ||
         (rc = dalloc(&a->grad, size_t(2) * m->cfg.nzf * m->P + size_t(5) * m->cfg.nzs * m->P)))
       return rc;
     // Q fields off the interior set are never written and must stay 0
@@ -1707,10 +1709,11 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
   double* g[7];
   for (int k = 0; k < 7; ++k) g[k] = grad_array(m, k);
   const float *c = C.rk_c, *w = C.rk_w;
-  const float* res = n % m->gap == 0 ? a->res + size_t(n / m->gap) * 3 * m->cfg.nx : nullptr;
   // mu = F^T lam and kb = c3 M mu: off the interface rows both were formed by
-  // the previous transposed step's last stage (zero before the first)
-  MFDM_CU(mfdm::adj::step_start(a->lam, L, C, a->tmp, res, a->mu, a->kb[0], a->mask, c[3], st));
+  // the previous transposed step's last stage (zero before the first); the
+  // time index comes from the device counter (n), which it leaves at n - 1
+  MFDM_CU(mfdm::adj::step_start(a->lam, L, C, a->tmp, a->res, m->gap, a->step, a->mu, a->kb[0],
+                                a->mask, c[3], st));
   // Each stage: once kb[kin] is complete, its sparse rows of L^T kb (side
   // stream) and its material-gradient accumulation (side_g) run beside the Q
   // fields and the transposed product on the main stream. The product writes
@@ -1738,6 +1741,21 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
   if ((rc = stage(d0, 0, 1, false, c[3], 0.f)) != MFDM_OK) return rc;
   // the step's stage inputs and kb are not reused before its last gradient ends
   MFDM_CU(cudaStreamWaitEvent(st, a->ev_g[1], 0));
+  return MFDM_OK;
+}
+
+// Transposed steps u1-1 .. u0 with stage inputs at base (4 sets per step), on
+// the high-priority stream, after setting the device step counter. (Captured
+// as a CUDA graph per segment shape the run measured 6 % slower: the chain's
+// stream priorities over the gradient stream do not carry into graph nodes.)
+int reverse_range(mfdm_model* m, int u0, int u1, float* base) {
+  AdjointState* a = m->adj;
+  const size_t len = size_t(a->L.len);
+  MFDM_CU(mfdm::adj::set_step(a->step, u1 - 1, a->hi));
+  for (int n = u1 - 1; n >= u0; --n) {
+    const int rc = reverse_step(m, n, base + size_t(n - u0) * 4 * len);
+    if (rc != MFDM_OK) return rc;
+  }
   return MFDM_OK;
 }
 
@@ -1926,10 +1944,8 @@ int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_
   // reverse steps u1-1..u0 from buffer b, once their recompute is done
   auto reverse = [&](int u0, int u1, int b) -> int {
     MFDM_CU(cudaStreamWaitEvent(hi, a->ev_seg[b], 0));
-    for (int n = u1 - 1; n >= u0; --n) {
-      int rc2;
-      if ((rc2 = reverse_step(m, n, buf_ptr(b) + size_t(n - u0) * 4 * len)) != MFDM_OK) return rc2;
-    }
+    int rc2;
+    if ((rc2 = reverse_range(m, u0, u1, buf_ptr(b))) != MFDM_OK) return rc2;
     MFDM_CU(cudaEventRecord(a->ev_rev[b], hi));
     return MFDM_OK;
   };
@@ -1939,8 +1955,7 @@ int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_
     if (k + a->nkeep >= ncp) {
       // kept by the forward pass
       float* base = a->keep + size_t(k + a->nkeep - ncp) * size_t(every) * 4 * len;
-      for (int n = t1 - 1; n >= t0; --n)
-        if ((rc = reverse_step(m, n, base + size_t(n - t0) * 4 * len)) != MFDM_OK) return rc;
+      if ((rc = reverse_range(m, t0, t1, base)) != MFDM_OK) return rc;
       continue;
     }
     if (inner < every) {
