@@ -2,6 +2,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
+#include <climits>
 
 #include "mfdm_adjoint.h"
 
@@ -196,102 +197,71 @@ __global__ void k_apply_t(const long long* __restrict__ rowptr, const int* __res
   if (lane == 0) y[row] = s;
 }
 
-// Receivers sample the filtered interface rows of columns 3..nx-4
-// (elsewhere the record is 0 whatever the state).
-// Residual injection at column ix (receiver rows: solid vx and vz on the
-// interface row, fluid p on the interface row).
-__device__ __forceinline__ void inject_col(float* lam, const SetLayout& L, const float* __restrict__ res,
-                                           int ix) {
-  const int nx = L.nx;
-  lam[L.off[3] + ix] += res[ix];
-  lam[L.off[4] + ix] += res[nx + ix];
-  lam[L.off[2] + (long long)(L.nzf - 1) * L.pitch[2] + ix] += res[2 * nx + ix];
-}
-
 struct W7 { float w[7]; };
 
 __device__ __forceinline__ long long iface_index(const SetLayout& L, int f, int ix) {
   return f < 3 ? L.off[f] + (long long)(L.nzf - 1) * L.pitch[f] + ix : L.off[f] + ix;
 }
 
-// Transposed continuity average of column ix, divided by the column's tap sum:
-// tmp[f][ix] = (A^T lam)_f / wsum(ix).
-__device__ __forceinline__ void filter_t_a_col(const float* lam, const SetLayout& L,
-                                               const float2* __restrict__ nrm, float* tmp,
-                                               const W7& w7, int ix) {
-  const int nx = L.nx;
-  float lv[8];
-#pragma unroll
-  for (int f = 0; f < 8; ++f) lv[f] = lam[iface_index(L, f, ix)];
-  const int klo = max(-3, 3 - ix), khi = min(3, nx - 4 - ix);
-  float wsum = 0.0f;
-  for (int k = klo; k <= khi; ++k) wsum += w7.w[k + 3];
-  const float2 n = __ldg(nrm + ix);
-#pragma unroll
-  for (int f = 0; f < 8; ++f) {
-    float e[8], u[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) e[q] = q == f ? 1.0f : 0.0f;
-    interface_average(n, e, u);
-    float t = 0.0f;
-#pragma unroll
-    for (int q = 0; q < 8; ++q) t = fmaf(lv[q], u[q], t);
-    tmp[f * nx + ix] = t / wsum;
-  }
-}
+constexpr int kStartThreads = 128;                    // columns of transposed averages per block
+constexpr int kStartCols = kStartThreads - 6;         // output columns per block (3-column halos)
 
-// Transposed smoothing: lam at interface cell (f, j) = sum_k w_k tmp[f][j - k].
-// The filtered interface cells also go to mu and kb (the step's mu = F^T lam
-// and kb = c M mu, formed off the interface rows by the previous step's last
-// transposed stage).
-__device__ __forceinline__ void filter_t_b_col(float* lam, const SetLayout& L, const float* tmp,
-                                               const W7& w7, float* mu, float* kb,
-                                               const uint8_t* __restrict__ mask, float c, int j) {
+// The start of one transposed step over the interface columns 3..nx-4, with
+// the smoothing halos recomputed per block (no grid-wide barrier):
+//   v_f(ix)   = lam_f(ix) (+ the step's residual on svx, svz, fp when res != null)
+//   tmp_f(ix) = (A^T v)_f (ix) / wsum(ix)          A: the continuity average
+//   s_f(j)    = sum_k w_k tmp_f(j - k), k = -3..3  (only ix in 3..nx-4)
+// s goes to mu and to kb = c M s; lam itself is only read (the step's first
+// transposed stage takes its lam from mu, where mu = lam off these cells).
+// Receivers sample the filtered interface rows of columns 3..nx-4 only, so the
+// residuals enter there (elsewhere the record is 0 whatever the state).
+__global__ void __launch_bounds__(kStartThreads) k_step_start(
+    const float* __restrict__ lam, SetLayout L, const float2* __restrict__ nrm, W7 w7,
+    const float* __restrict__ res, float* mu, float* kb, const uint8_t* __restrict__ mask, float c) {
+  __shared__ float tmp[8][kStartThreads];
   const int nx = L.nx;
+  const int ix = blockIdx.x * kStartCols + threadIdx.x;  // = output column j0 - 3 + threadIdx.x
+  if (ix >= 3 && ix <= nx - 4) {
+    float lv[8];
+#pragma unroll
+    for (int f = 0; f < 8; ++f) lv[f] = lam[iface_index(L, f, ix)];
+    if (res) {
+      lv[3] += __ldg(res + ix);
+      lv[4] += __ldg(res + nx + ix);
+      lv[2] += __ldg(res + 2 * nx + ix);
+    }
+    const int klo = max(-3, 3 - ix), khi = min(3, nx - 4 - ix);
+    float wsum = 0.0f;
+    for (int k = klo; k <= khi; ++k) wsum += w7.w[k + 3];
+    const float2 n = __ldg(nrm + ix);
+#pragma unroll
+    for (int f = 0; f < 8; ++f) {
+      float e[8], u[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) e[q] = q == f ? 1.0f : 0.0f;
+      interface_average(n, e, u);
+      float t = 0.0f;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) t = fmaf(lv[q], u[q], t);
+      tmp[f][threadIdx.x] = t / wsum;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 3 || threadIdx.x >= kStartThreads - 3 || ix < 3 || ix > nx - 4) return;
 #pragma unroll
   for (int f = 0; f < 8; ++f) {
     float s = 0.0f;
 #pragma unroll
     for (int k = -3; k <= 3; ++k) {
-      const int i = j - k;
-      if (i >= 3 && i <= nx - 4) s = fmaf(w7.w[k + 3], tmp[f * nx + i], s);
+      const int i = ix - k;
+      if (i >= 3 && i <= nx - 4) s = fmaf(w7.w[k + 3], tmp[f][threadIdx.x - k], s);
     }
-    const long long q = iface_index(L, f, j);
-    lam[q] = s;
+    const long long q = iface_index(L, f, ix);
     mu[q] = s;
     kb[q] = mask[q] ? c * s : 0.0f;
   }
 }
 
-// The start of one transposed step in one block (the interface columns only):
-// the residual injection (res != null), the transposed continuity average into
-// tmp, a block barrier, the transposed smoothing -- one launch instead of three
-// dependent ones.
-// The transposed step's time index n comes from the device counter `step`
-// (the residuals of step n are injected when n % gap == 0) and the step
-// leaves n - 1 behind, so a captured run of transposed steps replays for any
-// segment once the counter is set.
-__global__ void __launch_bounds__(1024) k_step_start(float* lam, SetLayout L,
-                                                     const float2* __restrict__ nrm, float* tmp,
-                                                     W7 w7, const float* __restrict__ res_all,
-                                                     int gap, int* step, float* mu, float* kb,
-                                                     const uint8_t* __restrict__ mask, float c) {
-  const int nx = L.nx;
-  const int n = *step;
-  const float* res = (res_all && gap > 0 && n % gap == 0) ? res_all + (size_t)(n / gap) * 3 * nx
-                                                           : nullptr;
-  for (int ix = 3 + threadIdx.x; ix <= nx - 4; ix += blockDim.x) {
-    if (res) inject_col(lam, L, res, ix);
-    filter_t_a_col(lam, L, nrm, tmp, w7, ix);
-  }
-  __syncthreads();  // tmp of every column written (global memory, one block)
-  for (int j = 3 + threadIdx.x; j <= nx - 4; j += blockDim.x)
-    filter_t_b_col(lam, L, tmp, w7, mu, kb, mask, c, j);
-  __syncthreads();  // every thread has read the counter
-  if (threadIdx.x == 0) *step = n - 1;
-}
-
-__global__ void k_set_int(int* p, int v) { *p = v; }
 
 __global__ void k_drop_count(const long long* __restrict__ rowptr, const int* __restrict__ col,
                              SetLayout L, unsigned long long* count) {
@@ -728,58 +698,68 @@ __device__ __forceinline__ float t_stencil(const SetLayout& L, const float* __re
   return DIR == kDirF ? s : -s;
 }
 
+constexpr int kRevBlock = 128;
+
 // One thread per row of L^T: the sparse rest plus, on main-field cells, the
 // transposed interior stencil; then the RK bookkeeping of the reverse stage.
 // MODE 0: y only; 1: lam += y and, with kbn, the start of the next transposed
-// step: mu = lam, kbn = w M lam; 2: lam += M y, kbn = M (w mu + c y); 3: lam += M y
+// step: mu = lam, kbn = w M lam; 2: lam += M y, kbn = M (w mu + c y); 3: lam += M y;
+// 4: MODE 2 with lam taken from mu (the step's first stage: the step start
+// wrote the filtered interface cells to mu only, and mu = lam elsewhere).
 // `t` holds the CSR part of every row (k_rows_csr; rows without entries keep 0).
+// Grid: x over the pitch of the main arrays; y over the 3 nz_f fluid rows and
+// the 5 nz_s solid rows (one row of one array each), then over the rest of the
+// set from `tail0` in runs of gridDim.x * kRevBlock elements (strips, bands,
+// padding), striding by gridDim.y.
 template <int DIR, int MODE>
-__global__ void k_reverse_h(const float* __restrict__ t, const float* __restrict__ qx,
-                            const float* __restrict__ qz, SetLayout L, float* y_or_lam,
-                            const uint8_t* __restrict__ mask, float* kbn, float* mu, float w,
-                            float cw) {
-  const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (j >= L.len) return;
-  float y = t[j];
-  // the RK operands first: their loads must not wait for a store
-  const float lam0 = MODE == 0 ? 0.f : y_or_lam[j];
-  const bool mk = MODE == 0 ? false : mask[j] != 0;
-  const float mu0 = MODE == 2 ? mu[j] : 0.f;
-  {
-    // the fluid block (3 arrays of nz_f rows) and the solid block (5 of nz_s)
-    // are contiguous at pitch P
-    const long long P = L.pitch[0], nf = (long long)L.nzf * P, ns = (long long)L.nzs * P;
-    long long rel = j - L.off[0];
-    int a = -1;
-    long long loc = 0;
-    if (rel >= 0 && rel < 3 * nf) {
-      a = int(rel / nf);
-      loc = rel - a * nf;
-    } else if ((rel = j - L.off[3]) >= 0 && rel < 5 * ns) {
-      a = 3 + int(rel / ns);
-      loc = rel - (a - 3) * ns;
+__global__ void __launch_bounds__(kRevBlock) k_reverse_h(
+    const float* __restrict__ t, const float* __restrict__ qx, const float* __restrict__ qz,
+    SetLayout L, long long tail0, int nyrows, float* y_or_lam, const uint8_t* __restrict__ mask,
+    float* kbn, float* mu, float w, float cw) {
+  const int nfr = 3 * L.nzf, nmain = nfr + 5 * L.nzs;
+  for (int yr = blockIdx.y; yr < nyrows; yr += gridDim.y) {
+    long long j;
+    int a = -1, r = 0, c = 0;
+    if (yr < nmain) {
+      c = blockIdx.x * kRevBlock + threadIdx.x;
+      if (c >= L.pitch[0]) continue;
+      if (yr < nfr) {
+        a = yr / L.nzf;
+        r = yr - a * L.nzf;
+      } else {
+        const int u = yr - nfr;
+        a = 3 + u / L.nzs;
+        r = u - (a - 3) * L.nzs;
+      }
+      j = L.off[a] + (long long)r * L.pitch[a] + c;
+    } else {
+      j = tail0 + (long long)(yr - nmain) * (gridDim.x * kRevBlock) + blockIdx.x * kRevBlock +
+          threadIdx.x;
+      if (j >= L.len) continue;
     }
-    if (a >= 0) {
-      const int r = int(loc / P), c = int(loc - r * P);
-      if (c < L.nx) y += t_stencil<DIR>(L, qx, qz, a, r, c);
+    float y = t[j];
+    // the RK operands first: their loads must not wait for a store
+    const float mu0 = (MODE == 2 || MODE == 4) ? mu[j] : 0.f;
+    const float lam0 = MODE == 0 ? 0.f : (MODE == 4 ? mu0 : y_or_lam[j]);
+    const bool mk = MODE == 0 ? false : mask[j] != 0;
+    if (a >= 0 && c < L.nx) y += t_stencil<DIR>(L, qx, qz, a, r, c);
+    if (MODE == 0) {
+      y_or_lam[j] = y;
+      continue;
     }
-  }
-  if (MODE == 0) {
-    y_or_lam[j] = y;
-    return;
-  }
-  const float m = mk ? 1.0f : 0.0f;
-  if (MODE == 1) {
-    const float l = lam0 + y;
-    y_or_lam[j] = l;
-    if (kbn) {
-      mu[j] = l;
-      kbn[j] = mk ? w * l : 0.0f;
+    const float m = mk ? 1.0f : 0.0f;
+    if (MODE == 1) {
+      const float l = lam0 + y;
+      y_or_lam[j] = l;
+      if (kbn) {
+        mu[j] = l;
+        kbn[j] = mk ? w * l : 0.0f;
+      }
+      continue;
     }
-    return;
+    y_or_lam[j] = lam0 + m * y;
+    if (MODE == 2 || MODE == 4) kbn[j] = m * fmaf(cw, y, w * mu0);
   }
-  y_or_lam[j] = lam0 + m * y;
-  if (MODE == 2) kbn[j] = m * fmaf(cw, y, w * mu0);
 }
 
 // The CSR part of L^T x on the rows that have entries, kLanes threads per row:
@@ -935,8 +915,17 @@ static cudaError_t hybrid_t(const HybridT& H, const Coef& C, const SetLayout& L,
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
-  k_reverse_h<DIR, MODE><<<unsigned((L.len + kBlock - 1) / kBlock), kBlock, 0, st>>>(
-      H.t, H.qx, H.qz, L, out, mask, kbn, mu, w, c);
+  // the main arrays are the fluid block [3][nz_f][P] at 0 and the solid block
+  // [5][nz_s][P] at off[3]; the rest of the set follows the solid block
+  const long long tail0 = L.off[3] + 5LL * L.nzs * L.pitch[3];
+  const int gx = (L.pitch[0] + kRevBlock - 1) / kRevBlock;
+  const long long run = (long long)gx * kRevBlock;
+  const long long ny = 3LL * L.nzf + 5LL * L.nzs + (L.len - tail0 + run - 1) / run;
+  if (L.off[0] != 0 || L.off[3] < 3LL * L.nzf * L.pitch[0] || tail0 > L.len || ny > INT_MAX)
+    return cudaErrorInvalidValue;
+  const unsigned gy = unsigned(ny < 65535 ? ny : 65535);
+  k_reverse_h<DIR, MODE><<<dim3(unsigned(gx), gy), kRevBlock, 0, st>>>(
+      H.t, H.qx, H.qz, L, tail0, int(ny), out, mask, kbn, mu, w, c);
   return cudaGetLastError();
 }
 
@@ -966,9 +955,13 @@ cudaError_t sparse_rows(const HybridT& H, const float* kb, cudaStream_t st) {
 
 cudaError_t reverse_stage(const HybridT& H, const Coef& C, const SetLayout& L, int dir,
                           const float* kb, float* lam, const uint8_t* mask, bool mask_lam,
-                          float* kbn, float* mu, float w, float c, bool q_ready,
+                          float* kbn, float* mu, float w, float c, bool q_ready, bool lam_from_mu,
                           cudaStream_t st) {
   if (!mask_lam) return hybrid_dir<1>(H, C, L, dir, kb, lam, mask, kbn, mu, w, c, q_ready, st);
+  if (lam_from_mu) {
+    if (!kbn) return cudaErrorInvalidValue;
+    return hybrid_dir<4>(H, C, L, dir, kb, lam, mask, kbn, mu, w, c, q_ready, st);
+  }
   if (kbn) return hybrid_dir<2>(H, C, L, dir, kb, lam, mask, kbn, mu, w, c, q_ready, st);
   return hybrid_dir<3>(H, C, L, dir, kb, lam, mask, kbn, mu, w, c, q_ready, st);
 }
@@ -981,21 +974,15 @@ cudaError_t apply_t(const HybridT& H, const Coef& C, const SetLayout& L, int dir
   return cudaGetLastError();
 }
 
-cudaError_t step_start(float* lam, const SetLayout& L, const Coef& C, float* tmp,
-                       const float* res_all, int gap, int* step, float* mu, float* kb,
-                       const uint8_t* mask, float c, cudaStream_t st) {
+cudaError_t step_start(const float* lam, const SetLayout& L, const Coef& C, const float* res,
+                       float* mu, float* kb, const uint8_t* mask, float c, cudaStream_t st) {
+  if (L.nx < 7) return cudaSuccess;  // no interface columns 3..nx-4
   // the filter taps (src/elements.cu:30-33), as the forward finish kernel uses them
   const W7 w7{{1.1e-13f, 1.678e-06f, 0.03419f, 0.93163f, 0.03419f, 1.678e-06f, 1.1e-13f}};
-  const int threads = L.nx < 1024 ? (L.nx + 31) / 32 * 32 : 1024;
-  k_step_start<<<1, threads, 0, st>>>(lam, L, C.nrm, tmp, w7, res_all, gap, step, mu, kb, mask, c);
+  const unsigned blocks = unsigned((L.nx - 6 + kStartCols - 1) / kStartCols);
+  k_step_start<<<blocks, kStartThreads, 0, st>>>(lam, L, C.nrm, w7, res, mu, kb, mask, c);
   return cudaGetLastError();
 }
-
-cudaError_t set_step(int* step, int n, cudaStream_t st) {
-  k_set_int<<<1, 1, 0, st>>>(step, n);
-  return cudaGetLastError();
-}
-
 
 template <int DIR, bool CPML>
 static cudaError_t gradient_t(const Coef& C, const SetLayout& L, const Fields& Y, const Fields& KB,

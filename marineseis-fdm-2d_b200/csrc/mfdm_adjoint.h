@@ -97,20 +97,21 @@ cudaError_t sort_rows(const CsrT& A, long long len, cudaStream_t st);
 cudaError_t drop_interior(const CsrT& full, const SetLayout& L, CsrT* rest,
                           unsigned long long* count, void** tmp, size_t* tmp_bytes, cudaStream_t st);
 
-// One reverse stage: y = L^T kb, lam += (mask_lam ? M : 1) y and, when kbn is
-// given, kbn = M (w mu + c y); without mask_lam (the step's last stage) and
-// with kbn, it also starts the next transposed step: mu = lam, kbn = w M lam.
-// q_ready: the Q fields of kb (written by gradient()) and its sparse rows
-// (sparse_rows()) are already in H.
 // The sparse rows of L^T kb into H.t (the rows listed in H.nzrow), so that a
 // stream other than the gradient's can form them concurrently.
 cudaError_t sparse_rows(const HybridT& H, const float* kb, cudaStream_t st);
 // The Q fields of kb into H.qx / H.qz (0 off the interior cells).
 cudaError_t q_fields(const HybridT& H, const Coef& C, const SetLayout& L, const float* kb,
                      cudaStream_t st);
+// One reverse stage: y = L^T kb, lam += (mask_lam ? M : 1) y and, when kbn is
+// given, kbn = M (w mu + c y); without mask_lam (the step's last stage) and
+// with kbn, it also starts the next transposed step: mu = lam, kbn = w M lam.
+// q_ready: the Q fields of kb (q_fields()) and its sparse rows (sparse_rows())
+// are already in H. lam_from_mu (with mask_lam and kbn: the step's first
+// stage) reads lam from mu, which holds the step start's filtered lam.
 cudaError_t reverse_stage(const HybridT& H, const Coef& C, const SetLayout& L, int dir,
                           const float* kb, float* lam, const uint8_t* mask, bool mask_lam,
-                          float* kbn, float* mu, float w, float c, bool q_ready,
+                          float* kbn, float* mu, float w, float c, bool q_ready, bool lam_from_mu,
                           cudaStream_t st);
 // Lists the rows of H->rest that have entries and allocates H->t (zeroed);
 // flag (len + 1) and tmp are scratch.
@@ -122,19 +123,14 @@ cudaError_t random_fill(float* x, long long n, unsigned seed, cudaStream_t st);
 cudaError_t apply_t(const HybridT& H, const Coef& C, const SetLayout& L, int dir, const float* x,
                     float* y, cudaStream_t st);
 
-// The start of one transposed step, in one launch: with res (one receiver
-// sample's residuals, svx, svz, fp rows of nx) it is added to lam; then
-// lam <- F^T lam on the interface rows (the transposed post-step filter; tmp
-// holds 8 * nx floats), and the filtered cells also get mu = lam and
-// kb = c M lam (the rest of both was formed by the previous transposed step).
-// The time index n is read from the device counter `step` (res_all: the
-// residuals of every sample, [ns][3][nx]; injected when n % gap == 0), which
-// the launch leaves at n - 1.
-cudaError_t step_start(float* lam, const SetLayout& L, const Coef& C, float* tmp,
-                       const float* res_all, int gap, int* step, float* mu, float* kb,
-                       const uint8_t* mask, float c, cudaStream_t st);
-// Sets the device counter of the transposed steps.
-cudaError_t set_step(int* step, int n, cudaStream_t st);
+// The start of one transposed step, in one launch: with res (the residuals of
+// the step's receiver sample, svx, svz, fp rows of nx) added to lam's
+// interface cells, the transposed post-step filter F^T lam of the interface
+// columns goes to mu and kb = c M mu there (off those cells both were formed
+// by the previous transposed step, with mu = lam). lam is only read: the step's
+// first transposed stage takes lam from mu (reverse_stage, lam_from_mu).
+cudaError_t step_start(const float* lam, const SetLayout& L, const Coef& C, const float* res,
+                       float* mu, float* kb, const uint8_t* mask, float c, cudaStream_t st);
 
 // Material gradients of one stage: g[m][cell] += kb . dL_dir/dm (Y) over the
 // cell's main fields (and the coupled interface column); Y is a set, kb a

@@ -179,7 +179,7 @@ struct AdjointState {
   mfdm::SetLayout L{};
   mfdm::HybridT H[2];      // transposed stage operators, F and B (shared Q buffers)
   uint8_t* mask = nullptr;
-  float *lam = nullptr, *mu = nullptr, *kb[2] = {nullptr, nullptr}, *tmp = nullptr;
+  float *lam = nullptr, *mu = nullptr, *kb[2] = {nullptr, nullptr};
   double* grad = nullptr;  // K, 1/rho_f [nz_f][P]; C11, C13, C33, C55, 1/rho_s [nz_s][P]
   bool grad_ready = false;  // grad holds a finished backward pass
   float* ckpt = nullptr;   // checkpoint sets
@@ -189,12 +189,15 @@ struct AdjointState {
   size_t seg_steps = 0;    // while this one is reversed (when the memory allows)
   float* keep = nullptr;   // stage inputs of the last `nkeep` segments, kept by the forward pass
   size_t keep_floats = 0;
-  // TMA maps of every kept step's four stage-input sets (stencil boxes) and of
-  // its first set as U^n (point-wise boxes): the kept steps run their stages
-  // in place in the keep buffer
+  // TMA maps of every step slot's four stage-input sets (stencil boxes) and of
+  // its first set as U^n (point-wise boxes), per buffer of slots (keep, seg,
+  // seg2): kept and recomputed steps run their stages in place in the slots
   struct SlotMaps { CUtensorMap fst[4], sst[4], fun, sun; };
-  std::vector<SlotMaps> keep_maps;
-  const float* keep_maps_for = nullptr;
+  struct SlotTable {
+    const float* base = nullptr;
+    std::vector<SlotMaps> maps;
+  };
+  SlotTable keep_tab, seg_tab[2];
   int nkeep = 0;
   float* res = nullptr;    // residual samples [ns][3][nx]
   float* inner = nullptr;  // second-level checkpoints of one segment
@@ -214,9 +217,7 @@ struct AdjointState {
   cudaEvent_t ev_rev[2] = {nullptr, nullptr};  // last reverse reading seg / seg2 done
   int nsteps = -1, every = 0;  // the forward run a backward pass may follow
   double build_ms = 0.0;       // operator assembly time (host clock)
-  int* step = nullptr;         // device time index of the transposed steps (step_start)
   ~AdjointState() {
-    cudaFree(step);
     for (auto& h : H) {
       cudaFree(h.rest.rowptr);
       cudaFree(h.rest.col);
@@ -227,7 +228,7 @@ struct AdjointState {
     cudaFree(H[0].qx);
     cudaFree(H[0].qz);
     cudaFree(mask); cudaFree(lam); cudaFree(mu); cudaFree(kb[0]); cudaFree(kb[1]);
-    cudaFree(tmp); cudaFree(grad); cudaFree(ckpt); cudaFree(seg); cudaFree(res); cudaFree(keep);
+    cudaFree(grad); cudaFree(ckpt); cudaFree(seg); cudaFree(res); cudaFree(keep);
     cudaFree(inner);
     cudaFree(scan_tmp);
     if (ev_kb) cudaEventDestroy(ev_kb);
@@ -453,12 +454,8 @@ int ensure_capacity(mfdm_model* m, int steps) {
 
 // Enqueues the five launches of one step. With `ev` (6 events) an event is
 // recorded before the first launch and after every launch.
-// With `save` (4 set-sized buffers) the four stage inputs are copied out as the
-// step runs (U, then the outputs of stages 0, 1 and 2), for the adjoint.
-int enqueue_step(mfdm_model* m, int it, cudaStream_t st, cudaEvent_t* ev = nullptr,
-                 float* const* save = nullptr) {
+int enqueue_step(mfdm_model* m, int it, cudaStream_t st, cudaEvent_t* ev = nullptr) {
   const int d0 = (it & 1) ? mfdm::kDirB : mfdm::kDirF, d1 = 1 - d0;
-  const size_t set_bytes = size_t(m->S[1].fvx - m->S[0].fvx) * sizeof(float);
   const Fields &U = m->S[0], &A = m->S[1], &B = m->S[2], &Acc = m->S[3];
   const Coef& C = m->C;
   // stage s reads in[s] and writes out[s]: U -> A -> B -> A -> U
@@ -467,7 +464,6 @@ int enqueue_step(mfdm_model* m, int it, cudaStream_t st, cudaEvent_t* ev = nullp
   const int in_set[4] = {0, 1, 2, 1};
   const int dir[4] = {d0, d1, d0, d1};
   if (ev) MFDM_CU(cudaEventRecord(ev[0], st));
-  if (save) MFDM_CU(cudaMemcpyAsync(save[0], U.fvx, set_bytes, cudaMemcpyDeviceToDevice, st));
   for (int s = 0; s < 4; ++s) {
     mfdm::StageMaps maps;
     maps.fin = m->fst[in_set[s]];
@@ -480,8 +476,6 @@ int enqueue_step(mfdm_model* m, int it, cudaStream_t st, cudaEvent_t* ev = nullp
     maps.scoef = m->sco;
     MFDM_CU(mfdm::launch_stage(C, *in[s], *out[s], U, Acc, maps, s, dir[s], st));
     if (ev) MFDM_CU(cudaEventRecord(ev[s + 1], st));
-    if (save && s < 3)
-      MFDM_CU(cudaMemcpyAsync(save[s + 1], out[s]->fvx, set_bytes, cudaMemcpyDeviceToDevice, st));
   }
   MFDM_CU(mfdm::launch_finish(C, U, st));
   if (ev) MFDM_CU(cudaEventRecord(ev[5], st));
@@ -1587,7 +1581,6 @@ int adjoint_prepare(mfdm_model* m) {
     if ((rc = dalloc(&a->mask, n)) || (rc = dalloc(&a->lam, n)) || (rc = dalloc(&a->mu, n)) ||
         (rc = dalloc(&a->H[0].qx, n)) || (rc = dalloc(&a->H[0].qz, n)) ||
         (rc = dalloc(&a->kb[0], n)) || (rc = dalloc(&a->kb[1], n)) ||
-        (rc = dalloc(&a->tmp, size_t(8) * m->cfg.nx)) || (rc = dalloc(&a->step, 1)) ||
         (rc = dalloc(&a->grad, size_t(2) * m->cfg.nzf * m->P + size_t(5) * m->cfg.nzs * m->P)))
       return rc;
     // Q fields off the interior set are never written and must stay 0
@@ -1636,46 +1629,49 @@ double* grad_array(mfdm_model* m, int k) {
   return m->adj->grad + (k < 2 ? size_t(k) * nf : 2 * nf + size_t(k - 2) * ns);
 }
 
-// Encodes the TMA maps of every step slot of the keep buffer (once per buffer).
-int keep_maps(mfdm_model* m, size_t nslots) {
-  AdjointState* a = m->adj;
-  if (a->keep_maps_for == a->keep && a->keep_maps.size() >= nslots) return MFDM_OK;
-  const mfdm::SetLayout& L = a->L;
+// Encodes the TMA maps of the first `nslots` step slots of the slot buffer at
+// `base` into `t` (once per buffer).
+int slot_maps(mfdm_model* m, AdjointState::SlotTable& t, const float* base, size_t nslots) {
+  if (t.base == base && t.maps.size() >= nslots) return MFDM_OK;
+  const mfdm::SetLayout& L = m->adj->L;
   const size_t len = size_t(L.len);
   const int P = m->P, nzf = m->cfg.nzf, nzs = m->cfg.nzs;
-  a->keep_maps.assign(nslots, AdjointState::SlotMaps{});
+  t.base = nullptr;
+  t.maps.assign(nslots, AdjointState::SlotMaps{});
   int rc;
   for (size_t j = 0; j < nslots; ++j) {
-    AdjointState::SlotMaps& M = a->keep_maps[j];
+    AdjointState::SlotMaps& M = t.maps[j];
     for (int s = 0; s < 4; ++s) {
-      const float* base = a->keep + (j * 4 + size_t(s)) * len;
-      if ((rc = encode_block(&M.fst[s], base + L.off[0], P, nzf, 3, mfdm::kStageSW, true, m->nshots, m->region)) ||
-          (rc = encode_block(&M.sst[s], base + L.off[3], P, nzs, 5, mfdm::kStageSW, true, m->nshots, m->region)))
+      const float* set = base + (j * 4 + size_t(s)) * len;
+      if ((rc = encode_block(&M.fst[s], set + L.off[0], P, nzf, 3, mfdm::kStageSW, true, m->nshots, m->region)) ||
+          (rc = encode_block(&M.sst[s], set + L.off[3], P, nzs, 5, mfdm::kStageSW, true, m->nshots, m->region)))
         return rc;
     }
-    const float* y1 = a->keep + j * 4 * len;
+    const float* y1 = base + j * 4 * len;
     if ((rc = encode_block(&M.fun, y1 + L.off[0], P, nzf, 3, mfdm::kStageTX, false, m->nshots, m->region)) ||
         (rc = encode_block(&M.sun, y1 + L.off[3], P, nzs, 5, mfdm::kStageTX, false, m->nshots, m->region)))
       return rc;
   }
-  a->keep_maps_for = a->keep;
+  t.base = base;
   return MFDM_OK;
 }
 
-// One step of a kept segment, run in place in its slot j: stage 0 reads U^n
-// from the slot's first set, stages 0-2 write the next three sets (the stage
-// inputs the backward pass reads), the last stage writes U^{n+1} into the next
-// slot's first set, or into the handle's state U after the run's last step.
-int enqueue_kept_step(mfdm_model* m, int it, size_t j, bool last_of_run, cudaStream_t st) {
+// One step run in place in slot j of a slot buffer (maps `t`): stage 0 reads
+// U^n from the slot's first set, stages 0-2 write the next three sets (the
+// stage inputs the backward pass reads), the last stage writes U^{n+1} into the
+// next slot's first set, or into the handle's state U after the run's last step.
+int enqueue_slot_step(mfdm_model* m, int it, const AdjointState::SlotTable& t, size_t j,
+                      bool last_of_run, cudaStream_t st) {
   AdjointState* a = m->adj;
   const mfdm::SetLayout& L = a->L;
   const size_t len = size_t(L.len);
+  float* base = const_cast<float*>(t.base);
   const int d0 = (it & 1) ? mfdm::kDirB : mfdm::kDirF, d1 = 1 - d0;
   const int dir[4] = {d0, d1, d0, d1};
   Fields Y[4];
-  for (int s = 0; s < 4; ++s) Y[s] = fields_at(L, a->keep + (j * 4 + size_t(s)) * len);
-  const Fields next = last_of_run ? m->S[0] : fields_at(L, a->keep + (j + 1) * 4 * len);
-  const AdjointState::SlotMaps& M = a->keep_maps[j];
+  for (int s = 0; s < 4; ++s) Y[s] = fields_at(L, base + (j * 4 + size_t(s)) * len);
+  const Fields next = last_of_run ? m->S[0] : fields_at(L, base + (j + 1) * 4 * len);
+  const AdjointState::SlotMaps& M = t.maps[j];
   const Fields& Acc = m->S[3];
   for (int s = 0; s < 4; ++s) {
     mfdm::StageMaps maps;
@@ -1711,15 +1707,15 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
   const float *c = C.rk_c, *w = C.rk_w;
   // mu = F^T lam and kb = c3 M mu: off the interface rows both were formed by
   // the previous transposed step's last stage (zero before the first); the
-  // time index comes from the device counter (n), which it leaves at n - 1
-  MFDM_CU(mfdm::adj::step_start(a->lam, L, C, a->tmp, a->res, m->gap, a->step, a->mu, a->kb[0],
-                                a->mask, c[3], st));
+  // residuals of step n enter when n is a receiver sample
+  const float* res = (n % m->gap == 0) ? a->res + size_t(n / m->gap) * 3 * size_t(m->cfg.nx) : nullptr;
+  MFDM_CU(mfdm::adj::step_start(a->lam, L, C, res, a->mu, a->kb[0], a->mask, c[3], st));
   // Each stage: once kb[kin] is complete, its sparse rows of L^T kb (side
   // stream) and its material-gradient accumulation (side_g) run beside the Q
   // fields and the transposed product on the main stream. The product writes
   // kb[1 - kin], which the previous stage's gradient reads: it waits for that
   // gradient (ev_g[1 - kin]; a never-recorded event is no wait).
-  auto stage = [&](int d, int sy, int kin, bool mask_lam, float ws, float cs) -> int {
+  auto stage = [&](int d, int sy, int kin, bool mask_lam, float ws, float cs, bool first) -> int {
     MFDM_CU(cudaEventRecord(a->ev_kb, st));
     MFDM_CU(cudaStreamWaitEvent(a->side, a->ev_kb, 0));
     MFDM_CU(mfdm::adj::sparse_rows(a->H[d], a->kb[kin], a->side));
@@ -1731,27 +1727,27 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
     MFDM_CU(cudaStreamWaitEvent(st, a->ev_rows, 0));
     MFDM_CU(cudaStreamWaitEvent(st, a->ev_g[1 - kin], 0));
     MFDM_CU(mfdm::adj::reverse_stage(a->H[d], C, L, d, a->kb[kin], a->lam, a->mask, mask_lam,
-                                     a->kb[1 - kin], a->mu, ws, cs, true, st));
+                                     a->kb[1 - kin], a->mu, ws, cs, true, first, st));
     return MFDM_OK;
   };
   int rc;
-  if ((rc = stage(d1, 3, 0, true, w[2], c[2])) != MFDM_OK) return rc;
-  if ((rc = stage(d0, 2, 1, true, w[1], c[1])) != MFDM_OK) return rc;
-  if ((rc = stage(d1, 1, 0, true, w[0], c[0])) != MFDM_OK) return rc;
-  if ((rc = stage(d0, 0, 1, false, c[3], 0.f)) != MFDM_OK) return rc;
+  // the first stage takes lam from mu (the step start leaves lam unfiltered)
+  if ((rc = stage(d1, 3, 0, true, w[2], c[2], true)) != MFDM_OK) return rc;
+  if ((rc = stage(d0, 2, 1, true, w[1], c[1], false)) != MFDM_OK) return rc;
+  if ((rc = stage(d1, 1, 0, true, w[0], c[0], false)) != MFDM_OK) return rc;
+  if ((rc = stage(d0, 0, 1, false, c[3], 0.f, false)) != MFDM_OK) return rc;
   // the step's stage inputs and kb are not reused before its last gradient ends
   MFDM_CU(cudaStreamWaitEvent(st, a->ev_g[1], 0));
   return MFDM_OK;
 }
 
 // Transposed steps u1-1 .. u0 with stage inputs at base (4 sets per step), on
-// the high-priority stream, after setting the device step counter. (Captured
-// as a CUDA graph per segment shape the run measured 6 % slower: the chain's
-// stream priorities over the gradient stream do not carry into graph nodes.)
+// the high-priority stream. (Captured as a CUDA graph per segment shape the
+// run measured 6 % slower: the chain's stream priorities over the gradient
+// stream do not carry into graph nodes.)
 int reverse_range(mfdm_model* m, int u0, int u1, float* base) {
   AdjointState* a = m->adj;
   const size_t len = size_t(a->L.len);
-  MFDM_CU(mfdm::adj::set_step(a->step, u1 - 1, a->hi));
   for (int n = u1 - 1; n >= u0; --n) {
     const int rc = reverse_step(m, n, base + size_t(n - u0) * 4 * len);
     if (rc != MFDM_OK) return rc;
@@ -1819,7 +1815,8 @@ int mfdm_adjoint_forward(mfdm_model* m, int nsteps, int ckpt_every) {
     // strips) must read 0, as in the handle's own sets
     MFDM_CU(cudaMemset(a->keep, 0, nkeep * seg_floats * sizeof(float)));
   }
-  if (nkeep > 0 && (rc = keep_maps(m, nkeep * size_t(ckpt_every))) != MFDM_OK) return rc;
+  if (nkeep > 0 && (rc = slot_maps(m, a->keep_tab, a->keep, nkeep * size_t(ckpt_every))) != MFDM_OK)
+    return rc;
   a->nkeep = int(nkeep);
   a->nsteps = -1;
   if ((rc = clear_state(m)) != MFDM_OK) return rc;
@@ -1835,7 +1832,8 @@ int mfdm_adjoint_forward(mfdm_model* m, int nsteps, int ckpt_every) {
                                 cudaMemcpyDeviceToDevice, m->stream));
       for (int j = 0; j < todo; ++j) {
         const bool last = k + 1 == ncp && j + 1 == todo;
-        if ((rc = enqueue_kept_step(m, m->host_step, j0 + size_t(j), last, m->stream)) != MFDM_OK)
+        if ((rc = enqueue_slot_step(m, m->host_step, a->keep_tab, j0 + size_t(j), last, m->stream)) !=
+            MFDM_OK)
           return rc;
         ++m->host_step;
       }
@@ -1892,8 +1890,12 @@ int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_
     a->seg2 = nullptr;
     a->seg_steps = 0;
     if ((rc = dalloc(&a->seg, size_t(inner) * 4 * len)) != MFDM_OK) return rc;
+    // cells a stage never writes must read 0, as in the handle's own sets
+    MFDM_CU(cudaMemset(a->seg, 0, size_t(inner) * 4 * len * sizeof(float)));
     a->seg_steps = size_t(inner);
   }
+  if (a->nkeep < ncp && (rc = slot_maps(m, a->seg_tab[0], a->seg, a->seg_steps)) != MFDM_OK)
+    return rc;
   if (a->nkeep < ncp && inner < every && ninner > a->inner_sets) {
     cudaFree(a->inner);
     a->inner = nullptr;
@@ -1921,22 +1923,24 @@ int mfdm_adjoint_backward(mfdm_model* m, const float* res_svx, const float* res_
       (void)cudaGetLastError();  // not enough memory for two: one buffer, no overlap
       a->seg2 = nullptr;
       dbl = false;
+    } else {
+      MFDM_CU(cudaMemset(a->seg2, 0, a->seg_steps * 4 * len * sizeof(float)));
     }
   }
+  if (dbl && (rc = slot_maps(m, a->seg_tab[1], a->seg2, a->seg_steps)) != MFDM_OK) return rc;
   auto buf_of = [&](int k) { return (dbl && (k & 1)) ? 1 : 0; };
   auto buf_ptr = [&](int b) { return b ? a->seg2 : a->seg; };
-  // restore checkpoint k and recompute steps u0..u1-1 keeping every stage
-  // input in buffer b (after the last reverse that read it)
+  // restore checkpoint k into the first slot of buffer b and recompute steps
+  // u0..u1-1 in place in its slots (after the last reverse that read it)
   auto recompute = [&](int k, int u0, int u1, int b, bool from_ckpt, const float* from) -> int {
     MFDM_CU(cudaStreamWaitEvent(st, a->ev_rev[b], 0));
-    MFDM_CU(cudaMemcpyAsync(m->S[0].fvx, from_ckpt ? a->ckpt + size_t(k) * len : from,
+    MFDM_CU(cudaMemcpyAsync(buf_ptr(b), from_ckpt ? a->ckpt + size_t(k) * len : from,
                             len * sizeof(float), cudaMemcpyDeviceToDevice, st));
     MFDM_CU(mfdm::launch_set_step(m->C, u0, st));
     for (int n = u0; n < u1; ++n) {
-      float* slot = buf_ptr(b) + size_t(n - u0) * 4 * len;
-      float* save[4] = {slot, slot + len, slot + 2 * len, slot + 3 * len};
       int rc2;
-      if ((rc2 = enqueue_step(m, n, st, nullptr, save)) != MFDM_OK) return rc2;
+      if ((rc2 = enqueue_slot_step(m, n, a->seg_tab[b], size_t(n - u0), n + 1 == u1, st)) != MFDM_OK)
+        return rc2;
     }
     MFDM_CU(cudaEventRecord(a->ev_seg[b], st));
     return MFDM_OK;
