@@ -430,6 +430,41 @@ def adjoint_rate(mfdm, device: int, nsteps: int = 4000, every: int = 50):
                               "adjoint_over_forward": round((kfwd + kbwd) / fwd, 3)}}
 
 
+def north_star_adjoint_rate(mfdm, device: int, nsteps: int = 400, every: int = 50):
+    """Adjoint cost at the 4096x2048 curvilinear size: `nsteps` RK4 steps,
+    checkpoint every `every`, every segment recomputed (one level, the next
+    segment recomputed into a second stage-input buffer while the current one
+    is reversed). Residuals: 1 % of the model's own records. Host wall time of
+    the synchronous calls, the second of two adjoint passes (the first also
+    assembles the transposed operators)."""
+    import torch
+    m = modelgen.curvilinear_4096x2048(nt=nsteps)
+    torch.cuda.synchronize(device)
+    free0, _ = torch.cuda.mem_get_info(device)
+    with mfdm.Solver.from_model(m, device=device) as s:
+        s.set_shot(0, reset=True)
+        s.step(16)
+        s.set_shot(0, reset=True)
+        t0 = time.perf_counter()
+        s.step(nsteps)
+        fwd = time.perf_counter() - t0
+        s.set_shot(0, reset=True)
+        rec = s.adjoint_forward(nsteps, every)
+        s.adjoint_backward_only({k: (0.01 * v).astype(np.float32) for k, v in rec.items()})
+        s.set_shot(0, reset=True)
+        t0 = time.perf_counter()
+        rec = s.adjoint_forward(nsteps, every)
+        afwd = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        s.adjoint_backward_only({k: (0.01 * v).astype(np.float32) for k, v in rec.items()})
+        bwd = time.perf_counter() - t0
+        used = free0 - torch.cuda.mem_get_info(device)[0]
+    return {"model": "curvilinear 4096x2048", "steps": nsteps, "ckpt_every": every,
+            "forward_s": round(fwd, 4), "adjoint_forward_s": round(afwd, 4),
+            "backward_s": round(bwd, 4), "adjoint_over_forward": round((afwd + bwd) / fwd, 3),
+            "device_gb_in_use": round(used / 1e9, 2)}
+
+
 def large_adjoint_rate(mfdm, device: int, nshots: int = 1, nsteps: int = 200, every: int = 100,
                        inner: int = 5, ckpt_probe_steps: int = 0):
     """The 8192 x 4096 batched-adjoint workload (von Kármán rough seafloor, Hurst
@@ -699,6 +734,7 @@ def main():
             fp64_error(mfdm, m_init, 400, local),
             note="forward state of the initial model; the gradient against the FP64 "
                  "adjoint oracle is checked in tests/test_gpu_adjoint.py (rel-L2 <= 1e-3)")
+        other["adjoint_4096x2048"] = north_star_adjoint_rate(mfdm, local)
         other["solid_only_2048x2048"] = solid_only_rate(mfdm, local)
         other["adjoint_8192x4096_rough_seafloor"] = large_adjoint_rate(mfdm, local)
         other["reference_cuda_build"] = reference_cuda_build([

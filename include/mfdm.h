@@ -256,8 +256,8 @@ int mfdm_adjoint_set_memory(mfdm_model* m, long long bytes);
  * recomputes and reverses one inner stretch at a time, so it holds
  * ceil(ckpt_every / inner_every) + 4 * inner_every states instead of
  * 4 * ckpt_every, for one more forward pass. 0 (the default): one level.
- * For example 8000 steps of an 8192x4096 model (about 1.1 GB per state) fit
- * in roughly 110 GB with ckpt_every 200 and inner_every 5. */
+ * For example 8000 steps of an 8192x4096 model (0.55 GB per state) held
+ * 66.6 GB of device memory in all with ckpt_every 200 and inner_every 5. */
 int mfdm_adjoint_set_inner(mfdm_model* m, int inner_every);
 
 /* Runs `nsteps` steps of the current shot from rest, storing the state every
