@@ -654,7 +654,7 @@ def main():
         return
 
     # ---- per-kernel durations (events around every launch) ----
-    nk = min(args.steps, 40)
+    nk = min(args.steps, 200)
     _, kms = solver.time_steps(nk, per_kernel=True)
     stage_ms = sum(kms[:4]) / nk  # the four stage launches of one step
     alg = algorithmic_bytes(model)

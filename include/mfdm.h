@@ -128,9 +128,10 @@ int mfdm_step(mfdm_model* m, int nsteps);
 
 /* Advances `nsteps` steps like mfdm_step and reports device time measured
  * with CUDA events on the handle's stream: *total_ms for the whole run. With
- * per_kernel != 0 the steps are launched one by one with an event pair around
- * every kernel, and kernel_ms[0..3] receive the summed time of the four RK
- * stage launches and kernel_ms[4] that of the filter/receiver launch. */
+ * per_kernel != 0 the steps are launched one by one (back to back, outside the
+ * graph) with an event between consecutive kernels, and kernel_ms[0..3] receive
+ * the summed time of the four RK stage launches and kernel_ms[4] that of the
+ * filter/receiver launch. */
 int mfdm_time_steps(mfdm_model* m, int nsteps, int per_kernel, float* total_ms, float* kernel_ms);
 
 /* Waits for the handle's stream. */

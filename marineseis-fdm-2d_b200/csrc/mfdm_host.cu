@@ -1038,19 +1038,34 @@ int mfdm_time_steps(mfdm_model* m, int nsteps, int per_kernel, float* total_ms, 
     MFDM_CU(cudaEventElapsedTime(total_ms, ev[6], ev[7]));
     return check_status(m);
   }
+  // the steps go back to back (no wait between them, as in a run), in chunks
+  // of kChunk steps with six events each
+  constexpr int kChunk = 256;
+  std::vector<cudaEvent_t> pool(size_t(std::min(nsteps, kChunk)) * 6, nullptr);
+  struct FreePool {
+    std::vector<cudaEvent_t>& p;
+    ~FreePool() { for (cudaEvent_t e : p) if (e) cudaEventDestroy(e); }
+  } fp{pool};
+  for (auto& e : pool) MFDM_CU(cudaEventCreate(&e));
   float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, tot = 0.f;
-  for (int k = 0; k < nsteps; ++k) {
-    if ((rc = enqueue_step(m, m->host_step, m->stream, ev)) != MFDM_OK) return rc;
-    ++m->host_step;
-    MFDM_CU(cudaEventSynchronize(ev[5]));
-    for (int i = 0; i < 5; ++i) {
-      float t = 0.f;
-      MFDM_CU(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
-      acc[i] += t;
+  for (int k0 = 0; k0 < nsteps; k0 += kChunk) {
+    const int n = std::min(kChunk, nsteps - k0);
+    for (int k = 0; k < n; ++k) {
+      if ((rc = enqueue_step(m, m->host_step, m->stream, &pool[size_t(k) * 6])) != MFDM_OK) return rc;
+      ++m->host_step;
     }
-    float t = 0.f;
-    MFDM_CU(cudaEventElapsedTime(&t, ev[0], ev[5]));
-    tot += t;
+    MFDM_CU(cudaEventSynchronize(pool[size_t(n - 1) * 6 + 5]));
+    for (int k = 0; k < n; ++k) {
+      const cudaEvent_t* e = &pool[size_t(k) * 6];
+      for (int i = 0; i < 5; ++i) {
+        float t = 0.f;
+        MFDM_CU(cudaEventElapsedTime(&t, e[i], e[i + 1]));
+        acc[i] += t;
+      }
+      float t = 0.f;
+      MFDM_CU(cudaEventElapsedTime(&t, e[0], e[5]));
+      tot += t;
+    }
   }
   for (int i = 0; i < 5; ++i) kernel_ms[i] = acc[i];
   *total_ms = tot;
