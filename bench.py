@@ -156,6 +156,16 @@ def algorithmic_bytes(m) -> int:
     return fluid + solid + strips * 16 * 4 * 4
 
 
+def batched_bytes(m, nshots: int) -> int:
+    """Bytes per step of `nshots` shots of one model when the coefficients are
+    read once for all shots (each shot still moves its own 16 state floats per
+    field and cell and its ADE memory)."""
+    state = m.nx * m.nz_f * 16 * 3 + m.nx * m.nz_s * 16 * 5
+    strips = 2 * m.npd * (m.nz_f - 3) + 2 * m.npd * (m.nz_s - 3) + m.npd * (m.nx - 6)
+    coef = m.nx * m.nz_f * 4 * 6 + m.nx * m.nz_s * 4 * 9
+    return (nshots * (state + strips * 16 * 4) + coef) * 4
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -334,12 +344,18 @@ def batched_rate(mfdm, model, device: int, warmup: int, nshots: int = 64, steps:
             t1, _ = s1.time_steps(steps)
             loop_ms += t1
     cells = model.cells * nshots * steps
+    peak, _ = peaks()
+    shared = batched_bytes(model, nshots) * steps / (tb / 1e3) / 1e9
+    unshared = algorithmic_bytes(model) * nshots * steps / (tb / 1e3) / 1e9
     return {"shots": nshots, "steps": steps, "ricker_hz": "U[10, 25], seed 2",
             "value": round(cells / (tb / 1e3) / 1e9, 3), "unit": "Gcell/s",
             "shot_steps_per_s": round(nshots * steps / (tb / 1e3), 1),
             "per_shot_loop_gcells": round(cells / (loop_ms / 1e3) / 1e9, 3),
             "speedup_vs_per_shot_loop": round(loop_ms / tb, 3),
-            "seg_rows": {"batch": tile_b, "per_shot": tile_1}}
+            "seg_rows": {"batch": tile_b, "per_shot": tile_1},
+            "roofline": {"bytes": "coefficients read once per segment for all shots",
+                         "achieved_gbs": round(shared, 1), "frac": round(shared / peak, 4),
+                         "frac_if_unshared": round(unshared / peak, 4)}}
 
 
 def uneven_rate(mfdm, device: int, nmodels: int = 32, steps: int = 128):
@@ -367,11 +383,14 @@ def uneven_rate(mfdm, device: int, nmodels: int = 32, steps: int = 128):
         for s in solvers:
             s.close()
     cells = sum(m.cells for m in models) * steps
+    peak, _ = peaks()
+    gbs = sum(algorithmic_bytes(m) for m in models) * steps / (tg / 1e3) / 1e9
     return {"models": nmodels, "steps": steps, "cells": sum(m.cells for m in models),
             "value": round(cells / (tg / 1e3) / 1e9, 3), "unit": "Gcell/s",
             "model_loop_gcells": round(cells / (loop_ms / 1e3) / 1e9, 3),
             "speedup_vs_model_loop": round(loop_ms / tg, 3),
-            "seg_rows": {str(r): tiles.count(r) for r in sorted(set(tiles))}}
+            "seg_rows": {str(r): tiles.count(r) for r in sorted(set(tiles))},
+            "roofline": {"achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}}
 
 
 def adjoint_rate(mfdm, device: int, nsteps: int = 4000, every: int = 50):
