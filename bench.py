@@ -727,9 +727,10 @@ def main():
         cpu = {"value": round(rate, 5), "unit": "Gcell/s", "cores": threads, "kind": "port",
                "sample": f"{n} RK4 steps of {args.workload} in {s:.1f} s (FP32 oracle, OpenMP)"}
 
-    # a second, smaller workload for context (configs[1]-sized)
+    # the other workloads, for context, on single-GPU runs only (a multi-GPU run
+    # would hold every GPU while rank 0 alone works through them)
     other = {}
-    if rank == 0 and args.workload == DEFAULT_WORKLOAD:
+    if rank == 0 and world == 1 and args.workload == DEFAULT_WORKLOAD:
         small = modelgen.curvilinear_1200x800(nt=10)
         with mfdm.Solver.from_model(small, device=local) as s2:
             s2.set_shot(0, reset=True)
