@@ -558,7 +558,7 @@ __device__ __forceinline__ void grad_iface(const Coef& C, const Fields& Y, const
 // rows 3..nz_f-2 and solid rows 1..nz_s-4; columns 3..nx-4. Interior cells also
 // write the Q fields of the stage adjoint (kb) for the transposed operator.
 template <int DIR, bool CPML>
-__global__ void __launch_bounds__(128) k_grad_cells(Coef C, SetLayout L, Fields Y, Fields KB,
+__global__ void __launch_bounds__(128, 6) k_grad_cells(Coef C, SetLayout L, Fields Y, Fields KB,
                                                     const float* __restrict__ kb, float* qx,
                                                     float* qz, Grad G) {
   const int ix = blockIdx.x * blockDim.x + threadIdx.x;
@@ -613,13 +613,21 @@ __global__ void __launch_bounds__(128) k_grad_cells(Coef C, SetLayout L, Fields 
   // C11, C33, C55 and 1/rho each reach a different output; C13 reaches sx and sz
   const SolidK o1 = solid_rhs<DIR, false, CPML>(C, A, iz, ix, side, bottom, xade, zade,
                                                 SolidCoefs{xix, xiz, zex, zez, 1.f, 1.f, 0.f, 1.f, 1.f});
-  const SolidK o2 = solid_rhs<DIR, false, CPML>(C, A, iz, ix, side, bottom, xade, zade,
-                                                SolidCoefs{xix, xiz, zex, zez, 0.f, 0.f, 1.f, 0.f, 0.f});
+  double t13;
+  if (!side && !bottom) {
+    // off the PML strips the stress RHS is sx = C11 X + C13 Z, sz = C13 X + C33 Z,
+    // so the unit-C13 outputs (Z, X) are the unit-C11/C33 ones swapped
+    t13 = ksx * o1.sz + ksz * o1.sx;
+  } else {
+    const SolidK o2 = solid_rhs<DIR, false, CPML>(C, A, iz, ix, side, bottom, xade, zade,
+                                                  SolidCoefs{xix, xiz, zex, zez, 0.f, 0.f, 1.f, 0.f, 0.f});
+    t13 = ksx * o2.sx + ksz * o2.sz;
+  }
   G.c11[m] = gc11 + ksx * o1.sx;
   G.c33[m] = gc33 + ksz * o1.sz;
   G.c55[m] = gc55 + ksxz * o1.sxz;
   G.rs[m] = grs + (kvx * o1.vx + kvz * o1.vz);
-  G.c13[m] = gc13 + (ksx * o2.sx + ksz * o2.sz);
+  G.c13[m] = gc13 + t13;
   if (qx) q_solid<CPML>(C, L, kb, qx, qz, nullptr, iz, ix, false);
 }
 
