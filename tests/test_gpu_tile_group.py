@@ -169,3 +169,23 @@ def test_stage_builds_agree(lib, cases, case):
             s.set_blocks_per_sm(5)
         s.set_blocks_per_sm(0)
         assert s.info()["blocks_per_sm"] == 3  # the default build
+
+
+def test_per_kernel_timing_steps_like_step(lib, cases):
+    """mfdm_time_steps with per-kernel events launches the steps one by one
+    (outside the captured graph, in chunks of 256): the same state as
+    mfdm_step, and the five kernel intervals tile each step's interval."""
+    model = cases.curv_small()
+    nt = 300
+    rec0, f0, _ = run(lib, model, nt)
+    with lib.Solver.from_model(model) as s:
+        s.set_shot(0, reset=True)
+        total, kms = s.time_steps(nt, per_kernel=True)
+        assert s.info()["step"] == nt
+        assert total > 0.0 and len(kms) == 5 and all(k > 0.0 for k in kms)
+        assert abs(sum(kms) - total) <= 1e-3 * total + 1e-3
+        rec = s.records()
+        for q in rec0:
+            assert np.array_equal(rec[q], rec0[q]), q
+        for n in lib.FIELDS:
+            assert np.array_equal(s.field(n), f0[n]), n
