@@ -594,8 +594,10 @@ def main():
     ap.add_argument("--seg-rows", type=int, default=0,
                     help="rows per segment block of the stage launches (0: the default for the grid)")
     ap.add_argument("--adjoint-profile", action="store_true",
-                    help="only a short adjoint run on the 800x400 model (16 steps, checkpoint "
+                    help="only a short adjoint run on a curvilinear model (16 steps, checkpoint "
                          "every 8, seeded residuals): a launch list of the adjoint kernels for ncu")
+    ap.add_argument("--adjoint-grid", type=int, nargs=2, default=[800, 400], metavar=("NX", "NZ"),
+                    help="grid of --adjoint-profile (default 800 400)")
     ap.add_argument("--large-adjoint", type=int, nargs=5, default=None,
                     metavar=("SHOTS", "STEPS", "EVERY", "INNER", "PROBE"),
                     help="only the 8192x4096 rough-seafloor adjoint: SHOTS shots of STEPS steps, "
@@ -630,7 +632,7 @@ def main():
     if args.adjoint_profile:
         mfdm = importlib.import_module("marineseis-fdm-2d_b200")
         mfdm.load_library()
-        m = modelgen.curvilinear(800, 400, nt=16)
+        m = modelgen.curvilinear(args.adjoint_grid[0], args.adjoint_grid[1], nt=16)
         with mfdm.Solver.from_model(m) as s:
             s.set_shot(0, reset=True)
             rec = s.adjoint_forward(16, 8)

@@ -2,7 +2,6 @@
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
-#include <climits>
 
 #include "mfdm_adjoint.h"
 
@@ -688,85 +687,173 @@ __device__ __forceinline__ void grad_iface(const Coef& C, const Fields& Y, const
   G.c13[si] += coupled(0.f, 0.f, 0.f, 0.f, 0.f, o2.sx, o2.sz, 0.f);
 }
 
-// Transposed interior stencil at input cell (a, r, c): D_F^T g (j) = sum_t a_t g(j - t),
-// D_B^T g (j) = -sum_t a_t g(j + t), taps t = -1..3 of the DRP pair.
-template <int DIR>
-__device__ __forceinline__ float t_stencil(const SetLayout& L, const float* __restrict__ qx,
-                                           const float* __restrict__ qz, int a, int r, int c) {
+// Transposed interior stencil at element j of a main array (row r of `rows`,
+// column c of nx, pitch P), addressed relative to j: D_F^T g (j) =
+// sum_t a_t g(j - t), D_B^T g (j) = -sum_t a_t g(j + t), taps t = -1..3 of
+// the DRP pair, along x in qx and along z in qz. CHECK: taps may leave the array.
+template <int DIR, bool CHECK>
+__device__ __forceinline__ float t_stencil(const float* __restrict__ qx, const float* __restrict__ qz,
+                                           long long j, int r, int c, int P, int rows, int nx) {
   const float at[5] = {kAm1, kA0, kA1, kA2, kA3};
-  const long long base = L.off[a];
-  const int P = L.pitch[a], rows = L.rows[a], ncols = L.ncols[a];
   float s = 0.0f;
 #pragma unroll
   for (int t = -1; t <= 3; ++t) {
-    const int cc = DIR == kDirF ? c - t : c + t, rr = DIR == kDirF ? r - t : r + t;
-    if (cc >= 0 && cc < ncols) s = fmaf(at[t + 1], __ldg(qx + base + (long long)r * P + cc), s);
-    if (rr >= 0 && rr < rows) s = fmaf(at[t + 1], __ldg(qz + base + (long long)rr * P + c), s);
+    const int d = DIR == kDirF ? -t : t;
+    if (!CHECK || (c + d >= 0 && c + d < nx)) s = fmaf(at[t + 1], __ldg(qx + j + d), s);
+    if (!CHECK || (r + d >= 0 && r + d < rows))
+      s = fmaf(at[t + 1], __ldg(qz + j + (long long)d * P), s);
   }
   return DIR == kDirF ? s : -s;
 }
 
 constexpr int kRevBlock = 128;
+constexpr int kRevVec = 4;  // consecutive elements per thread
 
-// One thread per row of L^T: the sparse rest plus, on main-field cells, the
-// transposed interior stencil; then the RK bookkeeping of the reverse stage.
+// The RK bookkeeping of one element of a reverse stage (see k_reverse_h).
+template <int MODE>
+__device__ __forceinline__ void rev_finish(float y, float lam0, float mu0, bool mk, float w,
+                                           float cw, bool has_kbn, float& lam, float& mu_out,
+                                           float& kbn_out) {
+  if (MODE == 0) {
+    lam = y;
+    return;
+  }
+  const float m = mk ? 1.0f : 0.0f;
+  if (MODE == 1) {
+    lam = lam0 + y;
+    if (has_kbn) {
+      mu_out = lam;
+      kbn_out = mk ? w * lam : 0.0f;
+    }
+    return;
+  }
+  lam = lam0 + m * y;
+  if (MODE == 2 || MODE == 4) kbn_out = m * fmaf(cw, y, w * mu0);
+}
+
+// One element, scalar loads (edges, padding and the rest of the set).
+// stencil: a main-array element at row r of `rows`, column c < nx.
+template <int DIR, int MODE>
+__device__ __forceinline__ void rev_one(const float* __restrict__ t, const float* __restrict__ qx,
+                                        const float* __restrict__ qz, long long j, bool stencil,
+                                        int r, int c, int P, int rows, int nx, float* y_or_lam,
+                                        const uint8_t* __restrict__ mask, float* kbn, float* mu,
+                                        float w, float cw) {
+  float y = t[j];
+  // the RK operands first: their loads must not wait for a store
+  const float mu0 = (MODE == 2 || MODE == 4) ? mu[j] : 0.f;
+  const float lam0 = MODE == 0 ? 0.f : (MODE == 4 ? mu0 : y_or_lam[j]);
+  const bool mk = MODE == 0 ? false : mask[j] != 0;
+  if (stencil) {
+    if (c >= 3 && c <= nx - 4 && r >= 3 && r <= rows - 4)
+      y += t_stencil<DIR, false>(qx, qz, j, r, c, P, rows, nx);
+    else
+      y += t_stencil<DIR, true>(qx, qz, j, r, c, P, rows, nx);
+  }
+  float lam = 0.f, mo = 0.f, ko = 0.f;
+  rev_finish<MODE>(y, lam0, mu0, mk, w, cw, kbn != nullptr, lam, mo, ko);
+  y_or_lam[j] = lam;
+  if (MODE == 1 && kbn) {
+    mu[j] = mo;
+    kbn[j] = ko;
+  }
+  if (MODE == 2 || MODE == 4) kbn[j] = ko;
+}
+
+__device__ __forceinline__ float f4(const float4& v, int k) {
+  return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
+}
+
+// One thread per kRevVec consecutive rows of L^T (j0 a multiple of kRevVec):
+// the sparse rest plus, on main-field cells, the transposed interior stencil;
+// then the RK bookkeeping of the reverse stage.
 // MODE 0: y only; 1: lam += y and, with kbn, the start of the next transposed
 // step: mu = lam, kbn = w M lam; 2: lam += M y, kbn = M (w mu + c y); 3: lam += M y;
 // 4: MODE 2 with lam taken from mu (the step's first stage: the step start
 // wrote the filtered interface cells to mu only, and mu = lam elsewhere).
 // `t` holds the CSR part of every row (k_rows_csr; rows without entries keep 0).
-// Grid: x over the pitch of the main arrays; y over the 3 nz_f fluid rows and
-// the 5 nz_s solid rows (one row of one array each), then over the rest of the
-// set from `tail0` in runs of gridDim.x * kRevBlock elements (strips, bands,
-// padding), striding by gridDim.y.
+// Grid: x over the pitch P of the main arrays (kRevVec columns a thread);
+// z < 8: main array z (the fluid block [3][nz_f][P] at 0, the solid block
+// [5][nz_s][P] at off[3]), y its row; z = 8: the rest of the set from `tail0`
+// in runs of gridDim.x * kRevBlock * kRevVec elements (strips, bands,
+// padding), striding by gridDim.y. Four columns whose stencils stay inside the
+// array take 16-byte loads and stores (every row starts 16-byte aligned: P
+// and the array offsets are multiples of 32 floats), with the taps of each
+// column summed in the same order as the scalar path.
 template <int DIR, int MODE>
 __global__ void __launch_bounds__(kRevBlock) k_reverse_h(
     const float* __restrict__ t, const float* __restrict__ qx, const float* __restrict__ qz,
-    SetLayout L, long long tail0, int nyrows, float* y_or_lam, const uint8_t* __restrict__ mask,
-    float* kbn, float* mu, float w, float cw) {
-  const int nfr = 3 * L.nzf, nmain = nfr + 5 * L.nzs;
-  for (int yr = blockIdx.y; yr < nyrows; yr += gridDim.y) {
-    long long j;
-    int a = -1, r = 0, c = 0;
-    if (yr < nmain) {
-      c = blockIdx.x * kRevBlock + threadIdx.x;
-      if (c >= L.pitch[0]) continue;
-      if (yr < nfr) {
-        a = yr / L.nzf;
-        r = yr - a * L.nzf;
-      } else {
-        const int u = yr - nfr;
-        a = 3 + u / L.nzs;
-        r = u - (a - 3) * L.nzs;
+    SetLayout L, long long tail0, float* y_or_lam, const uint8_t* __restrict__ mask, float* kbn,
+    float* mu, float w, float cw) {
+  const int a = blockIdx.z;
+  const int P = L.pitch[0], nx = L.nx;
+  if (a < 8) {
+    const bool fluid = a < 3;
+    const int rows = fluid ? L.nzf : L.nzs;
+    const int r = blockIdx.y, c0 = (blockIdx.x * kRevBlock + threadIdx.x) * kRevVec;
+    if (r >= rows || c0 >= P) return;
+    const long long j0 = fluid ? (long long)(a * L.nzf + r) * P + c0
+                               : L.off[3] + (long long)((a - 3) * L.nzs + r) * P + c0;
+    if (c0 >= 4 && c0 + kRevVec - 1 <= nx - 4 && r >= 3 && r <= rows - 4) {
+      const float4 tv = *reinterpret_cast<const float4*>(t + j0);
+      float4 lv = make_float4(0.f, 0.f, 0.f, 0.f), mv = lv;
+      uchar4 kv = make_uchar4(0, 0, 0, 0);
+      if (MODE == 2 || MODE == 4) mv = *reinterpret_cast<const float4*>(mu + j0);
+      if (MODE == 1 || MODE == 2 || MODE == 3) lv = *reinterpret_cast<const float4*>(y_or_lam + j0);
+      if (MODE == 4) lv = mv;
+      if (MODE != 0) kv = *reinterpret_cast<const uchar4*>(mask + j0);
+      // qx along the row: elements j0 - 4 .. j0 + 7 cover the taps of all four columns
+      const float4 xa = __ldg(reinterpret_cast<const float4*>(qx + j0 - 4));
+      const float4 xb = __ldg(reinterpret_cast<const float4*>(qx + j0));
+      const float4 xc = __ldg(reinterpret_cast<const float4*>(qx + j0 + 4));
+      float4 zr[5];
+#pragma unroll
+      for (int t5 = -1; t5 <= 3; ++t5) {
+        const int d = DIR == kDirF ? -t5 : t5;
+        zr[t5 + 1] = __ldg(reinterpret_cast<const float4*>(qz + j0 + (long long)d * P));
       }
-      j = L.off[a] + (long long)r * L.pitch[a] + c;
-    } else {
-      j = tail0 + (long long)(yr - nmain) * (gridDim.x * kRevBlock) + blockIdx.x * kRevBlock +
-          threadIdx.x;
-      if (j >= L.len) continue;
-    }
-    float y = t[j];
-    // the RK operands first: their loads must not wait for a store
-    const float mu0 = (MODE == 2 || MODE == 4) ? mu[j] : 0.f;
-    const float lam0 = MODE == 0 ? 0.f : (MODE == 4 ? mu0 : y_or_lam[j]);
-    const bool mk = MODE == 0 ? false : mask[j] != 0;
-    if (a >= 0 && c < L.nx) y += t_stencil<DIR>(L, qx, qz, a, r, c);
-    if (MODE == 0) {
-      y_or_lam[j] = y;
-      continue;
-    }
-    const float m = mk ? 1.0f : 0.0f;
-    if (MODE == 1) {
-      const float l = lam0 + y;
-      y_or_lam[j] = l;
-      if (kbn) {
-        mu[j] = l;
-        kbn[j] = mk ? w * l : 0.0f;
+      const float at[5] = {kAm1, kA0, kA1, kA2, kA3};
+      float yo[4], lo[4], mo[4], ko[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        float sum = 0.0f;
+#pragma unroll
+        for (int t5 = -1; t5 <= 3; ++t5) {
+          const int d = DIR == kDirF ? -t5 : t5;
+          const int q = k + d + 4;  // index in xa|xb|xc
+          const float xv = q < 4 ? f4(xa, q) : (q < 8 ? f4(xb, q - 4) : f4(xc, q - 8));
+          sum = fmaf(at[t5 + 1], xv, sum);
+          sum = fmaf(at[t5 + 1], f4(zr[t5 + 1], k), sum);
+        }
+        yo[k] = f4(tv, k) + (DIR == kDirF ? sum : -sum);
+        const unsigned char mb = k == 0 ? kv.x : (k == 1 ? kv.y : (k == 2 ? kv.z : kv.w));
+        mo[k] = 0.f;
+        ko[k] = 0.f;
+        rev_finish<MODE>(yo[k], f4(lv, k), f4(mv, k), mb != 0, w, cw, kbn != nullptr, lo[k],
+                         mo[k], ko[k]);
       }
-      continue;
+      *reinterpret_cast<float4*>(y_or_lam + j0) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+      if (MODE == 1 && kbn) {
+        *reinterpret_cast<float4*>(mu + j0) = make_float4(mo[0], mo[1], mo[2], mo[3]);
+        *reinterpret_cast<float4*>(kbn + j0) = make_float4(ko[0], ko[1], ko[2], ko[3]);
+      }
+      if (MODE == 2 || MODE == 4)
+        *reinterpret_cast<float4*>(kbn + j0) = make_float4(ko[0], ko[1], ko[2], ko[3]);
+      return;
     }
-    y_or_lam[j] = lam0 + m * y;
-    if (MODE == 2 || MODE == 4) kbn[j] = m * fmaf(cw, y, w * mu0);
+#pragma unroll 1
+    for (int k = 0; k < kRevVec && c0 + k < P; ++k)
+      rev_one<DIR, MODE>(t, qx, qz, j0 + k, c0 + k < nx, r, c0 + k, P, rows, nx, y_or_lam, mask,
+                         kbn, mu, w, cw);
+    return;
+  }
+  const long long run = (long long)gridDim.x * kRevBlock * kRevVec;
+  for (long long j = tail0 + (long long)blockIdx.y * run +
+                     (long long)(blockIdx.x * kRevBlock + threadIdx.x) * kRevVec;
+       j < L.len; j += (long long)gridDim.y * run) {
+#pragma unroll 1
+    for (int k = 0; k < kRevVec && j + k < L.len; ++k)
+      rev_one<DIR, MODE>(t, qx, qz, j + k, false, 0, 0, P, 0, nx, y_or_lam, mask, kbn, mu, w, cw);
   }
 }
 
@@ -926,14 +1013,17 @@ static cudaError_t hybrid_t(const HybridT& H, const Coef& C, const SetLayout& L,
   // the main arrays are the fluid block [3][nz_f][P] at 0 and the solid block
   // [5][nz_s][P] at off[3]; the rest of the set follows the solid block
   const long long tail0 = L.off[3] + 5LL * L.nzs * L.pitch[3];
-  const int gx = (L.pitch[0] + kRevBlock - 1) / kRevBlock;
-  const long long run = (long long)gx * kRevBlock;
-  const long long ny = 3LL * L.nzf + 5LL * L.nzs + (L.len - tail0 + run - 1) / run;
-  if (L.off[0] != 0 || L.off[3] < 3LL * L.nzf * L.pitch[0] || tail0 > L.len || ny > INT_MAX)
-    return cudaErrorInvalidValue;
-  const unsigned gy = unsigned(ny < 65535 ? ny : 65535);
-  k_reverse_h<DIR, MODE><<<dim3(unsigned(gx), gy), kRevBlock, 0, st>>>(
-      H.t, H.qx, H.qz, L, tail0, int(ny), out, mask, kbn, mu, w, c);
+  const int gx = (L.pitch[0] + kRevBlock * kRevVec - 1) / (kRevBlock * kRevVec);
+  const int gy = std::max(L.nzf, L.nzs);
+  bool ok = L.off[0] == 0 && L.off[3] >= 3LL * L.nzf * L.pitch[0] && tail0 <= L.len && gy <= 65535 &&
+            L.pitch[0] % 32 == 0 && L.off[3] % 32 == 0 && tail0 % kRevVec == 0;
+  for (int a = 0; a < 8; ++a)
+    ok = ok && L.pitch[a] == L.pitch[0] &&
+         L.off[a] == (a < 3 ? (long long)a * L.nzf * L.pitch[0]
+                            : L.off[3] + (long long)(a - 3) * L.nzs * L.pitch[0]);
+  if (!ok) return cudaErrorInvalidValue;
+  k_reverse_h<DIR, MODE><<<dim3(unsigned(gx), unsigned(gy), 9u), kRevBlock, 0, st>>>(
+      H.t, H.qx, H.qz, L, tail0, out, mask, kbn, mu, w, c);
   return cudaGetLastError();
 }
 
