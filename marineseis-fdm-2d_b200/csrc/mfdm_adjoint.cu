@@ -543,6 +543,33 @@ __global__ void k_qfields(Coef C, SetLayout L, const float* __restrict__ x, floa
   else q_solid<CPML>(C, L, x, qx, qz, t, row - L.nzf, c, ZERO);
 }
 
+// The Q fields of x (the grid rows below nz_f + nz_s, as k_qfields without
+// zeroing) and, in the grid rows after them, the probed sparse rows of L^T x
+// into t (kLanes threads a row), in one launch: both only read x, and they
+// write disjoint rows of t (the ADE rows of structured cells, the rows with
+// entries).
+template <bool CPML>
+__global__ void k_prepare(Coef C, SetLayout L, const float* __restrict__ x, float* qx, float* qz,
+                          float* t, const int* __restrict__ nzrow,
+                          const long long* __restrict__ rowptr, const int* __restrict__ col,
+                          const float* __restrict__ val, long long nrows) {
+  const int row = blockIdx.y, nq = L.nzf + L.nzs;
+  if (row < nq) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= L.nx) return;
+    if (row < L.nzf) q_fluid<CPML>(C, L, x, qx, qz, t, row, c, false);
+    else q_solid<CPML>(C, L, x, qx, qz, t, row - L.nzf, c, false);
+    return;
+  }
+  const long long g = ((long long)(row - nq) * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x;
+  const long long r = g / kLanes;
+  const int lane = threadIdx.x % kLanes;
+  if (r >= nrows) return;  // whole groups leave together
+  const int j = nzrow[r];
+  const float sum = row_dot(rowptr, col, val, x, j, lane);
+  if (lane == 0) t[j] = sum;
+}
+
 // ---- material gradients ----------------------------------------------------------
 
 struct Grad {
@@ -1004,7 +1031,7 @@ static cudaError_t hybrid_t(const HybridT& H, const Coef& C, const SetLayout& L,
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
-  if (H.nrows > 0 && !q_ready) {  // else formed by sparse_rows()
+  if (H.nrows > 0 && !q_ready) {  // else formed by prepare()
     k_rows_csr<<<unsigned((H.nrows * kLanes + kBlock - 1) / kBlock), kBlock, 0, st>>>(
         H.nzrow, H.rest.rowptr, H.rest.col, H.rest.val, kb, H.nrows, H.t);
     const cudaError_t e = cudaGetLastError();
@@ -1035,19 +1062,20 @@ static cudaError_t hybrid_dir(const HybridT& H, const Coef& C, const SetLayout& 
                       : hybrid_t<kDirB, MODE>(H, C, L, kb, out, mask, kbn, mu, w, c, q_ready, st);
 }
 
-cudaError_t q_fields(const HybridT& H, const Coef& C, const SetLayout& L, const float* kb,
-                     cudaStream_t st) {
-  // off the interior cells the Q buffers hold the zeros written when allocated
-  const dim3 gq(unsigned((L.nx + 127) / 128), unsigned(L.nzf + L.nzs));
-  if (L.cpml) k_qfields<true, false><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz, H.t);
-  else k_qfields<false, false><<<gq, 128, 0, st>>>(C, L, kb, H.qx, H.qz, H.t);
-  return cudaGetLastError();
-}
-
-cudaError_t sparse_rows(const HybridT& H, const float* kb, cudaStream_t st) {
-  if (H.nrows <= 0) return cudaSuccess;
-  k_rows_csr<<<unsigned((H.nrows * kLanes + kBlock - 1) / kBlock), kBlock, 0, st>>>(
-      H.nzrow, H.rest.rowptr, H.rest.col, H.rest.val, kb, H.nrows, H.t);
+cudaError_t prepare(const HybridT& H, const Coef& C, const SetLayout& L, const float* kb,
+                    cudaStream_t st) {
+  const unsigned gx = unsigned((L.nx + 127) / 128);
+  const long long per_row = (long long)gx * 128;
+  const long long ycsr = H.nrows > 0 ? (H.nrows * kLanes + per_row - 1) / per_row : 0;
+  const long long gy = L.nzf + L.nzs + ycsr;
+  if (gy > 65535) return cudaErrorInvalidValue;
+  const dim3 grid(gx, unsigned(gy));
+  if (L.cpml)
+    k_prepare<true><<<grid, 128, 0, st>>>(C, L, kb, H.qx, H.qz, H.t, H.nzrow, H.rest.rowptr,
+                                          H.rest.col, H.rest.val, H.nrows);
+  else
+    k_prepare<false><<<grid, 128, 0, st>>>(C, L, kb, H.qx, H.qz, H.t, H.nzrow, H.rest.rowptr,
+                                           H.rest.col, H.rest.val, H.nrows);
   return cudaGetLastError();
 }
 

@@ -97,17 +97,15 @@ cudaError_t sort_rows(const CsrT& A, long long len, cudaStream_t st);
 cudaError_t drop_interior(const CsrT& full, const SetLayout& L, CsrT* rest,
                           unsigned long long* count, void** tmp, size_t* tmp_bytes, cudaStream_t st);
 
-// The sparse rows of L^T kb into H.t (the rows listed in H.nzrow), so that a
-// stream other than the gradient's can form them concurrently.
-cudaError_t sparse_rows(const HybridT& H, const float* kb, cudaStream_t st);
-// The Q fields of kb into H.qx / H.qz (0 off the interior cells).
-cudaError_t q_fields(const HybridT& H, const Coef& C, const SetLayout& L, const float* kb,
-                     cudaStream_t st);
+// The Q fields of kb into H.qx / H.qz (the interior and strip cells; 0 off
+// them) and its sparse rows of L^T kb into H.t (the rows listed in H.nzrow),
+// in one launch.
+cudaError_t prepare(const HybridT& H, const Coef& C, const SetLayout& L, const float* kb,
+                    cudaStream_t st);
 // One reverse stage: y = L^T kb, lam += (mask_lam ? M : 1) y and, when kbn is
 // given, kbn = M (w mu + c y); without mask_lam (the step's last stage) and
 // with kbn, it also starts the next transposed step: mu = lam, kbn = w M lam.
-// q_ready: the Q fields of kb (q_fields()) and its sparse rows (sparse_rows())
-// are already in H. lam_from_mu (with mask_lam and kbn: the step's first
+// q_ready: the Q fields of kb and its sparse rows (prepare()) are already in H. lam_from_mu (with mask_lam and kbn: the step's first
 // stage) reads lam from mu, which holds the step start's filtered lam.
 cudaError_t reverse_stage(const HybridT& H, const Coef& C, const SetLayout& L, int dir,
                           const float* kb, float* lam, const uint8_t* mask, bool mask_lam,

@@ -206,12 +206,11 @@ struct AdjointState {
   void* scan_tmp = nullptr;
   size_t scan_bytes = 0;
   bool built = false;
-  // Streams of the backward steps: `hi` runs the transposed chain and `side`
-  // each stage's sparse rows of L^T kb, both at the highest priority; `side_g`
-  // the material-gradient accumulation (which nothing in the chain waits for)
-  // at the lowest, so its blocks take only the SMs the chain leaves idle.
-  cudaStream_t hi = nullptr, side = nullptr, side_g = nullptr;
-  cudaEvent_t ev_kb = nullptr, ev_rows = nullptr, ev_g[2] = {nullptr, nullptr};
+  // Streams of the backward steps: `hi` runs the transposed chain at the
+  // highest priority, `side_g` the material-gradient accumulation at the
+  // lowest, so its blocks take only the SMs the chain leaves idle.
+  cudaStream_t hi = nullptr, side_g = nullptr;
+  cudaEvent_t ev_kb = nullptr, ev_g[2] = {nullptr, nullptr};
   cudaEvent_t ev_enter = nullptr, ev_leave = nullptr;
   cudaEvent_t ev_seg[2] = {nullptr, nullptr};  // segment recomputed into seg / seg2
   cudaEvent_t ev_rev[2] = {nullptr, nullptr};  // last reverse reading seg / seg2 done
@@ -232,7 +231,6 @@ struct AdjointState {
     cudaFree(inner);
     cudaFree(scan_tmp);
     if (ev_kb) cudaEventDestroy(ev_kb);
-    if (ev_rows) cudaEventDestroy(ev_rows);
     if (ev_enter) cudaEventDestroy(ev_enter);
     if (ev_leave) cudaEventDestroy(ev_leave);
     for (cudaEvent_t e : ev_seg)
@@ -243,7 +241,6 @@ struct AdjointState {
     if (hi) cudaStreamDestroy(hi);
     for (cudaEvent_t e : ev_g)
       if (e) cudaEventDestroy(e);
-    if (side) cudaStreamDestroy(side);
     if (side_g) cudaStreamDestroy(side_g);
   }
 };
@@ -1604,14 +1601,12 @@ int adjoint_prepare(mfdm_model* m) {
     int least = 0, greatest = 0;
     MFDM_CU(cudaDeviceGetStreamPriorityRange(&least, &greatest));
     MFDM_CU(cudaStreamCreateWithPriority(&a->hi, cudaStreamNonBlocking, greatest));
-    MFDM_CU(cudaStreamCreateWithPriority(&a->side, cudaStreamNonBlocking, greatest));
     MFDM_CU(cudaStreamCreateWithPriority(&a->side_g, cudaStreamNonBlocking, least));
     MFDM_CU(cudaEventCreateWithFlags(&a->ev_enter, cudaEventDisableTiming));
     MFDM_CU(cudaEventCreateWithFlags(&a->ev_leave, cudaEventDisableTiming));
     for (cudaEvent_t& e : a->ev_seg) MFDM_CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (cudaEvent_t& e : a->ev_rev) MFDM_CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     MFDM_CU(cudaEventCreateWithFlags(&a->ev_kb, cudaEventDisableTiming));
-    MFDM_CU(cudaEventCreateWithFlags(&a->ev_rows, cudaEventDisableTiming));
     for (cudaEvent_t& e : a->ev_g) MFDM_CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
   if (!m->adj->built) return adjoint_build(m);
@@ -1725,21 +1720,17 @@ int reverse_step(mfdm_model* m, int n, float* slot) {
   // residuals of step n enter when n is a receiver sample
   const float* res = (n % m->gap == 0) ? a->res + size_t(n / m->gap) * 3 * size_t(m->cfg.nx) : nullptr;
   MFDM_CU(mfdm::adj::step_start(a->lam, L, C, res, a->mu, a->kb[0], a->mask, c[3], st));
-  // Each stage: once kb[kin] is complete, its sparse rows of L^T kb (side
-  // stream) and its material-gradient accumulation (side_g) run beside the Q
-  // fields and the transposed product on the main stream. The product writes
-  // kb[1 - kin], which the previous stage's gradient reads: it waits for that
-  // gradient (ev_g[1 - kin]; a never-recorded event is no wait).
+  // Each stage: once kb[kin] is complete, its Q fields and sparse rows of L^T
+  // kb (one launch) and the transposed product run on the main stream, and its
+  // material-gradient accumulation on side_g. The product writes kb[1 - kin],
+  // which the previous stage's gradient reads: it waits for that gradient
+  // (ev_g[1 - kin]; a never-recorded event is no wait).
   auto stage = [&](int d, int sy, int kin, bool mask_lam, float ws, float cs, bool first) -> int {
     MFDM_CU(cudaEventRecord(a->ev_kb, st));
-    MFDM_CU(cudaStreamWaitEvent(a->side, a->ev_kb, 0));
-    MFDM_CU(mfdm::adj::sparse_rows(a->H[d], a->kb[kin], a->side));
-    MFDM_CU(cudaEventRecord(a->ev_rows, a->side));
-    MFDM_CU(mfdm::adj::q_fields(a->H[d], C, L, a->kb[kin], st));
+    MFDM_CU(mfdm::adj::prepare(a->H[d], C, L, a->kb[kin], st));
     MFDM_CU(cudaStreamWaitEvent(a->side_g, a->ev_kb, 0));
     MFDM_CU(mfdm::adj::gradient(C, L, Y[sy], a->kb[kin], g, d, nullptr, a->side_g));
     MFDM_CU(cudaEventRecord(a->ev_g[kin], a->side_g));
-    MFDM_CU(cudaStreamWaitEvent(st, a->ev_rows, 0));
     MFDM_CU(cudaStreamWaitEvent(st, a->ev_g[1 - kin], 0));
     MFDM_CU(mfdm::adj::reverse_stage(a->H[d], C, L, d, a->kb[kin], a->lam, a->mask, mask_lam,
                                      a->kb[1 - kin], a->mu, ws, cs, true, first, st));
