@@ -393,7 +393,7 @@ def uneven_rate(mfdm, device: int, nmodels: int = 32, steps: int = 128):
             "roofline": {"achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}}
 
 
-def adjoint_rate(mfdm, device: int, nsteps: int = 4000, every: int = 50):
+def adjoint_rate(mfdm, device: int, nsteps: int = 4000, every: int = 50, repeats: int = 3):
     """Cost of the adjoint-state gradient against a plain forward run on the
     800x400 curvilinear model pair (4000 RK4 steps, checkpoint every 50): host
     wall time of the synchronous calls. The observed records come from the true
@@ -401,7 +401,9 @@ def adjoint_rate(mfdm, device: int, nsteps: int = 4000, every: int = 50):
     of the smoothed initial model's records against them. The adjoint's
     forward pass (with checkpoints) plus its backward pass is compared with
     mfdm_step over the same steps; the one-time operator assembly is listed
-    separately."""
+    separately. Each pass runs `repeats` times and the median is reported,
+    with every run listed (the backward enqueues ~40 host calls a step, so a
+    busy host can slow a single run)."""
     true, m = modelgen.adjoint_pair(800, 400, nt=nsteps)
     with mfdm.Solver.from_model(true, device=device) as st:
         st.set_shot(0, reset=True)
@@ -410,33 +412,40 @@ def adjoint_rate(mfdm, device: int, nsteps: int = 4000, every: int = 50):
     with mfdm.Solver.from_model(m, device=device) as s:
         s.set_shot(0, reset=True)
         s.step(64)
-        s.set_shot(0, reset=True)
-        t0 = time.perf_counter()
-        s.step(nsteps)
-        fwd = time.perf_counter() - t0
+        fwds, afwds, bwds = [], [], []
+        for _ in range(repeats):
+            s.set_shot(0, reset=True)
+            t0 = time.perf_counter()
+            s.step(nsteps)
+            fwds.append(time.perf_counter() - t0)
         t0 = time.perf_counter()
         s.adjoint_forward(nsteps, every)  # first call also assembles the operators
         first = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        rec = s.adjoint_forward(nsteps, every)
-        afwd = time.perf_counter() - t0
-        res = {k: (rec[k] - obs[k]).astype(np.float32) for k in rec}
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            rec = s.adjoint_forward(nsteps, every)
+            afwds.append(time.perf_counter() - t0)
+            res = {k: (rec[k] - obs[k]).astype(np.float32) for k in rec}
+            t0 = time.perf_counter()
+            grad = s.adjoint_backward(res)
+            bwds.append(time.perf_counter() - t0)
         misfit = 0.5 * sum(float(np.sum(np.float64(r) ** 2)) for r in res.values())
-        t0 = time.perf_counter()
-        grad = s.adjoint_backward(res)
-        bwd = time.perf_counter() - t0
+        fwd, afwd, bwd = (statistics.median(v) for v in (fwds, afwds, bwds))
         # the same with every segment's stage inputs kept in device memory
         # (no recompute; 4 * 4000 states of this model, about 85 GB of HBM)
         s.adjoint_memory(150 * 10 ** 9)
         t0 = time.perf_counter()
         s.adjoint_forward(nsteps, every)  # first: allocates the keep buffer, encodes its maps
         kfirst = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        s.adjoint_forward(nsteps, every)
-        kfwd = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        s.adjoint_backward(res)
-        kbwd = time.perf_counter() - t0
+        kfwds, kbwds = [], []
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            s.adjoint_forward(nsteps, every)
+            kfwds.append(time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            s.adjoint_backward(res)
+            kbwds.append(time.perf_counter() - t0)
+        kfwd, kbwd = statistics.median(kfwds), statistics.median(kbwds)
         s.adjoint_memory(0)
     # where the vs anomaly sits: the solid C55 gradient should be largest near it
     g55 = np.abs(grad["C55"])
@@ -447,6 +456,10 @@ def adjoint_rate(mfdm, device: int, nsteps: int = 4000, every: int = 50):
             "forward_s": round(fwd, 4), "adjoint_forward_s": round(afwd, 4),
             "backward_s": round(bwd, 4), "assembly_s": round(first - afwd, 4),
             "adjoint_over_forward": round((afwd + bwd) / fwd, 3),
+            "runs": {"forward_s": [round(v, 4) for v in fwds],
+                     "adjoint_forward_s": [round(v, 4) for v in afwds],
+                     "backward_s": [round(v, 4) for v in bwds],
+                     "kept_backward_s": [round(v, 4) for v in kbwds], "statistic": "median"},
             "kept_segments": {"adjoint_forward_s": round(kfwd, 4), "backward_s": round(kbwd, 4),
                               "keep_setup_s": round(kfirst - kfwd, 4),
                               "adjoint_over_forward": round((kfwd + kbwd) / fwd, 3)}}
