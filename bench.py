@@ -22,8 +22,8 @@ weak scaling, no data-path collective.
 other_workloads.reference_cuda_build: the reference's own CUDA build
          (oracle/_ref/main_debug, compiled from its sources) and this library's
          drop-in CLI on the same JSON models, per-step time from the difference
-         of median wall times of a short and a long run (start-up, model
-         loading and file output cancel), snapshots off.
+         of the fastest wall times of a short and a long run (start-up and
+         model loading cancel), snapshots off.
 fp64_error: relative L2 distance of every result to the FP64 oracle over a
          bounded number of steps (the largest over the state fields).
 """
