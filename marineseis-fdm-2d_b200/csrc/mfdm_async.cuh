@@ -37,12 +37,16 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
+// Suspend-time hint of mbarrier.try_wait in ns; 0 (the default) leaves the
+// suspension to the hardware's own time limit. Measured on the stage kernels:
+// no hint runs 0.7-1.9 % faster than a 20 us hint (1 us and 1 ms: as 20 us).
 #ifndef MFDM_WAIT_HINT_NS
-#define MFDM_WAIT_HINT_NS 20000  // suspend hint of mbarrier.try_wait (0: none)
+#define MFDM_WAIT_HINT_NS 0
 #endif
 
-// try_wait suspends the thread in hardware until the phase completes or the
-// hint (ns) elapses, instead of spinning on issue slots.
+// try_wait suspends the thread in hardware until the phase completes or a
+// time limit (the hint, or the hardware's) elapses, instead of spinning on
+// issue slots.
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   uint32_t ok;
 #if MFDM_WAIT_HINT_NS > 0
