@@ -234,3 +234,18 @@ def test_full_size_against_oracle(lib, oracle, modelgen):
         assert rel_l2(fields[n], ref["fluid"][q]) <= TOL, n
     for q, n in enumerate(("solid_vx", "solid_vz", "solid_sx", "solid_sz", "solid_sxz")):
         assert rel_l2(fields[n], ref["solid"][q]) <= TOL, n
+
+
+def test_largest_size_against_oracle(lib, oracle, modelgen):
+    """The 8192 x 4096 rough-seafloor model of the batched adjoint (33.6 M cells,
+    von Karman seafloor, flat side pads), first 20 steps of shot 0, every field
+    against the FP32 oracle: the index arithmetic and launch shapes at the
+    largest configured size."""
+    model = modelgen.rough_seafloor(8192, 4096, nt=20)
+    rec, fields, info = run_solver(lib, model, 20)
+    assert info["cells"] == model.cells
+    ref = oracle.forward(model, 20, oracle.record_gap(model.dt), 32, final_fields=True)
+    for q, n in enumerate(("fluid_vx", "fluid_vz", "fluid_p")):
+        assert rel_l2(fields[n], ref["fluid"][q]) <= TOL, n
+    for q, n in enumerate(("solid_vx", "solid_vz", "solid_sx", "solid_sz", "solid_sxz")):
+        assert rel_l2(fields[n], ref["solid"][q]) <= TOL, n
