@@ -214,16 +214,17 @@ constexpr int kStartCols = kStartThreads - 6;         // output columns per bloc
 // transposed stage takes its lam from mu, where mu = lam off these cells).
 // Receivers sample the filtered interface rows of columns 3..nx-4 only, so the
 // residuals enter there (elsewhere the record is 0 whatever the state).
-__global__ void __launch_bounds__(kStartThreads) k_step_start(
+// Threads (column t, field f): blockDim = (kStartThreads, 8).
+__global__ void __launch_bounds__(kStartThreads * 8) k_step_start(
     const float* __restrict__ lam, SetLayout L, const float2* __restrict__ nrm, W7 w7,
     const float* __restrict__ res, float* mu, float* kb, const uint8_t* __restrict__ mask, float c) {
   __shared__ float tmp[8][kStartThreads];
-  const int nx = L.nx;
+  const int nx = L.nx, f = threadIdx.y;
   const int ix = blockIdx.x * kStartCols + threadIdx.x;  // = output column j0 - 3 + threadIdx.x
   if (ix >= 3 && ix <= nx - 4) {
     float lv[8];
 #pragma unroll
-    for (int f = 0; f < 8; ++f) lv[f] = lam[iface_index(L, f, ix)];
+    for (int q = 0; q < 8; ++q) lv[q] = lam[iface_index(L, q, ix)];
     if (res) {
       lv[3] += __ldg(res + ix);
       lv[4] += __ldg(res + nx + ix);
@@ -233,32 +234,26 @@ __global__ void __launch_bounds__(kStartThreads) k_step_start(
     float wsum = 0.0f;
     for (int k = klo; k <= khi; ++k) wsum += w7.w[k + 3];
     const float2 n = __ldg(nrm + ix);
+    float e[8], u[8];
 #pragma unroll
-    for (int f = 0; f < 8; ++f) {
-      float e[8], u[8];
+    for (int q = 0; q < 8; ++q) e[q] = q == f ? 1.0f : 0.0f;
+    interface_average(n, e, u);
+    float t = 0.0f;
 #pragma unroll
-      for (int q = 0; q < 8; ++q) e[q] = q == f ? 1.0f : 0.0f;
-      interface_average(n, e, u);
-      float t = 0.0f;
-#pragma unroll
-      for (int q = 0; q < 8; ++q) t = fmaf(lv[q], u[q], t);
-      tmp[f][threadIdx.x] = t / wsum;
-    }
+    for (int q = 0; q < 8; ++q) t = fmaf(lv[q], u[q], t);
+    tmp[f][threadIdx.x] = t / wsum;
   }
   __syncthreads();
   if (threadIdx.x < 3 || threadIdx.x >= kStartThreads - 3 || ix < 3 || ix > nx - 4) return;
+  float s = 0.0f;
 #pragma unroll
-  for (int f = 0; f < 8; ++f) {
-    float s = 0.0f;
-#pragma unroll
-    for (int k = -3; k <= 3; ++k) {
-      const int i = ix - k;
-      if (i >= 3 && i <= nx - 4) s = fmaf(w7.w[k + 3], tmp[f][threadIdx.x - k], s);
-    }
-    const long long q = iface_index(L, f, ix);
-    mu[q] = s;
-    kb[q] = mask[q] ? c * s : 0.0f;
+  for (int k = -3; k <= 3; ++k) {
+    const int i = ix - k;
+    if (i >= 3 && i <= nx - 4) s = fmaf(w7.w[k + 3], tmp[f][threadIdx.x - k], s);
   }
+  const long long q = iface_index(L, f, ix);
+  mu[q] = s;
+  kb[q] = mask[q] ? c * s : 0.0f;
 }
 
 
@@ -1106,7 +1101,7 @@ cudaError_t step_start(const float* lam, const SetLayout& L, const Coef& C, cons
   // the filter taps (src/elements.cu:30-33), as the forward finish kernel uses them
   const W7 w7{{1.1e-13f, 1.678e-06f, 0.03419f, 0.93163f, 0.03419f, 1.678e-06f, 1.1e-13f}};
   const unsigned blocks = unsigned((L.nx - 6 + kStartCols - 1) / kStartCols);
-  k_step_start<<<blocks, kStartThreads, 0, st>>>(lam, L, C.nrm, w7, res, mu, kb, mask, c);
+  k_step_start<<<blocks, dim3(kStartThreads, 8), 0, st>>>(lam, L, C.nrm, w7, res, mu, kb, mask, c);
   return cudaGetLastError();
 }
 
