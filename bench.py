@@ -780,6 +780,14 @@ def main():
              (100, 1100), (200, 5200)),
             ("curvilinear_1200x800", lambda nt: modelgen.curvilinear_1200x800(nt=nt),
              (500, 4500), (1000, 21000))])
+        # the same against this library's device-timed step (CUDA events), which
+        # carries no process start-up jitter
+        dev_ms = {"curvilinear_4096x2048": ms / args.steps,
+                  "curvilinear_1200x800": other["curvilinear_1200x800"]["ms_per_step"]}
+        for name, row in other["reference_cuda_build"].items():
+            if isinstance(row, dict) and name in dev_ms and "reference" in row:
+                row["library_device_ms_per_step"] = round(dev_ms[name], 4)
+                row["speedup_device_timed"] = round(row["reference"]["ms_per_step"] / dev_ms[name], 2)
 
     clocks = clk.summary()
     solver.close()
