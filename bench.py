@@ -465,7 +465,7 @@ def adjoint_rate(mfdm, device: int, nsteps: int = 4000, every: int = 50, repeats
                               "adjoint_over_forward": round((kfwd + kbwd) / fwd, 3)}}
 
 
-def north_star_adjoint_rate(mfdm, device: int, nsteps: int = 400, every: int = 50):
+def adjoint_4096x2048_rate(mfdm, device: int, nsteps: int = 400, every: int = 50):
     """Adjoint cost at the 4096x2048 curvilinear size: `nsteps` RK4 steps,
     checkpoint every `every`, every segment recomputed (one level, the next
     segment recomputed into a second stage-input buffer while the current one
@@ -772,7 +772,7 @@ def main():
             fp64_error(mfdm, m_init, 400, local),
             note="forward state of the initial model; the gradient against the FP64 "
                  "adjoint oracle is checked in tests/test_gpu_adjoint.py (rel-L2 <= 1e-3)")
-        other["adjoint_4096x2048"] = north_star_adjoint_rate(mfdm, local)
+        other["adjoint_4096x2048"] = adjoint_4096x2048_rate(mfdm, local)
         other["solid_only_2048x2048"] = solid_only_rate(mfdm, local)
         other["adjoint_8192x4096_rough_seafloor"] = large_adjoint_rate(mfdm, local)
         other["reference_cuda_build"] = reference_cuda_build([
