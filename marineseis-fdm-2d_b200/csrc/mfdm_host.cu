@@ -1028,6 +1028,12 @@ int mfdm_time_steps(mfdm_model* m, int nsteps, int per_kernel, float* total_ms, 
   for (auto& e : ev) MFDM_CU(cudaEventCreate(&e));
   struct Free { cudaEvent_t* e; ~Free() { for (int i = 0; i < 8; ++i) cudaEventDestroy(e[i]); } } fr{ev};
   if (!per_kernel) {
+    // the time loop's graph is captured and uploaded before the timed region:
+    // a one-time setup (the first mfdm_step of 32 steps or more does it too)
+    if (!m->graph && nsteps >= kGraphSteps) {
+      if ((rc = capture_graph(m)) != MFDM_OK) return rc;
+      if (cudaGraphUpload(m->graph, m->stream) != cudaSuccess) (void)cudaGetLastError();
+    }
     MFDM_CU(cudaEventRecord(ev[6], m->stream));
     if ((rc = enqueue_steps(m, nsteps)) != MFDM_OK) return rc;
     MFDM_CU(cudaEventRecord(ev[7], m->stream));
